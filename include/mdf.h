@@ -1,0 +1,208 @@
+/*
+ * mdf.h — C ABI of the B200 force/energy engine (libmdf.so).
+ *
+ * Drop-in for the CPU energy/force path of prateekbansal97/MD.  In the
+ * reference that path is the private member functions of md::System
+ * (include/System/System.h:78-170): calculate_energies()
+ * (src/System/System.cpp:9-23), calculate_forces() (src/System/System.cpp:25-39),
+ * the pairlist build (src/System/NonBondedUtils.cpp:185-282) and the PME chain
+ * spread -> FFT -> solve -> FFT^-1 -> gather (src/System/PBC.cpp:183-653).  The
+ * reference keeps an empty CUDA slot for it (src/cuda/nonbonded_cuda.cu,
+ * CMakeLists.txt:140-160).
+ *
+ * Conventions (identical to the reference's):
+ *   - lengths in Angstrom, energies in kcal/mol, forces in kcal/mol/Angstrom
+ *     (forces, not gradients: System::forces_, include/System/System.h:175);
+ *   - positions and forces are 3N doubles, atom-major (x0 y0 z0 x1 ...);
+ *   - charges in the reference's internal unit, prmtop charge / 18.2206899283247
+ *     (src/AmberTopology/TopologyParser.cpp:52), with the Coulomb constant
+ *     passed in mdf_params.coulomb_const (18.2206899283247^2,
+ *     src/NonBonded/CoulombicEE.cpp:12);
+ *   - orthorhombic periodic box.
+ *
+ * Ownership: the caller owns every host array it passes; the library copies
+ * what it needs during the call.  The library owns all device memory.
+ * Threading: one context per host thread; a context is not internally
+ * synchronised.  Errors: every entry point returns an mdf_status (0 = OK);
+ * mdf_last_error() describes the last failure on that context.  There is no
+ * CPU fallback: without a usable CUDA device mdf_create fails with
+ * MDF_ERR_CUDA.
+ */
+#ifndef MDF_H
+#define MDF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MDF_API_VERSION 1
+
+typedef enum {
+    MDF_OK = 0,
+    MDF_ERR_INVALID = 1,     /* bad argument / inconsistent topology */
+    MDF_ERR_CUDA = 2,        /* CUDA runtime error or no device */
+    MDF_ERR_CAPACITY = 3,    /* a device list outgrew its buffer (retry grows it) */
+    MDF_ERR_NONFINITE = 4,   /* non-finite position or force detected */
+    MDF_ERR_OVERFLOW = 5,    /* fixed-point accumulator range exceeded */
+    MDF_ERR_TIMEOUT = 6,     /* a bounded device wait gave up */
+    MDF_ERR_STATE = 7,       /* call out of order (e.g. compute before positions) */
+    MDF_ERR_NOMEM = 8,       /* device or host allocation failed */
+    MDF_ERR_UNSUPPORTED = 9  /* option not supported by this build */
+} mdf_status;
+
+/* Which formulas to evaluate. */
+typedef enum {
+    /* The reference exactly as it runs: exclusion lists are whatever the host
+     * passes (the reference's loader leaves them empty), switched LJ, plain
+     * cutoff Coulomb forces, its torsion-force formulas, unwrapped improper
+     * energy, and the reference's energy terms reported side by side. */
+    MDF_SEM_REFERENCE = 0,
+    /* Textbook Amber/CHARMM physics: prmtop exclusions, scaled 1-4 pairs,
+     * -grad(E) torsion forces, erfc real-space Ewald + excluded-pair erf
+     * corrections + self energy + smooth PME reciprocal sum. */
+    MDF_SEM_PHYSICAL = 1
+} mdf_semantics;
+
+typedef enum {
+    MDF_PREC_FP64 = 0,   /* every kernel in double */
+    MDF_PREC_MIXED = 1   /* FP32 pair/spread/FFT/gather, int64 fixed-point forces,
+                            FP64 bonded terms, corrections and energy sums */
+} mdf_precision;
+
+/* Energy terms.  Which ones are filled depends on the semantics:
+ * REFERENCE: BOND..CMAP, VDW, EE (all-pairs plain Coulomb,
+ *   src/System/NonBondedEnergy.cpp:133-174), EE_PAIRLIST (:176-204),
+ *   EE_CUTOFF (:206-234), EE_DIRECT (:236-305), EE_SELF (:307-316).
+ * PHYSICAL: BOND..CMAP, VDW, VDW14, EE_DIRECT (erfc real space), EE14,
+ *   EE_EXCL (-erf correction over excluded pairs), EE_SELF, EE_RECIP. */
+enum {
+    MDF_E_BOND = 0, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
+    MDF_E_VDW, MDF_E_VDW14, MDF_E_EE, MDF_E_EE_PAIRLIST, MDF_E_EE_CUTOFF, MDF_E_EE_DIRECT,
+    MDF_E_EE14, MDF_E_EE_EXCL, MDF_E_EE_SELF, MDF_E_EE_RECIP,
+    MDF_E_COUNT
+};
+
+typedef struct {
+    double e[MDF_E_COUNT];
+    double total;        /* potential energy of the chosen semantics */
+    double virial[9];    /* reciprocal-space virial (PHYSICAL), row-major */
+} mdf_energies;
+
+/* Flattened topology.  All indices 0-based.  Term parameters are resolved
+ * per term (what the reference's term objects carry after
+ * src/AmberTopology/CreateBondedFromParsed.cpp). */
+typedef struct {
+    int32_t natoms;
+    const double *charge;          /* [natoms], internal charge unit */
+    const int32_t *type;           /* [natoms], 0-based atom type */
+    int32_t ntypes;
+    const int32_t *nb_index;       /* [ntypes*ntypes] NONBONDED_PARM_INDEX, 1-based, 0 = none */
+    int32_t n_ljpair;
+    const double *lj_a, *lj_b;     /* [n_ljpair] */
+    const double *lj14_a, *lj14_b; /* [n_ljpair] */
+
+    int32_t n_bonds;  const int32_t *bond_atoms;     const double *bond_k, *bond_r0;        /* 2/term */
+    int32_t n_ub;     const int32_t *ub_atoms;       const double *ub_k, *ub_r0;            /* 2/term */
+    int32_t n_angles; const int32_t *angle_atoms;    const double *angle_k, *angle_theta0;  /* 3/term */
+    int32_t n_dihedrals; const int32_t *dihedral_atoms;                                    /* 4/term */
+    const double *dihedral_k, *dihedral_n, *dihedral_phase;
+    int32_t n_impropers; const int32_t *improper_atoms;                                    /* 4/term */
+    const double *improper_k, *improper_phase;
+    int32_t n_cmaps;  const int32_t *cmap_atoms;     const int32_t *cmap_set;               /* 5/term, set 0-based */
+    int32_t cmap_nsets, cmap_res;
+    const double *cmap_coeff;      /* [nsets][res][res][16] bicubic coefficients
+                                      (src/AmberTopology/CreateNonBondedFromParsed.cpp:46-117) */
+
+    /* Pairs excluded from the ordinary nonbonded sum (i<j), and the subset
+     * that receives the scaled 1-4 interaction.  pairs14 must be a subset of
+     * excl_pairs. */
+    int32_t n_excl;   const int32_t *excl_pairs;     /* 2/pair */
+    int32_t n_pairs14; const int32_t *pairs14;       /* 2/pair */
+    const double *scee14, *scnb14;                   /* [n_pairs14] */
+} mdf_topology;
+
+/* Run parameters; mdf_params_default() gives the reference's init() values
+ * (src/System/init.cpp:15-23): cutoff 10, skin 2, switch 9, tolerance 1e-6. */
+typedef struct {
+    int32_t semantics;       /* mdf_semantics */
+    int32_t precision;       /* mdf_precision */
+    double box[3];
+    double cutoff;           /* LJ and Coulomb cutoff (reference: lj_cutoff_ = ee_cutoff_) */
+    double skin;             /* pairlist skin; list cutoff = cutoff + skin */
+    double switch_radius;    /* LJ potential switch start; <= 0 selects force-shifted LJ */
+    double ewald_tol;        /* alpha = sqrt(-ln(2 tol)) / cutoff (src/System/PBC.cpp:88-91) */
+    double ewald_alpha;      /* > 0 overrides ewald_tol */
+    int32_t grid[3];         /* PME mesh; 0 = the reference's formula (src/System/PBC.cpp:93-99) */
+    int32_t pme_order;       /* PHYSICAL B-spline order (4); REFERENCE uses its order-5 chain */
+    double coulomb_const;    /* 18.2206899283247^2 */
+    int32_t device;          /* CUDA device ordinal */
+    int32_t reserved[7];
+} mdf_params;
+
+/* Flags for mdf_compute. */
+#define MDF_COMPUTE_ENERGY 1u
+#define MDF_COMPUTE_FORCES 2u
+/* REFERENCE semantics: also run the reference's order-5 PME chain and make its
+ * forces available through mdf_get_pme_forces (the reference computes them in
+ * init() and then discards them, src/System/init.cpp:59-64 + System.cpp:28). */
+#define MDF_COMPUTE_PME_REFERENCE 4u
+
+typedef struct mdf_ctx mdf_ctx;
+
+/* Fill *p with the reference's defaults for the given box. */
+void mdf_params_default(mdf_params *p);
+
+/* Create a context on p->device and upload the topology. */
+int mdf_create(const mdf_topology *top, const mdf_params *p, mdf_ctx **out);
+void mdf_destroy(mdf_ctx *ctx);
+const char *mdf_last_error(const mdf_ctx *ctx);
+const char *mdf_status_string(int status);
+
+/* Host positions, 3N doubles (replaces topology_.get_coordinates()). */
+int mdf_set_positions(mdf_ctx *ctx, const double *xyz);
+/* Device positions, 3N doubles already on ctx's device. */
+int mdf_set_positions_device(mdf_ctx *ctx, const double *d_xyz);
+int mdf_set_box(mdf_ctx *ctx, const double box[3]);
+
+/* Cell sort + cluster-pair list with exclusion masks (replaces
+ * setup_pairlists / build_lj_pairlist, src/System/NonBondedUtils.cpp:49-57,185-282). */
+int mdf_build_pairlist(mdf_ctx *ctx);
+
+/* One evaluation.  forces_out: host 3N doubles or NULL; e_out: host or NULL.
+ * Replaces calculate_forces() + calculate_energies() (+ the PME chain). */
+int mdf_compute(mdf_ctx *ctx, uint32_t flags, double *forces_out, mdf_energies *e_out);
+
+/* Same evaluation, enqueued on the context's stream without a host sync; the
+ * results stay on the device until mdf_fetch / mdf_compute_device. */
+int mdf_compute_async(mdf_ctx *ctx, uint32_t flags);
+/* Wait for the last async evaluation and copy its results (either may be NULL). */
+int mdf_fetch(mdf_ctx *ctx, double *forces_out, mdf_energies *e_out);
+/* Device forces (3N doubles on ctx's device) of the last evaluation. */
+int mdf_forces_device(mdf_ctx *ctx, double *d_forces_out);
+
+/* REFERENCE semantics only: forces of the reference's order-5 PME chain from
+ * the last evaluation that asked for MDF_COMPUTE_PME_REFERENCE. */
+int mdf_get_pme_forces(mdf_ctx *ctx, double *forces_out);
+
+/* Use an existing CUDA stream (cudaStream_t passed as void*); NULL = the
+ * context's own stream. */
+int mdf_set_stream(mdf_ctx *ctx, void *stream);
+
+/* Sizes of the current pairlist (clusters, cluster pairs, atom pairs within
+ * the cutoff from the last evaluation or -1). */
+int mdf_pairlist_info(mdf_ctx *ctx, int64_t *n_clusters, int64_t *n_cluster_pairs,
+                      int64_t *n_pairs_in_cutoff);
+
+/* Kernel timings of the last evaluation in milliseconds, recorded with CUDA
+ * events when MDF timing is enabled (mdf_enable_timing). names[i] points to
+ * static strings. Returns the number of entries written. */
+int mdf_enable_timing(mdf_ctx *ctx, int enable);
+int mdf_kernel_times(mdf_ctx *ctx, const char **names, float *ms, int max_entries);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,335 @@
+"""Benchmark: force evaluations per second of the B200 engine at 100k atoms.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the 100 A periodic box of about 32,000 flexible 3-site waters plus a
+400-residue synthetic chain (99,844 atoms, seeded synthetic data), cutoff
+10 A, skin 2 A, LJ switch 9-10 A, Ewald tolerance 1e-5, PME grid 100^3 order
+4, PHYSICAL semantics, MIXED precision (FP32 pair/spread/FFT/gather, int64
+fixed-point forces, FP64 bonded/corrections/energy sums).  A step is one full
+energy + force evaluation on a pairlist built before the timed region (the
+build is timed separately and reported).
+
+value      device time of K steps with inputs resident in HBM (CUDA events on
+           the engine's stream around each step; L2 flushed between steps by a
+           256 MiB memset outside the events)
+e2e        the same evaluation through the C ABI from pinned host memory:
+           mdf_set_positions (3N doubles in) + mdf_compute (3N doubles and the
+           energy record out), wall clock per step
+roofline   the pair kernel (the dominant kernel), FP32-pipe bound: 60 FP32
+           flops per atom pair inside the cutoff over its mean CUDA-event
+           duration, against the measured FMA peak of the same GPU
+cpu_baseline / --impl reference
+           the unmodified reference (oracle/_ref/o1_harness, single-threaded
+           C++) on the same system: PME chain + list energies +
+           calculate_forces per step
+
+Multi-GPU (torchrun): each rank evaluates its own replica of the system (no
+data-path collective: a single 100k-atom system is not sharded), timings are
+max-reduced over ranks and value is the whole-job rate (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "force evals/s at 100k atoms: mixed vs FP64 GPU at ≤1e-5 rms rel force error"
+CONFIG = "c1"
+GRID = (100, 100, 100)
+FLOPS_PER_PAIR = 60.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            parts = [p.strip() for p in l.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_workload():
+    from md_b200 import abi, engine, synth, topology
+    s = synth.make_config(CONFIG)
+    flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    return s, flat
+
+
+def o1_files(s):
+    from md_b200 import synth
+    d = tempfile.mkdtemp(prefix="mdf_bench_")
+    return synth.write_files(s, d, stem=CONFIG)
+
+
+def reference_time(s, steps, warmup=1):
+    from oracle import oracle as O
+    prm, rst = o1_files(s)
+    r = O.bench_o1(prm, rst, GRID, steps, warmup=warmup, tol=1e-5)
+    return r
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    import platform
+    s, _ = build_workload()
+    budget_s = 120.0
+    per = 7.0      # seconds per reference evaluation at this size on a ~2.7 GHz core
+    k = max(1, min(args.steps, int(budget_s / per)))
+    w = 1 if args.warmup > 0 else 0
+    r = reference_time(s, k, warmup=w)
+    v = 1.0 / r["s_per_step"]
+    sample = ("%d full reference evaluations of the %d-atom system (PME chain at 100^3 + list energies + "
+              "calculate_forces; pairlist built once; O(N^2) calculate_EE_energy left out)" % (k, s.natoms))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": args.gpus,
+            "steps": k, "warmup": w, "ms_per_step": r["s_per_step"] * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "c1: 100 A box, %d atoms, PME 100^3" % s.natoms, "semantics": "reference as-is",
+                       "cpu": platform.processor() or platform.machine()},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": 1, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_breakdown_s": {k2: r[k2] for k2 in ("s_pme_chain", "s_list_energies", "s_calculate_forces",
+                                                          "s_pairlist")}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    from md_b200 import abi, engine
+    if ws > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+
+    s, flat = build_workload()
+    stream = torch.cuda.Stream(device=dev)
+    eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, ewald_tol=1e-5,
+                        grid=GRID, device=dev)
+    eng.set_stream(stream.cuda_stream)
+    eng.set_positions(s.coords)
+    t0 = time.perf_counter()
+    eng.build_pairlist()
+    torch.cuda.synchronize(dev)
+    t_build = time.perf_counter() - t0
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    eng.enable_timing(True)
+
+    # warm-up
+    for _ in range(max(3, args.warmup)):
+        eng.compute_async(energy=True)
+        eng.fetch(forces=False)
+
+    # timed region: per-step CUDA events on the engine stream, L2 flushed in between
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    ktimes = {}
+    launches0 = eng.launches()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ev[k][0].record(stream)
+            eng.compute_async(energy=True)
+            ev[k][1].record(stream)
+            eng.fetch(forces=False)
+            for name, ms in eng.kernel_times():
+                ktimes.setdefault(name, []).append(ms)
+        torch.cuda.synchronize(dev)
+    launches = eng.launches() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_total = sum(step_ms) / 1e3
+    if ws > 1:
+        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+    value = ws * args.steps / t_total
+    info = eng.pairlist_info()
+    pair_ms = float(np.mean(ktimes.get("pairs", [float("nan")])))
+
+    # e2e through the C ABI from pinned host buffers
+    pos_h = torch.from_numpy(np.ascontiguousarray(s.coords.reshape(-1))).pin_memory()
+    f_h = torch.empty(3 * s.natoms, dtype=torch.float64).pin_memory()
+    eng.enable_timing(False)
+    for _ in range(3):
+        eng.set_positions_ptr(pos_h.data_ptr())
+        eng.compute_into(f_h.data_ptr())
+    e2e_steps = max(10, args.steps // 2)
+    e2e_t = 0.0
+    for _ in range(e2e_steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        stream.synchronize()
+        a = time.perf_counter()
+        eng.set_positions_ptr(pos_h.data_ptr())
+        eng.compute_into(f_h.data_ptr())
+        e2e_t += time.perf_counter() - a
+    if ws > 1:
+        tt = torch.tensor([e2e_t], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e = ws * e2e_steps / e2e_t
+    F_mixed = f_h.numpy().reshape(-1, 3).copy()
+
+    # FP64 path on the same system (the metric's comparison), and its force error
+    fp64 = None
+    if not args.no_fp64:
+        eng64 = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_FP64,
+                              ewald_tol=1e-5, grid=GRID, device=dev)
+        eng64.set_stream(stream.cuda_stream)
+        eng64.set_positions(s.coords)
+        eng64.build_pairlist()
+        for _ in range(3):
+            eng64.compute_async(energy=True)
+            eng64.fetch(forces=False)
+        n64 = max(10, args.steps // 4)
+        ev64 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n64)]
+        for k in range(n64):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            ev64[k][0].record(stream)
+            eng64.compute_async(energy=True)
+            ev64[k][1].record(stream)
+            eng64.fetch(forces=False)
+        torch.cuda.synchronize(dev)
+        t64 = sum(a.elapsed_time(b) for a, b in ev64) / 1e3 / n64
+        _, F64 = eng64.compute()
+        err = float(np.linalg.norm(F_mixed - F64) / np.linalg.norm(F64))
+        fp64 = {"ms_per_step": t64 * 1e3, "value": 1.0 / t64, "mixed_over_fp64": (t_total / args.steps) ** -1 * t64,
+                "rms_rel_force_err_mixed_vs_fp64": err}
+        eng64.close()
+
+    peak = engine.probe_fma_tflops(dev, abi.MDF_PREC_MIXED)
+    achieved = FLOPS_PER_PAIR * info["pairs_in_cutoff"] / (pair_ms * 1e-3) / 1e12
+    kernel_ms = {k: float(np.mean(v)) for k, v in ktimes.items()}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            r = reference_time(s, 1, warmup=0)
+            cpu = {"value": 1.0 / r["s_per_step"], "unit": "evals/s", "cores": 1, "kind": "reference",
+                   "sample": "one full evaluation of the same %d-atom system by the unmodified reference "
+                             "(PME chain + list energies + calculate_forces, single-threaded; pairlist "
+                             "built once, O(N^2) calculate_EE_energy left out)" % s.natoms,
+                   "breakdown_s": {k2: r[k2] for k2 in ("s_pme_chain", "s_list_energies", "s_calculate_forces",
+                                                        "s_pairlist")}}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "evals/s", "cores": 1, "kind": "reference", "sample": "failed: %s" % e}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": t_total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "c1: 100 A cubic box, %d atoms (31,948 flexible waters + 400-residue chain), "
+                                   "cutoff 10 A, skin 2 A, LJ switch 9 A, Ewald tol 1e-5, PME 100^3 order 4, "
+                                   "PHYSICAL semantics, mixed precision" % s.natoms,
+                       "parallelism": "replicas x%d" % ws if ws > 1 else "single GPU",
+                       "l2": "flushed between steps (256 MiB memset outside the per-step events)",
+                       "pairlist_build_ms": t_build * 1e3, "clusters": info["clusters"],
+                       "cluster_pairs": info["cluster_pairs"], "pairs_in_cutoff": info["pairs_in_cutoff"]},
+            "roofline": {"kernel": "k_pairs (LJ + erfc Ewald pair kernel)", "bound": "fp32", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured FP32 FMA throughput of this GPU (mdf_probe_fma_tflops)",
+                         "work": "%g FP32 flops x %d pairs in cutoff per launch" % (FLOPS_PER_PAIR,
+                                                                                  info["pairs_in_cutoff"])},
+            "kernel_ms": kernel_ms,
+            "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": 3 * s.natoms * 8,
+                    "d2h_bytes_per_step": 3 * s.natoms * 8 + 26 * 8},
+            "fp64": fp64,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

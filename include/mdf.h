@@ -200,7 +200,19 @@ int mdf_pairlist_info(mdf_ctx *ctx, int64_t *n_clusters, int64_t *n_cluster_pair
  * events when MDF timing is enabled (mdf_enable_timing). names[i] points to
  * static strings. Returns the number of entries written. */
 int mdf_enable_timing(mdf_ctx *ctx, int enable);
+/* Number of kernels this context has launched for evaluations so far. */
+int64_t mdf_kernel_launches(const mdf_ctx *ctx);
 int mdf_kernel_times(mdf_ctx *ctx, const char **names, float *ms, int max_entries);
+
+/* Host-only utility: bicubic CMAP coefficients [nsets][res][res][16] from the
+ * energy grids [nsets][res*res], the reference's table build
+ * (src/AmberTopology/CreateNonBondedFromParsed.cpp:46-117). */
+int mdf_cmap_coefficients(int nsets, int res, const double *grids, double *coeff);
+
+/* Diagnostic: measured FMA throughput of the device's CUDA cores in TFLOP/s
+ * (an FMA counts 2), precision MDF_PREC_MIXED for FP32, MDF_PREC_FP64 for
+ * FP64.  The roofline denominator of the FP32-pipe-bound pair kernel. */
+int mdf_probe_fma_tflops(int device, int precision, double *tflops);
 
 #ifdef __cplusplus
 }

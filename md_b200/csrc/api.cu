@@ -1,0 +1,591 @@
+// C ABI of libmdf (include/mdf.h): context lifetime, uploads, evaluation
+// sequencing and result readback.  The evaluation replaces the reference's
+// System::calculate_forces() + calculate_energies() + PME chain
+// (src/System/System.cpp:9-39, src/System/init.cpp:59-64).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <set>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "mdf_device.cuh"
+#include "mdf_internal.cuh"
+
+namespace mdf {
+
+CudaError::CudaError(cudaError_t e, const char* what, const char* file, int line) : err(e)
+{
+    char buf[512];
+    snprintf(buf, sizeof(buf), "CUDA error %s (%s) at %s:%d: %s", cudaGetErrorName(e), cudaGetErrorString(e), file,
+             line, what);
+    msg = buf;
+}
+
+void mark(Ctx& c, const char* name)
+{
+    if (!c.timing) return;
+    if (c.nev >= (int)c.evpool.size()) {
+        cudaEvent_t ev;
+        MDF_CUDA_TRY(cudaEventCreate(&ev));
+        c.evpool.push_back(ev);
+        c.evname.push_back(name);
+    }
+    c.evname[c.nev] = name;
+    MDF_CUDA_TRY(cudaEventRecord(c.evpool[c.nev], c.stream));
+    ++c.nev;
+}
+
+__global__ void k_finalize(int N, int nslots, const unsigned long long* __restrict__ fatom,
+                           const unsigned long long* __restrict__ fslot, const int* __restrict__ atom_slot,
+                           double* __restrict__ out)
+{
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= N) return;
+    int s = atom_slot[a];
+    for (int k = 0; k < 3; ++k) {
+        long long v = (long long)fatom[(long long)k * N + a] + (long long)fslot[(long long)k * nslots + s];
+        out[3 * a + k] = (double)v * FORCE_ISCALE;
+    }
+}
+
+void launch_finalize(Ctx& c, double* d_forces, bool)
+{
+    k_finalize<<<grid_blocks(c.N, 256), 256, 0, c.stream>>>(c.N, c.n_slots, c.f_atom.p, c.f_slot.p, c.atom_slot.p,
+                                                            d_forces);
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 1;
+}
+
+static void check_index(const int32_t* a, long long n, int N, const char* what)
+{
+    for (long long i = 0; i < n; ++i)
+        if (a[i] < 0 || a[i] >= N) throw ApiError(MDF_ERR_INVALID, std::string("atom index out of range in ") + what);
+}
+
+void upload_topology(Ctx& c, const mdf_topology* t)
+{
+    cudaStream_t s = c.stream;
+    if (!t || t->natoms <= 0) throw ApiError(MDF_ERR_INVALID, "topology has no atoms");
+    if (!t->charge || !t->type || !t->nb_index || t->ntypes <= 0)
+        throw ApiError(MDF_ERR_INVALID, "topology misses charges, types or the nonbonded index");
+    c.N = t->natoms;
+    c.ntypes = t->ntypes;
+    c.ntp = t->ntypes + 1;
+    for (int i = 0; i < c.N; ++i)
+        if (t->type[i] < 0 || t->type[i] >= t->ntypes) throw ApiError(MDF_ERR_INVALID, "atom type out of range");
+    // pair tables over (ntypes + 1)^2, the extra type being cluster padding
+    std::vector<double2> ab(c.ntp * c.ntp, make_double2(0, 0)), ab14(c.ntp * c.ntp, make_double2(0, 0));
+    std::vector<float2> abf(c.ntp * c.ntp, make_float2(0, 0));
+    std::vector<int> valid(c.ntp * c.ntp, 0);
+    for (int i = 0; i < c.ntypes; ++i)
+        for (int j = 0; j < c.ntypes; ++j) {
+            int nb = t->nb_index[i * c.ntypes + j];
+            if (nb != t->nb_index[j * c.ntypes + i])
+                throw ApiError(MDF_ERR_UNSUPPORTED, "NONBONDED_PARM_INDEX is not symmetric");
+            if (nb < 0 || nb > t->n_ljpair) throw ApiError(MDF_ERR_INVALID, "NONBONDED_PARM_INDEX out of range");
+            if (nb == 0) continue;
+            int tp = i * c.ntp + j;
+            ab[tp] = make_double2(t->lj_a[nb - 1], t->lj_b[nb - 1]);
+            abf[tp] = make_float2((float)t->lj_a[nb - 1], (float)t->lj_b[nb - 1]);
+            if (t->lj14_a && t->lj14_b) ab14[tp] = make_double2(t->lj14_a[nb - 1], t->lj14_b[nb - 1]);
+            else ab14[tp] = ab[tp];
+            valid[tp] = 1;
+        }
+    c.ljAB.upload(ab.data(), ab.size(), s);
+    c.ljAB_f.upload(abf.data(), abf.size(), s);
+    c.lj14AB.upload(ab14.data(), ab14.size(), s);
+    c.ljvalid.upload(valid.data(), valid.size(), s);
+    c.q.upload(t->charge, c.N, s);
+    c.type.upload(t->type, c.N, s);
+
+    // bonded terms
+    auto pack2 = [](int n, const double* a, const double* b) {
+        std::vector<double2> v(n);
+        for (int i = 0; i < n; ++i) v[i] = make_double2(a[i], b[i]);
+        return v;
+    };
+    c.n_bonds = t->n_bonds; c.n_ub = t->n_ub; c.n_angles = t->n_angles;
+    c.n_dih = t->n_dihedrals; c.n_imp = t->n_impropers; c.n_cmap = t->n_cmaps;
+    check_index(t->bond_atoms, 2LL * c.n_bonds, c.N, "bonds");
+    check_index(t->ub_atoms, 2LL * c.n_ub, c.N, "Urey-Bradley");
+    check_index(t->angle_atoms, 3LL * c.n_angles, c.N, "angles");
+    check_index(t->dihedral_atoms, 4LL * c.n_dih, c.N, "dihedrals");
+    check_index(t->improper_atoms, 4LL * c.n_imp, c.N, "impropers");
+    check_index(t->cmap_atoms, 5LL * c.n_cmap, c.N, "CMAP");
+    c.bond_atoms.upload(t->bond_atoms, 2 * (size_t)c.n_bonds, s);
+    { auto v = pack2(c.n_bonds, t->bond_k, t->bond_r0); c.bond_par.upload(v.data(), v.size(), s); }
+    c.ub_atoms.upload(t->ub_atoms, 2 * (size_t)c.n_ub, s);
+    { auto v = pack2(c.n_ub, t->ub_k, t->ub_r0); c.ub_par.upload(v.data(), v.size(), s); }
+    c.angle_atoms.upload(t->angle_atoms, 3 * (size_t)c.n_angles, s);
+    { auto v = pack2(c.n_angles, t->angle_k, t->angle_theta0); c.angle_par.upload(v.data(), v.size(), s); }
+    c.dih_atoms.upload(t->dihedral_atoms, 4 * (size_t)c.n_dih, s);
+    {
+        std::vector<double> v(3 * (size_t)c.n_dih);
+        for (int i = 0; i < c.n_dih; ++i) {
+            v[3 * i] = t->dihedral_k[i]; v[3 * i + 1] = t->dihedral_n[i]; v[3 * i + 2] = t->dihedral_phase[i];
+        }
+        c.dih_par.upload(v.data(), v.size(), s);
+    }
+    c.imp_atoms.upload(t->improper_atoms, 4 * (size_t)c.n_imp, s);
+    { auto v = pack2(c.n_imp, t->improper_k, t->improper_phase); c.imp_par.upload(v.data(), v.size(), s); }
+    c.cmap_atoms.upload(t->cmap_atoms, 5 * (size_t)c.n_cmap, s);
+    c.cmap_set.upload(t->cmap_set, c.n_cmap, s);
+    c.cmap_res = t->cmap_res > 0 ? t->cmap_res : 24;
+    c.cmap_nsets = t->cmap_nsets;
+    for (int i = 0; i < c.n_cmap; ++i)
+        if (t->cmap_set[i] < 0 || t->cmap_set[i] >= c.cmap_nsets) throw ApiError(MDF_ERR_INVALID, "CMAP set out of range");
+    if (c.n_cmap > 0) {
+        if (!t->cmap_coeff) throw ApiError(MDF_ERR_INVALID, "CMAP coefficients missing");
+        c.cmap_coeff.upload(t->cmap_coeff, (size_t)c.cmap_nsets * c.cmap_res * c.cmap_res * 16, s);
+    }
+
+    // exclusions and 1-4 pairs
+    c.n_excl = t->n_excl;
+    c.n_14 = t->n_pairs14;
+    check_index(t->excl_pairs, 2LL * c.n_excl, c.N, "exclusions");
+    check_index(t->pairs14, 2LL * c.n_14, c.N, "1-4 pairs");
+    std::vector<int> ex(2 * (size_t)c.n_excl), is14(c.n_excl, 0);
+    std::set<std::pair<int, int>> s14;
+    for (int i = 0; i < c.n_14; ++i) {
+        int a = t->pairs14[2 * i], b = t->pairs14[2 * i + 1];
+        s14.insert({std::min(a, b), std::max(a, b)});
+    }
+    std::set<std::pair<int, int>> sex;
+    for (int i = 0; i < c.n_excl; ++i) {
+        int a = t->excl_pairs[2 * i], b = t->excl_pairs[2 * i + 1];
+        if (a == b) throw ApiError(MDF_ERR_INVALID, "excluded pair of an atom with itself");
+        ex[2 * i] = std::min(a, b);
+        ex[2 * i + 1] = std::max(a, b);
+        is14[i] = s14.count({ex[2 * i], ex[2 * i + 1]}) ? 1 : 0;
+        sex.insert({ex[2 * i], ex[2 * i + 1]});
+    }
+    for (auto& pr : s14)
+        if (!sex.count(pr)) throw ApiError(MDF_ERR_INVALID, "1-4 pair missing from the exclusion list");
+    c.excl_pairs.upload(ex.data(), ex.size(), s);
+    c.excl_is14.upload(is14.data(), is14.size(), s);
+    {
+        std::vector<int> p(2 * (size_t)c.n_14);
+        std::vector<double2> sc(c.n_14);
+        for (int i = 0; i < c.n_14; ++i) {
+            p[2 * i] = t->pairs14[2 * i];
+            p[2 * i + 1] = t->pairs14[2 * i + 1];
+            sc[i] = make_double2(t->scee14 ? t->scee14[i] : 1.0, t->scnb14 ? t->scnb14[i] : 1.0);
+        }
+        c.pairs14.upload(p.data(), p.size(), s);
+        c.p14_scale.upload(sc.data(), sc.size(), s);
+    }
+
+    // constant self energy: -k alpha / sqrt(pi) sum q^2 (src/System/NonBondedEnergy.cpp:307-316)
+    long double q2 = 0, qt = 0;
+    for (int i = 0; i < c.N; ++i) {
+        q2 += (long double)t->charge[i] * t->charge[i];
+        qt += t->charge[i];
+    }
+    c.e_self = (double)(-(long double)c.p.coulomb_const * (c.alpha / std::sqrt(M_PI)) * q2);
+    c.q_total = (double)qt;
+
+    c.xyz.alloc(3 * (size_t)c.N);
+    c.f_atom.alloc(3 * (size_t)c.N);
+    c.forces_out.alloc(3 * (size_t)c.N);
+    c.acc.alloc(NUM_ACC);
+    c.npairs_cut.alloc(1);
+    c.status.alloc(1);
+    MDF_CUDA_TRY(cudaStreamSynchronize(s));
+}
+
+static void eval_async(Ctx& c, uint32_t flags)
+{
+    if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
+    if (!c.have_list) build_pairlist(c);
+    cudaStream_t s = c.stream;
+    bool energy = (flags & MDF_COMPUTE_ENERGY) != 0;
+    bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
+    c.nev = 0;
+    mark(c, "start");
+    MDF_CUDA_TRY(cudaMemsetAsync(c.f_slot.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_slots, s));
+    MDF_CUDA_TRY(cudaMemsetAsync(c.f_atom.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.N, s));
+    MDF_CUDA_TRY(cudaMemsetAsync(c.acc.p, 0, sizeof(unsigned long long) * NUM_ACC, s));
+    MDF_CUDA_TRY(cudaMemsetAsync(c.npairs_cut.p, 0, sizeof(unsigned long long), s));
+    MDF_CUDA_TRY(cudaMemsetAsync(c.status.p, 0, sizeof(unsigned), s));
+    pack_positions(c);
+    mark(c, "pack");
+    launch_nonbonded(c, energy);
+    mark(c, "pairs");
+    launch_exclusions(c, energy);
+    mark(c, "excl_14");
+    launch_bonded(c, energy);
+    mark(c, "bonded");
+    if (phys || (flags & MDF_COMPUTE_PME_REFERENCE)) {
+        launch_pme(c, energy);
+        c.have_pme_ref = !phys;
+    }
+    launch_finalize(c, c.forces_out.p, false);
+    mark(c, "finalize");
+    MDF_CUDA_TRY(cudaMemcpyAsync(c.h_acc, c.acc.p, sizeof(unsigned long long) * NUM_ACC, cudaMemcpyDeviceToHost, s));
+    MDF_CUDA_TRY(cudaMemcpyAsync(c.h_status, c.status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    c.pending = true;
+    c.pending_flags = flags;
+}
+
+static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
+{
+    if (!c.pending) throw ApiError(MDF_ERR_STATE, "no evaluation to fetch");
+    MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    unsigned st = *c.h_status;
+    if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite force or energy contribution");
+    if (st & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "fixed-point accumulator range exceeded");
+    if (c.timing) {
+        c.tlast.clear();
+        for (int i = 1; i < c.nev; ++i) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, c.evpool[i - 1], c.evpool[i]);
+            c.tlast.emplace_back(c.evname[i], ms);
+        }
+    }
+    if (e_out) {
+        memset(e_out, 0, sizeof(*e_out));
+        if (c.pending_flags & MDF_COMPUTE_ENERGY) {
+            for (int k = 0; k < MDF_E_COUNT; ++k) e_out->e[k] = (double)(long long)c.h_acc[k] * ENERGY_ISCALE;
+            e_out->e[MDF_E_EE_SELF] += c.e_self;
+            bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
+            if (phys) {
+                double V = c.box[0] * c.box[1] * c.box[2];
+                e_out->e[MDF_E_EE_RECIP] +=
+                    -c.p.coulomb_const * M_PI * c.q_total * c.q_total / (2.0 * V * c.alpha * c.alpha);
+                const int vmap[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+                for (int k = 0; k < 9; ++k)
+                    e_out->virial[k] = (double)(long long)c.h_acc[ACC_VIR + vmap[k]] * ENERGY_ISCALE;
+                double tot = 0;
+                const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
+                                     MDF_E_VDW, MDF_E_VDW14, MDF_E_EE_DIRECT, MDF_E_EE14, MDF_E_EE_EXCL,
+                                     MDF_E_EE_SELF, MDF_E_EE_RECIP};
+                for (int k : terms) tot += e_out->e[k];
+                e_out->total = tot;
+            } else {
+                double tot = 0;
+                const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
+                                     MDF_E_VDW, MDF_E_EE};
+                for (int k : terms) tot += e_out->e[k];
+                e_out->total = tot;
+            }
+        }
+    }
+    if (forces_out)
+        MDF_CUDA_TRY(cudaMemcpy(forces_out, c.forces_out.p, sizeof(double) * 3 * (size_t)c.N, cudaMemcpyDeviceToHost));
+}
+
+}  // namespace mdf
+
+using namespace mdf;
+
+struct mdf_ctx {
+    Ctx c;
+};
+
+template <typename F>
+static int guarded(mdf_ctx* ctx, F&& f)
+{
+    try {
+        f();
+        if (ctx) ctx->c.last_error.clear();
+        return MDF_OK;
+    } catch (const ApiError& e) {
+        if (ctx) ctx->c.last_error = e.msg;
+        return e.status;
+    } catch (const CudaError& e) {
+        if (ctx) ctx->c.last_error = e.msg;
+        return MDF_ERR_CUDA;
+    } catch (const std::bad_alloc&) {
+        if (ctx) ctx->c.last_error = "host allocation failed";
+        return MDF_ERR_NOMEM;
+    } catch (const std::exception& e) {
+        if (ctx) ctx->c.last_error = e.what();
+        return MDF_ERR_INVALID;
+    }
+}
+
+static thread_local std::string g_create_error;
+
+extern "C" {
+
+void mdf_params_default(mdf_params* p)
+{
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->semantics = MDF_SEM_REFERENCE;
+    p->precision = MDF_PREC_FP64;
+    p->cutoff = 10.0;
+    p->skin = 2.0;
+    p->switch_radius = 9.0;
+    p->ewald_tol = 1e-6;
+    p->ewald_alpha = 0.0;
+    p->pme_order = 4;
+    long double r = 18.2206899283247L;
+    p->coulomb_const = (double)(r * r);
+    p->device = 0;
+}
+
+const char* mdf_status_string(int status)
+{
+    switch (status) {
+        case MDF_OK: return "MDF_OK";
+        case MDF_ERR_INVALID: return "MDF_ERR_INVALID";
+        case MDF_ERR_CUDA: return "MDF_ERR_CUDA";
+        case MDF_ERR_CAPACITY: return "MDF_ERR_CAPACITY";
+        case MDF_ERR_NONFINITE: return "MDF_ERR_NONFINITE";
+        case MDF_ERR_OVERFLOW: return "MDF_ERR_OVERFLOW";
+        case MDF_ERR_TIMEOUT: return "MDF_ERR_TIMEOUT";
+        case MDF_ERR_STATE: return "MDF_ERR_STATE";
+        case MDF_ERR_NOMEM: return "MDF_ERR_NOMEM";
+        case MDF_ERR_UNSUPPORTED: return "MDF_ERR_UNSUPPORTED";
+        default: return "MDF_ERR_UNKNOWN";
+    }
+}
+
+const char* mdf_last_error(const mdf_ctx* ctx)
+{
+    if (!ctx) return g_create_error.c_str();
+    return ctx->c.last_error.c_str();
+}
+
+int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
+{
+    if (!out || !top || !p) {
+        g_create_error = "null argument";
+        return MDF_ERR_INVALID;
+    }
+    *out = nullptr;
+    mdf_ctx* ctx = new mdf_ctx();
+    int rc = guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        c.p = *p;
+        if (c.p.semantics != MDF_SEM_REFERENCE && c.p.semantics != MDF_SEM_PHYSICAL)
+            throw ApiError(MDF_ERR_INVALID, "unknown semantics");
+        if (c.p.precision != MDF_PREC_FP64 && c.p.precision != MDF_PREC_MIXED)
+            throw ApiError(MDF_ERR_INVALID, "unknown precision");
+        if (!(c.p.cutoff > 0) || c.p.skin < 0) throw ApiError(MDF_ERR_INVALID, "bad cutoff or skin");
+        if (c.p.switch_radius > 0 && !(c.p.switch_radius < c.p.cutoff))
+            throw ApiError(MDF_ERR_INVALID, "lj_switch must be < lj_cutoff");
+        int ndev = 0;
+        cudaError_t e = cudaGetDeviceCount(&ndev);
+        if (e != cudaSuccess || ndev == 0) throw ApiError(MDF_ERR_CUDA, "no CUDA device available");
+        if (c.p.device < 0 || c.p.device >= ndev) throw ApiError(MDF_ERR_INVALID, "device ordinal out of range");
+        c.device = c.p.device;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        c.own_stream = true;
+        MDF_CUDA_TRY(cudaMallocHost((void**)&c.h_acc, sizeof(unsigned long long) * NUM_ACC));
+        MDF_CUDA_TRY(cudaMallocHost((void**)&c.h_status, sizeof(unsigned)));
+        for (int d = 0; d < 3; ++d) c.box[d] = c.p.box[d];
+        double tol = c.p.ewald_tol > 0 ? c.p.ewald_tol : 1e-6;
+        c.alpha = c.p.ewald_alpha > 0 ? c.p.ewald_alpha : std::sqrt(std::log(2 * tol) * -1) / c.p.cutoff;
+        upload_topology(c, top);
+        if (!(c.box[0] > 0 && c.box[1] > 0 && c.box[2] > 0))
+            throw ApiError(MDF_ERR_INVALID, "periodic box required");
+        setup_pme(c);
+    });
+    if (rc != MDF_OK) {
+        g_create_error = ctx->c.last_error;
+        mdf_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return MDF_OK;
+}
+
+void mdf_destroy(mdf_ctx* ctx)
+{
+    if (!ctx) return;
+    Ctx& c = ctx->c;
+    cudaSetDevice(c.device);
+    if (c.stream) cudaStreamSynchronize(c.stream);
+    for (auto& e : c.evpool) cudaEventDestroy(e);
+    c.q.release(); c.type.release(); c.ljAB.release(); c.ljAB_f.release(); c.lj14AB.release(); c.ljvalid.release();
+    c.bond_atoms.release(); c.ub_atoms.release(); c.angle_atoms.release(); c.dih_atoms.release();
+    c.imp_atoms.release(); c.cmap_atoms.release(); c.cmap_set.release(); c.bond_par.release(); c.ub_par.release();
+    c.angle_par.release(); c.imp_par.release(); c.dih_par.release(); c.cmap_coeff.release();
+    c.excl_pairs.release(); c.pairs14.release(); c.p14_scale.release(); c.excl_is14.release();
+    c.xyz.release(); c.atom_col.release(); c.col_count.release(); c.col_start.release(); c.col_cstart.release();
+    c.col_atoms.release(); c.slot_atom.release(); c.atom_slot.release(); c.slot_type.release(); c.center.release();
+    c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
+    c.ilist.release(); c.icount.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
+    c.f_atom.release(); c.acc.release(); c.npairs_cut.release(); c.forces_out.release(); c.forces_pme_ref.release();
+    c.status.release(); c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
+    c.rgrid_d.release();
+    for (int d = 0; d < 3; ++d) {
+        c.bmod[d].release(); c.bmod_f[d].release(); c.tw_d[d].release(); c.tw_f[d].release();
+    }
+    if (c.h_acc) cudaFreeHost(c.h_acc);
+    if (c.h_status) cudaFreeHost(c.h_status);
+    if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
+    delete ctx;
+}
+
+int mdf_set_positions(mdf_ctx* ctx, const double* xyz)
+{
+    if (!ctx || !xyz) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaMemcpyAsync(c.xyz.p, xyz, sizeof(double) * 3 * (size_t)c.N, cudaMemcpyHostToDevice, c.stream));
+        c.have_positions = true;
+    });
+}
+
+int mdf_set_positions_device(mdf_ctx* ctx, const double* d_xyz)
+{
+    if (!ctx || !d_xyz) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaMemcpyAsync(c.xyz.p, d_xyz, sizeof(double) * 3 * (size_t)c.N, cudaMemcpyDeviceToDevice,
+                                     c.stream));
+        c.have_positions = true;
+    });
+}
+
+int mdf_set_box(mdf_ctx* ctx, const double box[3])
+{
+    if (!ctx || !box) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        for (int d = 0; d < 3; ++d) {
+            if (!(box[d] > 0)) throw ApiError(MDF_ERR_INVALID, "box lengths must be positive");
+            c.box[d] = box[d];
+            c.p.box[d] = box[d];
+        }
+        c.have_list = false;
+        setup_pme(c);
+    });
+}
+
+int mdf_build_pairlist(mdf_ctx* ctx)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
+        build_pairlist(c);
+    });
+}
+
+int mdf_compute_async(mdf_ctx* ctx, uint32_t flags)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        eval_async(ctx->c, flags);
+    });
+}
+
+int mdf_fetch(mdf_ctx* ctx, double* forces_out, mdf_energies* e_out)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        fetch(ctx->c, forces_out, e_out);
+    });
+}
+
+int mdf_compute(mdf_ctx* ctx, uint32_t flags, double* forces_out, mdf_energies* e_out)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        eval_async(ctx->c, flags);
+        fetch(ctx->c, forces_out, e_out);
+    });
+}
+
+int mdf_forces_device(mdf_ctx* ctx, double* d_forces_out)
+{
+    if (!ctx || !d_forces_out) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaMemcpyAsync(d_forces_out, c.forces_out.p, sizeof(double) * 3 * (size_t)c.N,
+                                     cudaMemcpyDeviceToDevice, c.stream));
+    });
+}
+
+int mdf_get_pme_forces(mdf_ctx* ctx, double* forces_out)
+{
+    if (!ctx || !forces_out) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (!c.have_pme_ref) throw ApiError(MDF_ERR_STATE, "no reference PME evaluation available");
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        MDF_CUDA_TRY(cudaMemcpy(forces_out, c.forces_pme_ref.p, sizeof(double) * 3 * (size_t)c.N,
+                                cudaMemcpyDeviceToHost));
+    });
+}
+
+int mdf_set_stream(mdf_ctx* ctx, void* stream)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+        if (stream) {
+            c.stream = (cudaStream_t)stream;
+            c.own_stream = false;
+        } else {
+            MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+            c.own_stream = true;
+        }
+    });
+}
+
+int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pairs, int64_t* n_pairs_in_cutoff)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        if (n_clusters) *n_clusters = c.have_list ? c.n_clusters : -1;
+        if (n_cluster_pairs) *n_cluster_pairs = c.have_list ? c.n_entries : -1;
+        if (n_pairs_in_cutoff) {
+            unsigned long long v = 0;
+            if (c.have_list) {
+                MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+                MDF_CUDA_TRY(cudaMemcpy(&v, c.npairs_cut.p, sizeof(v), cudaMemcpyDeviceToHost));
+            }
+            *n_pairs_in_cutoff = c.have_list ? (int64_t)v : -1;
+        }
+    });
+}
+
+int64_t mdf_kernel_launches(const mdf_ctx* ctx)
+{
+    return ctx ? (int64_t)ctx->c.launches : -1;
+}
+
+int mdf_enable_timing(mdf_ctx* ctx, int enable)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    ctx->c.timing = enable != 0;
+    return MDF_OK;
+}
+
+int mdf_kernel_times(mdf_ctx* ctx, const char** names, float* ms, int max_entries)
+{
+    if (!ctx) return 0;
+    int n = 0;
+    for (auto& t : ctx->c.tlast) {
+        if (n >= max_entries) break;
+        if (names) names[n] = t.first;
+        if (ms) ms[n] = t.second;
+        ++n;
+    }
+    return n;
+}
+
+}  // extern "C"

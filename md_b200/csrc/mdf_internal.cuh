@@ -1,0 +1,225 @@
+// Internal declarations shared by the libmdf translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/mdf.h"
+
+namespace mdf {
+
+// ---------------------------------------------------------------- constants
+constexpr int CLUSTER = 8;                 // atoms per cluster
+constexpr double FORCE_SCALE = 4294967296.0;          // 2^32 fixed point for forces
+constexpr double FORCE_ISCALE = 1.0 / 4294967296.0;
+constexpr double ENERGY_SCALE = 4294967296.0;         // 2^32 fixed point for energies
+constexpr double ENERGY_ISCALE = 1.0 / 4294967296.0;
+constexpr double GRID_SCALE = 1099511627776.0;        // 2^40 fixed point for PME charge grid
+constexpr double GRID_ISCALE = 1.0 / 1099511627776.0;
+constexpr int NUM_ACC = MDF_E_COUNT + 6;   // energies + 6 virial components
+constexpr int ACC_VIR = MDF_E_COUNT;
+
+// device status bits
+enum : unsigned {
+    ST_NONFINITE = 1u,
+    ST_OVERFLOW = 2u,
+    ST_CAPACITY_PAIRS = 4u,
+    ST_CAPACITY_COLUMN = 8u,
+    ST_BAD_INDEX = 16u,
+};
+
+struct PairEntry {          // one cluster pair of the half list (16 B)
+    int j;                  // j cluster
+    int shift;              // periodic image code (sx+1) + 3 (sy+1) + 9 (sz+1)
+    unsigned long long mask;  // bit (ii*8 + jj): atom pair interacts
+};
+
+struct ILRange {            // one i cluster's span of entries
+    int i;
+    int start;
+    int count;
+    int pad;
+};
+
+// --------------------------------------------------------------- utilities
+#define MDF_CUDA_TRY(expr)                                                          \
+    do {                                                                            \
+        cudaError_t _e = (expr);                                                    \
+        if (_e != cudaSuccess) {                                                    \
+            throw mdf::CudaError(_e, #expr, __FILE__, __LINE__);                    \
+        }                                                                           \
+    } while (0)
+
+struct CudaError {
+    cudaError_t err;
+    std::string msg;
+    CudaError(cudaError_t e, const char* what, const char* file, int line);
+};
+
+struct ApiError {
+    int status;
+    std::string msg;
+    ApiError(int s, std::string m) : status(s), msg(std::move(m)) {}
+};
+
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        size_t bytes = count * sizeof(T);
+        if (bytes == 0) bytes = sizeof(T);
+        MDF_CUDA_TRY(cudaMalloc((void**)&p, bytes));
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <typename U>
+    void upload(const U* host, size_t count, cudaStream_t s) {
+        alloc(count);
+        if (count) MDF_CUDA_TRY(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, s));
+    }
+};
+
+// ----------------------------------------------------------- PME plan bits
+struct FFTPlan1D {
+    int n = 0;
+    int nstages = 0;
+    int radix[16];
+};
+
+// --------------------------------------------------------------- context
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    mdf_params p{};
+    int N = 0;
+    int ntypes = 0;
+    std::string last_error;
+
+    // topology on device
+    DevBuf<double> q;          // [N]
+    DevBuf<int> type;          // [N]
+    DevBuf<double2> ljAB;      // [(ntypes+1)^2] pair table (A,B); last row/col = padding type
+    DevBuf<float2> ljAB_f;
+    DevBuf<double2> lj14AB;    // same indexing, 1-4 tables
+    DevBuf<int> ljvalid;       // [(ntypes+1)^2] nb != 0
+    int ntp = 0;               // ntypes + 1 (padding type appended)
+
+    int n_bonds = 0, n_ub = 0, n_angles = 0, n_dih = 0, n_imp = 0, n_cmap = 0;
+    DevBuf<int> bond_atoms, ub_atoms, angle_atoms, dih_atoms, imp_atoms, cmap_atoms, cmap_set;
+    DevBuf<double2> bond_par, ub_par, angle_par, imp_par;
+    DevBuf<double> dih_par;    // 3 per term
+    DevBuf<double> cmap_coeff;
+    int cmap_res = 24, cmap_nsets = 0;
+
+    int n_excl = 0, n_14 = 0;
+    DevBuf<int> excl_pairs, pairs14;
+    DevBuf<double2> p14_scale;     // (scee, scnb)
+    DevBuf<int> excl_is14;         // per excluded pair: 1 if it is a 1-4 pair
+
+    double e_self = 0.0;           // constant for fixed charges
+    double q_total = 0.0;
+
+    // positions
+    DevBuf<double> xyz;            // [3N] raw as given
+    bool have_positions = false;
+    double box[3] = {0, 0, 0};
+
+    // clusters / pairlist
+    int ncol_x = 0, ncol_y = 0, ncols = 0;
+    int n_clusters = 0, n_slots = 0;
+    bool have_list = false;
+    DevBuf<int> atom_col;          // [N]
+    DevBuf<int> col_count, col_start, col_cstart;   // [ncols + 1]
+    DevBuf<int> col_atoms;         // [N] atoms bucketed by column
+    DevBuf<int> slot_atom;         // [n_slots]
+    DevBuf<int> atom_slot;         // [N]
+    DevBuf<int> slot_type;         // [n_slots]
+    DevBuf<double4> center;        // [n_clusters] (x,y,z,unused) cluster center
+    DevBuf<float4> bb_lo, bb_hi;   // [n_clusters] bounding boxes (wrapped coordinates)
+    DevBuf<float4> xq_f;           // [n_slots] offset from center + q (mixed)
+    DevBuf<double4> xq_d;          // [n_slots] (FP64)
+    DevBuf<int> cluster_col;       // [n_clusters]
+    DevBuf<ILRange> ilist;         // [n_clusters]
+    DevBuf<int> icount;            // [n_clusters + 1]
+    DevBuf<PairEntry> plist;       // [cap]
+    long long n_entries = 0;
+    DevBuf<int> scan_tmp;
+
+    // accumulators
+    DevBuf<unsigned long long> f_slot;   // [3 * n_slots] fixed point, SoA x|y|z
+    DevBuf<unsigned long long> f_atom;   // [3 * N]
+    DevBuf<unsigned long long> acc;      // [NUM_ACC] energies + virial, fixed point
+    DevBuf<unsigned long long> npairs_cut; // [1]
+    DevBuf<double> forces_out;           // [3N]
+    DevBuf<double> forces_pme_ref;       // [3N]
+    DevBuf<unsigned> status;             // [1]
+    unsigned long long* h_acc = nullptr; // pinned
+    unsigned* h_status = nullptr;        // pinned
+
+    // PME
+    int K[3] = {0, 0, 0};
+    int order = 4;
+    double alpha = 0.0;
+    DevBuf<unsigned long long> qgrid;    // [K0*K1*K2] fixed point
+    DevBuf<float2> cgrid_f;              // [K0*K1*(K2/2+1)]
+    DevBuf<double2> cgrid_d;
+    DevBuf<float> rgrid_f;               // [K0*K1*K2] potential
+    DevBuf<double> rgrid_d;
+    DevBuf<double> bmod[3];              // PHYSICAL: 1/|b(m)|^2 factors; REFERENCE: moduli
+    DevBuf<float> bmod_f[3];
+    DevBuf<double2> tw_d[3];             // twiddles per dimension
+    DevBuf<float2> tw_f[3];
+    FFTPlan1D plan[3];
+    // reference order-5 chain (REFERENCE semantics)
+    int Kref[3] = {0, 0, 0};
+    DevBuf<double> ref_grid;             // [K^3] double (real), used as spread target via fixed
+    DevBuf<unsigned long long> ref_qgrid;
+    DevBuf<double2> ref_cgrid;
+    DevBuf<double> ref_moduli[3];
+    DevBuf<double2> ref_tw[3];
+    FFTPlan1D ref_plan[3];
+    bool have_pme_ref = false;
+
+    // timing
+    bool timing = false;
+    std::vector<cudaEvent_t> evpool;          // reused timing events
+    std::vector<const char*> evname;
+    int nev = 0;
+    std::vector<std::pair<const char*, float>> tlast;
+    long long launches = 0;                   // kernels launched by evaluations
+
+    // last evaluation bookkeeping
+    bool pending = false;
+    uint32_t pending_flags = 0;
+};
+
+// ------------------------------------------------------ launch helpers (.cu)
+void upload_topology(Ctx& c, const mdf_topology* t);
+void build_pairlist(Ctx& c);
+void pack_positions(Ctx& c);
+void launch_nonbonded(Ctx& c, bool energy);
+void launch_exclusions(Ctx& c, bool energy);
+void launch_bonded(Ctx& c, bool energy);
+void setup_pme(Ctx& c);
+void launch_pme(Ctx& c, bool energy);
+void setup_pme_reference(Ctx& c);
+void launch_pme_reference(Ctx& c);
+void launch_finalize(Ctx& c, double* d_forces, bool pme_ref);
+void mark(Ctx& c, const char* name);
+
+// simple device-wide exclusive scan of ints (n up to a few million)
+void exclusive_scan_int(const int* d_in, int* d_out, int n, int* d_total_out, cudaStream_t s);
+
+int grid_blocks(long long n, int threads);
+
+}  // namespace mdf

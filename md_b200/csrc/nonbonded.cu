@@ -1,0 +1,454 @@
+// Nonbonded pair kernel and the FP64 excluded-pair / 1-4 kernels.
+//
+// Replaces, in REFERENCE semantics:
+//   calculate_LJ_energy_pairlist     src/System/NonBondedEnergy.cpp:79-131
+//   calculate_EE_energy (all pairs)  src/System/NonBondedEnergy.cpp:133-174
+//   calculate_EE_energy_pairlist     :176-204, ..._with_cutoff :206-234
+//   calculate_EE_ewald_direct_term   :236-305
+//   calculate_forces_LJ_pairlist     src/System/NonBondedForces.cpp:92-155
+//   calculate_forces_EE_pairlist     src/System/NonBondedForces.cpp:207-241
+// and in PHYSICAL semantics the erfc real-space Ewald sum with switched LJ,
+// the excluded-pair erf corrections and the scaled 1-4 pairs.
+//
+// Pair kernel layout: one warp per i cluster (8 atoms).  The warp walks the
+// cluster's half list four j clusters at a time; lane = (jslot, ii) with
+// jslot = lane/8 selecting the j cluster and ii = lane%8 the i atom.  The four
+// j clusters are staged in shared memory; in step t lane (jslot, ii) computes
+// the pair (ii, (ii+t)&7), so the eight lanes of a j slot touch eight different
+// j atoms at every step and the j-force accumulators simply rotate one lane
+// per step (3 shuffles per pair instead of a 3-level reduction).  i forces
+// stay in registers for the whole list; j forces go to int64 fixed-point
+// accumulators once per cluster pair.
+#include <cmath>
+
+#include "mdf_device.cuh"
+#include "mdf_internal.cuh"
+
+namespace mdf {
+
+constexpr int NB_WARPS = 8;
+constexpr int NB_THREADS = NB_WARPS * 32;
+
+template <typename R> struct V2;
+template <> struct V2<float> { using type = float2; };
+template <> struct V2<double> { using type = double2; };
+
+struct NBParams {
+    double box[3];
+    double rc, rc2, rsw, inv_sw, kc, alpha, rlist2;
+    int use_switch;
+    int ntp;
+    double ucut_pow6, ucut_pow12;   // rc^-6, rc^-12 (force-shift LJ)
+};
+
+// Abramowitz & Stegun 7.1.26 (Hastings): erfc(x) ~ t (a1 + t (a2 + ...)) e^{-x^2},
+// t = 1 / (1 + p x), |error| <= 1.5e-7.  Used by the FP32 pair kernel only.
+__device__ __forceinline__ float erfc_as(float t, float ex)
+{
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
+                a5 = 1.061405429f;
+    return t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5)))) * ex;
+}
+
+template <typename R, int SEM, bool ENERGY>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs(
+    int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist,
+    const typename V4<R>::type* __restrict__ xq, const int* __restrict__ stype, const double4* __restrict__ center,
+    const typename V2<R>::type* __restrict__ ljAB, const int* __restrict__ ljvalid, NBParams P,
+    unsigned long long* __restrict__ fslot, int nslots, unsigned long long* __restrict__ acc,
+    unsigned long long* __restrict__ npairs, unsigned* st)
+{
+    using V4t = typename V4<R>::type;
+    using V2t = typename V2<R>::type;
+    __shared__ V4t sx[NB_WARPS][4][CLUSTER + 1];
+    __shared__ int stj[NB_WARPS][4][CLUSTER];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * NB_WARPS + wib;
+    const int jslot = lane >> 3, ii = lane & 7;
+    const unsigned FULL = 0xffffffffu;
+
+    double e_lj = 0, e_dir = 0, e_all = 0, e_pl = 0, e_cut = 0;
+    long long npc = 0;
+    R fix = 0, fiy = 0, fiz = 0;
+    const R rc2 = (R)P.rc2, rsw = (R)P.rsw, inv_sw = (R)P.inv_sw, alpha = (R)P.alpha;
+    const R two_a_spi = (R)(2.0 * P.alpha / 1.7724538509055160273);
+
+    if (w < nlist) {
+        const ILRange L = ilist[w];
+        const int I = L.i;
+        const V4t xi = xq[I * CLUSTER + ii];
+        const int ti = stype[I * CLUSTER + ii];
+        const double4 cI = center[I];
+        const R qik = (R)P.kc * xi.w;
+        for (int b = 0; b < L.count; b += 4) {
+            const int e = b + jslot;
+            const bool valid = e < L.count;
+            PairEntry pe;
+            if (valid) {
+                pe = plist[L.start + e];
+            } else {
+                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+            }
+            const int J = pe.j;
+            sx[wib][jslot][ii] = xq[J * CLUSTER + ii];
+            stj[wib][jslot][ii] = stype[J * CLUSTER + ii];
+            const double4 cJ = center[J];
+            int ssx, ssy, ssz;
+            shift_decode(pe.shift, ssx, ssy, ssz);
+            const R xix = xi.x + (R)(cI.x - cJ.x - ssx * P.box[0]);
+            const R xiy = xi.y + (R)(cI.y - cJ.y - ssy * P.box[1]);
+            const R xiz = xi.z + (R)(cI.z - cJ.z - ssz * P.box[2]);
+            const unsigned long long mask = pe.mask;
+            __syncwarp();
+            R fjx = 0, fjy = 0, fjz = 0;
+            const int rot_src = (lane & ~7) | ((ii + 1) & 7);
+#pragma unroll
+            for (int t = 0; t < CLUSTER; ++t) {
+                const int jj = (ii + t) & 7;
+                const V4t xj = sx[wib][jslot][jj];
+                const R dx = xix - xj.x, dy = xiy - xj.y, dz = xiz - xj.z;
+                const R r2 = dx * dx + dy * dy + dz * dz;
+                bool on = ((mask >> (ii * 8 + jj)) & 1ull) && r2 <= rc2;
+                if (SEM == MDF_SEM_REFERENCE) on = on && r2 >= (R)1e-12;
+                if (on) {
+                    const int tj = stj[wib][jslot][jj];
+                    const int tp = ti * P.ntp + tj;
+                    R g = 0;
+                    if (SEM == MDF_SEM_PHYSICAL) {
+                        R rinv, r, rinv2;
+                        if (sizeof(R) == 4) {
+                            rinv = rsqrtf((float)r2);
+                        } else {
+                            rinv = (R)1 / sqrt((double)r2);
+                        }
+                        r = r2 * rinv;
+                        rinv2 = rinv * rinv;
+                        // Lennard-Jones 12-6, switched (or force-shifted)
+                        const V2t ab = ljAB[tp];
+                        const R rinv6 = rinv2 * rinv2 * rinv2;
+                        R U = (ab.x * rinv6 - ab.y) * rinv6;
+                        R G = ((R)12 * ab.x * rinv6 - (R)6 * ab.y) * rinv6 * rinv2;
+                        if (P.use_switch) {
+                            if (r > rsw) {
+                                const R x = (r - rsw) * inv_sw, x2 = x * x, x3 = x2 * x;
+                                const R S = (R)1 + x3 * ((R)-10 + x * ((R)15 - (R)6 * x));
+                                const R dS = x2 * ((R)-30 + x * ((R)60 - (R)30 * x)) * inv_sw;
+                                G = S * G - U * dS * rinv;
+                                U = U * S;
+                            }
+                        } else {
+                            const R uc = ab.x * (R)P.ucut_pow12 - ab.y * (R)P.ucut_pow6;
+                            const R gc = ((R)12 * ab.x * (R)P.ucut_pow12 - (R)6 * ab.y * (R)P.ucut_pow6) / (R)P.rc2;
+                            U = U - uc + (r - (R)P.rc) * (gc * (R)P.rc);
+                            G = G - gc * (R)P.rc * rinv;
+                        }
+                        // erfc real-space Ewald
+                        const R qq = qik * xj.w;
+                        const R ar = alpha * r;
+                        R erfcv, ex;
+                        if (sizeof(R) == 4) {
+                            ex = __expf(-(float)(ar * ar));
+                            const float tt = __fdividef(1.0f, 1.0f + 0.3275911f * (float)ar);
+                            erfcv = erfc_as(tt, (float)ex);
+                        } else {
+                            ex = exp(-(double)(ar * ar));
+                            erfcv = erfc((double)ar);
+                        }
+                        const R ec = qq * erfcv * rinv;
+                        g = G + (ec + qq * two_a_spi * ex) * rinv2;
+                        if (ENERGY) {
+                            e_lj += (double)U;
+                            e_dir += (double)ec;
+                            ++npc;
+                        }
+                    } else {
+                        // REFERENCE formulas, operation for operation
+                        const double r2d = (double)r2, r = sqrt(r2d);
+                        const double qq = (double)xi.w * (double)xj.w;
+                        const double ecoul = (qq / r) * P.kc;
+                        if (ENERGY) e_all += ecoul;
+                        if (ljvalid[tp]) {
+                            const V2t ab = ljAB[tp];
+                            const double A = (double)ab.x, B = (double)ab.y;
+                            const double i2 = 1.0 / r2d, i4 = i2 * i2, i6 = i4 * i2, i8 = i4 * i4, i12 = i6 * i6,
+                                         i14 = i12 * i2;
+                            double U = A * i12 - B * i6;
+                            double G = 12.0 * A * i14 - 6.0 * B * i8;
+                            if (P.use_switch) {
+                                double S = 1.0, dS = 0.0;
+                                if (r > P.rsw) {
+                                    if (r >= P.rc) {
+                                        S = 0.0;
+                                    } else {
+                                        const double x = (r - P.rsw) * P.inv_sw, x2 = x * x, x3 = x2 * x,
+                                                     x4 = x2 * x2, x5 = x4 * x;
+                                        S = 1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5;
+                                        dS = (-30.0 * x2 + 60.0 * x3 - 30.0 * x4) * P.inv_sw;
+                                    }
+                                }
+                                G = S * G - (U / r) * dS;
+                                U = U * S;
+                            } else {
+                                const double rc2d = P.rc2, c2 = 1.0 / rc2d, c4 = c2 * c2, c6 = c4 * c2, c8 = c4 * c4,
+                                             c12 = c6 * c6, c14 = c12 * c2;
+                                const double ucut = A * c12 - B * c6, gcut = 12.0 * A * c14 - 6.0 * B * c8;
+                                U = U - ucut + (r - P.rc) * (gcut * P.rc);
+                                G = G - gcut * (P.rc / r);
+                            }
+                            g = (R)(G + ((qq / (r2d * r)) * P.kc));
+                            if (ENERGY) {
+                                e_lj += U;
+                                e_pl += ecoul;
+                                e_cut += (qq * P.kc) * (1.0 / r - 1.0 / P.rc);
+                                e_dir += (qq / r) * erfc(P.alpha * r) * P.kc;
+                                ++npc;
+                            }
+                        }
+                    }
+                    fix += g * dx; fiy += g * dy; fiz += g * dz;
+                    fjx -= g * dx; fjy -= g * dy; fjz -= g * dz;
+                }
+                fjx = __shfl_sync(FULL, fjx, rot_src);
+                fjy = __shfl_sync(FULL, fjy, rot_src);
+                fjz = __shfl_sync(FULL, fjz, rot_src);
+            }
+            if (valid && (fjx != (R)0 || fjy != (R)0 || fjz != (R)0)) {
+                const int sl = J * CLUSTER + ii;
+                fx_add(fslot + sl, fjx, FORCE_SCALE, st);
+                fx_add(fslot + nslots + sl, fjy, FORCE_SCALE, st);
+                fx_add(fslot + 2 * nslots + sl, fjz, FORCE_SCALE, st);
+            }
+            __syncwarp();
+        }
+        fix += __shfl_xor_sync(FULL, fix, 8); fix += __shfl_xor_sync(FULL, fix, 16);
+        fiy += __shfl_xor_sync(FULL, fiy, 8); fiy += __shfl_xor_sync(FULL, fiy, 16);
+        fiz += __shfl_xor_sync(FULL, fiz, 8); fiz += __shfl_xor_sync(FULL, fiz, 16);
+        if (jslot == 0) {
+            const int sl = I * CLUSTER + ii;
+            fx_add(fslot + sl, fix, FORCE_SCALE, st);
+            fx_add(fslot + nslots + sl, fiy, FORCE_SCALE, st);
+            fx_add(fslot + 2 * nslots + sl, fiz, FORCE_SCALE, st);
+        }
+    }
+    if (ENERGY) {
+        if (SEM == MDF_SEM_PHYSICAL) {
+            const double v[2] = {e_lj, e_dir};
+            const int idx[2] = {MDF_E_VDW, MDF_E_EE_DIRECT};
+            block_acc_fixed<2>(v, acc, idx, ENERGY_SCALE, st);
+        } else {
+            const double v[5] = {e_lj, e_all, e_pl, e_cut, e_dir};
+            const int idx[5] = {MDF_E_VDW, MDF_E_EE, MDF_E_EE_PAIRLIST, MDF_E_EE_CUTOFF, MDF_E_EE_DIRECT};
+            block_acc_fixed<5>(v, acc, idx, ENERGY_SCALE, st);
+        }
+        long long np = warp_sum_ll(npc);
+        if (lane == 0 && np) atomicAdd(npairs, (unsigned long long)np);
+    }
+}
+
+// --------------------------------------------------------------- FP64 pairs
+__device__ __forceinline__ void pair_vec(const double* __restrict__ xyz, int a, int b, const NBParams& P,
+                                         double d[3])
+{
+    d[0] = min_image(xyz[3 * a] - xyz[3 * b], P.box[0]);
+    d[1] = min_image(xyz[3 * a + 1] - xyz[3 * b + 1], P.box[1]);
+    d[2] = min_image(xyz[3 * a + 2] - xyz[3 * b + 2], P.box[2]);
+}
+
+__device__ __forceinline__ void add_pair_force(unsigned long long* f, int N, int a, int b, double g, const double d[3],
+                                               unsigned* st)
+{
+    for (int k = 0; k < 3; ++k) {
+        fx_add(f + k * N + a, g * d[k], FORCE_SCALE, st);
+        fx_add(f + k * N + b, -g * d[k], FORCE_SCALE, st);
+    }
+}
+
+// Excluded pairs.  PHYSICAL: -k q q erf(alpha r)/r with its force (every
+// excluded pair, min image, no cutoff).  REFERENCE: the same energy for
+// excluded pairs that are not 1-4 (src/System/NonBondedEnergy.cpp:271-304),
+// no force.
+template <int SEM, bool ENERGY>
+__global__ void k_exclusions(int n, const int* __restrict__ pairs, const int* __restrict__ is14,
+                             const double* __restrict__ xyz, const double* __restrict__ q, NBParams P, int N,
+                             unsigned long long* __restrict__ fatom, unsigned long long* __restrict__ acc, unsigned* st)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (k < n && !(SEM == MDF_SEM_REFERENCE && is14[k])) {
+        int a = pairs[2 * k], b = pairs[2 * k + 1];
+        double d[3];
+        pair_vec(xyz, a, b, P, d);
+        double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], r = sqrt(r2);
+        if (SEM == MDF_SEM_PHYSICAL) {
+            double qq = q[a] * q[b] * P.kc, ar = P.alpha * r;
+            e = -qq * erf(ar) / r;
+            double g = (e + qq * (2.0 * P.alpha / 1.7724538509055160273) * exp(-ar * ar)) / r2;
+            add_pair_force(fatom, N, a, b, g, d, st);
+        } else {
+            e = -P.kc * (q[a] * q[b] / r) * erf(P.alpha * r);
+        }
+    }
+    if (ENERGY) {
+        const double v[1] = {e};
+        const int idx[1] = {SEM == MDF_SEM_PHYSICAL ? MDF_E_EE_EXCL : MDF_E_EE_DIRECT};
+        block_acc_fixed<1>(v, acc, idx, ENERGY_SCALE, st);
+    }
+}
+
+// 1-4 pairs.  PHYSICAL: k q q / (scee r) + (A14/r^12 - B14/r^6) / scnb.
+// REFERENCE: the reference's is14 branches of the list loops (A14/B14 with the
+// switch, Coulomb / scee, and CalculateEnergyEwaldDirectTerm_14's erf(r)).
+template <int SEM, bool ENERGY>
+__global__ void k_pairs14(int n, const int* __restrict__ pairs, const double2* __restrict__ scale,
+                          const double* __restrict__ xyz, const double* __restrict__ q, const int* __restrict__ type,
+                          const double2* __restrict__ lj14, const int* __restrict__ ljvalid, NBParams P, int N,
+                          unsigned long long* __restrict__ fatom, unsigned long long* __restrict__ acc, unsigned* st)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    double ev = 0, ec = 0, eall = 0, epl = 0, ecut = 0, edir = 0;
+    if (k < n) {
+        int a = pairs[2 * k], b = pairs[2 * k + 1];
+        double d[3];
+        pair_vec(xyz, a, b, P, d);
+        double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2], r = sqrt(r2);
+        double2 sc = scale[k];
+        int tp = type[a] * P.ntp + type[b];
+        double2 ab = lj14[tp];
+        double i2 = 1.0 / r2, i4 = i2 * i2, i6 = i4 * i2, i8 = i4 * i4, i12 = i6 * i6, i14 = i12 * i2;
+        if (SEM == MDF_SEM_PHYSICAL) {
+            double qq = q[a] * q[b] * P.kc / sc.x;
+            ec = qq / r;
+            double g = ec / r2;
+            if (ljvalid[tp]) {
+                ev = (ab.x * i12 - ab.y * i6) / sc.y;
+                g += (12.0 * ab.x * i14 - 6.0 * ab.y * i8) / sc.y;
+            }
+            add_pair_force(fatom, N, a, b, g, d, st);
+        } else {
+            double qq = q[a] * q[b];
+            double scee = sc.x;
+            if (r2 <= P.rc2 && r2 >= 1e-12) eall = (1.0 / scee) * ((qq / r) * P.kc);
+            bool in_list = r2 <= P.rlist2 && r2 > 1e-12 && ljvalid[tp];
+            if (in_list && r2 <= P.rc2 && r2 >= 1e-12) {
+                double U = ab.x * i12 - ab.y * i6, G = 12.0 * ab.x * i14 - 6.0 * ab.y * i8;
+                if (P.use_switch) {
+                    double S = 1.0, dS = 0.0;
+                    if (r > P.rsw) {
+                        if (r >= P.rc) S = 0.0;
+                        else {
+                            double x = (r - P.rsw) * P.inv_sw, x2 = x * x, x3 = x2 * x, x4 = x2 * x2, x5 = x4 * x;
+                            S = 1.0 - 10.0 * x3 + 15.0 * x4 - 6.0 * x5;
+                            dS = (-30.0 * x2 + 60.0 * x3 - 30.0 * x4) * P.inv_sw;
+                        }
+                    }
+                    G = S * G - (U / r) * dS;
+                    U = U * S;
+                } else {
+                    double c2 = 1.0 / P.rc2, c4 = c2 * c2, c6 = c4 * c2, c8 = c4 * c4, c12 = c6 * c6, c14 = c12 * c2;
+                    double ucut = ab.x * c12 - ab.y * c6, gcut = 12.0 * ab.x * c14 - 6.0 * ab.y * c8;
+                    U = U - ucut + (r - P.rc) * (gcut * P.rc);
+                    G = G - gcut * (P.rc / r);
+                }
+                ev = U;
+                epl = (1.0 / scee) * ((qq / r) * P.kc);
+                ecut = (1.0 / scee) * (qq * P.kc) * (1.0 / r - 1.0 / P.rc);
+                edir = ((1.0 / (scee * r)) - (erf(r) / r)) * (qq * P.kc);
+                double g = G + (1.0 / scee) * ((qq / (r2 * r)) * P.kc);
+                add_pair_force(fatom, N, a, b, g, d, st);
+            }
+        }
+    }
+    if (ENERGY) {
+        if (SEM == MDF_SEM_PHYSICAL) {
+            const double v[2] = {ev, ec};
+            const int idx[2] = {MDF_E_VDW14, MDF_E_EE14};
+            block_acc_fixed<2>(v, acc, idx, ENERGY_SCALE, st);
+        } else {
+            const double v[5] = {ev, eall, epl, ecut, edir};
+            const int idx[5] = {MDF_E_VDW, MDF_E_EE, MDF_E_EE_PAIRLIST, MDF_E_EE_CUTOFF, MDF_E_EE_DIRECT};
+            block_acc_fixed<5>(v, acc, idx, ENERGY_SCALE, st);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host
+static NBParams make_params(const Ctx& c)
+{
+    NBParams P;
+    for (int d = 0; d < 3; ++d) P.box[d] = c.box[d];
+    P.rc = c.p.cutoff;
+    P.rc2 = c.p.cutoff * c.p.cutoff;
+    P.use_switch = c.p.switch_radius > 0.0;
+    P.rsw = P.use_switch ? c.p.switch_radius : c.p.cutoff;
+    P.inv_sw = P.use_switch ? 1.0 / (c.p.cutoff - c.p.switch_radius) : 0.0;
+    P.kc = c.p.coulomb_const;
+    P.alpha = c.alpha;
+    double rl = c.p.cutoff + c.p.skin;
+    P.rlist2 = rl * rl;
+    P.ntp = c.ntp;
+    double i2 = 1.0 / P.rc2, i6 = i2 * i2 * i2;
+    P.ucut_pow6 = i6;
+    P.ucut_pow12 = i6 * i6;
+    return P;
+}
+
+template <typename R, int SEM>
+static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, const typename V2<R>::type* lj)
+{
+    NBParams P = make_params(c);
+    int nb = grid_blocks(c.n_clusters, NB_WARPS);
+    if (energy)
+        k_pairs<R, SEM, true><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, xq, c.slot_type.p,
+                                                               c.center.p, lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots,
+                                                               c.acc.p, c.npairs_cut.p, c.status.p);
+    else
+        k_pairs<R, SEM, false><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, xq,
+                                                                c.slot_type.p, c.center.p, lj, c.ljvalid.p, P,
+                                                                c.f_slot.p, c.n_slots, c.acc.p, c.npairs_cut.p,
+                                                                c.status.p);
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 1;
+}
+
+void launch_nonbonded(Ctx& c, bool energy)
+{
+    if (c.n_clusters == 0) return;
+    bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
+    if (c.p.precision == MDF_PREC_MIXED) {
+        if (phys) launch_pairs_t<float, MDF_SEM_PHYSICAL>(c, energy, c.xq_f.p, c.ljAB_f.p);
+        else launch_pairs_t<float, MDF_SEM_REFERENCE>(c, energy, c.xq_f.p, c.ljAB_f.p);
+    } else {
+        if (phys) launch_pairs_t<double, MDF_SEM_PHYSICAL>(c, energy, c.xq_d.p, c.ljAB.p);
+        else launch_pairs_t<double, MDF_SEM_REFERENCE>(c, energy, c.xq_d.p, c.ljAB.p);
+    }
+}
+
+void launch_exclusions(Ctx& c, bool energy)
+{
+    NBParams P = make_params(c);
+    const int th = 256;
+    bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
+    if (c.n_excl > 0) {
+        int nb = grid_blocks(c.n_excl, th);
+#define MDF_EXCL(S, E)                                                                                          \
+    k_exclusions<S, E><<<nb, th, 0, c.stream>>>(c.n_excl, c.excl_pairs.p, c.excl_is14.p, c.xyz.p, c.q.p, P, c.N, \
+                                                c.f_atom.p, c.acc.p, c.status.p)
+        if (phys) { if (energy) MDF_EXCL(MDF_SEM_PHYSICAL, true); else MDF_EXCL(MDF_SEM_PHYSICAL, false); }
+        else if (energy) MDF_EXCL(MDF_SEM_REFERENCE, true);
+#undef MDF_EXCL
+        if (phys || energy) c.launches += 1;
+    }
+    if (c.n_14 > 0) {
+        int nb = grid_blocks(c.n_14, th);
+#define MDF_P14(S, E)                                                                                             \
+    k_pairs14<S, E><<<nb, th, 0, c.stream>>>(c.n_14, c.pairs14.p, c.p14_scale.p, c.xyz.p, c.q.p, c.type.p,        \
+                                             c.lj14AB.p, c.ljvalid.p, P, c.N, c.f_atom.p, c.acc.p, c.status.p)
+        if (phys) { if (energy) MDF_P14(MDF_SEM_PHYSICAL, true); else MDF_P14(MDF_SEM_PHYSICAL, false); }
+        else { if (energy) MDF_P14(MDF_SEM_REFERENCE, true); else MDF_P14(MDF_SEM_REFERENCE, false); }
+#undef MDF_P14
+        c.launches += 1;
+    }
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+
+}  // namespace mdf

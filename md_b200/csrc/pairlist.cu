@@ -1,0 +1,529 @@
+// Cluster sort and cluster-pair list (replaces the reference's linked-list
+// cell pairlist, src/System/NonBondedUtils.cpp:185-282).
+//
+// Atoms are binned into x-y columns whose cross-section holds about one
+// cluster-height of atoms, sorted by z inside each column, and cut into
+// clusters of 8.  Every i cluster then gets the list of j clusters (j >= i,
+// half list) whose bounding boxes, in some periodic image, come within the
+// list cutoff (cutoff + skin).  Each entry carries a 64-bit mask of the atom
+// pairs that interact: padding slots, the lower triangle of the self pair and
+// excluded pairs are cleared.
+#include <algorithm>
+#include <cmath>
+
+#include "mdf_device.cuh"
+#include "mdf_internal.cuh"
+
+namespace mdf {
+
+int grid_blocks(long long n, int threads)
+{
+    long long b = (n + threads - 1) / threads;
+    return (int)std::max(1LL, b);
+}
+
+// ------------------------------------------------------------------ scan
+// Single-block exclusive scan; n up to a few million.
+__global__ void k_scan_1block(const int* __restrict__ in, int* __restrict__ out, int n, int* total)
+{
+    __shared__ int part[1024];
+    int tid = threadIdx.x;
+    int per = (n + blockDim.x - 1) / blockDim.x;
+    int b0 = tid * per, b1 = min(n, b0 + per);
+    int s = 0;
+    for (int i = b0; i < b1; ++i) s += in[i];
+    part[tid] = s;
+    __syncthreads();
+    // Hillis-Steele inclusive scan over the block partials
+    for (int o = 1; o < blockDim.x; o <<= 1) {
+        int v = tid >= o ? part[tid - o] : 0;
+        __syncthreads();
+        part[tid] += v;
+        __syncthreads();
+    }
+    int run = tid ? part[tid - 1] : 0;
+    for (int i = b0; i < b1; ++i) {
+        int v = in[i];
+        out[i] = run;
+        run += v;
+    }
+    if (tid == blockDim.x - 1 && total) *total = part[tid];
+}
+
+void exclusive_scan_int(const int* d_in, int* d_out, int n, int* d_total_out, cudaStream_t s)
+{
+    k_scan_1block<<<1, 1024, 0, s>>>(d_in, d_out, n, d_total_out);
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+
+// ------------------------------------------------------------- binning
+__global__ void k_assign_columns(int N, const double* __restrict__ xyz, double Lx, double Ly, int ncx, int ncy,
+                                 int* __restrict__ atom_col, int* __restrict__ col_count, unsigned* st)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2];
+    if (!isfinite(x) || !isfinite(y) || !isfinite(z)) {
+        status_set(st, ST_NONFINITE);
+        x = y = 0.0;
+    }
+    x = wrap_coord(x, Lx);
+    y = wrap_coord(y, Ly);
+    int cx = (int)(x * ncx / Lx), cy = (int)(y * ncy / Ly);
+    cx = min(max(cx, 0), ncx - 1);
+    cy = min(max(cy, 0), ncy - 1);
+    int col = cx + ncx * cy;
+    atom_col[i] = col;
+    atomicAdd(&col_count[col], 1);
+}
+
+__global__ void k_clusters_per_column(int ncols, const int* __restrict__ cnt, int* __restrict__ ncl)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < ncols) ncl[c] = (cnt[c] + CLUSTER - 1) / CLUSTER;
+}
+
+__global__ void k_bucket(int N, const int* __restrict__ atom_col, const int* __restrict__ col_start,
+                         int* __restrict__ col_fill, int* __restrict__ col_atoms)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int col = atom_col[i];
+    int pos = col_start[col] + atomicAdd(&col_fill[col], 1);
+    col_atoms[pos] = i;
+}
+
+constexpr int COL_MAX = 2048;   // atoms per column handled by the in-block sort
+
+// One block (1024 threads) per column: bitonic sort of (z, atom) keys, then
+// cut into clusters of 8.
+__global__ void __launch_bounds__(1024) k_sort_columns(const double* __restrict__ xyz, double Lz,
+                                                       const int* __restrict__ col_count,
+                                                       const int* __restrict__ col_start,
+                                                       const int* __restrict__ col_cstart,
+                                                       const int* __restrict__ col_atoms,
+                                                       int* __restrict__ slot_atom, int* __restrict__ atom_slot,
+                                                       int* __restrict__ cluster_col, unsigned* st)
+{
+    __shared__ unsigned long long key[COL_MAX];
+    int col = blockIdx.x, tid = threadIdx.x;
+    int n = col_count[col];
+    if (n > COL_MAX) {
+        if (tid == 0) status_set(st, ST_CAPACITY_COLUMN);
+        return;
+    }
+    int s0 = col_start[col];
+    // pad to the next power of two >= n (at least 2)
+    int m = 2;
+    while (m < n) m <<= 1;
+    for (int k = tid; k < m; k += blockDim.x) {
+        unsigned long long kk = ~0ull;
+        if (k < n) {
+            int a = col_atoms[s0 + k];
+            double zw = wrap_coord(xyz[3 * a + 2], Lz);
+            float zf = (float)zw;
+            if (!(zf >= 0.0f)) zf = 0.0f;
+            kk = ((unsigned long long)__float_as_uint(zf) << 32) | (unsigned)a;
+        }
+        key[k] = kk;
+    }
+    for (int size = 2; size <= m; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            __syncthreads();
+            for (int t = tid; t < (m >> 1); t += blockDim.x) {
+                int i = 2 * t - (t & (stride - 1));
+                int j = i + stride;
+                bool asc = (i & size) == 0;
+                unsigned long long a = key[i], b = key[j];
+                if ((a > b) == asc) {
+                    key[i] = b;
+                    key[j] = a;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    int c0 = col_cstart[col];
+    int ncl = (n + CLUSTER - 1) / CLUSTER;
+    for (int k = tid; k < ncl * CLUSTER; k += blockDim.x) {
+        int cl = c0 + k / CLUSTER;
+        int slot = cl * CLUSTER + (k % CLUSTER);
+        if (k < n) {
+            int a = (int)(key[k] & 0xffffffffu);
+            slot_atom[slot] = a;
+            atom_slot[a] = slot;
+        } else {
+            slot_atom[slot] = -1;
+        }
+        if ((k % CLUSTER) == 0) cluster_col[cl] = col;
+    }
+}
+
+// Cluster bounding boxes (wrapped coordinates) and centres; center.w = number
+// of real atoms in the cluster.
+__global__ void k_cluster_geom(int ncl, const double* __restrict__ xyz, double Lx, double Ly, double Lz,
+                               const int* __restrict__ slot_atom, double4* __restrict__ center,
+                               float4* __restrict__ bb_lo, float4* __restrict__ bb_hi)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncl) return;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    int nv = 0;
+    for (int k = 0; k < CLUSTER; ++k) {
+        int a = slot_atom[c * CLUSTER + k];
+        if (a < 0) continue;
+        ++nv;
+        double p[3] = {wrap_coord(xyz[3 * a], Lx), wrap_coord(xyz[3 * a + 1], Ly), wrap_coord(xyz[3 * a + 2], Lz)};
+        for (int d = 0; d < 3; ++d) {
+            lo[d] = fmin(lo[d], p[d]);
+            hi[d] = fmax(hi[d], p[d]);
+        }
+    }
+    if (nv == 0) {
+        for (int d = 0; d < 3; ++d) lo[d] = hi[d] = 0.0;
+    }
+    center[c] = make_double4(0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2]), (double)nv);
+    bb_lo[c] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]), __double2float_rd(lo[2]), 0.f);
+    bb_hi[c] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]), __double2float_ru(hi[2]), 0.f);
+}
+
+// Per-evaluation packing: cluster-ordered offsets from the cluster centre
+// (min image, so atoms crossing the box edge between rebuilds stay whole)
+// plus charge, in the working precision.
+template <typename R>
+__global__ void k_pack(int nslots, const double* __restrict__ xyz, const double* __restrict__ q,
+                       const int* __restrict__ slot_atom, const double4* __restrict__ center, double Lx, double Ly,
+                       double Lz, typename V4<R>::type* __restrict__ xq, unsigned* st)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    int a = slot_atom[s];
+    typename V4<R>::type v;
+    if (a < 0) {
+        v.x = v.y = v.z = v.w = (R)0;
+    } else {
+        double4 c = center[s / CLUSTER];
+        double dx = min_image(xyz[3 * a] - c.x, Lx), dy = min_image(xyz[3 * a + 1] - c.y, Ly),
+               dz = min_image(xyz[3 * a + 2] - c.z, Lz);
+        if (!isfinite(dx + dy + dz)) status_set(st, ST_NONFINITE);
+        v.x = (R)dx;
+        v.y = (R)dy;
+        v.z = (R)dz;
+        v.w = (R)q[a];
+    }
+    xq[s] = v;
+}
+
+__global__ void k_slot_type(int nslots, const int* __restrict__ slot_atom, const int* __restrict__ type, int pad_type,
+                            int* __restrict__ slot_type)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    int a = slot_atom[s];
+    slot_type[s] = a < 0 ? pad_type : type[a];
+}
+
+// -------------------------------------------------------- pair search
+struct SearchGeom {
+    double L[3];
+    double colw[3];
+    int ncx, ncy;
+    int Rx, Ry;
+    float rlist2;
+    float rlist;
+};
+
+__device__ __forceinline__ unsigned long long entry_mask(int nvi, int nvj, bool self_pair)
+{
+    unsigned long long row = (nvj >= 8) ? 0xffull : ((1ull << nvj) - 1ull);
+    unsigned long long m = 0;
+    for (int ii = 0; ii < nvi; ++ii) {
+        unsigned long long r = row;
+        if (self_pair) r &= ~((2ull << ii) - 1ull);   // keep jj > ii
+        m |= r << (8 * ii);
+    }
+    return m;
+}
+
+// One warp per i cluster.  FILL=false: count entries into icount[i];
+// FILL=true: write them at ilist[i].start (deterministic lane-major order).
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_pair_search(int ncl, SearchGeom g, const int* __restrict__ cluster_col,
+                                                     const int* __restrict__ col_cstart,
+                                                     const float4* __restrict__ bb_lo, const float4* __restrict__ bb_hi,
+                                                     const double4* __restrict__ center, int* __restrict__ icount,
+                                                     const int* __restrict__ istart, PairEntry* __restrict__ out,
+                                                     long long cap, ILRange* __restrict__ ilist, unsigned* st)
+{
+    int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (I >= ncl) return;
+    int col = cluster_col[I];
+    int cx = col % g.ncx, cy = col / g.ncx;
+    float4 lo = bb_lo[I], hi = bb_hi[I];
+    int nvi = (int)center[I].w;
+    int nxc = 2 * g.Rx + 1, nyc = 2 * g.Ry + 1;
+    int ncombo = nxc * nyc * 3;
+    float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
+    int cnt = 0;
+    long long base = 0;
+    // FILL runs two sweeps: count this lane's entries, then write them after
+    // the lane-exclusive prefix
+    for (int sweep = FILL ? 0 : 1; sweep < 2; ++sweep) {
+        if (FILL && sweep == 1) {
+            // lane-exclusive prefix
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            base = (long long)istart[I] + (incl - cnt);
+            if (lane == 31) {
+                ILRange r;
+                r.i = I;
+                r.start = istart[I];
+                r.count = incl;
+                r.pad = 0;
+                ilist[I] = r;
+            }
+            cnt = 0;
+        }
+        for (int combo = lane; combo < ncombo; combo += 32) {
+            int szi = combo % 3;
+            int rest = combo / 3;
+            int dcx = rest % nxc - g.Rx;
+            int dcy = rest / nxc - g.Ry;
+            int jx = cx + dcx, jy = cy + dcy;
+            int sx = jx < 0 ? -1 : (jx >= g.ncx ? 1 : 0);
+            int sy = jy < 0 ? -1 : (jy >= g.ncy ? 1 : 0);
+            jx -= sx * g.ncx;
+            jy -= sy * g.ncy;
+            int sz = szi - 1;
+            float cxl = (float)(jx * g.colw[0] + sx * g.L[0]), cxh = (float)((jx + 1) * g.colw[0] + sx * g.L[0]);
+            float cyl = (float)(jy * g.colw[1] + sy * g.L[1]), cyh = (float)((jy + 1) * g.colw[1] + sy * g.L[1]);
+            float gx = fmaxf(0.f, fmaxf(cxl - hi.x, lo.x - cxh));
+            float gy = fmaxf(0.f, fmaxf(cyl - hi.y, lo.y - cyh));
+            if (gx * gx + gy * gy > g.rlist2) continue;
+            float zmin = lo.z - g.rlist - sz * Lz, zmax = hi.z + g.rlist - sz * Lz;
+            if (zmax < -1.0f || zmin > Lz + 1.0f) continue;
+            int jcol = jx + g.ncx * jy;
+            int c0 = col_cstart[jcol], c1 = col_cstart[jcol + 1];
+            // first cluster whose hi.z >= zmin
+            int a = c0, b = c1;
+            while (a < b) {
+                int mid = (a + b) >> 1;
+                if (bb_hi[mid].z < zmin) a = mid + 1;
+                else b = mid;
+            }
+            for (int J = a; J < c1; ++J) {
+                float4 jl = bb_lo[J], jh = bb_hi[J];
+                if (jl.z > zmax) break;
+                float ox = sx * Lx, oy = sy * Ly, oz = sz * Lz;
+                float dx = fmaxf(0.f, fmaxf(jl.x + ox - hi.x, lo.x - (jh.x + ox)));
+                float dy = fmaxf(0.f, fmaxf(jl.y + oy - hi.y, lo.y - (jh.y + oy)));
+                float dz = fmaxf(0.f, fmaxf(jl.z + oz - hi.z, lo.z - (jh.z + oz)));
+                if (dx * dx + dy * dy + dz * dz > g.rlist2) continue;
+                int code = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+                if (J < I || (J == I && code < 13)) continue;
+                if (FILL && sweep == 1) {
+                    long long pos = base + cnt;
+                    if (pos < cap) {
+                        PairEntry e;
+                        e.j = J;
+                        e.shift = code;
+                        e.mask = entry_mask(nvi, (int)center[J].w, J == I && code == 13);
+                        out[pos] = e;
+                    } else {
+                        status_set(st, ST_CAPACITY_PAIRS);
+                    }
+                }
+                ++cnt;
+            }
+        }
+    }
+    if (!FILL) {
+        int tot = cnt;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+        if (lane == 0) icount[I] = tot;
+    }
+}
+
+// Clear the mask bit of every excluded pair in the entry that holds it.
+__global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const int* __restrict__ atom_slot,
+                                  const double* __restrict__ xyz, const double4* __restrict__ center, double Lx,
+                                  double Ly, double Lz, const ILRange* __restrict__ ilist,
+                                  PairEntry* __restrict__ plist)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nexcl) return;
+    int a = excl[2 * k], b = excl[2 * k + 1];
+    int sa = atom_slot[a], sb = atom_slot[b];
+    int Ia = sa / CLUSTER, la = sa % CLUSTER, Ib = sb / CLUSTER, lb = sb % CLUSTER;
+    double4 ca = center[Ia], cb = center[Ib];
+    // list-geometry positions: centre + min-image offset
+    double pa[3] = {ca.x + min_image(xyz[3 * a] - ca.x, Lx), ca.y + min_image(xyz[3 * a + 1] - ca.y, Ly),
+                    ca.z + min_image(xyz[3 * a + 2] - ca.z, Lz)};
+    double pb[3] = {cb.x + min_image(xyz[3 * b] - cb.x, Lx), cb.y + min_image(xyz[3 * b + 1] - cb.y, Ly),
+                    cb.z + min_image(xyz[3 * b + 2] - cb.z, Lz)};
+    // J atoms sit at p + s L in I's frame: s = round((p_I - p_J) / L)
+    int s[3] = {(int)round((pa[0] - pb[0]) / Lx), (int)round((pa[1] - pb[1]) / Ly), (int)round((pa[2] - pb[2]) / Lz)};
+    if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) return;  // never listed
+    int I, J, bit;
+    int code = (s[0] + 1) + 3 * (s[1] + 1) + 9 * (s[2] + 1);
+    if (Ia < Ib) {
+        I = Ia; J = Ib; bit = la * 8 + lb;
+    } else if (Ia > Ib) {
+        I = Ib; J = Ia; bit = lb * 8 + la; code = 26 - code;
+    } else {
+        I = J = Ia;
+        if (code == 13) bit = min(la, lb) * 8 + max(la, lb);
+        else if (code > 13) bit = la * 8 + lb;
+        else { bit = lb * 8 + la; code = 26 - code; }
+    }
+    ILRange r = ilist[I];
+    for (int e = r.start; e < r.start + r.count; ++e) {
+        if (plist[e].j == J && plist[e].shift == code) {
+            atomicAnd(&plist[e].mask, ~(1ull << bit));
+            break;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host
+static double atom_density(const Ctx& c)
+{
+    return (double)c.N / (c.box[0] * c.box[1] * c.box[2]);
+}
+
+void pack_positions(Ctx& c)
+{
+    int th = 256;
+    if (c.p.precision == MDF_PREC_MIXED) {
+        k_pack<float><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.xyz.p, c.q.p, c.slot_atom.p,
+                                                                         c.center.p, c.box[0], c.box[1], c.box[2],
+                                                                         c.xq_f.p, c.status.p);
+    } else {
+        k_pack<double><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.xyz.p, c.q.p, c.slot_atom.p,
+                                                                          c.center.p, c.box[0], c.box[1], c.box[2],
+                                                                          c.xq_d.p, c.status.p);
+    }
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 1;
+}
+
+void build_pairlist(Ctx& c)
+{
+    cudaStream_t s = c.stream;
+    const int th = 256;
+    double rlist = c.p.cutoff + c.p.skin;
+    for (int d = 0; d < 3; ++d)
+        if (!(c.box[d] >= 2.0 * c.p.cutoff))
+            throw ApiError(MDF_ERR_INVALID, "box edge shorter than twice the cutoff (minimum image undefined)");
+    // column cross-section ~ one cluster of atoms per column-height cube
+    double rho = atom_density(c);
+    double side = std::cbrt((double)CLUSTER / std::max(rho, 1e-6));
+    for (int attempt = 0; attempt < 6; ++attempt) {
+        c.ncol_x = std::max(1, (int)std::floor(c.box[0] / side));
+        c.ncol_y = std::max(1, (int)std::floor(c.box[1] / side));
+        double wx = c.box[0] / c.ncol_x, wy = c.box[1] / c.ncol_y;
+        int Rx = (int)std::floor(rlist / wx) + 1, Ry = (int)std::floor(rlist / wy) + 1;
+        if (Rx >= c.ncol_x || Ry >= c.ncol_y) {
+            // columns too wide for the one-image search: use more, thinner columns
+            side *= 0.75;
+            if (attempt == 5) throw ApiError(MDF_ERR_INVALID, "box too small for the list cutoff");
+            continue;
+        }
+        c.ncols = c.ncol_x * c.ncol_y;
+        c.col_count.alloc(c.ncols + 1);
+        c.col_start.alloc(c.ncols + 1);
+        c.col_cstart.alloc(c.ncols + 1);
+        c.scan_tmp.alloc(c.ncols + 1);
+        c.atom_col.alloc(c.N);
+        c.col_atoms.alloc(c.N);
+        c.atom_slot.alloc(c.N);
+        MDF_CUDA_TRY(cudaMemsetAsync(c.col_count.p, 0, sizeof(int) * (c.ncols + 1), s));
+        MDF_CUDA_TRY(cudaMemsetAsync(c.status.p, 0, sizeof(unsigned), s));
+        k_assign_columns<<<grid_blocks(c.N, th), th, 0, s>>>(c.N, c.xyz.p, c.box[0], c.box[1], c.ncol_x, c.ncol_y,
+                                                             c.atom_col.p, c.col_count.p, c.status.p);
+        exclusive_scan_int(c.col_count.p, c.col_start.p, c.ncols + 1, nullptr, s);
+        k_clusters_per_column<<<grid_blocks(c.ncols + 1, th), th, 0, s>>>(c.ncols + 1, c.col_count.p, c.scan_tmp.p);
+        exclusive_scan_int(c.scan_tmp.p, c.col_cstart.p, c.ncols + 1, nullptr, s);
+        int ncl = 0;
+        MDF_CUDA_TRY(cudaMemcpyAsync(&ncl, c.col_cstart.p + c.ncols, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MDF_CUDA_TRY(cudaMemsetAsync(c.scan_tmp.p, 0, sizeof(int) * (c.ncols + 1), s));
+        k_bucket<<<grid_blocks(c.N, th), th, 0, s>>>(c.N, c.atom_col.p, c.col_start.p, c.scan_tmp.p, c.col_atoms.p);
+        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        c.n_clusters = ncl;
+        c.n_slots = ncl * CLUSTER;
+        c.slot_atom.alloc(c.n_slots);
+        c.cluster_col.alloc(ncl);
+        k_sort_columns<<<c.ncols, 1024, 0, s>>>(c.xyz.p, c.box[2], c.col_count.p, c.col_start.p, c.col_cstart.p,
+                                                c.col_atoms.p, c.slot_atom.p, c.atom_slot.p, c.cluster_col.p,
+                                                c.status.p);
+        unsigned st = 0;
+        MDF_CUDA_TRY(cudaMemcpyAsync(&st, c.status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite position");
+        if (st & ST_CAPACITY_COLUMN) {
+            side *= 0.7;   // too many atoms in a column: thinner columns
+            if (attempt == 5) throw ApiError(MDF_ERR_CAPACITY, "column too populated for the in-block sort");
+            continue;
+        }
+        // geometry
+        c.center.alloc(ncl);
+        c.bb_lo.alloc(ncl);
+        c.bb_hi.alloc(ncl);
+        k_cluster_geom<<<grid_blocks(ncl, th), th, 0, s>>>(ncl, c.xyz.p, c.box[0], c.box[1], c.box[2], c.slot_atom.p,
+                                                           c.center.p, c.bb_lo.p, c.bb_hi.p);
+        c.slot_type.alloc(c.n_slots);
+        k_slot_type<<<grid_blocks(c.n_slots, th), th, 0, s>>>(c.n_slots, c.slot_atom.p, c.type.p, c.ntp - 1,
+                                                              c.slot_type.p);
+        if (c.p.precision == MDF_PREC_MIXED) c.xq_f.alloc(c.n_slots);
+        else c.xq_d.alloc(c.n_slots);
+        MDF_CUDA_TRY(cudaGetLastError());
+
+        SearchGeom g;
+        for (int d = 0; d < 3; ++d) g.L[d] = c.box[d];
+        g.colw[0] = c.box[0] / c.ncol_x;
+        g.colw[1] = c.box[1] / c.ncol_y;
+        g.colw[2] = c.box[2];
+        g.ncx = c.ncol_x;
+        g.ncy = c.ncol_y;
+        g.Rx = Rx;
+        g.Ry = Ry;
+        // bounding boxes are rounded outward to float; pad the list radius a hair
+        g.rlist = (float)(rlist * (1.0 + 1e-6));
+        g.rlist2 = g.rlist * g.rlist;
+        c.icount.alloc(ncl + 1);
+        c.ilist.alloc(ncl);
+        MDF_CUDA_TRY(cudaMemsetAsync(c.icount.p, 0, sizeof(int) * (ncl + 1), s));
+        int wblocks = grid_blocks((long long)ncl * 32, th);
+        k_pair_search<false><<<wblocks, th, 0, s>>>(ncl, g, c.cluster_col.p, c.col_cstart.p, c.bb_lo.p, c.bb_hi.p,
+                                                    c.center.p, c.icount.p, nullptr, nullptr, 0, nullptr, c.status.p);
+        c.scan_tmp.alloc(ncl + 1);
+        exclusive_scan_int(c.icount.p, c.scan_tmp.p, ncl + 1, nullptr, s);
+        int total = 0;
+        MDF_CUDA_TRY(cudaMemcpyAsync(&total, c.scan_tmp.p + ncl, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        c.n_entries = total;
+        c.plist.alloc((size_t)total + 1);
+        k_pair_search<true><<<wblocks, th, 0, s>>>(ncl, g, c.cluster_col.p, c.col_cstart.p, c.bb_lo.p, c.bb_hi.p,
+                                                   c.center.p, nullptr, c.scan_tmp.p, c.plist.p, total, c.ilist.p,
+                                                   c.status.p);
+        if (c.n_excl > 0)
+            k_exclusion_masks<<<grid_blocks(c.n_excl, th), th, 0, s>>>(c.n_excl, c.excl_pairs.p, c.atom_slot.p,
+                                                                      c.xyz.p, c.center.p, c.box[0], c.box[1],
+                                                                      c.box[2], c.ilist.p, c.plist.p);
+        MDF_CUDA_TRY(cudaGetLastError());
+        MDF_CUDA_TRY(cudaMemcpyAsync(&st, c.status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        if (st & ST_CAPACITY_PAIRS) throw ApiError(MDF_ERR_CAPACITY, "pair list capacity exceeded");
+        c.f_slot.alloc((size_t)3 * c.n_slots);
+        c.have_list = true;
+        return;
+    }
+}
+
+}  // namespace mdf

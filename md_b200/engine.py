@@ -1,0 +1,221 @@
+"""Python binding of libmdf (ctypes over include/mdf.h).
+
+This is plumbing for tests, the benchmark and Python users; the product is
+the C ABI.  There is no CPU fallback: without the built library or without a
+CUDA device every call raises MDFError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_LIB = None
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmdf.so")
+
+EXPORTS = [
+    "mdf_params_default", "mdf_create", "mdf_destroy", "mdf_last_error", "mdf_status_string",
+    "mdf_set_positions", "mdf_set_positions_device", "mdf_set_box", "mdf_build_pairlist", "mdf_compute",
+    "mdf_compute_async", "mdf_fetch", "mdf_forces_device", "mdf_get_pme_forces", "mdf_set_stream",
+    "mdf_pairlist_info", "mdf_enable_timing", "mdf_kernel_times", "mdf_cmap_coefficients",
+    "mdf_kernel_launches", "mdf_probe_fma_tflops",
+]
+
+
+class MDFError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__("%s: %s" % (abi.STATUS.get(status, status), message))
+        self.status = status
+
+
+def library(path=None):
+    """Load libmdf.so (building it first if the sources are present and it is missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        from . import build as _build
+        _build.build()
+    lib = C.CDLL(path)
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int32)
+    lib.mdf_params_default.argtypes = [C.POINTER(abi.mdf_params)]
+    lib.mdf_params_default.restype = None
+    lib.mdf_create.argtypes = [C.POINTER(abi.mdf_topology), C.POINTER(abi.mdf_params), C.POINTER(C.c_void_p)]
+    lib.mdf_destroy.argtypes = [C.c_void_p]
+    lib.mdf_destroy.restype = None
+    lib.mdf_last_error.argtypes = [C.c_void_p]
+    lib.mdf_last_error.restype = C.c_char_p
+    lib.mdf_status_string.argtypes = [C.c_int]
+    lib.mdf_status_string.restype = C.c_char_p
+    lib.mdf_set_positions.argtypes = [C.c_void_p, dp]
+    lib.mdf_set_positions_device.argtypes = [C.c_void_p, C.c_void_p]
+    lib.mdf_set_box.argtypes = [C.c_void_p, dp]
+    lib.mdf_build_pairlist.argtypes = [C.c_void_p]
+    lib.mdf_compute.argtypes = [C.c_void_p, C.c_uint32, dp, C.POINTER(abi.mdf_energies)]
+    lib.mdf_compute_async.argtypes = [C.c_void_p, C.c_uint32]
+    lib.mdf_fetch.argtypes = [C.c_void_p, dp, C.POINTER(abi.mdf_energies)]
+    lib.mdf_forces_device.argtypes = [C.c_void_p, C.c_void_p]
+    lib.mdf_get_pme_forces.argtypes = [C.c_void_p, dp]
+    lib.mdf_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    lib.mdf_pairlist_info.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.mdf_enable_timing.argtypes = [C.c_void_p, C.c_int]
+    lib.mdf_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int]
+    lib.mdf_cmap_coefficients.argtypes = [C.c_int, C.c_int, dp, dp]
+    lib.mdf_kernel_launches.argtypes = [C.c_void_p]
+    lib.mdf_kernel_launches.restype = C.c_int64
+    lib.mdf_probe_fma_tflops.argtypes = [C.c_int, C.c_int, dp]
+    _LIB = lib
+    return lib
+
+
+def cmap_coefficients(nsets, res, grids):
+    """Bicubic CMAP coefficient table through the C ABI (host only, no GPU)."""
+    g = np.ascontiguousarray(grids, dtype=np.float64)
+    out = np.zeros(nsets * res * res * 16)
+    rc = library().mdf_cmap_coefficients(nsets, res, g.ctypes.data_as(C.POINTER(C.c_double)),
+                                         out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise MDFError(rc, "mdf_cmap_coefficients")
+    return out
+
+
+def probe_fma_tflops(device=0, precision=abi.MDF_PREC_MIXED):
+    """Measured CUDA-core FMA throughput (TFLOP/s) of the device."""
+    v = C.c_double(0)
+    rc = library().mdf_probe_fma_tflops(device, precision, C.byref(v))
+    if rc != 0:
+        raise MDFError(rc, "mdf_probe_fma_tflops")
+    return v.value
+
+
+def default_params():
+    p = abi.mdf_params()
+    library().mdf_params_default(C.byref(p))
+    return p
+
+
+class Engine:
+    """One libmdf context (one system on one GPU)."""
+
+    def __init__(self, flat, box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, cutoff=10.0,
+                 skin=2.0, switch_radius=9.0, ewald_tol=1e-5, ewald_alpha=0.0, grid=(0, 0, 0), pme_order=4,
+                 device=0):
+        self.lib = library()
+        self.flat = flat
+        self.natoms = flat.natoms
+        p = default_params()
+        p.semantics, p.precision = int(semantics), int(precision)
+        for k in range(3):
+            p.box[k] = float(box[k])
+            p.grid[k] = int(grid[k])
+        p.cutoff, p.skin, p.switch_radius = float(cutoff), float(skin), float(switch_radius)
+        p.ewald_tol, p.ewald_alpha, p.pme_order, p.device = float(ewald_tol), float(ewald_alpha), int(pme_order), int(device)
+        self.params = p
+        h = C.c_void_p()
+        rc = self.lib.mdf_create(C.byref(flat.struct()), C.byref(p), C.byref(h))
+        if rc != 0:
+            raise MDFError(rc, self.lib.mdf_last_error(None).decode())
+        self.h = h
+        self._f = np.zeros((self.natoms, 3))
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise MDFError(rc, "%s: %s" % (what, self.lib.mdf_last_error(self.h).decode()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_positions(self, xyz):
+        x = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1)
+        if x.size != 3 * self.natoms:
+            raise ValueError("expected %d coordinates" % (3 * self.natoms))
+        self._check(self.lib.mdf_set_positions(self.h, x.ctypes.data_as(C.POINTER(C.c_double))), "set_positions")
+
+    def set_positions_ptr(self, host_ptr):
+        """Host positions from a raw pointer (e.g. pinned memory)."""
+        self._check(self.lib.mdf_set_positions(self.h, C.cast(C.c_void_p(host_ptr), C.POINTER(C.c_double))),
+                    "set_positions")
+
+    def compute_into(self, forces_ptr, energy=True):
+        """mdf_compute writing forces to a raw host pointer; returns energies."""
+        flags = abi.MDF_COMPUTE_FORCES | (abi.MDF_COMPUTE_ENERGY if energy else 0)
+        e = abi.mdf_energies()
+        self._check(self.lib.mdf_compute(self.h, flags, C.cast(C.c_void_p(forces_ptr), C.POINTER(C.c_double)),
+                                         C.byref(e)), "compute")
+        return e
+
+    def launches(self):
+        return int(self.lib.mdf_kernel_launches(self.h))
+
+    def set_positions_device(self, ptr):
+        self._check(self.lib.mdf_set_positions_device(self.h, C.c_void_p(ptr)), "set_positions_device")
+
+    def set_box(self, box):
+        b = np.ascontiguousarray(box, dtype=np.float64)
+        self._check(self.lib.mdf_set_box(self.h, b.ctypes.data_as(C.POINTER(C.c_double))), "set_box")
+
+    def set_stream(self, stream_ptr):
+        self._check(self.lib.mdf_set_stream(self.h, C.c_void_p(stream_ptr)), "set_stream")
+
+    def build_pairlist(self):
+        self._check(self.lib.mdf_build_pairlist(self.h), "build_pairlist")
+
+    def compute(self, energy=True, forces=True, pme_reference=False):
+        flags = (abi.MDF_COMPUTE_ENERGY if energy else 0) | (abi.MDF_COMPUTE_FORCES if forces else 0)
+        if pme_reference:
+            flags |= abi.MDF_COMPUTE_PME_REFERENCE
+        e = abi.mdf_energies()
+        f = np.zeros((self.natoms, 3)) if forces else None
+        fp = f.ctypes.data_as(C.POINTER(C.c_double)) if forces else None
+        self._check(self.lib.mdf_compute(self.h, flags, fp, C.byref(e)), "compute")
+        out = e.as_dict() if energy else None
+        if energy:
+            out["virial"] = np.array(e.virial[:]).reshape(3, 3)
+        return out, f
+
+    def compute_async(self, energy=True, pme_reference=False):
+        flags = abi.MDF_COMPUTE_FORCES | (abi.MDF_COMPUTE_ENERGY if energy else 0)
+        if pme_reference:
+            flags |= abi.MDF_COMPUTE_PME_REFERENCE
+        self._check(self.lib.mdf_compute_async(self.h, flags), "compute_async")
+
+    def fetch(self, forces=True, energy=True):
+        e = abi.mdf_energies()
+        f = np.zeros((self.natoms, 3)) if forces else None
+        fp = f.ctypes.data_as(C.POINTER(C.c_double)) if forces else None
+        self._check(self.lib.mdf_fetch(self.h, fp, C.byref(e) if energy else None), "fetch")
+        return (e.as_dict() if energy else None), f
+
+    def forces_device(self, ptr):
+        self._check(self.lib.mdf_forces_device(self.h, C.c_void_p(ptr)), "forces_device")
+
+    def pme_forces(self):
+        f = np.zeros((self.natoms, 3))
+        self._check(self.lib.mdf_get_pme_forces(self.h, f.ctypes.data_as(C.POINTER(C.c_double))), "pme_forces")
+        return f
+
+    def pairlist_info(self):
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(self.lib.mdf_pairlist_info(self.h, C.byref(a), C.byref(b), C.byref(c)), "pairlist_info")
+        return dict(clusters=a.value, cluster_pairs=b.value, pairs_in_cutoff=c.value)
+
+    def enable_timing(self, on=True):
+        self._check(self.lib.mdf_enable_timing(self.h, 1 if on else 0), "enable_timing")
+
+    def kernel_times(self):
+        names = (C.c_char_p * 32)()
+        ms = (C.c_float * 32)()
+        n = self.lib.mdf_kernel_times(self.h, names, ms, 32)
+        return [(names[i].decode(), ms[i]) for i in range(n)]

@@ -241,7 +241,8 @@ def make_system(name, box, n_waters, n_residues, seed, atoms_per_residue=10,
         hsh.add(chain_pos[0], 0)
         for i in range(1, n_chain):
             r = bond_r0_c[chain_bond_type[i - 1]] * (1.0 + rng.normal(0, 0.02))
-            best, best_score = None, -1.0
+            best, best_score = None, -1e9
+            fallback = None
             for attempt in range(60):
                 if i == 1:
                     v = rng.normal(size=3); v /= np.linalg.norm(v)
@@ -252,6 +253,7 @@ def make_system(name, box, n_waters, n_residues, seed, atoms_per_residue=10,
                     a = chain_pos[i - 3] if i >= 3 else chain_pos[i - 2] + np.array([0.3, 0.7, 0.1])
                     cand = _place_next(a, chain_pos[i - 2], chain_pos[i - 1], r, th, ph)
                 if np.any(np.abs(cand - center) > 0.62 * box):
+                    fallback = cand
                     continue
                 near = [t for t in hsh.near(cand, 2.7) if t < i - 3]
                 if not near:
@@ -260,6 +262,8 @@ def make_system(name, box, n_waters, n_residues, seed, atoms_per_residue=10,
                 score = -len(near)
                 if score > best_score or best is None:
                     best, best_score = cand, score
+            if best is None:
+                best = fallback
             chain_pos[i] = best
             hsh.add(best, i)
 
@@ -503,10 +507,12 @@ CONFIGS = {
     # small cases the oracle finishes in well under a second
     "tiny": dict(box=22.0, n_waters=300, n_residues=3, seed=11),
     "small": dict(box=30.0, n_waters=800, n_residues=8, seed=12),
-    # 66 A cube, 9,000 waters + 120-residue chain (about 28k atoms)
-    "c0": dict(box=66.0, n_waters=9000, n_residues=120, seed=1000),
-    # 100 A cube, about 32,000 waters + 400-residue chain (about 100k atoms)
-    "c1": dict(box=100.0, n_waters=32000, n_residues=400, seed=1001),
+    # 66 A cube, about 9,000 waters (after removing those overlapping the
+    # chain) + a 120-residue chain: about 28k atoms
+    "c0": dict(box=66.0, n_waters=10050, n_residues=120, seed=1000),
+    # 100 A cube, about 32,000 waters (after overlap removal) + a 400-residue
+    # chain: about 100k atoms
+    "c1": dict(box=100.0, n_waters=35300, n_residues=400, seed=1001),
     # 215 A cube of about 320,000 waters (about 960k atoms)
     "c4": dict(box=215.0, n_waters=320000, n_residues=0, seed=1004),
 }

@@ -1,0 +1,199 @@
+"""GPU parity: libmdf (through its C ABI) against the oracles.
+
+Tolerances:
+  REFERENCE, FP64 vs the unmodified reference (golden O1 fixtures):
+      energies 1e-9 relative, forces 1e-9 rms relative (spec: 1e-6 / 1e-5);
+      the reference's PME-chain forces 1e-8 (the GPU charge grid is int64
+      fixed point at 2^-40).
+  PHYSICAL, FP64 vs O2: energies 1e-9 relative, forces 1e-9 rms relative.
+  PHYSICAL, MIXED vs O2: forces <= 1e-5 rms relative (the target), total
+      energy 1e-6 relative.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from md_b200 import abi, engine, synth
+from oracle import oracle as O
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+REF, PHYS = abi.MDF_SEM_REFERENCE, abi.MDF_SEM_PHYSICAL
+FP64, MIXED = abi.MDF_PREC_FP64, abi.MDF_PREC_MIXED
+E_REF_TERMS = ["bond", "angle", "dihedral", "ub", "improper", "cmap", "vdw", "ee", "ee_pairlist", "ee_cutoff",
+               "ee_direct", "ee_self"]
+E_PHYS_TERMS = ["bond", "angle", "dihedral", "ub", "improper", "cmap", "vdw", "vdw14", "ee_direct", "ee14",
+                "ee_excl", "ee_self", "ee_recip"]
+
+
+def make_engine(s, sem, prec, grid, tol=1e-5, **kw):
+    flat = H.flat(s, sem, engine.cmap_coefficients)
+    eng = engine.Engine(flat, s.box, semantics=sem, precision=prec, ewald_tol=tol, grid=grid, **kw)
+    eng.set_positions(s.coords)
+    eng.build_pairlist()
+    return eng, flat
+
+
+@pytest.mark.parametrize("case", ["tiny", "tiny_sentinel", "small", "c0"])
+def test_reference_fp64_matches_reference_cpu(case):
+    g = H.golden(case)
+    m = g["meta"]
+    s = H.system(m["config"], m["sentinels"])
+    eng, _ = make_engine(s, REF, FP64, m["grid"])
+    E, F = eng.compute(pme_reference=True)
+    for k in E_REF_TERMS:
+        assert H.rel(E[k], g["energies"][k]) < 1e-9, (k, E[k], g["energies"][k])
+    H.check_forces_vs_golden(F, g, 1e-9, "forces")
+    H.check_forces_vs_golden(eng.pme_forces(), g, 1e-8, "forces_pme")
+    eng.close()
+
+
+@pytest.mark.parametrize("cfg", ["tiny", "small", "c0"])
+def test_physical_fp64_matches_o2(cfg):
+    s = H.system(cfg)
+    grid = synth.GRIDS[cfg]
+    eng, flat = make_engine(s, PHYS, FP64, grid)
+    E, F = eng.compute()
+    p = O.make_params(PHYS, s.box, grid, H.alpha_for(1e-5), H.KC)
+    e2, f2, vir2, _, np2 = O.evaluate(flat, p, s.coords)
+    for k in E_PHYS_TERMS:
+        ref = e2[abi.E_INDEX[k]]
+        assert abs(E[k] - ref) <= 1e-9 * max(abs(ref), 1.0), (k, E[k], ref)
+    assert H.frel(F, f2) < 1e-9
+    assert np.allclose(E["virial"].ravel(), vir2, rtol=1e-9, atol=1e-7)
+    assert eng.pairlist_info()["pairs_in_cutoff"] == np2
+    eng.close()
+
+
+@pytest.mark.parametrize("cfg", ["small", "c0", "c1"])
+def test_mixed_precision_force_error_below_1e5(cfg):
+    s = H.system(cfg)
+    grid = synth.GRIDS[cfg]
+    eng, flat = make_engine(s, PHYS, MIXED, grid)
+    E, F = eng.compute()
+    p = O.make_params(PHYS, s.box, grid, H.alpha_for(1e-5), H.KC)
+    e2, f2, _, _, _ = O.evaluate(flat, p, s.coords)
+    err = H.frel(F, f2)
+    assert err <= 1e-5, err
+    tot2 = sum(e2[abi.E_INDEX[k]] for k in E_PHYS_TERMS)
+    assert H.rel(E["total"], tot2) < 1e-6
+    eng.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_bit_reproducible(prec):
+    s = H.system("small")
+    eng, _ = make_engine(s, PHYS, prec, (32, 32, 32))
+    E1, F1 = eng.compute()
+    E2, F2 = eng.compute()
+    assert np.array_equal(F1, F2)
+    assert all(E1[k] == E2[k] for k in E_PHYS_TERMS)
+    # a fresh context (fresh pairlist build) gives the same bits too
+    eng2, _ = make_engine(s, PHYS, prec, (32, 32, 32))
+    E3, F3 = eng2.compute()
+    assert np.array_equal(F1, F3)
+    eng.close(); eng2.close()
+
+
+def test_periodic_images_of_positions_give_identical_results():
+    """Whole-box shifts of individual molecules change nothing (min image)."""
+    s = H.system("small")
+    eng, flat = make_engine(s, PHYS, FP64, (32, 32, 32))
+    E1, F1 = eng.compute()
+    x = s.coords.copy()
+    nchain = s.meta["n_chain"]
+    # shift every water molecule by a random whole-box vector
+    rng = np.random.default_rng(3)
+    for w in range(nchain, s.natoms, 3):
+        x[w:w + 3] += rng.integers(-2, 3, 3) * s.box
+    eng.set_positions(x)
+    eng.build_pairlist()
+    E2, F2 = eng.compute()
+    assert H.frel(F2, F1) < 1e-12
+    assert H.rel(E2["total"], E1["total"]) < 1e-12
+    eng.close()
+
+
+def test_list_reuse_within_skin_matches_rebuild():
+    s = H.system("small")
+    eng, flat = make_engine(s, PHYS, FP64, (32, 32, 32))
+    rng = np.random.default_rng(5)
+    x = s.coords + rng.uniform(-0.4, 0.4, s.coords.shape)   # < skin/2
+    eng.set_positions(x)
+    E1, F1 = eng.compute()           # old list
+    eng.build_pairlist()
+    E2, F2 = eng.compute()           # new list
+    assert H.frel(F1, F2) < 1e-12
+    assert H.rel(E1["total"], E2["total"]) < 1e-12
+    eng.close()
+
+
+def test_force_shifted_lj_and_noncubic_box():
+    s = synth.make_system("nc", (31.0, 27.5, 36.0), 900, 6, seed=77)
+    grid = (32, 27, 36)
+    flat = H.flat(s, PHYS, engine.cmap_coefficients)
+    eng = engine.Engine(flat, s.box, semantics=PHYS, precision=FP64, ewald_tol=1e-5, grid=grid, switch_radius=0.0)
+    eng.set_positions(s.coords)
+    E, F = eng.compute()
+    p = O.make_params(PHYS, s.box, grid, H.alpha_for(1e-5), H.KC, switch=0.0)
+    e2, f2, _, _, _ = O.evaluate(flat, p, s.coords)
+    assert H.frel(F, f2) < 1e-9
+    for k in E_PHYS_TERMS:
+        ref = e2[abi.E_INDEX[k]]
+        assert abs(E[k] - ref) <= 1e-9 * max(abs(ref), 1.0), k
+    eng.close()
+
+
+def test_smallest_box_two_cutoffs():
+    """Box edge exactly twice the cutoff: several images per cluster pair."""
+    s = synth.make_system("b20", 20.0, 250, 2, seed=8)
+    flat = H.flat(s, PHYS, engine.cmap_coefficients)
+    eng = engine.Engine(flat, s.box, semantics=PHYS, precision=FP64, ewald_tol=1e-5, grid=(20, 20, 20))
+    eng.set_positions(s.coords)
+    E, F = eng.compute()
+    p = O.make_params(PHYS, s.box, (20, 20, 20), H.alpha_for(1e-5), H.KC)
+    e2, f2, _, _, np2 = O.evaluate(flat, p, s.coords)
+    assert H.frel(F, f2) < 1e-9
+    assert eng.pairlist_info()["pairs_in_cutoff"] == np2
+    eng.close()
+
+
+def test_pure_water_no_bonded_chain():
+    s = synth.make_system("w", 24.0, 460, 0, seed=9)
+    eng, flat = make_engine(s, PHYS, MIXED, (24, 24, 24))
+    E, F = eng.compute()
+    p = O.make_params(PHYS, s.box, (24, 24, 24), H.alpha_for(1e-5), H.KC)
+    e2, f2, _, _, _ = O.evaluate(flat, p, s.coords)
+    assert H.frel(F, f2) < 1e-5
+    eng.close()
+
+
+def test_nacl_madelung_on_gpu():
+    x, q, box = H.nacl_crystal(4, 5.64)
+    flat = H.simple_flat(q)
+    eng = engine.Engine(flat, box, semantics=PHYS, precision=FP64, ewald_alpha=0.42, grid=(64, 64, 64),
+                        switch_radius=0.0)
+    eng.set_positions(x)
+    E, F = eng.compute()
+    etot = E["ee_direct"] + E["ee_recip"] + E["ee_self"]
+    M = -etot / (len(q) / 2) * (5.64 / 2) / H.KC
+    assert abs(M - H.MADELUNG_NACL) < 2e-6
+    assert np.abs(F).max() < 1e-6          # perfect lattice: no net force
+    eng.close()
+
+
+def test_nonfinite_position_reported_not_faulted():
+    s = H.system("tiny")
+    eng, _ = make_engine(s, PHYS, MIXED, (24, 24, 24))
+    x = s.coords.copy()
+    x[5, 1] = np.nan
+    eng.set_positions(x)
+    with pytest.raises(engine.MDFError) as e:
+        eng.compute()
+    assert e.value.status == 4
+    # the context stays usable
+    eng.set_positions(s.coords)
+    E, F = eng.compute()
+    assert np.isfinite(F).all()
+    eng.close()

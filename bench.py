@@ -59,7 +59,32 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--profile", metavar="CONFIG", default=None,
+                    help="profiling run: build CONFIG (tiny, small, c0, c1, c4), run --warmup + --steps "
+                         "evaluations, print the per-phase times and exit (for ncu)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     return ap.parse_args()
+
+
+def run_profile(args):
+    """Plain evaluation loop for profilers: no timing bookkeeping of our own."""
+    import torch
+    from md_b200 import abi, engine, synth, topology
+    s = synth.make_config(args.profile)
+    flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    prec = abi.MDF_PREC_MIXED if args.precision == "mixed" else abi.MDF_PREC_FP64
+    eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=prec, ewald_tol=1e-5,
+                        grid=synth.GRIDS[args.profile])
+    eng.set_positions(s.coords)
+    eng.build_pairlist()
+    for _ in range(args.warmup + args.steps):
+        eng.compute_async(energy=True)
+        eng.fetch(forces=False)
+    eng.enable_timing(True)
+    eng.compute()
+    print(json.dumps({"profile": args.profile, "natoms": s.natoms, "precision": args.precision,
+                      "pairlist": eng.pairlist_info(), "phase_ms": dict(eng.kernel_times())}))
+    eng.close()
 
 
 def dist_setup(args):
@@ -171,6 +196,9 @@ def run_reference_arm(args, rank):
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
+    if args.profile:
+        run_profile(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args, rank)
         return

@@ -139,7 +139,16 @@ typedef struct {
     int32_t pme_order;       /* PHYSICAL B-spline order (4); REFERENCE uses its order-5 chain */
     double coulomb_const;    /* 18.2206899283247^2 */
     int32_t device;          /* CUDA device ordinal */
-    int32_t reserved[7];
+    /* Dynamic pruning of the cluster-pair list: every prune_every evaluations
+     * the entries whose closest atom pair lies beyond cutoff + prune_margin
+     * are dropped from the list the pair kernel walks (the outer list keeps
+     * them).  prune_every = 1, prune_margin = 0 prunes against the current
+     * positions at every evaluation (exact); larger intervals need a margin
+     * of at least twice the largest displacement between prunes.
+     * prune_every = 0 disables pruning. */
+    int32_t prune_every;
+    double prune_margin;
+    int32_t reserved[4];
 } mdf_params;
 
 /* Flags for mdf_compute. */
@@ -191,10 +200,11 @@ int mdf_get_pme_forces(mdf_ctx *ctx, double *forces_out);
  * context's own stream. */
 int mdf_set_stream(mdf_ctx *ctx, void *stream);
 
-/* Sizes of the current pairlist (clusters, cluster pairs, atom pairs within
- * the cutoff from the last evaluation or -1). */
+/* Sizes of the current pairlist: clusters, cluster pairs of the outer list,
+ * cluster pairs kept by the last prune, and atom pairs within the cutoff that
+ * the last evaluation computed (-1 where unknown).  Any pointer may be NULL. */
 int mdf_pairlist_info(mdf_ctx *ctx, int64_t *n_clusters, int64_t *n_cluster_pairs,
-                      int64_t *n_pairs_in_cutoff);
+                      int64_t *n_cluster_pairs_pruned, int64_t *n_pairs_in_cutoff);
 
 /* Kernel timings of the last evaluation in milliseconds, recorded with CUDA
  * events when MDF timing is enabled (mdf_enable_timing). names[i] points to

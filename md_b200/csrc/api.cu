@@ -212,6 +212,14 @@ static void eval_async(Ctx& c, uint32_t flags)
     MDF_CUDA_TRY(cudaMemsetAsync(c.status.p, 0, sizeof(unsigned), s));
     pack_positions(c);
     mark(c, "pack");
+    if (c.p.prune_every > 0) {
+        if (!c.pruned_valid || c.since_prune >= c.p.prune_every) {
+            prune_pairlist(c);
+            c.since_prune = 0;
+        }
+        ++c.since_prune;
+        mark(c, "prune");
+    }
     launch_nonbonded(c, energy);
     mark(c, "pairs");
     launch_exclusions(c, energy);
@@ -326,6 +334,8 @@ void mdf_params_default(mdf_params* p)
     long double r = 18.2206899283247L;
     p->coulomb_const = (double)(r * r);
     p->device = 0;
+    p->prune_every = 1;
+    p->prune_margin = 0.0;
 }
 
 const char* mdf_status_string(int status)
@@ -412,6 +422,7 @@ void mdf_destroy(mdf_ctx* ctx)
     c.col_atoms.release(); c.slot_atom.release(); c.atom_slot.release(); c.slot_type.release(); c.center.release();
     c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
     c.ilist.release(); c.icount.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
+    c.plist_in.release(); c.ilist_in.release(); c.n_in.release();
     c.f_atom.release(); c.acc.release(); c.npairs_cut.release(); c.forces_out.release(); c.forces_pme_ref.release();
     c.status.release(); c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
     c.rgrid_d.release();
@@ -544,7 +555,8 @@ int mdf_set_stream(mdf_ctx* ctx, void* stream)
     });
 }
 
-int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pairs, int64_t* n_pairs_in_cutoff)
+int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pairs, int64_t* n_cluster_pairs_pruned,
+                      int64_t* n_pairs_in_cutoff)
 {
     if (!ctx) return MDF_ERR_INVALID;
     return guarded(ctx, [&] {
@@ -552,6 +564,15 @@ int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pair
         MDF_CUDA_TRY(cudaSetDevice(c.device));
         if (n_clusters) *n_clusters = c.have_list ? c.n_clusters : -1;
         if (n_cluster_pairs) *n_cluster_pairs = c.have_list ? c.n_entries : -1;
+        if (n_cluster_pairs_pruned) {
+            unsigned long long v = 0;
+            bool ok = c.have_list && c.pruned_valid && c.p.prune_every > 0;
+            if (ok) {
+                MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+                MDF_CUDA_TRY(cudaMemcpy(&v, c.n_in.p, sizeof(v), cudaMemcpyDeviceToHost));
+            }
+            *n_cluster_pairs_pruned = ok ? (int64_t)v : -1;
+        }
         if (n_pairs_in_cutoff) {
             unsigned long long v = 0;
             if (c.have_list) {

@@ -151,8 +151,13 @@ struct Ctx {
     DevBuf<int> cluster_col;       // [n_clusters]
     DevBuf<ILRange> ilist;         // [n_clusters]
     DevBuf<int> icount;            // [n_clusters + 1]
-    DevBuf<PairEntry> plist;       // [cap]
+    DevBuf<PairEntry> plist;       // [cap] outer list (cutoff + skin)
     long long n_entries = 0;
+    DevBuf<PairEntry> plist_in;    // pruned list the pair kernel walks (same offsets as plist)
+    DevBuf<ILRange> ilist_in;
+    DevBuf<unsigned long long> n_in;   // [1] entries kept by the last prune
+    int since_prune = 0;
+    bool pruned_valid = false;
     DevBuf<int> scan_tmp;
 
     // accumulators
@@ -207,6 +212,7 @@ struct Ctx {
 void upload_topology(Ctx& c, const mdf_topology* t);
 void build_pairlist(Ctx& c);
 void pack_positions(Ctx& c);
+void prune_pairlist(Ctx& c);
 void launch_nonbonded(Ctx& c, bool energy);
 void launch_exclusions(Ctx& c, bool energy);
 void launch_bonded(Ctx& c, bool energy);

@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
     const unsigned FULL = 0xffffffffu;
 
     double e_lj = 0, e_dir = 0, e_all = 0, e_pl = 0, e_cut = 0;
-    long long npc = 0;
+    int npc = 0;
     R fix = 0, fiy = 0, fiz = 0;
     const R rc2 = (R)P.rc2, rsw = (R)P.rsw, inv_sw = (R)P.inv_sw, alpha = (R)P.alpha;
     const R two_a_spi = (R)(2.0 * P.alpha / 1.7724538509055160273);
@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
             const unsigned long long mask = pe.mask;
             __syncwarp();
             R fjx = 0, fjy = 0, fjz = 0;
+            R el_e = 0, ed_e = 0;   // this entry's energies in working precision; summed in FP64 below
             const int rot_src = (lane & ~7) | ((ii + 1) & 7);
 #pragma unroll
             for (int t = 0; t < CLUSTER; ++t) {
@@ -157,8 +158,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
                         const R ec = qq * erfcv * rinv;
                         g = G + (ec + qq * two_a_spi * ex) * rinv2;
                         if (ENERGY) {
-                            e_lj += (double)U;
-                            e_dir += (double)ec;
+                            el_e += U;
+                            ed_e += ec;
                             ++npc;
                         }
                     } else {
@@ -212,6 +213,10 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
                 fjy = __shfl_sync(FULL, fjy, rot_src);
                 fjz = __shfl_sync(FULL, fjz, rot_src);
             }
+            if (ENERGY && SEM == MDF_SEM_PHYSICAL) {
+                e_lj += (double)el_e;
+                e_dir += (double)ed_e;
+            }
             if (valid && (fjx != (R)0 || fjy != (R)0 || fjz != (R)0)) {
                 const int sl = J * CLUSTER + ii;
                 fx_add(fslot + sl, fjx, FORCE_SCALE, st);
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
             const int idx[5] = {MDF_E_VDW, MDF_E_EE, MDF_E_EE_PAIRLIST, MDF_E_EE_CUTOFF, MDF_E_EE_DIRECT};
             block_acc_fixed<5>(v, acc, idx, ENERGY_SCALE, st);
         }
-        long long np = warp_sum_ll(npc);
+        long long np = warp_sum_ll((long long)npc);
         if (lane == 0 && np) atomicAdd(npairs, (unsigned long long)np);
     }
 }
@@ -397,15 +402,17 @@ static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, 
 {
     NBParams P = make_params(c);
     int nb = grid_blocks(c.n_clusters, NB_WARPS);
+    const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
+    const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
+    const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     if (energy)
-        k_pairs<R, SEM, true><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, xq, c.slot_type.p,
-                                                               c.center.p, lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots,
-                                                               c.acc.p, c.npairs_cut.p, c.status.p);
+        k_pairs<R, SEM, true><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
+                                                               lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
+                                                               c.npairs_cut.p, c.status.p);
     else
-        k_pairs<R, SEM, false><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, xq,
-                                                                c.slot_type.p, c.center.p, lj, c.ljvalid.p, P,
-                                                                c.f_slot.p, c.n_slots, c.acc.p, c.npairs_cut.p,
-                                                                c.status.p);
+        k_pairs<R, SEM, false><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
+                                                                lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
+                                                                c.npairs_cut.p, c.status.p);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
 }

@@ -391,6 +391,87 @@ __global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const
     }
 }
 
+// ------------------------------------------------------------- pruning
+// One warp per i cluster, one lane per outer entry: keep the entries with at
+// least one unmasked atom pair inside rcut (current positions), compacted in
+// list order into the same offsets of the pruned list.
+template <typename R>
+__global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restrict__ ilist,
+                                               const PairEntry* __restrict__ plist,
+                                               const typename V4<R>::type* __restrict__ xq,
+                                               const double4* __restrict__ center, double Lx, double Ly, double Lz,
+                                               R rcut2, ILRange* __restrict__ ilist_in,
+                                               PairEntry* __restrict__ plist_in, unsigned long long* __restrict__ n_in)
+{
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (I >= ncl) return;
+    const ILRange L = ilist[I];
+    R xi[CLUSTER], yi[CLUSTER], zi[CLUSTER];
+#pragma unroll
+    for (int k = 0; k < CLUSTER; ++k) {
+        typename V4<R>::type v = xq[I * CLUSTER + k];
+        xi[k] = v.x; yi[k] = v.y; zi[k] = v.z;
+    }
+    const double4 cI = center[I];
+    int kept = 0;
+    for (int base = 0; base < L.count; base += 32) {
+        const int e = base + lane;
+        bool keep = false;
+        PairEntry pe;
+        pe.j = 0; pe.shift = 13; pe.mask = 0ull;
+        if (e < L.count) {
+            pe = plist[L.start + e];
+            const int J = pe.j;
+            int sx, sy, sz;
+            shift_decode(pe.shift, sx, sy, sz);
+            const double4 cJ = center[J];
+            const R dcx = (R)(cI.x - cJ.x - sx * Lx), dcy = (R)(cI.y - cJ.y - sy * Ly), dcz = (R)(cI.z - cJ.z - sz * Lz);
+            const unsigned long long m = pe.mask;
+#pragma unroll
+            for (int jj = 0; jj < CLUSTER; ++jj) {
+                typename V4<R>::type v = xq[J * CLUSTER + jj];
+                const R xj = v.x - dcx, yj = v.y - dcy, zj = v.z - dcz;
+#pragma unroll
+                for (int ii = 0; ii < CLUSTER; ++ii) {
+                    const R dx = xi[ii] - xj, dy = yi[ii] - yj, dz = zi[ii] - zj;
+                    const R r2 = dx * dx + dy * dy + dz * dz;
+                    keep |= ((m >> (ii * 8 + jj)) & 1ull) && r2 < rcut2;
+                }
+            }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) plist_in[L.start + kept + __popc(bal & ((1u << lane) - 1u))] = pe;
+        kept += __popc(bal);
+    }
+    if (lane == 0) {
+        ILRange r;
+        r.i = I; r.start = L.start; r.count = kept; r.pad = 0;
+        ilist_in[I] = r;
+        if (kept) atomicAdd(n_in, (unsigned long long)kept);
+    }
+}
+
+void prune_pairlist(Ctx& c)
+{
+    const int th = 256;
+    // a hair above the cutoff so working-precision rounding never drops a pair at r ~ rc
+    double rc = c.p.cutoff + std::max(0.0, c.p.prune_margin) + 0.02;
+    MDF_CUDA_TRY(cudaMemsetAsync(c.n_in.p, 0, sizeof(unsigned long long), c.stream));
+    int blocks = grid_blocks((long long)c.n_clusters * 32, th);
+    if (c.p.precision == MDF_PREC_MIXED)
+        k_prune<float><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_f.p, c.center.p, c.box[0],
+                                                   c.box[1], c.box[2], (float)(rc * rc), c.ilist_in.p, c.plist_in.p,
+                                                   c.n_in.p);
+    else
+        k_prune<double><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_d.p, c.center.p,
+                                                    c.box[0], c.box[1], c.box[2], rc * rc, c.ilist_in.p, c.plist_in.p,
+                                                    c.n_in.p);
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 1;
+    c.pruned_valid = true;
+}
+
 // ------------------------------------------------------------------ host
 static double atom_density(const Ctx& c)
 {
@@ -521,6 +602,11 @@ void build_pairlist(Ctx& c)
         MDF_CUDA_TRY(cudaStreamSynchronize(s));
         if (st & ST_CAPACITY_PAIRS) throw ApiError(MDF_ERR_CAPACITY, "pair list capacity exceeded");
         c.f_slot.alloc((size_t)3 * c.n_slots);
+        c.plist_in.alloc((size_t)total + 1);
+        c.ilist_in.alloc(ncl);
+        c.n_in.alloc(1);
+        c.pruned_valid = false;
+        c.since_prune = 0;
         c.have_list = true;
         return;
     }

@@ -61,7 +61,7 @@ def library(path=None):
     lib.mdf_forces_device.argtypes = [C.c_void_p, C.c_void_p]
     lib.mdf_get_pme_forces.argtypes = [C.c_void_p, dp]
     lib.mdf_set_stream.argtypes = [C.c_void_p, C.c_void_p]
-    lib.mdf_pairlist_info.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    lib.mdf_pairlist_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int64)] * 4
     lib.mdf_enable_timing.argtypes = [C.c_void_p, C.c_int]
     lib.mdf_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int]
     lib.mdf_cmap_coefficients.argtypes = [C.c_int, C.c_int, dp, dp]
@@ -103,7 +103,7 @@ class Engine:
 
     def __init__(self, flat, box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, cutoff=10.0,
                  skin=2.0, switch_radius=9.0, ewald_tol=1e-5, ewald_alpha=0.0, grid=(0, 0, 0), pme_order=4,
-                 device=0):
+                 device=0, prune_every=1, prune_margin=0.0):
         self.lib = library()
         self.flat = flat
         self.natoms = flat.natoms
@@ -114,6 +114,7 @@ class Engine:
             p.grid[k] = int(grid[k])
         p.cutoff, p.skin, p.switch_radius = float(cutoff), float(skin), float(switch_radius)
         p.ewald_tol, p.ewald_alpha, p.pme_order, p.device = float(ewald_tol), float(ewald_alpha), int(pme_order), int(device)
+        p.prune_every, p.prune_margin = int(prune_every), float(prune_margin)
         self.params = p
         h = C.c_void_p()
         rc = self.lib.mdf_create(C.byref(flat.struct()), C.byref(p), C.byref(h))
@@ -207,9 +208,10 @@ class Engine:
         return f
 
     def pairlist_info(self):
-        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
-        self._check(self.lib.mdf_pairlist_info(self.h, C.byref(a), C.byref(b), C.byref(c)), "pairlist_info")
-        return dict(clusters=a.value, cluster_pairs=b.value, pairs_in_cutoff=c.value)
+        a, b, p, c = C.c_int64(), C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(self.lib.mdf_pairlist_info(self.h, C.byref(a), C.byref(b), C.byref(p), C.byref(c)),
+                    "pairlist_info")
+        return dict(clusters=a.value, cluster_pairs=b.value, cluster_pairs_pruned=p.value, pairs_in_cutoff=c.value)
 
     def enable_timing(self, on=True):
         self._check(self.lib.mdf_enable_timing(self.h, 1 if on else 0), "enable_timing")

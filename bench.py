@@ -338,7 +338,10 @@ def main():
                        "parallelism": "replicas x%d" % ws if ws > 1 else "single GPU",
                        "l2": "flushed between steps (256 MiB memset outside the per-step events)",
                        "pairlist_build_ms": t_build * 1e3, "clusters": info["clusters"],
-                       "cluster_pairs": info["cluster_pairs"], "pairs_in_cutoff": info["pairs_in_cutoff"]},
+                       "cluster_pairs": info["cluster_pairs"],
+                       "cluster_pairs_pruned": info["cluster_pairs_pruned"],
+                       "prune": "every evaluation, exact (margin 0)",
+                       "pairs_in_cutoff": info["pairs_in_cutoff"]},
             "roofline": {"kernel": "k_pairs (LJ + erfc Ewald pair kernel)", "bound": "fp32", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured FP32 FMA throughput of this GPU (mdf_probe_fma_tflops)",

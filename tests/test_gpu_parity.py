@@ -200,9 +200,10 @@ def test_nonfinite_position_reported_not_faulted():
 
 
 @pytest.mark.parametrize("prec", [FP64, MIXED])
-def test_pruned_list_gives_identical_bits(prec):
+def test_pruned_list_matches_unpruned(prec):
     """Pruning only drops cluster pairs without an atom pair inside the
-    cutoff, so the pruned evaluation reproduces the unpruned one bit for bit."""
+    cutoff: the pruned evaluation equals the unpruned one up to the order in
+    which the pair kernel sums (entries move between lanes)."""
     s = H.system("small")
     flat = H.flat(s, PHYS, engine.cmap_coefficients)
     out = []
@@ -216,8 +217,9 @@ def test_pruned_list_gives_identical_bits(prec):
             assert 0 < info["cluster_pairs_pruned"] < info["cluster_pairs"]
         eng.close()
     (E0, F0), (E1, F1) = out
-    assert np.array_equal(F0, F1)
-    assert all(E0[k] == E1[k] for k in E_PHYS_TERMS)
+    tol = 1e-12 if prec == FP64 else 1e-6
+    assert H.frel(F1, F0) < tol
+    assert all(abs(E0[k] - E1[k]) <= tol * max(1.0, abs(E0[k])) for k in E_PHYS_TERMS)
 
 
 def test_prune_interval_with_margin_tracks_moving_atoms():
@@ -235,6 +237,6 @@ def test_prune_interval_with_margin_tracks_moving_atoms():
         b.set_positions(x)
         Ea, Fa = a.compute()
         Eb, Fb = b.compute()
-        assert np.array_equal(Fa, Fb), step
+        assert H.frel(Fa, Fb) < 1e-12, step
         x = x + rng.uniform(-0.1, 0.1, x.shape)
     a.close(); b.close()

@@ -419,7 +419,7 @@ void mdf_destroy(mdf_ctx* ctx)
     c.angle_par.release(); c.imp_par.release(); c.dih_par.release(); c.cmap_coeff.release();
     c.excl_pairs.release(); c.pairs14.release(); c.p14_scale.release(); c.excl_is14.release();
     c.xyz.release(); c.atom_col.release(); c.col_count.release(); c.col_start.release(); c.col_cstart.release();
-    c.col_atoms.release(); c.slot_atom.release(); c.atom_slot.release(); c.slot_type.release(); c.center.release();
+    c.col_atoms.release(); c.slot_atom.release(); c.atom_slot.release(); c.slot_type.release(); c.center.release(); c.centerf.release();
     c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
     c.ilist.release(); c.icount.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
     c.plist_in.release(); c.ilist_in.release(); c.n_in.release();

@@ -32,6 +32,17 @@ __device__ __forceinline__ void fx_add(unsigned long long* a, float v, double sc
 
 __device__ __forceinline__ long long to_fixed(double v, double scale) { return __double2ll_rn(v * scale); }
 
+// FP32 force contribution straight to 2^-32 fixed point (the scaling is exact).
+__device__ __forceinline__ void fx_add_force_f(unsigned long long* a, float v, unsigned* st)
+{
+    const float s = v * 4294967296.0f;
+    if (!(fabsf(s) < 9.2e18f)) {
+        status_set(st, isfinite(v) ? ST_OVERFLOW : ST_NONFINITE);
+        return;
+    }
+    atomicAdd(a, (unsigned long long)__float2ll_rn(s));
+}
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll

@@ -144,7 +144,9 @@ struct Ctx {
     DevBuf<int> slot_atom;         // [n_slots]
     DevBuf<int> atom_slot;         // [N]
     DevBuf<int> slot_type;         // [n_slots]
-    DevBuf<double4> center;        // [n_clusters] (x,y,z,unused) cluster center
+    DevBuf<double4> center;        // [n_clusters] (x,y,z,n_real_atoms) cluster centre
+    DevBuf<float4> centerf;        // the same centres, exact in FP32 (they lie on a 2^-k grid)
+    double center_quantum = 0.0;
     DevBuf<float4> bb_lo, bb_hi;   // [n_clusters] bounding boxes (wrapped coordinates)
     DevBuf<float4> xq_f;           // [n_slots] offset from center + q (mixed)
     DevBuf<double4> xq_d;          // [n_slots] (FP64)

@@ -250,6 +250,146 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
     }
 }
 
+// ------------------------------------------------- FP32 PHYSICAL pair kernel
+// Periodic image offsets s*L of the 27 shift codes as an FP32 hi + lo pair.
+struct ShiftTable {
+    float v[27][6];   // hi.x hi.y hi.z lo.x lo.y lo.z
+};
+
+// The mixed-precision production kernel (PHYSICAL semantics).  Same warp
+// layout as k_pairs; differences that matter for speed and accuracy:
+//  * cluster centres lie on a 2^-k grid and are exact in FP32, so the centre
+//    difference is exact and the image offset enters as hi + lo: the pair
+//    vector carries ~1e-6 A rounding, not the 1e-5 A of raw FP32 coordinates;
+//  * the lane's row of the 8x8 mask is rotated once per entry so step t tests
+//    bit t;
+//  * the pair arithmetic is branch-free (inactive pairs are selected out);
+//  * energies are summed in FP32 per entry and in FP64 across entries.
+template <bool ENERGY, bool SWITCH>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
+    int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
+    const int* __restrict__ stype, const float4* __restrict__ centerf, const float2* __restrict__ ljAB, NBParams P,
+    ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots, unsigned long long* __restrict__ acc,
+    unsigned long long* __restrict__ npairs, unsigned* st)
+{
+    __shared__ float4 sx[NB_WARPS][4][CLUSTER + 1];
+    __shared__ int stj[NB_WARPS][4][CLUSTER];
+    __shared__ float sh[27][6];
+    for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
+    __syncthreads();
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * NB_WARPS + wib;
+    const int jslot = lane >> 3, ii = lane & 7;
+    const unsigned FULL = 0xffffffffu;
+    const float rc2 = (float)P.rc2, rsw = (float)P.rsw, inv_sw = (float)P.inv_sw, alpha = (float)P.alpha;
+    const float two_a_spi = (float)(2.0 * P.alpha / 1.7724538509055160273);
+    const float uc6 = (float)P.ucut_pow6, uc12 = (float)P.ucut_pow12, rcf = (float)P.rc, rc2f = (float)P.rc2;
+    double e_lj = 0, e_dir = 0;
+    int npc = 0;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+
+    if (w < nlist) {
+        const ILRange L = ilist[w];
+        const int I = L.i;
+        const float4 xi = xq[I * CLUSTER + ii];
+        const int trow = stype[I * CLUSTER + ii] * P.ntp;
+        const float4 cI = centerf[I];
+        const float qik = (float)P.kc * xi.w;
+        const int rot_src = (lane & ~7) | ((ii + 1) & 7);
+        for (int b = 0; b < L.count; b += 4) {
+            const int e = b + jslot;
+            PairEntry pe;
+            if (e < L.count) {
+                pe = plist[L.start + e];
+            } else {
+                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+            }
+            const int J = pe.j;
+            sx[wib][jslot][ii] = xq[J * CLUSTER + ii];
+            stj[wib][jslot][ii] = stype[J * CLUSTER + ii];
+            const float4 cJ = centerf[J];
+            const float* s6 = sh[pe.shift];
+            const float xix = xi.x + (((cI.x - cJ.x) - s6[0]) - s6[3]);
+            const float xiy = xi.y + (((cI.y - cJ.y) - s6[1]) - s6[4]);
+            const float xiz = xi.z + (((cI.z - cJ.z) - s6[2]) - s6[5]);
+            const unsigned rowm = (unsigned)(pe.mask >> (ii * 8)) & 0xffu;
+            const unsigned rot = ((rowm >> ii) | (rowm << (8 - ii))) & 0xffu;
+            __syncwarp();
+            float fjx = 0.f, fjy = 0.f, fjz = 0.f, el = 0.f, ed = 0.f;
+#pragma unroll
+            for (int t = 0; t < CLUSTER; ++t) {
+                const int jj = (ii + t) & 7;
+                const float4 xj = sx[wib][jslot][jj];
+                const float dx = xix - xj.x, dy = xiy - xj.y, dz = xiz - xj.z;
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                const bool on = ((rot >> t) & 1u) && r2 <= rc2;
+                const float r2s = on ? r2 : 1.0f;
+                const float rinv = rsqrtf(r2s);
+                const float r = r2s * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
+                const float2 ab = __ldg(&ljAB[trow + stj[wib][jslot][jj]]);
+                float U = (ab.x * rinv6 - ab.y) * rinv6;
+                float G = (12.f * ab.x * rinv6 - 6.f * ab.y) * rinv6 * rinv2;
+                if (SWITCH) {
+                    const float x = fmaxf(0.f, (r - rsw) * inv_sw), x2 = x * x, x3 = x2 * x;
+                    const float S = 1.f + x3 * (-10.f + x * (15.f - 6.f * x));
+                    const float dS = x2 * (-30.f + x * (60.f - 30.f * x)) * inv_sw;
+                    G = S * G - U * dS * rinv;
+                    U = U * S;
+                } else {
+                    const float uc = ab.x * uc12 - ab.y * uc6;
+                    const float gc = (12.f * ab.x * uc12 - 6.f * ab.y * uc6) / rc2f;
+                    U = U - uc + (r - rcf) * (gc * rcf);
+                    G = G - gc * rcf * rinv;
+                }
+                const float qq = qik * xj.w;
+                const float ar = alpha * r;
+                const float ex = __expf(-ar * ar);
+                const float erfcv = erfc_as(__fdividef(1.0f, 1.0f + 0.3275911f * ar), ex);
+                const float ec = qq * erfcv * rinv;
+                float g = G + (ec + qq * two_a_spi * ex) * rinv2;
+                g = on ? g : 0.f;
+                if (ENERGY) {
+                    el += on ? U : 0.f;
+                    ed += on ? ec : 0.f;
+                    npc += on ? 1 : 0;
+                }
+                fix += g * dx; fiy += g * dy; fiz += g * dz;
+                fjx -= g * dx; fjy -= g * dy; fjz -= g * dz;
+                fjx = __shfl_sync(FULL, fjx, rot_src);
+                fjy = __shfl_sync(FULL, fjy, rot_src);
+                fjz = __shfl_sync(FULL, fjz, rot_src);
+            }
+            if (ENERGY) {
+                e_lj += (double)el;
+                e_dir += (double)ed;
+            }
+            if (e < L.count && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
+                const int sl = J * CLUSTER + ii;
+                fx_add_force_f(fslot + sl, fjx, st);
+                fx_add_force_f(fslot + nslots + sl, fjy, st);
+                fx_add_force_f(fslot + 2 * nslots + sl, fjz, st);
+            }
+            __syncwarp();
+        }
+        fix += __shfl_xor_sync(FULL, fix, 8); fix += __shfl_xor_sync(FULL, fix, 16);
+        fiy += __shfl_xor_sync(FULL, fiy, 8); fiy += __shfl_xor_sync(FULL, fiy, 16);
+        fiz += __shfl_xor_sync(FULL, fiz, 8); fiz += __shfl_xor_sync(FULL, fiz, 16);
+        if (jslot == 0) {
+            const int sl = I * CLUSTER + ii;
+            fx_add_force_f(fslot + sl, fix, st);
+            fx_add_force_f(fslot + nslots + sl, fiy, st);
+            fx_add_force_f(fslot + 2 * nslots + sl, fiz, st);
+        }
+    }
+    if (ENERGY) {
+        const double v[2] = {e_lj, e_dir};
+        const int idx[2] = {MDF_E_VDW, MDF_E_EE_DIRECT};
+        block_acc_fixed<2>(v, acc, idx, ENERGY_SCALE, st);
+        long long np = warp_sum_ll((long long)npc);
+        if (lane == 0 && np) atomicAdd(npairs, (unsigned long long)np);
+    }
+}
+
 // --------------------------------------------------------------- FP64 pairs
 __device__ __forceinline__ void pair_vec(const double* __restrict__ xyz, int a, int b, const NBParams& P,
                                          double d[3])
@@ -417,12 +557,49 @@ static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, 
     c.launches += 1;
 }
 
+static ShiftTable make_shift_table(const Ctx& c)
+{
+    ShiftTable t;
+    for (int code = 0; code < 27; ++code) {
+        int s[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+        for (int d = 0; d < 3; ++d) {
+            double v = s[d] * c.box[d];
+            float hi = (float)v;
+            t.v[code][d] = hi;
+            t.v[code][3 + d] = (float)(v - (double)hi);
+        }
+    }
+    return t;
+}
+
+static void launch_pairs_f32(Ctx& c, bool energy)
+{
+    NBParams P = make_params(c);
+    ShiftTable sh = make_shift_table(c);
+    int nb = grid_blocks(c.n_clusters, NB_WARPS);
+    const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
+    const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
+    const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
+#define MDF_PF32(E, S)                                                                                           \
+    k_pairs_f32<E, S><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p, c.centerf.p, \
+                                                       c.ljAB_f.p, P, sh, c.f_slot.p, c.n_slots, c.acc.p,         \
+                                                       c.npairs_cut.p, c.status.p)
+    if (energy) {
+        if (P.use_switch) MDF_PF32(true, true); else MDF_PF32(true, false);
+    } else {
+        if (P.use_switch) MDF_PF32(false, true); else MDF_PF32(false, false);
+    }
+#undef MDF_PF32
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 1;
+}
+
 void launch_nonbonded(Ctx& c, bool energy)
 {
     if (c.n_clusters == 0) return;
     bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
     if (c.p.precision == MDF_PREC_MIXED) {
-        if (phys) launch_pairs_t<float, MDF_SEM_PHYSICAL>(c, energy, c.xq_f.p, c.ljAB_f.p);
+        if (phys) launch_pairs_f32(c, energy);
         else launch_pairs_t<float, MDF_SEM_REFERENCE>(c, energy, c.xq_f.p, c.ljAB_f.p);
     } else {
         if (phys) launch_pairs_t<double, MDF_SEM_PHYSICAL>(c, energy, c.xq_d.p, c.ljAB.p);

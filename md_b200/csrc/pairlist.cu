@@ -162,8 +162,8 @@ __global__ void __launch_bounds__(1024) k_sort_columns(const double* __restrict_
 // Cluster bounding boxes (wrapped coordinates) and centres; center.w = number
 // of real atoms in the cluster.
 __global__ void k_cluster_geom(int ncl, const double* __restrict__ xyz, double Lx, double Ly, double Lz,
-                               const int* __restrict__ slot_atom, double4* __restrict__ center,
-                               float4* __restrict__ bb_lo, float4* __restrict__ bb_hi)
+                               double quantum, const int* __restrict__ slot_atom, double4* __restrict__ center,
+                               float4* __restrict__ centerf, float4* __restrict__ bb_lo, float4* __restrict__ bb_hi)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncl) return;
@@ -182,7 +182,12 @@ __global__ void k_cluster_geom(int ncl, const double* __restrict__ xyz, double L
     if (nv == 0) {
         for (int d = 0; d < 3; ++d) lo[d] = hi[d] = 0.0;
     }
-    center[c] = make_double4(0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]), 0.5 * (lo[2] + hi[2]), (double)nv);
+    // centres on a 2^-k grid fine enough that they are exact in FP32, so the
+    // FP32 pair kernel forms centre differences without rounding
+    double cc[3];
+    for (int d = 0; d < 3; ++d) cc[d] = rint(0.5 * (lo[d] + hi[d]) / quantum) * quantum;
+    center[c] = make_double4(cc[0], cc[1], cc[2], (double)nv);
+    centerf[c] = make_float4((float)cc[0], (float)cc[1], (float)cc[2], (float)nv);
     bb_lo[c] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]), __double2float_rd(lo[2]), 0.f);
     bb_hi[c] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]), __double2float_ru(hi[2]), 0.f);
 }
@@ -392,9 +397,12 @@ __global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const
 }
 
 // ------------------------------------------------------------- pruning
-// One warp per i cluster, one lane per outer entry: keep the entries with at
-// least one unmasked atom pair inside rcut (current positions), compacted in
-// list order into the same offsets of the pruned list.
+// One warp per i cluster, four entries at a time in the pair kernel's layout
+// (lane = jslot*8 + ii): the eight j atoms of each entry are staged in shared
+// memory with coalesced loads, every lane tests its i atom against them, and
+// an entry is kept when any unmasked atom pair lies inside rcut (current
+// positions).  Kept entries are compacted, in list order, into the same
+// offsets of the pruned list.
 template <typename R>
 __global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restrict__ ilist,
                                                const PairEntry* __restrict__ plist,
@@ -403,46 +411,46 @@ __global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restric
                                                R rcut2, ILRange* __restrict__ ilist_in,
                                                PairEntry* __restrict__ plist_in, unsigned long long* __restrict__ n_in)
 {
+    using V4t = typename V4<R>::type;
+    __shared__ V4t sj[8][4][CLUSTER + 1];
+    const int wib = threadIdx.x >> 5;
     const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, jslot = lane >> 3, ii = lane & 7;
     if (I >= ncl) return;
     const ILRange L = ilist[I];
-    R xi[CLUSTER], yi[CLUSTER], zi[CLUSTER];
-#pragma unroll
-    for (int k = 0; k < CLUSTER; ++k) {
-        typename V4<R>::type v = xq[I * CLUSTER + k];
-        xi[k] = v.x; yi[k] = v.y; zi[k] = v.z;
-    }
+    const V4t xi = xq[I * CLUSTER + ii];
     const double4 cI = center[I];
     int kept = 0;
-    for (int base = 0; base < L.count; base += 32) {
-        const int e = base + lane;
-        bool keep = false;
+    for (int base = 0; base < L.count; base += 4) {
+        const int e = base + jslot;
         PairEntry pe;
-        pe.j = 0; pe.shift = 13; pe.mask = 0ull;
-        if (e < L.count) {
-            pe = plist[L.start + e];
-            const int J = pe.j;
-            int sx, sy, sz;
-            shift_decode(pe.shift, sx, sy, sz);
-            const double4 cJ = center[J];
-            const R dcx = (R)(cI.x - cJ.x - sx * Lx), dcy = (R)(cI.y - cJ.y - sy * Ly), dcz = (R)(cI.z - cJ.z - sz * Lz);
-            const unsigned long long m = pe.mask;
+        pe.j = I; pe.shift = 13; pe.mask = 0ull;
+        if (e < L.count) pe = plist[L.start + e];
+        const int J = pe.j;
+        sj[wib][jslot][ii] = xq[J * CLUSTER + ii];
+        int sx, sy, sz;
+        shift_decode(pe.shift, sx, sy, sz);
+        const double4 cJ = center[J];
+        const R xx = xi.x + (R)(cI.x - cJ.x - sx * Lx), yy = xi.y + (R)(cI.y - cJ.y - sy * Ly),
+                zz = xi.z + (R)(cI.z - cJ.z - sz * Lz);
+        const unsigned row = (unsigned)(pe.mask >> (ii * 8)) & 0xffu;
+        __syncwarp();
+        bool near = false;
 #pragma unroll
-            for (int jj = 0; jj < CLUSTER; ++jj) {
-                typename V4<R>::type v = xq[J * CLUSTER + jj];
-                const R xj = v.x - dcx, yj = v.y - dcy, zj = v.z - dcz;
-#pragma unroll
-                for (int ii = 0; ii < CLUSTER; ++ii) {
-                    const R dx = xi[ii] - xj, dy = yi[ii] - yj, dz = zi[ii] - zj;
-                    const R r2 = dx * dx + dy * dy + dz * dz;
-                    keep |= ((m >> (ii * 8 + jj)) & 1ull) && r2 < rcut2;
-                }
-            }
+        for (int jj = 0; jj < CLUSTER; ++jj) {
+            const V4t v = sj[wib][jslot][jj];
+            const R dx = xx - v.x, dy = yy - v.y, dz = zz - v.z;
+            near |= ((row >> jj) & 1u) && (dx * dx + dy * dy + dz * dz < rcut2);
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (keep) plist_in[L.start + kept + __popc(bal & ((1u << lane) - 1u))] = pe;
-        kept += __popc(bal);
+        const unsigned bal = __ballot_sync(0xffffffffu, near);
+        // keep[k] = any lane of j slot k found a pair
+        unsigned keep = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) keep |= ((bal >> (8 * k)) & 0xffu) ? (1u << k) : 0u;
+        if (ii == 0 && ((keep >> jslot) & 1u))
+            plist_in[L.start + kept + __popc(keep & ((1u << jslot) - 1u))] = pe;
+        kept += __popc(keep);
+        __syncwarp();
     }
     if (lane == 0) {
         ILRange r;
@@ -556,8 +564,15 @@ void build_pairlist(Ctx& c)
         c.center.alloc(ncl);
         c.bb_lo.alloc(ncl);
         c.bb_hi.alloc(ncl);
-        k_cluster_geom<<<grid_blocks(ncl, th), th, 0, s>>>(ncl, c.xyz.p, c.box[0], c.box[1], c.box[2], c.slot_atom.p,
-                                                           c.center.p, c.bb_lo.p, c.bb_hi.p);
+        c.centerf.alloc(ncl);
+        {
+            // largest power-of-two quantum keeping every centre exact in FP32 (24-bit significand)
+            double lmax = std::max(c.box[0], std::max(c.box[1], c.box[2]));
+            c.center_quantum = std::ldexp(1.0, (int)std::ceil(std::log2(lmax + 1.0)) - 24);
+        }
+        k_cluster_geom<<<grid_blocks(ncl, th), th, 0, s>>>(ncl, c.xyz.p, c.box[0], c.box[1], c.box[2],
+                                                           c.center_quantum, c.slot_atom.p, c.center.p, c.centerf.p,
+                                                           c.bb_lo.p, c.bb_hi.p);
         c.slot_type.alloc(c.n_slots);
         k_slot_type<<<grid_blocks(c.n_slots, th), th, 0, s>>>(c.n_slots, c.slot_atom.p, c.type.p, c.ntp - 1,
                                                               c.slot_type.p);

@@ -699,9 +699,11 @@ static void ref_w5_spread_host(double u, double th[5])
 static int lines_per_block(int n, size_t csize)
 {
     // two ping-pong buffers + twiddles within 48 KB
+    // few lines per block: many small blocks keep every SM busy on these
+    // latency-bound, L2-resident passes
     size_t budget = 46 * 1024;
     int lp = (int)((budget / csize - n) / (2 * (size_t)n));
-    return std::max(1, std::min(16, lp));
+    return std::max(1, std::min(4, lp));
 }
 
 void setup_pme(Ctx& c)

@@ -38,23 +38,29 @@ void mark(Ctx& c, const char* name)
     ++c.nev;
 }
 
-__global__ void k_finalize(int N, int nslots, const unsigned long long* __restrict__ fatom,
-                           const unsigned long long* __restrict__ fslot, const int* __restrict__ atom_slot,
-                           double* __restrict__ out)
+// Forces out in atom order, and every accumulator cleared for the next
+// evaluation (read-and-clear: an evaluation needs no memsets).  The scalar
+// block was copied to the host before this kernel runs.
+__global__ void k_finalize(int N, int nslots, unsigned long long* __restrict__ fatom,
+                           unsigned long long* __restrict__ fslot, const int* __restrict__ atom_slot,
+                           double* __restrict__ out, unsigned long long* __restrict__ scal)
 {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < NUM_SCAL) scal[a] = 0ull;
     if (a >= N) return;
     int s = atom_slot[a];
     for (int k = 0; k < 3; ++k) {
         long long v = (long long)fatom[(long long)k * N + a] + (long long)fslot[(long long)k * nslots + s];
+        fatom[(long long)k * N + a] = 0ull;
+        fslot[(long long)k * nslots + s] = 0ull;
         out[3 * a + k] = (double)v * FORCE_ISCALE;
     }
 }
 
 void launch_finalize(Ctx& c, double* d_forces, bool)
 {
-    k_finalize<<<grid_blocks(c.N, 256), 256, 0, c.stream>>>(c.N, c.n_slots, c.f_atom.p, c.f_slot.p, c.atom_slot.p,
-                                                            d_forces);
+    k_finalize<<<grid_blocks(std::max(c.N, NUM_SCAL), 256), 256, 0, c.stream>>>(
+        c.N, c.n_slots, c.f_atom.p, c.f_slot.p, c.atom_slot.p, d_forces, c.scal.p);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
 }
@@ -190,13 +196,15 @@ void upload_topology(Ctx& c, const mdf_topology* t)
     c.xyz.alloc(3 * (size_t)c.N);
     c.f_atom.alloc(3 * (size_t)c.N);
     c.forces_out.alloc(3 * (size_t)c.N);
-    c.acc.alloc(NUM_ACC);
-    c.npairs_cut.alloc(1);
-    c.status.alloc(1);
+    c.scal.alloc(NUM_SCAL);
+    c.acc.p = c.scal.p;
+    c.npairs_cut.p = c.scal.p + NUM_ACC;
+    c.status.p = reinterpret_cast<unsigned*>(c.scal.p + NUM_ACC + 1);
+    c.need_clear = true;
     MDF_CUDA_TRY(cudaStreamSynchronize(s));
 }
 
-static void eval_async(Ctx& c, uint32_t flags)
+static void eval_async_impl(Ctx& c, uint32_t flags)
 {
     if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
     if (!c.have_list) build_pairlist(c);
@@ -205,11 +213,13 @@ static void eval_async(Ctx& c, uint32_t flags)
     bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
     c.nev = 0;
     mark(c, "start");
-    MDF_CUDA_TRY(cudaMemsetAsync(c.f_slot.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_slots, s));
-    MDF_CUDA_TRY(cudaMemsetAsync(c.f_atom.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.N, s));
-    MDF_CUDA_TRY(cudaMemsetAsync(c.acc.p, 0, sizeof(unsigned long long) * NUM_ACC, s));
-    MDF_CUDA_TRY(cudaMemsetAsync(c.npairs_cut.p, 0, sizeof(unsigned long long), s));
-    MDF_CUDA_TRY(cudaMemsetAsync(c.status.p, 0, sizeof(unsigned), s));
+    if (c.need_clear) {
+        // first evaluation on these buffers (later ones are cleared by k_finalize)
+        MDF_CUDA_TRY(cudaMemsetAsync(c.f_slot.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_slots, s));
+        MDF_CUDA_TRY(cudaMemsetAsync(c.f_atom.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.N, s));
+        MDF_CUDA_TRY(cudaMemsetAsync(c.scal.p, 0, sizeof(unsigned long long) * NUM_SCAL, s));
+        c.need_clear = false;
+    }
     pack_positions(c);
     mark(c, "pack");
     if (c.p.prune_every > 0) {
@@ -230,19 +240,28 @@ static void eval_async(Ctx& c, uint32_t flags)
         launch_pme(c, energy);
         c.have_pme_ref = !phys;
     }
+    MDF_CUDA_TRY(cudaMemcpyAsync(c.h_scal, c.scal.p, sizeof(unsigned long long) * NUM_SCAL, cudaMemcpyDeviceToHost, s));
     launch_finalize(c, c.forces_out.p, false);
     mark(c, "finalize");
-    MDF_CUDA_TRY(cudaMemcpyAsync(c.h_acc, c.acc.p, sizeof(unsigned long long) * NUM_ACC, cudaMemcpyDeviceToHost, s));
-    MDF_CUDA_TRY(cudaMemcpyAsync(c.h_status, c.status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     c.pending = true;
     c.pending_flags = flags;
+}
+
+static void eval_async(Ctx& c, uint32_t flags)
+{
+    try {
+        eval_async_impl(c, flags);
+    } catch (...) {
+        c.need_clear = true;
+        throw;
+    }
 }
 
 static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
 {
     if (!c.pending) throw ApiError(MDF_ERR_STATE, "no evaluation to fetch");
     MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    unsigned st = *c.h_status;
+    unsigned st = (unsigned)c.h_scal[NUM_ACC + 1];
     if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite force or energy contribution");
     if (st & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "fixed-point accumulator range exceeded");
     if (c.timing) {
@@ -256,7 +275,7 @@ static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
     if (e_out) {
         memset(e_out, 0, sizeof(*e_out));
         if (c.pending_flags & MDF_COMPUTE_ENERGY) {
-            for (int k = 0; k < MDF_E_COUNT; ++k) e_out->e[k] = (double)(long long)c.h_acc[k] * ENERGY_ISCALE;
+            for (int k = 0; k < MDF_E_COUNT; ++k) e_out->e[k] = (double)(long long)c.h_scal[k] * ENERGY_ISCALE;
             e_out->e[MDF_E_EE_SELF] += c.e_self;
             bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
             if (phys) {
@@ -265,7 +284,7 @@ static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
                     -c.p.coulomb_const * M_PI * c.q_total * c.q_total / (2.0 * V * c.alpha * c.alpha);
                 const int vmap[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
                 for (int k = 0; k < 9; ++k)
-                    e_out->virial[k] = (double)(long long)c.h_acc[ACC_VIR + vmap[k]] * ENERGY_ISCALE;
+                    e_out->virial[k] = (double)(long long)c.h_scal[ACC_VIR + vmap[k]] * ENERGY_ISCALE;
                 double tot = 0;
                 const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
                                      MDF_E_VDW, MDF_E_VDW14, MDF_E_EE_DIRECT, MDF_E_EE14, MDF_E_EE_EXCL,
@@ -387,8 +406,8 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         MDF_CUDA_TRY(cudaSetDevice(c.device));
         MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
-        MDF_CUDA_TRY(cudaMallocHost((void**)&c.h_acc, sizeof(unsigned long long) * NUM_ACC));
-        MDF_CUDA_TRY(cudaMallocHost((void**)&c.h_status, sizeof(unsigned)));
+        MDF_CUDA_TRY(cudaMallocHost((void**)&c.h_scal, sizeof(unsigned long long) * NUM_SCAL));
+        memset(c.h_scal, 0, sizeof(unsigned long long) * NUM_SCAL);
         for (int d = 0; d < 3; ++d) c.box[d] = c.p.box[d];
         double tol = c.p.ewald_tol > 0 ? c.p.ewald_tol : 1e-6;
         c.alpha = c.p.ewald_alpha > 0 ? c.p.ewald_alpha : std::sqrt(std::log(2 * tol) * -1) / c.p.cutoff;
@@ -422,15 +441,14 @@ void mdf_destroy(mdf_ctx* ctx)
     c.col_atoms.release(); c.slot_atom.release(); c.atom_slot.release(); c.slot_type.release(); c.center.release(); c.centerf.release();
     c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
     c.ilist.release(); c.icount.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
-    c.plist_in.release(); c.ilist_in.release(); c.n_in.release();
-    c.f_atom.release(); c.acc.release(); c.npairs_cut.release(); c.forces_out.release(); c.forces_pme_ref.release();
-    c.status.release(); c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
+    c.plist_in.release(); c.ilist_in.release(); c.n_in.release(); c.cur_lo.release(); c.cur_hi.release();
+    c.f_atom.release(); c.scal.release(); c.forces_out.release(); c.forces_pme_ref.release();
+    c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
     c.rgrid_d.release();
     for (int d = 0; d < 3; ++d) {
         c.bmod[d].release(); c.bmod_f[d].release(); c.tw_d[d].release(); c.tw_f[d].release();
     }
-    if (c.h_acc) cudaFreeHost(c.h_acc);
-    if (c.h_status) cudaFreeHost(c.h_status);
+    if (c.h_scal) cudaFreeHost(c.h_scal);
     if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
     delete ctx;
 }
@@ -574,12 +592,9 @@ int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pair
             *n_cluster_pairs_pruned = ok ? (int64_t)v : -1;
         }
         if (n_pairs_in_cutoff) {
-            unsigned long long v = 0;
-            if (c.have_list) {
-                MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
-                MDF_CUDA_TRY(cudaMemcpy(&v, c.npairs_cut.p, sizeof(v), cudaMemcpyDeviceToHost));
-            }
-            *n_pairs_in_cutoff = c.have_list ? (int64_t)v : -1;
+            // from the host copy of the last evaluation's scalar block
+            MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+            *n_pairs_in_cutoff = (c.have_list && c.pending) ? (int64_t)c.h_scal[NUM_ACC] : -1;
         }
     });
 }

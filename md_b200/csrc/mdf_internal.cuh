@@ -20,6 +20,7 @@ constexpr double GRID_SCALE = 1099511627776.0;        // 2^40 fixed point for PM
 constexpr double GRID_ISCALE = 1.0 / 1099511627776.0;
 constexpr int NUM_ACC = MDF_E_COUNT + 6;   // energies + 6 virial components
 constexpr int ACC_VIR = MDF_E_COUNT;
+constexpr int NUM_SCAL = NUM_ACC + 2;      // + pairs in cutoff + status word
 
 // device status bits
 enum : unsigned {
@@ -88,6 +89,12 @@ struct DevBuf {
     }
 };
 
+// Non-owning view into a DevBuf.
+template <typename T>
+struct DevView {
+    T* p = nullptr;
+};
+
 // ----------------------------------------------------------- PME plan bits
 struct FFTPlan1D {
     int n = 0;
@@ -148,6 +155,7 @@ struct Ctx {
     DevBuf<float4> centerf;        // the same centres, exact in FP32 (they lie on a 2^-k grid)
     double center_quantum = 0.0;
     DevBuf<float4> bb_lo, bb_hi;   // [n_clusters] bounding boxes (wrapped coordinates)
+    DevBuf<float4> cur_lo, cur_hi; // [n_clusters] current boxes in the cluster frame (per evaluation)
     DevBuf<float4> xq_f;           // [n_slots] offset from center + q (mixed)
     DevBuf<double4> xq_d;          // [n_slots] (FP64)
     DevBuf<int> cluster_col;       // [n_clusters]
@@ -162,16 +170,19 @@ struct Ctx {
     bool pruned_valid = false;
     DevBuf<int> scan_tmp;
 
-    // accumulators
+    // accumulators.  The force accumulators are cleared by the kernel that
+    // reads them (k_finalize); the scalar block is copied to the host and then
+    // cleared by k_finalize too, so an evaluation needs no memsets.
     DevBuf<unsigned long long> f_slot;   // [3 * n_slots] fixed point, SoA x|y|z
     DevBuf<unsigned long long> f_atom;   // [3 * N]
-    DevBuf<unsigned long long> acc;      // [NUM_ACC] energies + virial, fixed point
-    DevBuf<unsigned long long> npairs_cut; // [1]
+    DevBuf<unsigned long long> scal;     // [NUM_SCAL]: energies + virial | pairs in cutoff | status
+    DevView<unsigned long long> acc;     // = scal[0 .. NUM_ACC)
+    DevView<unsigned long long> npairs_cut;  // = scal[NUM_ACC]
+    DevView<unsigned> status;            // = (unsigned*)&scal[NUM_ACC + 1]
     DevBuf<double> forces_out;           // [3N]
     DevBuf<double> forces_pme_ref;       // [3N]
-    DevBuf<unsigned> status;             // [1]
-    unsigned long long* h_acc = nullptr; // pinned
-    unsigned* h_status = nullptr;        // pinned
+    unsigned long long* h_scal = nullptr;  // pinned copy of scal after each evaluation
+    bool need_clear = true;              // accumulators not known to be zero
 
     // PME
     int K[3] = {0, 0, 0};

@@ -195,28 +195,48 @@ __global__ void k_cluster_geom(int ncl, const double* __restrict__ xyz, double L
 // Per-evaluation packing: cluster-ordered offsets from the cluster centre
 // (min image, so atoms crossing the box edge between rebuilds stay whole)
 // plus charge, in the working precision.
+// Also the cluster's current bounding box in its own frame (FP32, rounded
+// outward) for the prune's box test.  blockDim.x must be a multiple of 32.
 template <typename R>
 __global__ void k_pack(int nslots, const double* __restrict__ xyz, const double* __restrict__ q,
                        const int* __restrict__ slot_atom, const double4* __restrict__ center, double Lx, double Ly,
-                       double Lz, typename V4<R>::type* __restrict__ xq, unsigned* st)
+                       double Lz, typename V4<R>::type* __restrict__ xq, float4* __restrict__ cur_lo,
+                       float4* __restrict__ cur_hi, unsigned* st)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nslots) return;
-    int a = slot_atom[s];
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool inside = s < nslots;
+    const int a = inside ? slot_atom[s] : -1;
     typename V4<R>::type v;
+    float lo[3] = {3.0e38f, 3.0e38f, 3.0e38f}, hi[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
     if (a < 0) {
         v.x = v.y = v.z = v.w = (R)0;
     } else {
         double4 c = center[s / CLUSTER];
-        double dx = min_image(xyz[3 * a] - c.x, Lx), dy = min_image(xyz[3 * a + 1] - c.y, Ly),
-               dz = min_image(xyz[3 * a + 2] - c.z, Lz);
-        if (!isfinite(dx + dy + dz)) status_set(st, ST_NONFINITE);
-        v.x = (R)dx;
-        v.y = (R)dy;
-        v.z = (R)dz;
+        double d[3] = {min_image(xyz[3 * a] - c.x, Lx), min_image(xyz[3 * a + 1] - c.y, Ly),
+                       min_image(xyz[3 * a + 2] - c.z, Lz)};
+        if (!isfinite(d[0] + d[1] + d[2])) status_set(st, ST_NONFINITE);
+        v.x = (R)d[0];
+        v.y = (R)d[1];
+        v.z = (R)d[2];
         v.w = (R)q[a];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = __double2float_rd(d[k]);
+            hi[k] = __double2float_ru(d[k]);
+        }
     }
-    xq[s] = v;
+    if (inside) xq[s] = v;
+    // min/max over the 8 slots of the cluster (8 consecutive lanes)
+#pragma unroll
+    for (int o = 1; o < CLUSTER; o <<= 1)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = fminf(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = fmaxf(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+    if (inside && (s % CLUSTER) == 0) {
+        cur_lo[s / CLUSTER] = make_float4(lo[0], lo[1], lo[2], 0.f);
+        cur_hi[s / CLUSTER] = make_float4(hi[0], hi[1], hi[2], 0.f);
+    }
 }
 
 __global__ void k_slot_type(int nslots, const int* __restrict__ slot_atom, const int* __restrict__ type, int pad_type,
@@ -397,60 +417,93 @@ __global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const
 }
 
 // ------------------------------------------------------------- pruning
-// One warp per i cluster, four entries at a time in the pair kernel's layout
-// (lane = jslot*8 + ii): the eight j atoms of each entry are staged in shared
-// memory with coalesced loads, every lane tests its i atom against them, and
-// an entry is kept when any unmasked atom pair lies inside rcut (current
-// positions).  Kept entries are compacted, in list order, into the same
-// offsets of the pruned list.
+// Two levels.  One lane per outer entry: reject the entry when the current
+// bounding boxes of the two clusters (k_pack) are rcut apart.  Surviving
+// entries are then tested atom pair by atom pair in the pair kernel's layout
+// (lane = jslot*8 + ii, j atoms staged in shared memory with coalesced loads),
+// four at a time, and kept when any unmasked pair lies inside rcut.  Kept
+// entries are compacted, in list order, into the same offsets of the pruned
+// list.  Image offsets use the exact-FP32 centres plus the hi/lo shift table.
+struct PruneShifts {
+    float v[27][6];
+};
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restrict__ ilist,
                                                const PairEntry* __restrict__ plist,
                                                const typename V4<R>::type* __restrict__ xq,
-                                               const double4* __restrict__ center, double Lx, double Ly, double Lz,
-                                               R rcut2, ILRange* __restrict__ ilist_in,
-                                               PairEntry* __restrict__ plist_in, unsigned long long* __restrict__ n_in)
+                                               const float4* __restrict__ centerf, const float4* __restrict__ cur_lo,
+                                               const float4* __restrict__ cur_hi, PruneShifts shifts, float rcut2,
+                                               ILRange* __restrict__ ilist_in, PairEntry* __restrict__ plist_in,
+                                               unsigned long long* __restrict__ n_in)
 {
     using V4t = typename V4<R>::type;
     __shared__ V4t sj[8][4][CLUSTER + 1];
+    __shared__ PairEntry cand[8][32];
+    __shared__ float sh[27][6];
+    for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
+    __syncthreads();
     const int wib = threadIdx.x >> 5;
     const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31, jslot = lane >> 3, ii = lane & 7;
     if (I >= ncl) return;
     const ILRange L = ilist[I];
     const V4t xi = xq[I * CLUSTER + ii];
-    const double4 cI = center[I];
+    const float4 cI = centerf[I], ilo = cur_lo[I], ihi = cur_hi[I];
     int kept = 0;
-    for (int base = 0; base < L.count; base += 4) {
-        const int e = base + jslot;
+    for (int base = 0; base < L.count; base += 32) {
+        // level 1: box test, one entry per lane
+        const int e = base + lane;
+        bool cand_ok = false;
         PairEntry pe;
         pe.j = I; pe.shift = 13; pe.mask = 0ull;
-        if (e < L.count) pe = plist[L.start + e];
-        const int J = pe.j;
-        sj[wib][jslot][ii] = xq[J * CLUSTER + ii];
-        int sx, sy, sz;
-        shift_decode(pe.shift, sx, sy, sz);
-        const double4 cJ = center[J];
-        const R xx = xi.x + (R)(cI.x - cJ.x - sx * Lx), yy = xi.y + (R)(cI.y - cJ.y - sy * Ly),
-                zz = xi.z + (R)(cI.z - cJ.z - sz * Lz);
-        const unsigned row = (unsigned)(pe.mask >> (ii * 8)) & 0xffu;
-        __syncwarp();
-        bool near = false;
-#pragma unroll
-        for (int jj = 0; jj < CLUSTER; ++jj) {
-            const V4t v = sj[wib][jslot][jj];
-            const R dx = xx - v.x, dy = yy - v.y, dz = zz - v.z;
-            near |= ((row >> jj) & 1u) && (dx * dx + dy * dy + dz * dz < rcut2);
+        if (e < L.count) {
+            pe = plist[L.start + e];
+            const float4 cJ = centerf[pe.j], jlo = cur_lo[pe.j], jhi = cur_hi[pe.j];
+            const float* s6 = sh[pe.shift];
+            // J's frame origin seen from I's frame
+            const float ox = -(((cI.x - cJ.x) - s6[0]) - s6[3]);
+            const float oy = -(((cI.y - cJ.y) - s6[1]) - s6[4]);
+            const float oz = -(((cI.z - cJ.z) - s6[2]) - s6[5]);
+            const float gx = fmaxf(0.f, fmaxf(jlo.x + ox - ihi.x, ilo.x - (jhi.x + ox)));
+            const float gy = fmaxf(0.f, fmaxf(jlo.y + oy - ihi.y, ilo.y - (jhi.y + oy)));
+            const float gz = fmaxf(0.f, fmaxf(jlo.z + oz - ihi.z, ilo.z - (jhi.z + oz)));
+            cand_ok = gx * gx + gy * gy + gz * gz < rcut2;
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, near);
-        // keep[k] = any lane of j slot k found a pair
-        unsigned keep = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) keep |= ((bal >> (8 * k)) & 0xffu) ? (1u << k) : 0u;
-        if (ii == 0 && ((keep >> jslot) & 1u))
-            plist_in[L.start + kept + __popc(keep & ((1u << jslot) - 1u))] = pe;
-        kept += __popc(keep);
+        const unsigned cb = __ballot_sync(0xffffffffu, cand_ok);
+        if (cand_ok) cand[wib][__popc(cb & ((1u << lane) - 1u))] = pe;
+        const int ncand = __popc(cb);
         __syncwarp();
+        // level 2: atom pairs of the candidates, four entries at a time
+        for (int cbase = 0; cbase < ncand; cbase += 4) {
+            const int ce = cbase + jslot;
+            PairEntry q;
+            q.j = I; q.shift = 13; q.mask = 0ull;
+            if (ce < ncand) q = cand[wib][ce];
+            sj[wib][jslot][ii] = xq[q.j * CLUSTER + ii];
+            const float4 cJ = centerf[q.j];
+            const float* s6 = sh[q.shift];
+            const R xx = xi.x + (R)(((cI.x - cJ.x) - s6[0]) - s6[3]);
+            const R yy = xi.y + (R)(((cI.y - cJ.y) - s6[1]) - s6[4]);
+            const R zz = xi.z + (R)(((cI.z - cJ.z) - s6[2]) - s6[5]);
+            const unsigned row = (unsigned)(q.mask >> (ii * 8)) & 0xffu;
+            __syncwarp();
+            bool near = false;
+#pragma unroll
+            for (int jj = 0; jj < CLUSTER; ++jj) {
+                const V4t v = sj[wib][jslot][jj];
+                const R dx = xx - v.x, dy = yy - v.y, dz = zz - v.z;
+                near |= ((row >> jj) & 1u) && (dx * dx + dy * dy + dz * dz < (R)rcut2);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, near);
+            unsigned keep = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) keep |= ((bal >> (8 * k)) & 0xffu) ? (1u << k) : 0u;
+            if (ii == 0 && ((keep >> jslot) & 1u))
+                plist_in[L.start + kept + __popc(keep & ((1u << jslot) - 1u))] = q;
+            kept += __popc(keep);
+            __syncwarp();
+        }
     }
     if (lane == 0) {
         ILRange r;
@@ -465,16 +518,26 @@ void prune_pairlist(Ctx& c)
     const int th = 256;
     // a hair above the cutoff so working-precision rounding never drops a pair at r ~ rc
     double rc = c.p.cutoff + std::max(0.0, c.p.prune_margin) + 0.02;
+    PruneShifts sh;
+    for (int code = 0; code < 27; ++code) {
+        int sv[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+        for (int d = 0; d < 3; ++d) {
+            double v = sv[d] * c.box[d];
+            float hi = (float)v;
+            sh.v[code][d] = hi;
+            sh.v[code][3 + d] = (float)(v - (double)hi);
+        }
+    }
     MDF_CUDA_TRY(cudaMemsetAsync(c.n_in.p, 0, sizeof(unsigned long long), c.stream));
     int blocks = grid_blocks((long long)c.n_clusters * 32, th);
     if (c.p.precision == MDF_PREC_MIXED)
-        k_prune<float><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_f.p, c.center.p, c.box[0],
-                                                   c.box[1], c.box[2], (float)(rc * rc), c.ilist_in.p, c.plist_in.p,
-                                                   c.n_in.p);
+        k_prune<float><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_f.p, c.centerf.p,
+                                                   c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc), c.ilist_in.p,
+                                                   c.plist_in.p, c.n_in.p);
     else
-        k_prune<double><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_d.p, c.center.p,
-                                                    c.box[0], c.box[1], c.box[2], rc * rc, c.ilist_in.p, c.plist_in.p,
-                                                    c.n_in.p);
+        k_prune<double><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_d.p, c.centerf.p,
+                                                    c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc), c.ilist_in.p,
+                                                    c.plist_in.p, c.n_in.p);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
     c.pruned_valid = true;
@@ -492,11 +555,12 @@ void pack_positions(Ctx& c)
     if (c.p.precision == MDF_PREC_MIXED) {
         k_pack<float><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.xyz.p, c.q.p, c.slot_atom.p,
                                                                          c.center.p, c.box[0], c.box[1], c.box[2],
-                                                                         c.xq_f.p, c.status.p);
+                                                                         c.xq_f.p, c.cur_lo.p, c.cur_hi.p, c.status.p);
     } else {
         k_pack<double><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.xyz.p, c.q.p, c.slot_atom.p,
                                                                           c.center.p, c.box[0], c.box[1], c.box[2],
-                                                                          c.xq_d.p, c.status.p);
+                                                                          c.xq_d.p, c.cur_lo.p, c.cur_hi.p,
+                                                                          c.status.p);
     }
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
@@ -564,6 +628,8 @@ void build_pairlist(Ctx& c)
         c.center.alloc(ncl);
         c.bb_lo.alloc(ncl);
         c.bb_hi.alloc(ncl);
+        c.cur_lo.alloc(ncl);
+        c.cur_hi.alloc(ncl);
         c.centerf.alloc(ncl);
         {
             // largest power-of-two quantum keeping every centre exact in FP32 (24-bit significand)
@@ -617,6 +683,7 @@ void build_pairlist(Ctx& c)
         MDF_CUDA_TRY(cudaStreamSynchronize(s));
         if (st & ST_CAPACITY_PAIRS) throw ApiError(MDF_ERR_CAPACITY, "pair list capacity exceeded");
         c.f_slot.alloc((size_t)3 * c.n_slots);
+        c.need_clear = true;   // slot layout changed: clear the accumulators before the next evaluation
         c.plist_in.alloc((size_t)total + 1);
         c.ilist_in.alloc(ncl);
         c.n_in.alloc(1);

@@ -43,10 +43,14 @@ void mark(Ctx& c, const char* name)
 // block was copied to the host before this kernel runs.
 __global__ void k_finalize(int N, int nslots, unsigned long long* __restrict__ fatom,
                            unsigned long long* __restrict__ fslot, const int* __restrict__ atom_slot,
-                           double* __restrict__ out, unsigned long long* __restrict__ scal)
+                           double* __restrict__ out, unsigned long long* __restrict__ scal,
+                           unsigned long long* __restrict__ host_scal)
 {
     int a = blockIdx.x * blockDim.x + threadIdx.x;
-    if (a < NUM_SCAL) scal[a] = 0ull;
+    if (a < NUM_SCAL) {
+        host_scal[a] = scal[a];   // mapped pinned memory: no copy-engine round trip
+        scal[a] = 0ull;
+    }
     if (a >= N) return;
     int s = atom_slot[a];
     for (int k = 0; k < 3; ++k) {
@@ -60,7 +64,7 @@ __global__ void k_finalize(int N, int nslots, unsigned long long* __restrict__ f
 void launch_finalize(Ctx& c, double* d_forces, bool)
 {
     k_finalize<<<grid_blocks(std::max(c.N, NUM_SCAL), 256), 256, 0, c.stream>>>(
-        c.N, c.n_slots, c.f_atom.p, c.f_slot.p, c.atom_slot.p, d_forces, c.scal.p);
+        c.N, c.n_slots, c.f_atom.p, c.f_slot.p, c.atom_slot.p, d_forces, c.scal.p, c.d_hscal);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
 }
@@ -240,7 +244,6 @@ static void eval_async_impl(Ctx& c, uint32_t flags)
         launch_pme(c, energy);
         c.have_pme_ref = !phys;
     }
-    MDF_CUDA_TRY(cudaMemcpyAsync(c.h_scal, c.scal.p, sizeof(unsigned long long) * NUM_SCAL, cudaMemcpyDeviceToHost, s));
     launch_finalize(c, c.forces_out.p, false);
     mark(c, "finalize");
     c.pending = true;
@@ -406,8 +409,9 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         MDF_CUDA_TRY(cudaSetDevice(c.device));
         MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
-        MDF_CUDA_TRY(cudaMallocHost((void**)&c.h_scal, sizeof(unsigned long long) * NUM_SCAL));
+        MDF_CUDA_TRY(cudaHostAlloc((void**)&c.h_scal, sizeof(unsigned long long) * NUM_SCAL, cudaHostAllocMapped));
         memset(c.h_scal, 0, sizeof(unsigned long long) * NUM_SCAL);
+        MDF_CUDA_TRY(cudaHostGetDevicePointer((void**)&c.d_hscal, c.h_scal, 0));
         for (int d = 0; d < 3; ++d) c.box[d] = c.p.box[d];
         double tol = c.p.ewald_tol > 0 ? c.p.ewald_tol : 1e-6;
         c.alpha = c.p.ewald_alpha > 0 ? c.p.ewald_alpha : std::sqrt(std::log(2 * tol) * -1) / c.p.cutoff;

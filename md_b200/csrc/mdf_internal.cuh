@@ -181,7 +181,8 @@ struct Ctx {
     DevView<unsigned> status;            // = (unsigned*)&scal[NUM_ACC + 1]
     DevBuf<double> forces_out;           // [3N]
     DevBuf<double> forces_pme_ref;       // [3N]
-    unsigned long long* h_scal = nullptr;  // pinned copy of scal after each evaluation
+    unsigned long long* h_scal = nullptr;  // mapped pinned copy of scal, written by k_finalize
+    unsigned long long* d_hscal = nullptr; // its device address
     bool need_clear = true;              // accumulators not known to be zero
 
     // PME

@@ -417,13 +417,14 @@ __global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const
 }
 
 // ------------------------------------------------------------- pruning
-// Two levels.  One lane per outer entry: reject the entry when the current
-// bounding boxes of the two clusters (k_pack) are rcut apart.  Surviving
-// entries are then tested atom pair by atom pair in the pair kernel's layout
-// (lane = jslot*8 + ii, j atoms staged in shared memory with coalesced loads),
-// four at a time, and kept when any unmasked pair lies inside rcut.  Kept
-// entries are compacted, in list order, into the same offsets of the pruned
-// list.  Image offsets use the exact-FP32 centres plus the hi/lo shift table.
+// Two levels, one lane per outer entry.  Level 1 rejects the entry when the
+// current bounding boxes of the two clusters (k_pack) are rcut apart.  Level 2
+// loads the entry's eight j atoms (independent loads, all in flight at once),
+// skips every j atom farther than rcut from the i cluster's box, and tests the
+// rest against the eight i atoms (held in registers by every lane), stopping
+// at the first unmasked pair inside rcut.  Kept entries are compacted, in
+// list order, into the same offsets of the pruned list.  Image offsets use the
+// exact-FP32 centres plus the hi/lo shift table.
 struct PruneShifts {
     float v[27][6];
 };
@@ -438,23 +439,24 @@ __global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restric
                                                unsigned long long* __restrict__ n_in)
 {
     using V4t = typename V4<R>::type;
-    __shared__ V4t sj[8][4][CLUSTER + 1];
-    __shared__ PairEntry cand[8][32];
     __shared__ float sh[27][6];
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
     __syncthreads();
-    const int wib = threadIdx.x >> 5;
     const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31, jslot = lane >> 3, ii = lane & 7;
+    const int lane = threadIdx.x & 31;
     if (I >= ncl) return;
     const ILRange L = ilist[I];
-    const V4t xi = xq[I * CLUSTER + ii];
+    R xi[CLUSTER], yi[CLUSTER], zi[CLUSTER];
+#pragma unroll
+    for (int k = 0; k < CLUSTER; ++k) {
+        const V4t v = xq[I * CLUSTER + k];
+        xi[k] = v.x; yi[k] = v.y; zi[k] = v.z;
+    }
     const float4 cI = centerf[I], ilo = cur_lo[I], ihi = cur_hi[I];
     int kept = 0;
     for (int base = 0; base < L.count; base += 32) {
-        // level 1: box test, one entry per lane
         const int e = base + lane;
-        bool cand_ok = false;
+        bool keep = false;
         PairEntry pe;
         pe.j = I; pe.shift = 13; pe.mask = 0ull;
         if (e < L.count) {
@@ -468,42 +470,29 @@ __global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restric
             const float gx = fmaxf(0.f, fmaxf(jlo.x + ox - ihi.x, ilo.x - (jhi.x + ox)));
             const float gy = fmaxf(0.f, fmaxf(jlo.y + oy - ihi.y, ilo.y - (jhi.y + oy)));
             const float gz = fmaxf(0.f, fmaxf(jlo.z + oz - ihi.z, ilo.z - (jhi.z + oz)));
-            cand_ok = gx * gx + gy * gy + gz * gz < rcut2;
-        }
-        const unsigned cb = __ballot_sync(0xffffffffu, cand_ok);
-        if (cand_ok) cand[wib][__popc(cb & ((1u << lane) - 1u))] = pe;
-        const int ncand = __popc(cb);
-        __syncwarp();
-        // level 2: atom pairs of the candidates, four entries at a time
-        for (int cbase = 0; cbase < ncand; cbase += 4) {
-            const int ce = cbase + jslot;
-            PairEntry q;
-            q.j = I; q.shift = 13; q.mask = 0ull;
-            if (ce < ncand) q = cand[wib][ce];
-            sj[wib][jslot][ii] = xq[q.j * CLUSTER + ii];
-            const float4 cJ = centerf[q.j];
-            const float* s6 = sh[q.shift];
-            const R xx = xi.x + (R)(((cI.x - cJ.x) - s6[0]) - s6[3]);
-            const R yy = xi.y + (R)(((cI.y - cJ.y) - s6[1]) - s6[4]);
-            const R zz = xi.z + (R)(((cI.z - cJ.z) - s6[2]) - s6[5]);
-            const unsigned row = (unsigned)(q.mask >> (ii * 8)) & 0xffu;
-            __syncwarp();
-            bool near = false;
+            if (gx * gx + gy * gy + gz * gz < rcut2) {
+                V4t vj[CLUSTER];
 #pragma unroll
-            for (int jj = 0; jj < CLUSTER; ++jj) {
-                const V4t v = sj[wib][jslot][jj];
-                const R dx = xx - v.x, dy = yy - v.y, dz = zz - v.z;
-                near |= ((row >> jj) & 1u) && (dx * dx + dy * dy + dz * dz < (R)rcut2);
+                for (int jj = 0; jj < CLUSTER; ++jj) vj[jj] = xq[pe.j * CLUSTER + jj];
+                const unsigned long long m = pe.mask;
+                for (int jj = 0; jj < CLUSTER && !keep; ++jj) {
+                    const float px = (float)vj[jj].x + ox, py = (float)vj[jj].y + oy, pz = (float)vj[jj].z + oz;
+                    const float bx = fmaxf(0.f, fmaxf(ilo.x - px, px - ihi.x));
+                    const float by = fmaxf(0.f, fmaxf(ilo.y - py, py - ihi.y));
+                    const float bz = fmaxf(0.f, fmaxf(ilo.z - pz, pz - ihi.z));
+                    if (bx * bx + by * by + bz * bz >= rcut2) continue;
+                    const R qx = vj[jj].x + (R)ox, qy = vj[jj].y + (R)oy, qz = vj[jj].z + (R)oz;
+#pragma unroll
+                    for (int ii = 0; ii < CLUSTER; ++ii) {
+                        const R dx = xi[ii] - qx, dy = yi[ii] - qy, dz = zi[ii] - qz;
+                        keep |= ((m >> (ii * 8 + jj)) & 1ull) && (dx * dx + dy * dy + dz * dz < (R)rcut2);
+                    }
+                }
             }
-            const unsigned bal = __ballot_sync(0xffffffffu, near);
-            unsigned keep = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) keep |= ((bal >> (8 * k)) & 0xffu) ? (1u << k) : 0u;
-            if (ii == 0 && ((keep >> jslot) & 1u))
-                plist_in[L.start + kept + __popc(keep & ((1u << jslot) - 1u))] = q;
-            kept += __popc(keep);
-            __syncwarp();
         }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (keep) plist_in[L.start + kept + __popc(bal & ((1u << lane) - 1u))] = pe;
+        kept += __popc(bal);
     }
     if (lane == 0) {
         ILRange r;

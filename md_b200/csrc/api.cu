@@ -448,9 +448,9 @@ void mdf_destroy(mdf_ctx* ctx)
     c.plist_in.release(); c.ilist_in.release(); c.n_in.release(); c.cur_lo.release(); c.cur_hi.release();
     c.f_atom.release(); c.scal.release(); c.forces_out.release(); c.forces_pme_ref.release();
     c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
-    c.rgrid_d.release();
+    c.rgrid_d.release(); c.infl_f.release(); c.infl_d.release();
     for (int d = 0; d < 3; ++d) {
-        c.bmod[d].release(); c.bmod_f[d].release(); c.tw_d[d].release(); c.tw_f[d].release();
+        c.tw_d[d].release(); c.tw_f[d].release(); c.fft_tab[d].release(); c.mvec[d].release();
     }
     if (c.h_scal) cudaFreeHost(c.h_scal);
     if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);

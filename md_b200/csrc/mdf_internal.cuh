@@ -99,7 +99,10 @@ struct DevView {
 struct FFTPlan1D {
     int n = 0;
     int nstages = 0;
-    int radix[16];
+    int radix[12];
+    int ns[12];     // product of the radices before stage s
+    int toff[12];   // offset of stage s in the per-butterfly index table
+    int ntab = 0;   // entries of the index table
 };
 
 // --------------------------------------------------------------- context
@@ -194,20 +197,14 @@ struct Ctx {
     DevBuf<double2> cgrid_d;
     DevBuf<float> rgrid_f;               // [K0*K1*K2] potential
     DevBuf<double> rgrid_d;
-    DevBuf<double> bmod[3];              // PHYSICAL: 1/|b(m)|^2 factors; REFERENCE: moduli
-    DevBuf<float> bmod_f[3];
     DevBuf<double2> tw_d[3];             // twiddles per dimension
     DevBuf<float2> tw_f[3];
     FFTPlan1D plan[3];
-    // reference order-5 chain (REFERENCE semantics)
-    int Kref[3] = {0, 0, 0};
-    DevBuf<double> ref_grid;             // [K^3] double (real), used as spread target via fixed
-    DevBuf<unsigned long long> ref_qgrid;
-    DevBuf<double2> ref_cgrid;
-    DevBuf<double> ref_moduli[3];
-    DevBuf<double2> ref_tw[3];
-    FFTPlan1D ref_plan[3];
-    bool have_pme_ref = false;
+    DevBuf<int2> fft_tab[3];             // per-butterfly (twiddle step, output index) per dimension
+    DevBuf<float> infl_f;                // influence function [ky][kz][kx] (mixed)
+    DevBuf<double> infl_d;               // influence function [ky][kz][kx] (FP64 / reference solve)
+    DevBuf<double> mvec[3];              // m_d = signed frequency / L_d per grid index
+    bool have_pme_ref = false;           // forces_pme_ref holds the reference chain's forces
 
     // timing
     bool timing = false;
@@ -232,8 +229,6 @@ void launch_exclusions(Ctx& c, bool energy);
 void launch_bonded(Ctx& c, bool energy);
 void setup_pme(Ctx& c);
 void launch_pme(Ctx& c, bool energy);
-void setup_pme_reference(Ctx& c);
-void launch_pme_reference(Ctx& c);
 void launch_finalize(Ctx& c, double* d_forces, bool pme_ref);
 void mark(Ctx& c, const char* name);
 

@@ -1,7 +1,7 @@
 // Particle-mesh Ewald: charge spread, hand-written 3-D FFT, reciprocal
 // convolution with the FP64 energy/virial reduction, and force gather.
 //
-// PHYSICAL semantics: smooth PME of order n (Essmann et al., J. Chem. Phys.
+// PHYSICAL semantics: smooth PME of order 4 (Essmann et al., J. Chem. Phys.
 // 103, 8577 (1995)): E = 1/2 sum_m c(m) |S(m)|^2 with
 // c(m) = k/(pi V) exp(-pi^2 m^2/alpha^2)/m^2 * B1 B2 B3, B_d = 1/|b_d(m_d)|^2.
 // REFERENCE semantics: the reference's own chain, order 5 with its weights and
@@ -11,10 +11,13 @@
 // returned separately for parity checks.
 //
 // FFT: mixed-radix Stockham autosort in shared memory (radix 4/2/3/5 and a
-// generic small-prime butterfly), one kernel per dimension:
+// generic small-prime butterfly).  Every butterfly's twiddle step and output
+// index come from a table built on the host, so the passes do no integer
+// division.  One kernel per dimension:
 //   z: real -> half complex, two real lines packed per complex transform
 //   y: complex, LP consecutive kz columns per block (coalesced along kz)
-//   x: complex forward, convolution, complex inverse in one kernel
+//   x: complex forward, convolution with the precomputed influence function
+//      (+ FP64 energy and virial), complex inverse - one kernel
 //   y: inverse
 //   z: half complex -> real
 // The charge grid is accumulated in int64 fixed point (2^-40), so the spread
@@ -32,10 +35,15 @@ template <typename R> struct CT;
 template <> struct CT<float> { using type = float2; };
 template <> struct CT<double> { using type = double2; };
 
+constexpr int FFT_THREADS = 128;
+
 struct FFTDesc {
     int n;
     int nst;
-    int radix[16];
+    int radix[12];
+    int ns[12];
+    int toff[12];
+    int ntab;
 };
 
 template <typename C>
@@ -67,8 +75,7 @@ __device__ __forceinline__ void small_dft(C* v, int Rr, bool inverse, const C* t
         C a = v[0], b = v[1], c = v[2], d = v[3];
         C t0 = {a.x + c.x, a.y + c.y}, t1 = {a.x - c.x, a.y - c.y};
         C t2 = {b.x + d.x, b.y + d.y}, t3 = {b.x - d.x, b.y - d.y};
-        // multiply t3 by -i (forward) or +i (inverse)
-        C t3r = {-s * t3.y, s * t3.x};
+        C t3r = {-s * t3.y, s * t3.x};   // t3 * (-i) forward, * (+i) inverse
         v[0].x = t0.x + t2.x; v[0].y = t0.y + t2.y;
         v[2].x = t0.x - t2.x; v[2].y = t0.y - t2.y;
         v[1].x = t1.x + t3r.x; v[1].y = t1.y + t3r.y;
@@ -91,7 +98,6 @@ __device__ __forceinline__ void small_dft(C* v, int Rr, bool inverse, const C* t
         v[0].x = a.x + b1.x + b2.x; v[0].y = a.y + b1.y + b2.y;
         C m1 = {a.x + c1 * b1.x + c2 * b2.x, a.y + c1 * b1.y + c2 * b2.y};
         C m2 = {a.x + c2 * b1.x + c1 * b2.x, a.y + c2 * b1.y + c1 * b2.y};
-        // i * (s1 d1 + s2 d2), i * (s2 d1 - s1 d2)
         C n1 = {s1 * d1.x + s2 * d2.x, s1 * d1.y + s2 * d2.y};
         C n2 = {s2 * d1.x - s1 * d2.x, s2 * d1.y - s1 * d2.y};
         v[1].x = m1.x - n1.y; v[1].y = m1.y + n1.x;
@@ -99,9 +105,9 @@ __device__ __forceinline__ void small_dft(C* v, int Rr, bool inverse, const C* t
         v[2].x = m2.x - n2.y; v[2].y = m2.y + n2.x;
         v[3].x = m2.x + n2.y; v[3].y = m2.y - n2.x;
     } else {
-        // generic prime radix via the line's twiddle table: W_R^q = W_n^{q n/R}
+        // generic prime radix through the line's twiddle table: W_R^q = W_n^{q n/R}
         C out[32];
-        int step = n / Rr;
+        const int step = n / Rr;
         for (int t = 0; t < Rr; ++t) {
             C acc = {0, 0};
             for (int r = 0; r < Rr; ++r) {
@@ -117,190 +123,189 @@ __device__ __forceinline__ void small_dft(C* v, int Rr, bool inverse, const C* t
     }
 }
 
-// One Stockham stage with a compile-time radix (registers only).
+// One Stockham stage (radix known at compile time) on this thread's line:
+// butterflies j = lt, lt + tpl, ...; tab[j] = (twiddle step k*n/(Ns R), output index).
 template <typename C, typename R, int RR>
-__device__ __forceinline__ void stockham_stage(const C* a, C* b, int nl, int n, int Ns, const C* tw, bool inverse)
+__device__ __forceinline__ void stage_fixed(const C* in, C* out, int n, int Ns, const C* tw, const int2* tab, int lt,
+                                            int tpl, bool inverse)
 {
     const int nb = n / RR;
-    const int step = n / (Ns * RR);
-    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-        const int line = t / nb, j = t - line * nb;
-        const C* in = a + line * n;
-        C* out = b + line * n;
-        const int k = j % Ns;
+    for (int j = lt; j < nb; j += tpl) {
+        const int2 t = tab[j];
         C v[RR];
 #pragma unroll
         for (int r = 0; r < RR; ++r) {
             C x = in[j + r * nb];
-            if (r && k) {
-                C w = tw[(r * k * step) % n];
+            if (r && t.x) {
+                C w = tw[r * t.x];
                 if (inverse) w = cconj(w);
                 x = cmul(x, w);
             }
             v[r] = x;
         }
         small_dft<C, R>(v, RR, inverse, tw, n);
-        const int idxD = (j / Ns) * Ns * RR + k;
 #pragma unroll
-        for (int r = 0; r < RR; ++r) out[idxD + r * Ns] = v[r];
+        for (int r = 0; r < RR; ++r) out[t.y + r * Ns] = v[r];
     }
 }
 
-// Generic prime radix (7..31), runtime-sized.
 template <typename C, typename R>
-__device__ void stockham_stage_generic(const C* a, C* b, int nl, int n, int Ns, int Rr, const C* tw, bool inverse)
+__device__ void stage_generic(const C* in, C* out, int n, int Rr, int Ns, const C* tw, const int2* tab, int lt,
+                              int tpl, bool inverse)
 {
     const int nb = n / Rr;
-    const int step = n / (Ns * Rr);
-    for (int t = threadIdx.x; t < nl * nb; t += blockDim.x) {
-        const int line = t / nb, j = t - line * nb;
-        const C* in = a + line * n;
-        C* out = b + line * n;
-        const int k = j % Ns;
+    for (int j = lt; j < nb; j += tpl) {
+        const int2 t = tab[j];
         C v[32];
         for (int r = 0; r < Rr; ++r) {
             C x = in[j + r * nb];
-            if (r && k) {
-                C w = tw[(r * k * step) % n];
+            if (r && t.x) {
+                C w = tw[r * t.x];
                 if (inverse) w = cconj(w);
                 x = cmul(x, w);
             }
             v[r] = x;
         }
         small_dft<C, R>(v, Rr, inverse, tw, n);
-        const int idxD = (j / Ns) * Ns * Rr + k;
-        for (int r = 0; r < Rr; ++r) out[idxD + r * Ns] = v[r];
+        for (int r = 0; r < Rr; ++r) out[t.y + r * Ns] = v[r];
     }
 }
 
-// Stockham autosort FFT of nl lines stored [line][n] in shared memory.
-// tw[q] = exp(-2 pi i q / n).  Returns the buffer holding the result.
+// Stockham FFT of the block's lines stored [line][n] in shared memory; this
+// thread works on line `line` with lane lt of tpl.  Returns the result buffer.
 template <typename C, typename R>
-__device__ C* fft_lines(C* a, C* b, int nl, const FFTDesc& d, const C* tw, bool inverse)
+__device__ C* fft_lines(C* a, C* b, const FFTDesc& d, const C* tw, const int2* tab, int line, int lt, int tpl,
+                        bool inverse)
 {
-    int Ns = 1;
     const int n = d.n;
     for (int s = 0; s < d.nst; ++s) {
         const int Rr = d.radix[s];
+        const C* in = a + line * n;
+        C* out = b + line * n;
+        const int2* ts = tab + d.toff[s];
         switch (Rr) {
-            case 2: stockham_stage<C, R, 2>(a, b, nl, n, Ns, tw, inverse); break;
-            case 3: stockham_stage<C, R, 3>(a, b, nl, n, Ns, tw, inverse); break;
-            case 4: stockham_stage<C, R, 4>(a, b, nl, n, Ns, tw, inverse); break;
-            case 5: stockham_stage<C, R, 5>(a, b, nl, n, Ns, tw, inverse); break;
-            default: stockham_stage_generic<C, R>(a, b, nl, n, Ns, Rr, tw, inverse); break;
+            case 2: stage_fixed<C, R, 2>(in, out, n, d.ns[s], tw, ts, lt, tpl, inverse); break;
+            case 3: stage_fixed<C, R, 3>(in, out, n, d.ns[s], tw, ts, lt, tpl, inverse); break;
+            case 4: stage_fixed<C, R, 4>(in, out, n, d.ns[s], tw, ts, lt, tpl, inverse); break;
+            case 5: stage_fixed<C, R, 5>(in, out, n, d.ns[s], tw, ts, lt, tpl, inverse); break;
+            default: stage_generic<C, R>(in, out, n, Rr, d.ns[s], tw, ts, lt, tpl, inverse); break;
         }
         __syncthreads();
-        C* tmp = a;
+        C* t = a;
         a = b;
-        b = tmp;
-        Ns *= Rr;
+        b = t;
     }
     return a;
 }
 
+// shared memory: twiddles [n] | index table [ntab] | two line buffers [LP][n]
 template <typename C>
-__device__ void load_tw(C* s_tw, const C* __restrict__ g_tw, int n)
+__device__ __forceinline__ void fft_smem_setup(unsigned char* raw, const FFTDesc& d, const C* __restrict__ g_tw,
+                                               const int2* __restrict__ g_tab, int LP, C*& tw, int2*& tab, C*& bufA,
+                                               C*& bufB)
 {
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s_tw[i] = g_tw[i];
+    tw = reinterpret_cast<C*>(raw);
+    bufA = tw + d.n;
+    bufB = bufA + LP * d.n;
+    tab = reinterpret_cast<int2*>(bufB + LP * d.n);
+    for (int i = threadIdx.x; i < d.n; i += blockDim.x) tw[i] = g_tw[i];
+    for (int i = threadIdx.x; i < d.ntab; i += blockDim.x) tab[i] = g_tab[i];
 }
 
 // ------------------------------------------------------------- z passes
 template <typename R>
-__global__ void k_fft_z_r2c(const unsigned long long* __restrict__ qgrid, typename CT<R>::type* __restrict__ cgrid,
-                            int nlines, int K2, FFTDesc dz, const typename CT<R>::type* __restrict__ twz, int LP)
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const unsigned long long* __restrict__ qgrid,
+                                                           typename CT<R>::type* __restrict__ cgrid, int nlines,
+                                                           FFTDesc dz, const typename CT<R>::type* __restrict__ twz,
+                                                           const int2* __restrict__ tabz, int LP)
 {
     using C = typename CT<R>::type;
-    extern __shared__ unsigned char smem_raw[];
-    C* s_tw = reinterpret_cast<C*>(smem_raw);
-    C* bufA = s_tw + K2;
-    C* bufB = bufA + LP * K2;
-    load_tw(s_tw, twz, K2);
-    const long long line0 = (long long)blockIdx.x * 2 * LP;
-    for (int e = threadIdx.x; e < 2 * LP * K2; e += blockDim.x) {
-        int rl = e / K2, z = e - rl * K2;
-        long long g = line0 + rl;
-        R v = 0;
-        if (g < nlines) v = (R)((double)(long long)qgrid[g * K2 + z] * GRID_ISCALE);
-        R* comp = reinterpret_cast<R*>(&bufA[(rl >> 1) * K2 + z]);
-        comp[rl & 1] = v;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw, *bufA, *bufB;
+    int2* tab;
+    fft_smem_setup(smem_raw, dz, twz, tabz, LP, tw, tab, bufA, bufB);
+    const int K2 = dz.n, Kc = K2 / 2 + 1;
+    const int tpl = blockDim.x / LP, line = threadIdx.x / tpl, lt = threadIdx.x - line * tpl;
+    const long long g0 = (long long)blockIdx.x * 2 * LP + 2 * line;   // this thread's pair of real lines
+    for (int z = lt; z < K2; z += tpl) {
+        C v;
+        v.x = g0 < nlines ? (R)((double)(long long)qgrid[g0 * K2 + z] * GRID_ISCALE) : (R)0;
+        v.y = g0 + 1 < nlines ? (R)((double)(long long)qgrid[(g0 + 1) * K2 + z] * GRID_ISCALE) : (R)0;
+        bufA[line * K2 + z] = v;
     }
     __syncthreads();
-    C* res = fft_lines<C, R>(bufA, bufB, LP, dz, s_tw, false);
-    const int Kc = K2 / 2 + 1;
-    for (int e = threadIdx.x; e < LP * Kc; e += blockDim.x) {
-        int p = e / Kc, k = e - p * Kc;
-        C Z = res[p * K2 + k], Zc = cconj(res[p * K2 + (K2 - k) % K2]);
-        C A = {(R)0.5 * (Z.x + Zc.x), (R)0.5 * (Z.y + Zc.y)};
-        C B = {(R)0.5 * (Z.y - Zc.y), (R)-0.5 * (Z.x - Zc.x)};
-        long long g = line0 + 2 * p;
-        if (g < nlines) cgrid[g * Kc + k] = A;
-        if (g + 1 < nlines) cgrid[(g + 1) * Kc + k] = B;
+    const C* res = fft_lines<C, R>(bufA, bufB, dz, tw, tab, line, lt, tpl, false);
+    for (int k = lt; k < Kc; k += tpl) {
+        const C Z = res[line * K2 + k], Zc = cconj(res[line * K2 + (k == 0 ? 0 : K2 - k)]);
+        const C A = {(R)0.5 * (Z.x + Zc.x), (R)0.5 * (Z.y + Zc.y)};
+        const C B = {(R)0.5 * (Z.y - Zc.y), (R)-0.5 * (Z.x - Zc.x)};
+        if (g0 < nlines) cgrid[g0 * Kc + k] = A;
+        if (g0 + 1 < nlines) cgrid[(g0 + 1) * Kc + k] = B;
     }
 }
 
 template <typename R>
-__global__ void k_fft_z_c2r(const typename CT<R>::type* __restrict__ cgrid, R* __restrict__ rgrid, int nlines, int K2,
-                            FFTDesc dz, const typename CT<R>::type* __restrict__ twz, int LP)
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const typename CT<R>::type* __restrict__ cgrid,
+                                                           R* __restrict__ rgrid, int nlines, FFTDesc dz,
+                                                           const typename CT<R>::type* __restrict__ twz,
+                                                           const int2* __restrict__ tabz, int LP)
 {
     using C = typename CT<R>::type;
-    extern __shared__ unsigned char smem_raw[];
-    C* s_tw = reinterpret_cast<C*>(smem_raw);
-    C* bufA = s_tw + K2;
-    C* bufB = bufA + LP * K2;
-    load_tw(s_tw, twz, K2);
-    const long long line0 = (long long)blockIdx.x * 2 * LP;
-    const int Kc = K2 / 2 + 1;
-    for (int e = threadIdx.x; e < LP * K2; e += blockDim.x) {
-        int p = e / K2, k = e - p * K2;
-        long long g = line0 + 2 * p;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw, *bufA, *bufB;
+    int2* tab;
+    fft_smem_setup(smem_raw, dz, twz, tabz, LP, tw, tab, bufA, bufB);
+    const int K2 = dz.n, Kc = K2 / 2 + 1;
+    const int tpl = blockDim.x / LP, line = threadIdx.x / tpl, lt = threadIdx.x - line * tpl;
+    const long long g0 = (long long)blockIdx.x * 2 * LP + 2 * line;
+    for (int k = lt; k < K2; k += tpl) {
+        const int kk = k < Kc ? k : K2 - k;
         C A = {0, 0}, B = {0, 0};
-        int kk = k < Kc ? k : K2 - k;
-        if (g < nlines) A = cgrid[g * Kc + kk];
-        if (g + 1 < nlines) B = cgrid[(g + 1) * Kc + kk];
+        if (g0 < nlines) A = cgrid[g0 * Kc + kk];
+        if (g0 + 1 < nlines) B = cgrid[(g0 + 1) * Kc + kk];
         if (k >= Kc) {
             A = cconj(A);
             B = cconj(B);
         }
-        C Z = {A.x - B.y, A.y + B.x};
-        bufA[p * K2 + k] = Z;
+        const C Z = {A.x - B.y, A.y + B.x};
+        bufA[line * K2 + k] = Z;
     }
     __syncthreads();
-    C* res = fft_lines<C, R>(bufA, bufB, LP, dz, s_tw, true);
-    for (int e = threadIdx.x; e < LP * K2; e += blockDim.x) {
-        int p = e / K2, k = e - p * K2;
-        long long g = line0 + 2 * p;
-        C Z = res[p * K2 + k];
-        if (g < nlines) rgrid[g * K2 + k] = Z.x;
-        if (g + 1 < nlines) rgrid[(g + 1) * K2 + k] = Z.y;
+    const C* res = fft_lines<C, R>(bufA, bufB, dz, tw, tab, line, lt, tpl, true);
+    for (int k = lt; k < K2; k += tpl) {
+        const C Z = res[line * K2 + k];
+        if (g0 < nlines) rgrid[g0 * K2 + k] = Z.x;
+        if (g0 + 1 < nlines) rgrid[(g0 + 1) * K2 + k] = Z.y;
     }
 }
 
 // ------------------------------------------------------------- y pass
 template <typename R>
-__global__ void k_fft_y(typename CT<R>::type* __restrict__ cgrid, int K1, int Kc, FFTDesc dy,
-                        const typename CT<R>::type* __restrict__ twy, int LP, bool inverse)
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_y(typename CT<R>::type* __restrict__ cgrid, int Kc, FFTDesc dy,
+                                                       const typename CT<R>::type* __restrict__ twy,
+                                                       const int2* __restrict__ taby, int LP, int lp_shift,
+                                                       bool inverse)
 {
     using C = typename CT<R>::type;
-    extern __shared__ unsigned char smem_raw[];
-    C* s_tw = reinterpret_cast<C*>(smem_raw);
-    C* bufA = s_tw + K1;
-    C* bufB = bufA + LP * K1;
-    load_tw(s_tw, twy, K1);
-    const int x = blockIdx.y;
-    const int kz0 = blockIdx.x * LP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw, *bufA, *bufB;
+    int2* tab;
+    fft_smem_setup(smem_raw, dy, twy, taby, LP, tw, tab, bufA, bufB);
+    const int K1 = dy.n;
+    const int x = blockIdx.y, kz0 = blockIdx.x * LP;
     const long long base = (long long)x * K1 * Kc;
+    // loads: consecutive threads take consecutive kz (coalesced)
     for (int e = threadIdx.x; e < LP * K1; e += blockDim.x) {
-        int y = e / LP, l = e - y * LP;
-        int kz = kz0 + l;
+        const int y = e >> lp_shift, l = e & (LP - 1), kz = kz0 + l;
         C v = {0, 0};
         if (kz < Kc) v = cgrid[base + (long long)y * Kc + kz];
         bufA[l * K1 + y] = v;
     }
     __syncthreads();
-    C* res = fft_lines<C, R>(bufA, bufB, LP, dy, s_tw, inverse);
+    const int tpl = blockDim.x / LP, line = threadIdx.x / tpl, lt = threadIdx.x - line * tpl;
+    const C* res = fft_lines<C, R>(bufA, bufB, dy, tw, tab, line, lt, tpl, inverse);
     for (int e = threadIdx.x; e < LP * K1; e += blockDim.x) {
-        int y = e / LP, l = e - y * LP;
-        int kz = kz0 + l;
+        const int y = e >> lp_shift, l = e & (LP - 1), kz = kz0 + l;
         if (kz < Kc) cgrid[base + (long long)y * Kc + kz] = res[l * K1 + y];
     }
 }
@@ -308,93 +313,67 @@ __global__ void k_fft_y(typename CT<R>::type* __restrict__ cgrid, int K1, int Kc
 // ------------------------------------------- x pass + convolution + inverse
 struct ConvParams {
     int K[3];
-    double L[3];
-    double fac;       // PHYSICAL: k/(pi V); REFERENCE: 4 pi / V
-    double pa2;       // PHYSICAL: pi^2/alpha^2; REFERENCE: 1/(4 alpha^2)
-    double norm;      // REFERENCE: 1/(K0 K1 K2)
-    int reference;
+    double pa2;       // pi^2 / alpha^2 (virial factor)
+    int reference;    // REFERENCE solve: no energy or virial
 };
 
 template <typename R, bool ENERGY>
-__global__ void k_fft_x_conv(typename CT<R>::type* __restrict__ cgrid, int K1, int Kc, FFTDesc dx,
-                             const typename CT<R>::type* __restrict__ twx, int LP, ConvParams cp,
-                             const R* __restrict__ b0, const R* __restrict__ b1, const R* __restrict__ b2,
-                             unsigned long long* __restrict__ acc, unsigned* st)
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv(
+    typename CT<R>::type* __restrict__ cgrid, int K1, int Kc, FFTDesc dx, const typename CT<R>::type* __restrict__ twx,
+    const int2* __restrict__ tabx, int LP, int lp_shift, ConvParams cp, const R* __restrict__ infl,
+    const double* __restrict__ mx, const double* __restrict__ my, const double* __restrict__ mz,
+    unsigned long long* __restrict__ acc, unsigned* st)
 {
     using C = typename CT<R>::type;
-    extern __shared__ unsigned char smem_raw[];
-    const int K0 = cp.K[0];
-    C* s_tw = reinterpret_cast<C*>(smem_raw);
-    C* bufA = s_tw + K0;
-    C* bufB = bufA + LP * K0;
-    load_tw(s_tw, twx, K0);
-    const int y = blockIdx.y;
-    const int kz0 = blockIdx.x * LP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *tw, *bufA, *bufB;
+    int2* tab;
+    fft_smem_setup(smem_raw, dx, twx, tabx, LP, tw, tab, bufA, bufB);
+    const int K0 = dx.n;
+    const int y = blockIdx.y, kz0 = blockIdx.x * LP;
     const long long stride = (long long)K1 * Kc;
     for (int e = threadIdx.x; e < LP * K0; e += blockDim.x) {
-        int x = e / LP, l = e - x * LP;
-        int kz = kz0 + l;
+        const int x = e >> lp_shift, l = e & (LP - 1), kz = kz0 + l;
         C v = {0, 0};
         if (kz < Kc) v = cgrid[x * stride + (long long)y * Kc + kz];
         bufA[l * K0 + x] = v;
     }
     __syncthreads();
-    C* res = fft_lines<C, R>(bufA, bufB, LP, dx, s_tw, false);
+    const int tpl = blockDim.x / LP, line = threadIdx.x / tpl, lt = threadIdx.x - line * tpl;
+    C* res = fft_lines<C, R>(bufA, bufB, dx, tw, tab, line, lt, tpl, false);
     C* other = (res == bufA) ? bufB : bufA;
     double e_sum = 0, w6[6] = {0, 0, 0, 0, 0, 0};
-    const int my_i = (y <= cp.K[1] / 2) ? y : y - cp.K[1];
-    for (int e = threadIdx.x; e < LP * K0; e += blockDim.x) {
-        int l = e / K0, kx = e - l * K0;
-        int kz = kz0 + l;
-        C S = res[l * K0 + kx];
-        if (kz >= Kc) continue;
-        int mx_i = (kx <= K0 / 2) ? kx : kx - K0;
-        if (!cp.reference) {
-            double mx = mx_i / cp.L[0], my = my_i / cp.L[1], mz = kz / cp.L[2];
-            double m2 = mx * mx + my * my + mz * mz;
-            R c;
-            if (kx == 0 && y == 0 && kz == 0) {
-                c = 0;
-            } else {
-                c = (R)(cp.fac * exp(-cp.pa2 * m2) / m2) * b0[kx] * b1[y] * b2[kz];
-                if (ENERGY) {
-                    double wgt = (kz == 0 || ((cp.K[2] & 1) == 0 && kz == cp.K[2] / 2)) ? 1.0 : 2.0;
-                    double s2 = (double)S.x * S.x + (double)S.y * S.y;
-                    double em = 0.5 * (double)c * s2 * wgt;
-                    e_sum += em;
-                    double vf = 2.0 * (1.0 + cp.pa2 * m2) / m2;
-                    double mv[3] = {mx, my, mz};
-                    int q = 0;
-                    for (int a = 0; a < 3; ++a)
-                        for (int b = a; b < 3; ++b) w6[q++] += em * ((a == b ? 1.0 : 0.0) - vf * mv[a] * mv[b]);
-                }
+    const int kz = kz0 + line;
+    if (kz < Kc) {
+        // influence function laid out [ky][kz][kx]: this line is contiguous
+        const R* fl = infl + ((long long)y * Kc + kz) * K0;
+        const double wgt = (kz == 0 || ((cp.K[2] & 1) == 0 && kz == cp.K[2] / 2)) ? 1.0 : 2.0;
+        for (int kx = lt; kx < K0; kx += tpl) {
+            C S = res[line * K0 + kx];
+            const R c = fl[kx];
+            if (ENERGY && !cp.reference && c != (R)0) {
+                const double s2 = (double)S.x * S.x + (double)S.y * S.y;
+                const double em = 0.5 * (double)c * s2 * wgt;
+                e_sum += em;
+                const double m[3] = {mx[kx], my[y], mz[kz]};
+                const double m2 = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+                const double vf = 2.0 * (1.0 + cp.pa2 * m2) / m2;
+                int q = 0;
+#pragma unroll
+                for (int a = 0; a < 3; ++a)
+#pragma unroll
+                    for (int b = a; b < 3; ++b) w6[q++] += em * ((a == b ? 1.0 : 0.0) - vf * m[a] * m[b]);
             }
             S.x *= c;
             S.y *= c;
-        } else {
-            // src/System/PBC.cpp:511-563
-            const double PI = 3.14159265358979323846;
-            double kxv = 2.0 * PI * mx_i / cp.L[0], kyv = 2.0 * PI * my_i / cp.L[1], kzv = 2.0 * PI * kz / cp.L[2];
-            double ksq = kxv * kxv + kyv * kyv + kzv * kzv;
-            if (ksq < 1e-10) {
-                S.x = 0;
-                S.y = 0;
-            } else {
-                double infl = cp.fac * exp(ksq * (-cp.pa2)) / ksq;
-                double bc = 1.0 / ((double)b0[kx] * (double)b1[y] * (double)b2[kz]);
-                double sc = infl * bc * cp.norm;
-                S.x = (R)(S.x * sc);
-                S.y = (R)(S.y * sc);
-            }
+            res[line * K0 + kx] = S;
         }
-        res[l * K0 + kx] = S;
     }
     __syncthreads();
-    C* out = fft_lines<C, R>(res, other, LP, dx, s_tw, true);
+    const C* out = fft_lines<C, R>(res, other, dx, tw, tab, line, lt, tpl, true);
     for (int e = threadIdx.x; e < LP * K0; e += blockDim.x) {
-        int x = e / LP, l = e - x * LP;
-        int kz = kz0 + l;
-        if (kz < Kc) cgrid[x * stride + (long long)y * Kc + kz] = out[l * K0 + x];
+        const int x = e >> lp_shift, l = e & (LP - 1), kzz = kz0 + l;
+        if (kzz < Kc) cgrid[x * stride + (long long)y * Kc + kzz] = out[l * K0 + x];
     }
     if (ENERGY && !cp.reference) {
         const double v[7] = {e_sum, w6[0], w6[1], w6[2], w6[3], w6[4], w6[5]};
@@ -530,7 +509,7 @@ __global__ void k_gather4(int nslots, const int* __restrict__ slot_atom, const d
 
 // The reference's order-5 weights (src/System/PBC.cpp:329-356 for the spread,
 // :359-401 for the gather; the two differ in operation order).
-__device__ __forceinline__ void ref_w5_spread(double u, double th[5])
+__host__ __device__ __forceinline__ void ref_w5_spread(double u, double th[5])
 {
     double c0 = 1.0 - u, c1 = u;
     double w0 = (1.0 / 2.0) * ((1.0 - u) * c0);
@@ -635,21 +614,38 @@ __global__ void k_gather_ref5(int N, const double* __restrict__ xyz, const doubl
 }
 
 // ------------------------------------------------------------------ host
-static FFTPlan1D make_plan(int n)
+static FFTPlan1D make_plan(int n, std::vector<int2>& tab)
 {
     FFTPlan1D p;
     p.n = n;
     p.nstages = 0;
     int m = n;
-    while (m % 4 == 0) { p.radix[p.nstages++] = 4; m /= 4; }
-    while (m % 2 == 0) { p.radix[p.nstages++] = 2; m /= 2; }
+    auto push = [&](int f) {
+        if (p.nstages >= 12) throw ApiError(MDF_ERR_UNSUPPORTED, "PME grid size has too many factors");
+        p.radix[p.nstages++] = f;
+        m /= f;
+    };
+    while (m % 4 == 0) push(4);
+    while (m % 2 == 0) push(2);
     for (int f = 3; f <= 31 && m > 1; f += 2)
-        while (m % f == 0) {
-            if (p.nstages >= 16) throw ApiError(MDF_ERR_UNSUPPORTED, "FFT size has too many factors");
-            p.radix[p.nstages++] = f;
-            m /= f;
-        }
+        while (m % f == 0) push(f);
     if (m != 1) throw ApiError(MDF_ERR_UNSUPPORTED, "PME grid size has a prime factor above 31");
+    // per-butterfly table: Stockham stage s with radix R, Ns = product of the
+    // earlier radices, butterfly j: twiddle step (j mod Ns) * n/(Ns R) and
+    // output index (j div Ns) Ns R + (j mod Ns)
+    tab.clear();
+    int Ns = 1;
+    for (int s = 0; s < p.nstages; ++s) {
+        const int R = p.radix[s], nb = n / R, step = n / (Ns * R);
+        p.ns[s] = Ns;
+        p.toff[s] = (int)tab.size();
+        for (int j = 0; j < nb; ++j) {
+            const int k = j % Ns;
+            tab.push_back(make_int2(k * step, (j / Ns) * Ns * R + k));
+        }
+        Ns *= R;
+    }
+    p.ntab = (int)tab.size();
     return p;
 }
 
@@ -658,7 +654,12 @@ static FFTDesc to_desc(const FFTPlan1D& p)
     FFTDesc d;
     d.n = p.n;
     d.nst = p.nstages;
-    for (int i = 0; i < 16; ++i) d.radix[i] = i < p.nstages ? p.radix[i] : 1;
+    for (int i = 0; i < 12; ++i) {
+        d.radix[i] = i < p.nstages ? p.radix[i] : 1;
+        d.ns[i] = i < p.nstages ? p.ns[i] : 1;
+        d.toff[i] = i < p.nstages ? p.toff[i] : 0;
+    }
+    d.ntab = p.ntab;
     return d;
 }
 
@@ -671,7 +672,7 @@ static void make_twiddles(int n, std::vector<double2>& tw)
     }
 }
 
-// Cardinal B-spline M_n at integer points 1..n-1 (Essmann eq. 4.1 recursion).
+// Cardinal B-spline M_n (Essmann et al. eq. 4.1 recursion).
 static double cardinal_bspline(int n, double x)
 {
     if (x <= 0.0 || x >= n) return 0.0;
@@ -679,31 +680,26 @@ static double cardinal_bspline(int n, double x)
     return (x * cardinal_bspline(n - 1, x) + (n - x) * cardinal_bspline(n - 1, x - 1.0)) / (n - 1);
 }
 
-static void ref_w5_spread_host(double u, double th[5])
+// lines per block (power of two dividing FFT_THREADS) within 46 KB of shared memory
+static int lines_per_block(const FFTPlan1D& p, size_t csize)
 {
-    double c0 = 1.0 - u, c1 = u;
-    double w0 = (1.0 / 2.0) * ((1.0 - u) * c0);
-    double w1 = (1.0 / 2.0) * ((1.0 + u) * c0 + (2.0 - u) * c1);
-    double w2 = (1.0 / 2.0) * ((1.0 + u) * c1);
-    double x0 = (1.0 / 3.0) * ((1.0 - u) * w0);
-    double x1 = (1.0 / 3.0) * ((2.0 + u) * w0 + (2.0 - u) * w1);
-    double x2 = (1.0 / 3.0) * ((1.0 + u) * w1 + (3.0 - u) * w2);
-    double x3 = (1.0 / 3.0) * ((2.0 + u) * w2);
-    th[0] = (1.0 / 4.0) * ((1.0 - u) * x0);
-    th[1] = (1.0 / 4.0) * ((3.0 + u) * x0 + (2.0 - u) * x1);
-    th[2] = (1.0 / 4.0) * ((2.0 + u) * x1 + (3.0 - u) * x2);
-    th[3] = (1.0 / 4.0) * ((1.0 + u) * x2 + (4.0 - u) * x3);
-    th[4] = (1.0 / 4.0) * ((3.0 + u) * x3);
+    for (int lp = 4; lp >= 1; lp >>= 1) {
+        size_t bytes = csize * ((size_t)p.n + 2 * (size_t)lp * p.n) + sizeof(int2) * (size_t)p.ntab;
+        if (bytes <= 46 * 1024) return lp;
+    }
+    return 1;
 }
 
-static int lines_per_block(int n, size_t csize)
+static size_t fft_smem(const FFTPlan1D& p, size_t csize, int lp)
 {
-    // two ping-pong buffers + twiddles within 48 KB
-    // few lines per block: many small blocks keep every SM busy on these
-    // latency-bound, L2-resident passes
-    size_t budget = 46 * 1024;
-    int lp = (int)((budget / csize - n) / (2 * (size_t)n));
-    return std::max(1, std::min(4, lp));
+    return csize * ((size_t)p.n + 2 * (size_t)lp * p.n) + sizeof(int2) * (size_t)p.ntab;
+}
+
+static int ilog2(int v)
+{
+    int s = 0;
+    while ((1 << s) < v) ++s;
+    return s;
 }
 
 void setup_pme(Ctx& c)
@@ -717,12 +713,18 @@ void setup_pme(Ctx& c)
         }
         if (K < 5) throw ApiError(MDF_ERR_INVALID, "PME grid dimension below 5");
         c.K[d] = K;
-        c.plan[d] = make_plan(K);
+        std::vector<int2> tab;
+        c.plan[d] = make_plan(K, tab);
+        c.fft_tab[d].upload(tab.data(), tab.size(), c.stream);
+        std::vector<double> mv(K);
+        for (int k = 0; k < K; ++k) mv[k] = ((k <= K / 2) ? k : k - K) / c.box[d];
+        c.mvec[d].upload(mv.data(), K, c.stream);
     }
     c.order = ref ? 5 : (c.p.pme_order > 0 ? c.p.pme_order : 4);
     if (!ref && c.order != 4) throw ApiError(MDF_ERR_UNSUPPORTED, "PHYSICAL PME supports order 4");
-    long long ntot = (long long)c.K[0] * c.K[1] * c.K[2];
-    long long nc = (long long)c.K[0] * c.K[1] * (c.K[2] / 2 + 1);
+    const int K0 = c.K[0], K1 = c.K[1], K2 = c.K[2], Kc = K2 / 2 + 1;
+    long long ntot = (long long)K0 * K1 * K2;
+    long long nc = (long long)K0 * K1 * Kc;
     c.qgrid.alloc(ntot);
     bool mixed = c.p.precision == MDF_PREC_MIXED && !ref;
     if (mixed) {
@@ -732,9 +734,12 @@ void setup_pme(Ctx& c)
         c.cgrid_d.alloc(nc);
         c.rgrid_d.alloc(ntot);
     }
+    // per-dimension factors: PHYSICAL 1/|b(m)|^2, REFERENCE the reference's moduli
+    std::vector<double> bfac[3];
     for (int d = 0; d < 3; ++d) {
         int K = c.K[d];
-        std::vector<double> b(K);
+        std::vector<double>& b = bfac[d];
+        b.assign(K, 0.0);
         if (!ref) {
             // 1/|b(m)|^2 = |sum_{k=0}^{n-2} M_n(k+1) e^{2 pi i m k/K}|^2, zeros bridged
             for (int m = 0; m < K; ++m) {
@@ -750,9 +755,9 @@ void setup_pme(Ctx& c)
                 if (b[m] < 1e-7) b[m] = 0.5 * (b[(m - 1 + K) % K] + b[(m + 1) % K]);
             for (int m = 0; m < K; ++m) b[m] = 1.0 / b[m];
         } else {
-            // the reference's moduli: |r2c of theta5(0) at 0,1,2,-1,-2|^2 (src/System/PBC.cpp:455-490)
+            // |r2c of theta5(0) placed at 0,1,2,-1,-2|^2 (src/System/PBC.cpp:455-490)
             double th[5];
-            ref_w5_spread_host(0.0, th);
+            ref_w5_spread(0.0, th);
             std::vector<double> rd(K, 0.0);
             rd[0] = th[2]; rd[1] = th[3]; rd[2] = th[4]; rd[K - 1] = th[1]; rd[K - 2] = th[0];
             for (int i = 0; i < K / 2 + 1; ++i) {
@@ -770,18 +775,49 @@ void setup_pme(Ctx& c)
         std::vector<double2> tw;
         make_twiddles(K, tw);
         if (mixed) {
-            std::vector<float> bf(K);
             std::vector<float2> twf(K);
-            for (int i = 0; i < K; ++i) {
-                bf[i] = (float)b[i];
-                twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
-            }
-            c.bmod_f[d].upload(bf.data(), K, c.stream);
+            for (int i = 0; i < K; ++i) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
             c.tw_f[d].upload(twf.data(), K, c.stream);
         } else {
-            c.bmod[d].upload(b.data(), K, c.stream);
             c.tw_d[d].upload(tw.data(), K, c.stream);
         }
+    }
+    // influence function, laid out [ky][kz][kx] (the x pass reads lines along kx)
+    std::vector<double> infl((size_t)K1 * Kc * K0);
+    const double V = c.box[0] * c.box[1] * c.box[2];
+    for (int ky = 0; ky < K1; ++ky) {
+        const int my_i = (ky <= K1 / 2) ? ky : ky - K1;
+        for (int kz = 0; kz < Kc; ++kz)
+            for (int kx = 0; kx < K0; ++kx) {
+                const int mx_i = (kx <= K0 / 2) ? kx : kx - K0;
+                double v;
+                if (!ref) {
+                    const double mx = mx_i / c.box[0], my = my_i / c.box[1], mz = kz / c.box[2];
+                    const double m2 = mx * mx + my * my + mz * mz;
+                    if (kx == 0 && ky == 0 && kz == 0) v = 0.0;
+                    else
+                        v = c.p.coulomb_const / (M_PI * V) * std::exp(-M_PI * M_PI * m2 / (c.alpha * c.alpha)) / m2 *
+                            bfac[0][kx] * bfac[1][ky] * bfac[2][kz];
+                } else {
+                    // src/System/PBC.cpp:511-563: 4 pi / V exp(-k^2/(4 alpha^2)) / k^2 / moduli / N
+                    const double kxv = 2.0 * M_PI * mx_i / c.box[0], kyv = 2.0 * M_PI * my_i / c.box[1],
+                                 kzv = 2.0 * M_PI * kz / c.box[2];
+                    const double ksq = kxv * kxv + kyv * kyv + kzv * kzv;
+                    if (ksq < 1e-10) v = 0.0;
+                    else {
+                        const double influence = 4.0 * M_PI / V * std::exp(ksq * (-1.0 / (4.0 * c.alpha * c.alpha))) / ksq;
+                        const double b_corr = 1.0 / (bfac[0][kx] * bfac[1][ky] * bfac[2][kz]);
+                        v = influence * b_corr * (1.0 / (double)ntot);
+                    }
+                }
+                infl[((size_t)ky * Kc + kz) * K0 + kx] = v;
+            }
+    }
+    if (mixed) {
+        std::vector<float> f(infl.begin(), infl.end());
+        c.infl_f.upload(f.data(), f.size(), c.stream);
+    } else {
+        c.infl_d.upload(infl.data(), infl.size(), c.stream);
     }
     MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
 }
@@ -795,19 +831,17 @@ static void run_pme(Ctx& c, bool energy)
     C* cg;
     R* rg;
     const C *twx, *twy, *twz;
-    const R *b0, *b1, *b2;
+    const R* infl;
     if (sizeof(R) == 4) {
         cg = reinterpret_cast<C*>(c.cgrid_f.p); rg = reinterpret_cast<R*>(c.rgrid_f.p);
         twx = reinterpret_cast<const C*>(c.tw_f[0].p); twy = reinterpret_cast<const C*>(c.tw_f[1].p);
         twz = reinterpret_cast<const C*>(c.tw_f[2].p);
-        b0 = reinterpret_cast<const R*>(c.bmod_f[0].p); b1 = reinterpret_cast<const R*>(c.bmod_f[1].p);
-        b2 = reinterpret_cast<const R*>(c.bmod_f[2].p);
+        infl = reinterpret_cast<const R*>(c.infl_f.p);
     } else {
         cg = reinterpret_cast<C*>(c.cgrid_d.p); rg = reinterpret_cast<R*>(c.rgrid_d.p);
         twx = reinterpret_cast<const C*>(c.tw_d[0].p); twy = reinterpret_cast<const C*>(c.tw_d[1].p);
         twz = reinterpret_cast<const C*>(c.tw_d[2].p);
-        b0 = reinterpret_cast<const R*>(c.bmod[0].p); b1 = reinterpret_cast<const R*>(c.bmod[1].p);
-        b2 = reinterpret_cast<const R*>(c.bmod[2].p);
+        infl = reinterpret_cast<const R*>(c.infl_d.p);
     }
     GridGeom g;
     for (int d = 0; d < 3; ++d) {
@@ -825,58 +859,40 @@ static void run_pme(Ctx& c, bool energy)
         k_spread_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, g, c.qgrid.p);
     }
     mark(c, "pme_spread");
-    const int fth = 128;
+    const FFTDesc dx = to_desc(c.plan[0]), dy = to_desc(c.plan[1]), dz = to_desc(c.plan[2]);
     // z forward (real -> half complex)
-    {
-        int LP = lines_per_block(K2, sizeof(C));
-        size_t sm = sizeof(C) * ((size_t)K2 + 2 * (size_t)LP * K2);
-        int nlines = K0 * K1;
-        int nb = (nlines + 2 * LP - 1) / (2 * LP);
-        k_fft_z_r2c<R><<<nb, fth, sm, c.stream>>>(c.qgrid.p, cg, nlines, K2, to_desc(c.plan[2]), twz, LP);
-    }
+    const int LPz = lines_per_block(c.plan[2], sizeof(C));
+    const size_t smz = fft_smem(c.plan[2], sizeof(C), LPz);
+    const int nlines = K0 * K1;
+    const int nbz = (nlines + 2 * LPz - 1) / (2 * LPz);
+    k_fft_z_r2c<R><<<nbz, FFT_THREADS, smz, c.stream>>>(c.qgrid.p, cg, nlines, dz, twz, c.fft_tab[2].p, LPz);
     // y forward
-    int LPy = lines_per_block(K1, sizeof(C));
-    size_t smy = sizeof(C) * ((size_t)K1 + 2 * (size_t)LPy * K1);
-    dim3 gy((Kc + LPy - 1) / LPy, K0);
-    k_fft_y<R><<<gy, fth, smy, c.stream>>>(cg, K1, Kc, to_desc(c.plan[1]), twy, LPy, false);
+    const int LPy = lines_per_block(c.plan[1], sizeof(C));
+    const size_t smy = fft_smem(c.plan[1], sizeof(C), LPy);
+    const dim3 gy((Kc + LPy - 1) / LPy, K0);
+    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(cg, Kc, dy, twy, c.fft_tab[1].p, LPy, ilog2(LPy), false);
     // x forward + convolution + x inverse
     {
-        int LP = lines_per_block(K0, sizeof(C));
-        size_t sm = sizeof(C) * ((size_t)K0 + 2 * (size_t)LP * K0);
-        dim3 gx((Kc + LP - 1) / LP, K1);
+        const int LP = lines_per_block(c.plan[0], sizeof(C));
+        const size_t sm = fft_smem(c.plan[0], sizeof(C), LP);
+        const dim3 gx((Kc + LP - 1) / LP, K1);
         ConvParams cp;
-        for (int d = 0; d < 3; ++d) {
-            cp.K[d] = c.K[d];
-            cp.L[d] = c.box[d];
-        }
-        double V = c.box[0] * c.box[1] * c.box[2];
+        for (int d = 0; d < 3; ++d) cp.K[d] = c.K[d];
+        cp.pa2 = M_PI * M_PI / (c.alpha * c.alpha);
         cp.reference = ref ? 1 : 0;
-        if (!ref) {
-            cp.fac = c.p.coulomb_const / (M_PI * V);
-            cp.pa2 = M_PI * M_PI / (c.alpha * c.alpha);
-            cp.norm = 1.0;
-        } else {
-            cp.fac = 4.0 * M_PI / V;
-            cp.pa2 = 1.0 / (4.0 * c.alpha * c.alpha);
-            cp.norm = 1.0 / (double)ntot;
-        }
         if (energy)
-            k_fft_x_conv<R, true><<<gx, fth, sm, c.stream>>>(cg, K1, Kc, to_desc(c.plan[0]), twx, LP, cp, b0, b1, b2,
-                                                            c.acc.p, c.status.p);
+            k_fft_x_conv<R, true><<<gx, FFT_THREADS, sm, c.stream>>>(cg, K1, Kc, dx, twx, c.fft_tab[0].p, LP,
+                                                                     ilog2(LP), cp, infl, c.mvec[0].p, c.mvec[1].p,
+                                                                     c.mvec[2].p, c.acc.p, c.status.p);
         else
-            k_fft_x_conv<R, false><<<gx, fth, sm, c.stream>>>(cg, K1, Kc, to_desc(c.plan[0]), twx, LP, cp, b0, b1,
-                                                             b2, c.acc.p, c.status.p);
+            k_fft_x_conv<R, false><<<gx, FFT_THREADS, sm, c.stream>>>(cg, K1, Kc, dx, twx, c.fft_tab[0].p, LP,
+                                                                      ilog2(LP), cp, infl, c.mvec[0].p, c.mvec[1].p,
+                                                                      c.mvec[2].p, c.acc.p, c.status.p);
     }
     // y inverse
-    k_fft_y<R><<<gy, fth, smy, c.stream>>>(cg, K1, Kc, to_desc(c.plan[1]), twy, LPy, true);
+    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(cg, Kc, dy, twy, c.fft_tab[1].p, LPy, ilog2(LPy), true);
     // z inverse (half complex -> real)
-    {
-        int LP = lines_per_block(K2, sizeof(C));
-        size_t sm = sizeof(C) * ((size_t)K2 + 2 * (size_t)LP * K2);
-        int nlines = K0 * K1;
-        int nb = (nlines + 2 * LP - 1) / (2 * LP);
-        k_fft_z_c2r<R><<<nb, fth, sm, c.stream>>>(cg, rg, nlines, K2, to_desc(c.plan[2]), twz, LP);
-    }
+    k_fft_z_c2r<R><<<nbz, FFT_THREADS, smz, c.stream>>>(cg, rg, nlines, dz, twz, c.fft_tab[2].p, LPz);
     mark(c, "pme_fft_conv");
     if (!ref) {
         k_gather4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, g, rg,

@@ -224,6 +224,28 @@ int mdf_cmap_coefficients(int nsets, int res, const double *grids, double *coeff
  * FP64.  The roofline denominator of the FP32-pipe-bound pair kernel. */
 int mdf_probe_fma_tflops(int device, int precision, double *tflops);
 
+/* No counterpart in the reference.
+ *
+ * Bonded terms only (bond, Urey-Bradley, angle, dihedral, improper, CMAP) of
+ * the context's current positions, computed without any device allocation:
+ * the fixed-point force and energy accumulators live in one static device
+ * array of the library, MDF_NOALLOC_MAX_ATOMS atoms at most (3 MiB of int64
+ * plus the energy words).  A context with more atoms gets MDF_ERR_INVALID
+ * before any device work.
+ *
+ * d_forces: device array [3 * natoms] (x,y,z per atom), overwritten; may be
+ * NULL without MDF_COMPUTE_FORCES.  energies: host struct, may be NULL; the
+ * bonded entries of e[] and their sum in total are set, the rest zeroed.
+ * The call runs on the context's stream and returns after it has finished.
+ *
+ * The first call on a device looks up the static array's device address
+ * (cudaGetSymbolAddress) and keeps it; make that first call before any
+ * stream capture.  The array is shared by every context on the device, so
+ * calls that overlap in time (other threads, other streams) race and corrupt
+ * each other's results: serialise them. */
+#define MDF_NOALLOC_MAX_ATOMS 131072
+int mdf_compute_bonded_noalloc(mdf_ctx *ctx, uint32_t flags, double *d_forces, mdf_energies *energies);
+
 #ifdef __cplusplus
 }
 #endif

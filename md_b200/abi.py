@@ -13,6 +13,8 @@ E_NAMES = ["bond", "angle", "dihedral", "ub", "improper", "cmap", "vdw", "vdw14"
 E_INDEX = {n: i for i, n in enumerate(E_NAMES)}
 MDF_E_COUNT = len(E_NAMES)
 
+MDF_OK, MDF_ERR_INVALID, MDF_ERR_CUDA, MDF_ERR_CAPACITY = 0, 1, 2, 3
+MDF_NOALLOC_MAX_ATOMS = 131072   # include/mdf.h: scratch limit of mdf_compute_bonded_noalloc
 MDF_COMPUTE_ENERGY = 1
 MDF_COMPUTE_FORCES = 2
 MDF_COMPUTE_PME_REFERENCE = 4

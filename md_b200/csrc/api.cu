@@ -311,10 +311,6 @@ static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
 
 using namespace mdf;
 
-struct mdf_ctx {
-    Ctx c;
-};
-
 template <typename F>
 static int guarded(mdf_ctx* ctx, F&& f)
 {

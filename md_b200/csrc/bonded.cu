@@ -303,4 +303,32 @@ void launch_bonded(Ctx& c, bool energy)
     c.launches += 1;
 }
 
+// The same kernel with caller-supplied accumulators: f [3 * N] fixed-point
+// forces (SoA x|y|z), acc the energy words, st the status word.
+void launch_bonded_into(Ctx& c, bool energy, unsigned long long* f, unsigned long long* acc, unsigned* st)
+{
+    BondedArgs A;
+    A.n[0] = c.n_bonds; A.n[1] = c.n_ub; A.n[2] = c.n_angles; A.n[3] = c.n_dih; A.n[4] = c.n_imp; A.n[5] = c.n_cmap;
+    const int th = 256;
+    A.blk0[0] = 0;
+    for (int s = 0; s < 6; ++s) A.blk0[s + 1] = A.blk0[s] + (A.n[s] + th - 1) / th;
+    const int nblk = A.blk0[6];
+    if (nblk == 0) return;
+    A.bond_atoms = c.bond_atoms.p; A.ub_atoms = c.ub_atoms.p; A.angle_atoms = c.angle_atoms.p;
+    A.dih_atoms = c.dih_atoms.p; A.imp_atoms = c.imp_atoms.p; A.cmap_atoms = c.cmap_atoms.p;
+    A.cmap_set = c.cmap_set.p;
+    A.bond_par = c.bond_par.p; A.ub_par = c.ub_par.p; A.angle_par = c.angle_par.p; A.imp_par = c.imp_par.p;
+    A.dih_par = c.dih_par.p; A.cmap_coeff = c.cmap_coeff.p; A.cmap_res = c.cmap_res;
+    A.xyz = c.xyz.p;
+    A.N = c.N;
+    if (c.p.semantics == MDF_SEM_PHYSICAL) {
+        if (energy) k_bonded<true, true><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
+        else k_bonded<true, false><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
+    } else {
+        if (energy) k_bonded<false, true><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
+        else k_bonded<false, false><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
+    }
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+
 }  // namespace mdf

@@ -227,6 +227,7 @@ void prune_pairlist(Ctx& c);
 void launch_nonbonded(Ctx& c, bool energy);
 void launch_exclusions(Ctx& c, bool energy);
 void launch_bonded(Ctx& c, bool energy);
+void launch_bonded_into(Ctx& c, bool energy, unsigned long long* f, unsigned long long* acc, unsigned* st);
 void setup_pme(Ctx& c);
 void launch_pme(Ctx& c, bool energy);
 void launch_finalize(Ctx& c, double* d_forces, bool pme_ref);
@@ -238,3 +239,8 @@ void exclusive_scan_int(const int* d_in, int* d_out, int n, int* d_total_out, cu
 int grid_blocks(long long n, int threads);
 
 }  // namespace mdf
+
+// The opaque handle of the C ABI.
+struct mdf_ctx {
+    mdf::Ctx c;
+};

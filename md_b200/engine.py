@@ -21,7 +21,7 @@ EXPORTS = [
     "mdf_set_positions", "mdf_set_positions_device", "mdf_set_box", "mdf_build_pairlist", "mdf_compute",
     "mdf_compute_async", "mdf_fetch", "mdf_forces_device", "mdf_get_pme_forces", "mdf_set_stream",
     "mdf_pairlist_info", "mdf_enable_timing", "mdf_kernel_times", "mdf_cmap_coefficients",
-    "mdf_kernel_launches", "mdf_probe_fma_tflops",
+    "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_compute_bonded_noalloc",
 ]
 
 
@@ -68,6 +68,7 @@ def library(path=None):
     lib.mdf_kernel_launches.argtypes = [C.c_void_p]
     lib.mdf_kernel_launches.restype = C.c_int64
     lib.mdf_probe_fma_tflops.argtypes = [C.c_int, C.c_int, dp]
+    lib.mdf_compute_bonded_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(abi.mdf_energies)]
     _LIB = lib
     return lib
 
@@ -201,6 +202,15 @@ class Engine:
 
     def forces_device(self, ptr):
         self._check(self.lib.mdf_forces_device(self.h, C.c_void_p(ptr)), "forces_device")
+
+    def bonded_noalloc(self, forces_ptr, energy=True):
+        """Bonded terms only, with the library's static scratch (no device
+        allocation); forces_ptr is a device array [3 natoms] or 0."""
+        e = abi.mdf_energies()
+        flags = (abi.MDF_COMPUTE_ENERGY if energy else 0) | (abi.MDF_COMPUTE_FORCES if forces_ptr else 0)
+        self._check(self.lib.mdf_compute_bonded_noalloc(self.h, flags, C.c_void_p(forces_ptr or None), C.byref(e)),
+                    "compute_bonded_noalloc")
+        return e.as_dict() if energy else None
 
     def pme_forces(self):
         f = np.zeros((self.natoms, 3))

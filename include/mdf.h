@@ -201,8 +201,9 @@ int mdf_get_pme_forces(mdf_ctx *ctx, double *forces_out);
 int mdf_set_stream(mdf_ctx *ctx, void *stream);
 
 /* Sizes of the current pairlist: clusters, cluster pairs of the outer list,
- * cluster pairs kept by the last prune, and atom pairs within the cutoff that
- * the last evaluation computed (-1 where unknown).  Any pointer may be NULL. */
+ * cluster pairs kept by the last prune, and atom pairs within the cutoff as
+ * counted by the first evaluation after the last pairlist build (-1 where
+ * unknown).  Any pointer may be NULL. */
 int mdf_pairlist_info(mdf_ctx *ctx, int64_t *n_clusters, int64_t *n_cluster_pairs,
                       int64_t *n_cluster_pairs_pruned, int64_t *n_pairs_in_cutoff);
 

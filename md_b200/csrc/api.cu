@@ -52,13 +52,19 @@ __global__ void k_finalize(int N, int nslots, unsigned long long* __restrict__ f
         scal[a] = 0ull;
     }
     if (a >= N) return;
-    int s = atom_slot[a];
+    const int s = atom_slot[a];
+    // all loads before any store, so the six loads are in flight together
+    long long v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        v[k] = (long long)fatom[(long long)k * N + a] + (long long)fslot[(long long)k * nslots + s];
+#pragma unroll
     for (int k = 0; k < 3; ++k) {
-        long long v = (long long)fatom[(long long)k * N + a] + (long long)fslot[(long long)k * nslots + s];
         fatom[(long long)k * N + a] = 0ull;
         fslot[(long long)k * nslots + s] = 0ull;
-        out[3 * a + k] = (double)v * FORCE_ISCALE;
     }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[3 * a + k] = (double)v[k] * FORCE_ISCALE;
 }
 
 void launch_finalize(Ctx& c, double* d_forces, bool)
@@ -442,7 +448,7 @@ void mdf_destroy(mdf_ctx* ctx)
     c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
     c.ilist.release(); c.icount.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
     c.plist_in.release(); c.ilist_in.release(); c.n_in.release(); c.cur_lo.release(); c.cur_hi.release();
-    c.f_atom.release(); c.scal.release(); c.forces_out.release(); c.forces_pme_ref.release();
+    c.f_atom.release(); c.scal.release(); c.npairs_dev.release(); c.forces_out.release(); c.forces_pme_ref.release();
     c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
     c.rgrid_d.release(); c.infl_f.release(); c.infl_d.release();
     for (int d = 0; d < 3; ++d) {
@@ -592,9 +598,13 @@ int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pair
             *n_cluster_pairs_pruned = ok ? (int64_t)v : -1;
         }
         if (n_pairs_in_cutoff) {
-            // from the host copy of the last evaluation's scalar block
-            MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
-            *n_pairs_in_cutoff = (c.have_list && c.pending) ? (int64_t)c.h_scal[NUM_ACC] : -1;
+            unsigned long long v = 0;
+            const bool ok = c.have_list && c.counted;
+            if (ok) {
+                MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+                MDF_CUDA_TRY(cudaMemcpy(&v, c.npairs_dev.p, sizeof(v), cudaMemcpyDeviceToHost));
+            }
+            *n_pairs_in_cutoff = ok ? (int64_t)v : -1;
         }
     });
 }

@@ -180,7 +180,10 @@ struct Ctx {
     DevBuf<unsigned long long> f_atom;   // [3 * N]
     DevBuf<unsigned long long> scal;     // [NUM_SCAL]: energies + virial | pairs in cutoff | status
     DevView<unsigned long long> acc;     // = scal[0 .. NUM_ACC)
-    DevView<unsigned long long> npairs_cut;  // = scal[NUM_ACC]
+    DevView<unsigned long long> npairs_cut;  // = scal[NUM_ACC] (unused word)
+    DevBuf<unsigned long long> npairs_dev;   // [1] atom pairs within the cutoff (first evaluation after a build)
+    bool count_next = false;             // the next evaluation counts them
+    bool counted = false;                // npairs_dev holds a count for the current list
     DevView<unsigned> status;            // = (unsigned*)&scal[NUM_ACC + 1]
     DevBuf<double> forces_out;           // [3N]
     DevBuf<double> forces_pme_ref;       // [3N]

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
     const typename V4<R>::type* __restrict__ xq, const int* __restrict__ stype, const double4* __restrict__ center,
     const typename V2<R>::type* __restrict__ ljAB, const int* __restrict__ ljvalid, NBParams P,
     unsigned long long* __restrict__ fslot, int nslots, unsigned long long* __restrict__ acc,
-    unsigned long long* __restrict__ npairs, unsigned* st)
+    unsigned long long* __restrict__ npairs, int count, unsigned* st)
 {
     using V4t = typename V4<R>::type;
     using V2t = typename V2<R>::type;
@@ -160,8 +160,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
                         if (ENERGY) {
                             el_e += U;
                             ed_e += ec;
-                            ++npc;
                         }
+                        ++npc;
                     } else {
                         // REFERENCE formulas, operation for operation
                         const double r2d = (double)r2, r = sqrt(r2d);
@@ -202,8 +202,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
                                 e_pl += ecoul;
                                 e_cut += (qq * P.kc) * (1.0 / r - 1.0 / P.rc);
                                 e_dir += (qq / r) * erfc(P.alpha * r) * P.kc;
-                                ++npc;
                             }
+                            ++npc;
                         }
                     }
                     fix += g * dx; fiy += g * dy; fiz += g * dz;
@@ -245,6 +245,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
             const int idx[5] = {MDF_E_VDW, MDF_E_EE, MDF_E_EE_PAIRLIST, MDF_E_EE_CUTOFF, MDF_E_EE_DIRECT};
             block_acc_fixed<5>(v, acc, idx, ENERGY_SCALE, st);
         }
+    }
+    if (count) {
         long long np = warp_sum_ll((long long)npc);
         if (lane == 0 && np) atomicAdd(npairs, (unsigned long long)np);
     }
@@ -265,7 +267,7 @@ struct ShiftTable {
 //    bit t;
 //  * the pair arithmetic is branch-free (inactive pairs are selected out);
 //  * energies are summed in FP32 per entry and in FP64 across entries.
-template <bool ENERGY, bool SWITCH>
+template <bool ENERGY, bool SWITCH, bool COUNT>
 __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
     int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
     const int* __restrict__ stype, const float4* __restrict__ centerf, const float2* __restrict__ ljAB, NBParams P,
@@ -351,8 +353,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
                 if (ENERGY) {
                     el += on ? U : 0.f;
                     ed += on ? ec : 0.f;
-                    npc += on ? 1 : 0;
                 }
+                if (COUNT) npc += on ? 1 : 0;
                 fix += g * dx; fiy += g * dy; fiz += g * dz;
                 fjx -= g * dx; fjy -= g * dy; fjz -= g * dz;
                 fjx = __shfl_sync(FULL, fjx, rot_src);
@@ -385,6 +387,8 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
         const double v[2] = {e_lj, e_dir};
         const int idx[2] = {MDF_E_VDW, MDF_E_EE_DIRECT};
         block_acc_fixed<2>(v, acc, idx, ENERGY_SCALE, st);
+    }
+    if (COUNT) {
         long long np = warp_sum_ll((long long)npc);
         if (lane == 0 && np) atomicAdd(npairs, (unsigned long long)np);
     }
@@ -537,6 +541,17 @@ static NBParams make_params(const Ctx& c)
     return P;
 }
 
+// Atom pairs within the cutoff are counted by the first evaluation after a
+// pairlist build only (the count costs instructions in the pair loop).
+static bool begin_pair_count(Ctx& c)
+{
+    if (!c.count_next) return false;
+    MDF_CUDA_TRY(cudaMemsetAsync(c.npairs_dev.p, 0, sizeof(unsigned long long), c.stream));
+    c.count_next = false;
+    c.counted = true;
+    return true;
+}
+
 template <typename R, int SEM>
 static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, const typename V2<R>::type* lj)
 {
@@ -545,14 +560,15 @@ static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, 
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
     const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
+    const int count = begin_pair_count(c) ? 1 : 0;
     if (energy)
         k_pairs<R, SEM, true><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
                                                                lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
-                                                               c.npairs_cut.p, c.status.p);
+                                                               c.npairs_dev.p, count, c.status.p);
     else
         k_pairs<R, SEM, false><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
                                                                 lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
-                                                                c.npairs_cut.p, c.status.p);
+                                                                c.npairs_dev.p, count, c.status.p);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
 }
@@ -580,15 +596,19 @@ static void launch_pairs_f32(Ctx& c, bool energy)
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
     const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
-#define MDF_PF32(E, S)                                                                                           \
-    k_pairs_f32<E, S><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p, c.centerf.p, \
-                                                       c.ljAB_f.p, P, sh, c.f_slot.p, c.n_slots, c.acc.p,         \
-                                                       c.npairs_cut.p, c.status.p)
+    const bool count = begin_pair_count(c);
+#define MDF_PF32(E, S, K)                                                                                           \
+    k_pairs_f32<E, S, K><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p,            \
+                                                          c.centerf.p, c.ljAB_f.p, P, sh, c.f_slot.p, c.n_slots,   \
+                                                          c.acc.p, c.npairs_dev.p, c.status.p)
+#define MDF_PF32_K(E, S) \
+    do { if (count) MDF_PF32(E, S, true); else MDF_PF32(E, S, false); } while (0)
     if (energy) {
-        if (P.use_switch) MDF_PF32(true, true); else MDF_PF32(true, false);
+        if (P.use_switch) MDF_PF32_K(true, true); else MDF_PF32_K(true, false);
     } else {
-        if (P.use_switch) MDF_PF32(false, true); else MDF_PF32(false, false);
+        if (P.use_switch) MDF_PF32_K(false, true); else MDF_PF32_K(false, false);
     }
+#undef MDF_PF32_K
 #undef MDF_PF32
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;

@@ -429,14 +429,25 @@ struct PruneShifts {
     float v[27][6];
 };
 
+// Dynamic pruning: keep the outer-list entries that have at least one atom
+// pair within the prune radius at the current positions.  Warp per i cluster.
+// The warp loads 32 entries at once (one per lane), drops those whose current
+// cluster boxes are farther apart than the radius, and checks the remaining
+// candidates four at a time with lane = (candidate, j atom): each lane tests
+// its j atom against the eight i atoms held in registers, and one ballot gives
+// the four keep flags.  The test ignores the entry's exclusion mask (an entry
+// whose only close pairs are excluded is kept; the pair kernel applies the
+// mask), so it keeps a superset of the exact set.  Distances use
+// |a - b|^2 = |a|^2 + |b|^2 - 2 a.b: three FMAs and a min per pair, the
+// rounding (~1e-4 A^2 at these magnitudes) far inside the radius' margin.
+// Kept entries are written in order, packed from the i cluster's start offset
+// in the outer list.
 template <typename R>
-__global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restrict__ ilist,
-                                               const PairEntry* __restrict__ plist,
-                                               const typename V4<R>::type* __restrict__ xq,
-                                               const float4* __restrict__ centerf, const float4* __restrict__ cur_lo,
-                                               const float4* __restrict__ cur_hi, PruneShifts shifts, float rcut2,
-                                               ILRange* __restrict__ ilist_in, PairEntry* __restrict__ plist_in,
-                                               unsigned long long* __restrict__ n_in)
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
+    int ncl, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist,
+    const typename V4<R>::type* __restrict__ xq, const float4* __restrict__ centerf,
+    const float4* __restrict__ cur_lo, const float4* __restrict__ cur_hi, PruneShifts shifts, float rcut2,
+    ILRange* __restrict__ ilist_in, PairEntry* __restrict__ plist_in, unsigned long long* __restrict__ n_in)
 {
     using V4t = typename V4<R>::type;
     __shared__ float sh[27][6];
@@ -445,54 +456,65 @@ __global__ void __launch_bounds__(256) k_prune(int ncl, const ILRange* __restric
     const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (I >= ncl) return;
+    const int slot = lane >> 3, jj = lane & 7;
+    const unsigned below = (1u << lane) - 1u;
     const ILRange L = ilist[I];
-    R xi[CLUSTER], yi[CLUSTER], zi[CLUSTER];
+    R ax[CLUSTER], ay[CLUSTER], az[CLUSTER], an[CLUSTER];   // -2 x_i and |x_i|^2
 #pragma unroll
     for (int k = 0; k < CLUSTER; ++k) {
         const V4t v = xq[I * CLUSTER + k];
-        xi[k] = v.x; yi[k] = v.y; zi[k] = v.z;
+        ax[k] = (R)-2 * v.x; ay[k] = (R)-2 * v.y; az[k] = (R)-2 * v.z;
+        an[k] = v.x * v.x + v.y * v.y + v.z * v.z;
     }
     const float4 cI = centerf[I], ilo = cur_lo[I], ihi = cur_hi[I];
+    const R rc2 = (R)rcut2;
     int kept = 0;
     for (int base = 0; base < L.count; base += 32) {
-        const int e = base + lane;
-        bool keep = false;
-        PairEntry pe;
-        pe.j = I; pe.shift = 13; pe.mask = 0ull;
-        if (e < L.count) {
-            pe = plist[L.start + e];
-            const float4 cJ = centerf[pe.j], jlo = cur_lo[pe.j], jhi = cur_hi[pe.j];
-            const float* s6 = sh[pe.shift];
-            // J's frame origin seen from I's frame
-            const float ox = -(((cI.x - cJ.x) - s6[0]) - s6[3]);
-            const float oy = -(((cI.y - cJ.y) - s6[1]) - s6[4]);
-            const float oz = -(((cI.z - cJ.z) - s6[2]) - s6[5]);
-            const float gx = fmaxf(0.f, fmaxf(jlo.x + ox - ihi.x, ilo.x - (jhi.x + ox)));
-            const float gy = fmaxf(0.f, fmaxf(jlo.y + oy - ihi.y, ilo.y - (jhi.y + oy)));
-            const float gz = fmaxf(0.f, fmaxf(jlo.z + oz - ihi.z, ilo.z - (jhi.z + oz)));
-            if (gx * gx + gy * gy + gz * gz < rcut2) {
-                V4t vj[CLUSTER];
+        const bool have = base + lane < L.count;
+        PairEntry my;
+        my.j = I; my.shift = 13; my.mask = 0ull;
+        if (have) my = plist[L.start + base + lane];
+        // this lane's entry: J's frame origin seen from I's frame, and the box test
+        const float4 cJ = centerf[my.j], jlo = cur_lo[my.j], jhi = cur_hi[my.j];
+        const float* s6 = sh[my.shift];
+        const float ox = -(((cI.x - cJ.x) - s6[0]) - s6[3]);
+        const float oy = -(((cI.y - cJ.y) - s6[1]) - s6[4]);
+        const float oz = -(((cI.z - cJ.z) - s6[2]) - s6[5]);
+        const float gx = fmaxf(0.f, fmaxf(jlo.x + ox - ihi.x, ilo.x - (jhi.x + ox)));
+        const float gy = fmaxf(0.f, fmaxf(jlo.y + oy - ihi.y, ilo.y - (jhi.y + oy)));
+        const float gz = fmaxf(0.f, fmaxf(jlo.z + oz - ihi.z, ilo.z - (jhi.z + oz)));
+        const bool cand = have && my.mask != 0ull && gx * gx + gy * gy + gz * gz < rcut2;
+        unsigned todo = __ballot_sync(0xffffffffu, cand);
+        unsigned keepmask = 0u;
+        while (todo) {
+            // this lane's candidate: the (slot+1)-th lowest pending entry
+            unsigned x = todo;
+            if (slot >= 1) x &= x - 1u;
+            if (slot >= 2) x &= x - 1u;
+            if (slot >= 3) x &= x - 1u;
+            const bool valid = x != 0u;
+            const int s = valid ? __ffs(x) - 1 : 0;
+            const int j = __shfl_sync(0xffffffffu, my.j, s);
+            const R px = (R)__shfl_sync(0xffffffffu, ox, s), py = (R)__shfl_sync(0xffffffffu, oy, s),
+                    pz = (R)__shfl_sync(0xffffffffu, oz, s);
+            const V4t vj = xq[j * CLUSTER + jj];
+            const R qx = vj.x + px, qy = vj.y + py, qz = vj.z + pz;
+            const R thr = rc2 - (qx * qx + qy * qy + qz * qz);
+            R m = fma(ax[0], qx, fma(ay[0], qy, fma(az[0], qz, an[0])));
 #pragma unroll
-                for (int jj = 0; jj < CLUSTER; ++jj) vj[jj] = xq[pe.j * CLUSTER + jj];
-                const unsigned long long m = pe.mask;
-                for (int jj = 0; jj < CLUSTER && !keep; ++jj) {
-                    const float px = (float)vj[jj].x + ox, py = (float)vj[jj].y + oy, pz = (float)vj[jj].z + oz;
-                    const float bx = fmaxf(0.f, fmaxf(ilo.x - px, px - ihi.x));
-                    const float by = fmaxf(0.f, fmaxf(ilo.y - py, py - ihi.y));
-                    const float bz = fmaxf(0.f, fmaxf(ilo.z - pz, pz - ihi.z));
-                    if (bx * bx + by * by + bz * bz >= rcut2) continue;
-                    const R qx = vj[jj].x + (R)ox, qy = vj[jj].y + (R)oy, qz = vj[jj].z + (R)oz;
-#pragma unroll
-                    for (int ii = 0; ii < CLUSTER; ++ii) {
-                        const R dx = xi[ii] - qx, dy = yi[ii] - qy, dz = zi[ii] - qz;
-                        keep |= ((m >> (ii * 8 + jj)) & 1ull) && (dx * dx + dy * dy + dz * dz < (R)rcut2);
-                    }
-                }
-            }
+            for (int ii = 1; ii < CLUSTER; ++ii) m = fmin(m, fma(ax[ii], qx, fma(ay[ii], qy, fma(az[ii], qz, an[ii]))));
+            const unsigned b = __ballot_sync(0xffffffffu, valid && m < thr);
+            // lane L's own entry, if pending and among the four: its rank is its slot
+            const unsigned rank = __popc(todo & below);
+            if (((todo >> lane) & 1u) && rank < 4u && ((b >> (8u * rank)) & 0xffu)) keepmask |= 1u << lane;
+            todo &= todo - 1u;
+            todo &= todo - 1u;
+            todo &= todo - 1u;
+            todo &= todo - 1u;
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, keep);
-        if (keep) plist_in[L.start + kept + __popc(bal & ((1u << lane) - 1u))] = pe;
-        kept += __popc(bal);
+        keepmask = __ballot_sync(0xffffffffu, (keepmask >> lane) & 1u);
+        if ((keepmask >> lane) & 1u) plist_in[L.start + kept + __popc(keepmask & below)] = my;
+        kept += __popc(keepmask);
     }
     if (lane == 0) {
         ILRange r;
@@ -557,6 +579,9 @@ void pack_positions(Ctx& c)
 
 void build_pairlist(Ctx& c)
 {
+    c.npairs_dev.alloc(1);
+    c.count_next = true;
+    c.counted = false;
     cudaStream_t s = c.stream;
     const int th = 256;
     double rlist = c.p.cutoff + c.p.skin;

@@ -230,6 +230,27 @@ static void eval_async_impl(Ctx& c, uint32_t flags)
         MDF_CUDA_TRY(cudaMemsetAsync(c.scal.p, 0, sizeof(unsigned long long) * NUM_SCAL, s));
         c.need_clear = false;
     }
+    // The PME chain only reads positions and charges and adds into the
+    // fixed-point accumulators, so it runs on the side stream while the main
+    // stream packs, prunes and runs the pair, exclusion and bonded kernels; the
+    // main stream waits for it before k_finalize.  With timing enabled every
+    // kernel runs on the main stream so the per-phase times are separable.
+    const bool want_pme = phys || (flags & MDF_COMPUTE_PME_REFERENCE);
+    const bool overlap = want_pme && !c.timing;
+    if (overlap) {
+        MDF_CUDA_TRY(cudaEventRecord(c.ev_fork, s));
+        MDF_CUDA_TRY(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+        c.stream = c.side;
+        try {
+            launch_pme(c, energy);
+        } catch (...) {
+            c.stream = s;
+            throw;
+        }
+        c.stream = s;
+        c.have_pme_ref = !phys;
+        MDF_CUDA_TRY(cudaEventRecord(c.ev_join, c.side));
+    }
     pack_positions(c);
     mark(c, "pack");
     if (c.p.prune_every > 0) {
@@ -246,10 +267,11 @@ static void eval_async_impl(Ctx& c, uint32_t flags)
     mark(c, "excl_14");
     launch_bonded(c, energy);
     mark(c, "bonded");
-    if (phys || (flags & MDF_COMPUTE_PME_REFERENCE)) {
+    if (want_pme && !overlap) {
         launch_pme(c, energy);
         c.have_pme_ref = !phys;
     }
+    if (overlap) MDF_CUDA_TRY(cudaStreamWaitEvent(s, c.ev_join, 0));
     launch_finalize(c, c.forces_out.p, false);
     mark(c, "finalize");
     c.pending = true;
@@ -411,6 +433,9 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         MDF_CUDA_TRY(cudaSetDevice(c.device));
         MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
+        MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+        MDF_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
+        MDF_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
         MDF_CUDA_TRY(cudaHostAlloc((void**)&c.h_scal, sizeof(unsigned long long) * NUM_SCAL, cudaHostAllocMapped));
         memset(c.h_scal, 0, sizeof(unsigned long long) * NUM_SCAL);
         MDF_CUDA_TRY(cudaHostGetDevicePointer((void**)&c.d_hscal, c.h_scal, 0));
@@ -456,6 +481,9 @@ void mdf_destroy(mdf_ctx* ctx)
     }
     if (c.h_scal) cudaFreeHost(c.h_scal);
     if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
+    if (c.side) cudaStreamDestroy(c.side);
+    if (c.ev_fork) cudaEventDestroy(c.ev_fork);
+    if (c.ev_join) cudaEventDestroy(c.ev_join);
     delete ctx;
 }
 

@@ -110,6 +110,8 @@ struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side = nullptr;         // the PME chain runs here, concurrently with the pair kernel
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     mdf_params p{};
     int N = 0;
     int ntypes = 0;

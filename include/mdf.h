@@ -225,6 +225,22 @@ int mdf_cmap_coefficients(int nsets, int res, const double *grids, double *coeff
  * FP64.  The roofline denominator of the FP32-pipe-bound pair kernel. */
 int mdf_probe_fma_tflops(int device, int precision, double *tflops);
 
+/* Replace the per-atom charges (internal unit, [natoms]) and/or the LJ A/B
+ * coefficients ([n_ljpair], indexed by NONBONDED_PARM_INDEX - 1) of the
+ * context; NULL keeps the current values (lj_a and lj_b go together).  The
+ * 1-4 coefficients are kept.  Positions and the pairlist are unchanged. */
+int mdf_set_parameters(mdf_ctx *ctx, const double *charge, const double *lj_a, const double *lj_b);
+
+/* Backward (vector-Jacobian product) of one PHYSICAL evaluation at the
+ * current positions: for a loss L(F, E) with dL_dF = dL/dF ([3N], forces as
+ * mdf_compute returns them; NULL = 0) and dL_dE = dL/dE (total energy),
+ * writes dL/dq ([natoms]), dL/dA and dL/dB ([n_ljpair], the main LJ table per
+ * NONBONDED_PARM_INDEX - 1 entry).  Any output may be NULL.  The pair kernel is
+ * recomputed; nothing from the forward evaluation is needed.  Positions and
+ * bonded terms are constants here.  REFERENCE semantics return
+ * MDF_ERR_UNSUPPORTED (their forces are not the gradient of their energy). */
+int mdf_backward(mdf_ctx *ctx, const double *dL_dF, double dL_dE, double *dL_dq, double *dL_dA, double *dL_dB);
+
 /* No counterpart in the reference.
  *
  * Bonded terms only (bond, Urey-Bradley, angle, dihedral, improper, CMAP) of

@@ -81,6 +81,48 @@ static void check_index(const int32_t* a, long long n, int N, const char* what)
         if (a[i] < 0 || a[i] >= N) throw ApiError(MDF_ERR_INVALID, std::string("atom index out of range in ") + what);
 }
 
+// Pair tables over (ntypes + 1)^2, the extra type being cluster padding, from
+// the LJ coefficients per NONBONDED_PARM_INDEX entry; also the table mapping a
+// type pair to its 0-based entry (-1: no LJ).
+void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b)
+{
+    cudaStream_t s = c.stream;
+    const int ntp = c.ntp;
+    std::vector<double2> ab(ntp * ntp, make_double2(0, 0)), ab14(ntp * ntp, make_double2(0, 0));
+    std::vector<float2> abf(ntp * ntp, make_float2(0, 0));
+    std::vector<int> valid(ntp * ntp, 0), idx(ntp * ntp, -1);
+    for (int i = 0; i < c.ntypes; ++i)
+        for (int j = 0; j < c.ntypes; ++j) {
+            const int nb = c.h_nb_index[i * c.ntypes + j];
+            if (nb == 0) continue;
+            const int tp = i * ntp + j;
+            ab[tp] = make_double2(lj_a[nb - 1], lj_b[nb - 1]);
+            abf[tp] = make_float2((float)lj_a[nb - 1], (float)lj_b[nb - 1]);
+            ab14[tp] = make_double2(c.h_lj14a[nb - 1], c.h_lj14b[nb - 1]);
+            valid[tp] = 1;
+            idx[tp] = nb - 1;
+        }
+    c.ljAB.upload(ab.data(), ab.size(), s);
+    c.ljAB_f.upload(abf.data(), abf.size(), s);
+    c.lj14AB.upload(ab14.data(), ab14.size(), s);
+    c.ljvalid.upload(valid.data(), valid.size(), s);
+    c.nbidx.upload(idx.data(), idx.size(), s);
+    MDF_CUDA_TRY(cudaStreamSynchronize(s));
+}
+
+// Charge-dependent constants: self energy -k alpha / sqrt(pi) sum q^2
+// (src/System/NonBondedEnergy.cpp:307-316) and the net charge.
+void set_charge_constants(Ctx& c, const double* charge)
+{
+    long double q2 = 0, qt = 0;
+    for (int i = 0; i < c.N; ++i) {
+        q2 += (long double)charge[i] * charge[i];
+        qt += charge[i];
+    }
+    c.e_self = (double)(-(long double)c.p.coulomb_const * (c.alpha / std::sqrt(M_PI)) * q2);
+    c.q_total = (double)qt;
+}
+
 void upload_topology(Ctx& c, const mdf_topology* t)
 {
     cudaStream_t s = c.stream;
@@ -92,28 +134,23 @@ void upload_topology(Ctx& c, const mdf_topology* t)
     c.ntp = t->ntypes + 1;
     for (int i = 0; i < c.N; ++i)
         if (t->type[i] < 0 || t->type[i] >= t->ntypes) throw ApiError(MDF_ERR_INVALID, "atom type out of range");
-    // pair tables over (ntypes + 1)^2, the extra type being cluster padding
-    std::vector<double2> ab(c.ntp * c.ntp, make_double2(0, 0)), ab14(c.ntp * c.ntp, make_double2(0, 0));
-    std::vector<float2> abf(c.ntp * c.ntp, make_float2(0, 0));
-    std::vector<int> valid(c.ntp * c.ntp, 0);
+    c.n_ljpair = t->n_ljpair;
+    c.h_nb_index.assign(t->nb_index, t->nb_index + (size_t)c.ntypes * c.ntypes);
     for (int i = 0; i < c.ntypes; ++i)
         for (int j = 0; j < c.ntypes; ++j) {
             int nb = t->nb_index[i * c.ntypes + j];
             if (nb != t->nb_index[j * c.ntypes + i])
                 throw ApiError(MDF_ERR_UNSUPPORTED, "NONBONDED_PARM_INDEX is not symmetric");
             if (nb < 0 || nb > t->n_ljpair) throw ApiError(MDF_ERR_INVALID, "NONBONDED_PARM_INDEX out of range");
-            if (nb == 0) continue;
-            int tp = i * c.ntp + j;
-            ab[tp] = make_double2(t->lj_a[nb - 1], t->lj_b[nb - 1]);
-            abf[tp] = make_float2((float)t->lj_a[nb - 1], (float)t->lj_b[nb - 1]);
-            if (t->lj14_a && t->lj14_b) ab14[tp] = make_double2(t->lj14_a[nb - 1], t->lj14_b[nb - 1]);
-            else ab14[tp] = ab[tp];
-            valid[tp] = 1;
         }
-    c.ljAB.upload(ab.data(), ab.size(), s);
-    c.ljAB_f.upload(abf.data(), abf.size(), s);
-    c.lj14AB.upload(ab14.data(), ab14.size(), s);
-    c.ljvalid.upload(valid.data(), valid.size(), s);
+    if (t->lj14_a && t->lj14_b) {
+        c.h_lj14a.assign(t->lj14_a, t->lj14_a + c.n_ljpair);
+        c.h_lj14b.assign(t->lj14_b, t->lj14_b + c.n_ljpair);
+    } else {
+        c.h_lj14a.assign(t->lj_a, t->lj_a + c.n_ljpair);
+        c.h_lj14b.assign(t->lj_b, t->lj_b + c.n_ljpair);
+    }
+    set_lj_tables(c, t->lj_a, t->lj_b);
     c.q.upload(t->charge, c.N, s);
     c.type.upload(t->type, c.N, s);
 
@@ -194,14 +231,7 @@ void upload_topology(Ctx& c, const mdf_topology* t)
         c.p14_scale.upload(sc.data(), sc.size(), s);
     }
 
-    // constant self energy: -k alpha / sqrt(pi) sum q^2 (src/System/NonBondedEnergy.cpp:307-316)
-    long double q2 = 0, qt = 0;
-    for (int i = 0; i < c.N; ++i) {
-        q2 += (long double)t->charge[i] * t->charge[i];
-        qt += t->charge[i];
-    }
-    c.e_self = (double)(-(long double)c.p.coulomb_const * (c.alpha / std::sqrt(M_PI)) * q2);
-    c.q_total = (double)qt;
+    set_charge_constants(c, t->charge);
 
     c.xyz.alloc(3 * (size_t)c.N);
     c.f_atom.alloc(3 * (size_t)c.N);
@@ -634,6 +664,40 @@ int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pair
             }
             *n_pairs_in_cutoff = ok ? (int64_t)v : -1;
         }
+    });
+}
+
+int mdf_set_parameters(mdf_ctx* ctx, const double* charge, const double* lj_a, const double* lj_b)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        if ((lj_a == nullptr) != (lj_b == nullptr)) throw ApiError(MDF_ERR_INVALID, "give both lj_a and lj_b or neither");
+        if (charge) {
+            for (int i = 0; i < c.N; ++i)
+                if (!std::isfinite(charge[i])) throw ApiError(MDF_ERR_INVALID, "non-finite charge");
+            c.q.upload(charge, c.N, c.stream);
+            set_charge_constants(c, charge);
+        }
+        if (lj_a) {
+            for (int k = 0; k < c.n_ljpair; ++k)
+                if (!std::isfinite(lj_a[k]) || !std::isfinite(lj_b[k]))
+                    throw ApiError(MDF_ERR_INVALID, "non-finite LJ coefficient");
+            set_lj_tables(c, lj_a, lj_b);
+        }
+        MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    });
+}
+
+int mdf_backward(mdf_ctx* ctx, const double* dL_dF, double dL_dE, double* dL_dq, double* dL_dA, double* dL_dB)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        backward(c, dL_dF, dL_dE, dL_dq, dL_dA, dL_dB);
     });
 }
 

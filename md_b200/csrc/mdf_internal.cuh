@@ -125,6 +125,10 @@ struct Ctx {
     DevBuf<double2> lj14AB;    // same indexing, 1-4 tables
     DevBuf<int> ljvalid;       // [(ntypes+1)^2] nb != 0
     int ntp = 0;               // ntypes + 1 (padding type appended)
+    int n_ljpair = 0;
+    std::vector<int> h_nb_index;         // [ntypes^2] NONBONDED_PARM_INDEX (host copy)
+    std::vector<double> h_lj14a, h_lj14b;  // [n_ljpair] 1-4 coefficients (host copy)
+    DevBuf<int> nbidx;                   // [(ntypes+1)^2] 0-based LJ entry of a type pair, -1 = none
 
     int n_bonds = 0, n_ub = 0, n_angles = 0, n_dih = 0, n_imp = 0, n_cmap = 0;
     DevBuf<int> bond_atoms, ub_atoms, angle_atoms, dih_atoms, imp_atoms, cmap_atoms, cmap_set;
@@ -211,6 +215,14 @@ struct Ctx {
     DevBuf<double> mvec[3];              // m_d = signed frequency / L_d per grid index
     bool have_pme_ref = false;           // forces_pme_ref holds the reference chain's forces
 
+    // adjoint (mdf_backward)
+    DevBuf<double> adj_v;                // [3N] dL/dF, atom order, normalised
+    DevBuf<float4> adj_vs_f;             // [n_slots] the same per slot (mixed)
+    DevBuf<double4> adj_vs_d;            // [n_slots] (FP64)
+    DevBuf<unsigned long long> adj_dq_slot, adj_dq_atom;   // fixed-point dL/dq
+    DevBuf<double> adj_dab;              // [2 n_ljpair] dL/dA | dL/dB
+    DevBuf<double> adj_dq;               // [N] dL/dq out
+
     // timing
     bool timing = false;
     std::vector<cudaEvent_t> evpool;          // reused timing events
@@ -226,6 +238,10 @@ struct Ctx {
 
 // ------------------------------------------------------ launch helpers (.cu)
 void upload_topology(Ctx& c, const mdf_topology* t);
+void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b);
+void set_charge_constants(Ctx& c, const double* charge);
+void backward(Ctx& c, const double* dL_dF, double dL_dE, double* dL_dq, double* dL_dA, double* dL_dB);
+void pme_adjoint(Ctx& c, double gE, double vscale);
 void build_pairlist(Ctx& c);
 void pack_positions(Ctx& c);
 void prune_pairlist(Ctx& c);

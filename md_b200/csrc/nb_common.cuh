@@ -1,0 +1,40 @@
+// Definitions shared by the pair kernel (nonbonded.cu) and its adjoint
+// (adjoint.cu).
+#pragma once
+
+#include "mdf_internal.cuh"
+
+namespace mdf {
+
+constexpr int NB_WARPS = 8;
+constexpr int NB_THREADS = NB_WARPS * 32;
+
+template <typename R> struct V2;
+template <> struct V2<float> { using type = float2; };
+template <> struct V2<double> { using type = double2; };
+
+struct NBParams {
+    double box[3];
+    double rc, rc2, rsw, inv_sw, kc, alpha, rlist2;
+    int use_switch;
+    int ntp;
+    double ucut_pow6, ucut_pow12;   // rc^-6, rc^-12 (force-shift LJ)
+};
+
+// Abramowitz & Stegun 7.1.26 (Hastings): erfc(x) ~ t (a1 + t (a2 + ...)) e^{-x^2},
+// t = 1 / (1 + p x), |error| <= 1.5e-7.  Used by the FP32 pair kernel only.
+__device__ __forceinline__ float erfc_as(float t, float ex)
+{
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
+                a5 = 1.061405429f;
+    return t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5)))) * ex;
+}
+
+struct ShiftTable {
+    float v[27][6];   // hi.x hi.y hi.z lo.x lo.y lo.z
+};
+
+NBParams make_params(const Ctx& c);
+ShiftTable make_shift_table(const Ctx& c);
+
+}  // namespace mdf

@@ -23,32 +23,9 @@
 
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
+#include "nb_common.cuh"
 
 namespace mdf {
-
-constexpr int NB_WARPS = 8;
-constexpr int NB_THREADS = NB_WARPS * 32;
-
-template <typename R> struct V2;
-template <> struct V2<float> { using type = float2; };
-template <> struct V2<double> { using type = double2; };
-
-struct NBParams {
-    double box[3];
-    double rc, rc2, rsw, inv_sw, kc, alpha, rlist2;
-    int use_switch;
-    int ntp;
-    double ucut_pow6, ucut_pow12;   // rc^-6, rc^-12 (force-shift LJ)
-};
-
-// Abramowitz & Stegun 7.1.26 (Hastings): erfc(x) ~ t (a1 + t (a2 + ...)) e^{-x^2},
-// t = 1 / (1 + p x), |error| <= 1.5e-7.  Used by the FP32 pair kernel only.
-__device__ __forceinline__ float erfc_as(float t, float ex)
-{
-    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f, a4 = -1.453152027f,
-                a5 = 1.061405429f;
-    return t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5)))) * ex;
-}
 
 template <typename R, int SEM, bool ENERGY>
 __global__ void __launch_bounds__(NB_THREADS) k_pairs(
@@ -254,9 +231,6 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
 
 // ------------------------------------------------- FP32 PHYSICAL pair kernel
 // Periodic image offsets s*L of the 27 shift codes as an FP32 hi + lo pair.
-struct ShiftTable {
-    float v[27][6];   // hi.x hi.y hi.z lo.x lo.y lo.z
-};
 
 // The mixed-precision production kernel (PHYSICAL semantics).  Same warp
 // layout as k_pairs; differences that matter for speed and accuracy:
@@ -521,7 +495,7 @@ __global__ void k_pairs14(int n, const int* __restrict__ pairs, const double2* _
 }
 
 // ------------------------------------------------------------------ host
-static NBParams make_params(const Ctx& c)
+NBParams make_params(const Ctx& c)
 {
     NBParams P;
     for (int d = 0; d < 3; ++d) P.box[d] = c.box[d];
@@ -573,7 +547,7 @@ static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, 
     c.launches += 1;
 }
 
-static ShiftTable make_shift_table(const Ctx& c)
+ShiftTable make_shift_table(const Ctx& c)
 {
     ShiftTable t;
     for (int code = 0; code < 27; ++code) {

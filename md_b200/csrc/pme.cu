@@ -822,55 +822,56 @@ void setup_pme(Ctx& c)
     MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
 }
 
+// Device buffers of one precision.
 template <typename R>
-static void run_pme(Ctx& c, bool energy)
-{
+struct PmeBufs {
     using C = typename CT<R>::type;
-    const bool ref = c.p.semantics == MDF_SEM_REFERENCE;
-    const int K0 = c.K[0], K1 = c.K[1], K2 = c.K[2], Kc = K2 / 2 + 1;
     C* cg;
     R* rg;
     const C *twx, *twy, *twz;
     const R* infl;
-    if (sizeof(R) == 4) {
-        cg = reinterpret_cast<C*>(c.cgrid_f.p); rg = reinterpret_cast<R*>(c.rgrid_f.p);
-        twx = reinterpret_cast<const C*>(c.tw_f[0].p); twy = reinterpret_cast<const C*>(c.tw_f[1].p);
-        twz = reinterpret_cast<const C*>(c.tw_f[2].p);
-        infl = reinterpret_cast<const R*>(c.infl_f.p);
-    } else {
-        cg = reinterpret_cast<C*>(c.cgrid_d.p); rg = reinterpret_cast<R*>(c.rgrid_d.p);
-        twx = reinterpret_cast<const C*>(c.tw_d[0].p); twy = reinterpret_cast<const C*>(c.tw_d[1].p);
-        twz = reinterpret_cast<const C*>(c.tw_d[2].p);
-        infl = reinterpret_cast<const R*>(c.infl_d.p);
-    }
     GridGeom g;
-    for (int d = 0; d < 3; ++d) {
-        g.K[d] = c.K[d];
-        g.L[d] = c.box[d];
-        g.scale[d] = (double)c.K[d] / c.box[d];
+    explicit PmeBufs(Ctx& c)
+    {
+        if (sizeof(R) == 4) {
+            cg = reinterpret_cast<C*>(c.cgrid_f.p); rg = reinterpret_cast<R*>(c.rgrid_f.p);
+            twx = reinterpret_cast<const C*>(c.tw_f[0].p); twy = reinterpret_cast<const C*>(c.tw_f[1].p);
+            twz = reinterpret_cast<const C*>(c.tw_f[2].p);
+            infl = reinterpret_cast<const R*>(c.infl_f.p);
+        } else {
+            cg = reinterpret_cast<C*>(c.cgrid_d.p); rg = reinterpret_cast<R*>(c.rgrid_d.p);
+            twx = reinterpret_cast<const C*>(c.tw_d[0].p); twy = reinterpret_cast<const C*>(c.tw_d[1].p);
+            twz = reinterpret_cast<const C*>(c.tw_d[2].p);
+            infl = reinterpret_cast<const R*>(c.infl_d.p);
+        }
+        for (int d = 0; d < 3; ++d) {
+            g.K[d] = c.K[d];
+            g.L[d] = c.box[d];
+            g.scale[d] = (double)c.K[d] / c.box[d];
+        }
     }
-    long long ntot = (long long)K0 * K1 * K2;
-    MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
-    const int th = 256;
-    if (!ref) {
-        k_spread4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, g,
-                                                                      c.qgrid.p, c.status.p);
-    } else {
-        k_spread_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, g, c.qgrid.p);
-    }
-    mark(c, "pme_spread");
+};
+
+// Fixed-point charge grid (c.qgrid) -> real potential grid: z, y, x + influence
+// function (+ energy and virial), y^-1, z^-1.  Five launches.
+template <typename R>
+static void conv_chain(Ctx& c, const PmeBufs<R>& B, bool energy)
+{
+    using C = typename CT<R>::type;
+    const bool ref = c.p.semantics == MDF_SEM_REFERENCE;
+    const int K0 = c.K[0], K1 = c.K[1], K2 = c.K[2], Kc = K2 / 2 + 1;
     const FFTDesc dx = to_desc(c.plan[0]), dy = to_desc(c.plan[1]), dz = to_desc(c.plan[2]);
     // z forward (real -> half complex)
     const int LPz = lines_per_block(c.plan[2], sizeof(C));
     const size_t smz = fft_smem(c.plan[2], sizeof(C), LPz);
     const int nlines = K0 * K1;
     const int nbz = (nlines + 2 * LPz - 1) / (2 * LPz);
-    k_fft_z_r2c<R><<<nbz, FFT_THREADS, smz, c.stream>>>(c.qgrid.p, cg, nlines, dz, twz, c.fft_tab[2].p, LPz);
+    k_fft_z_r2c<R><<<nbz, FFT_THREADS, smz, c.stream>>>(c.qgrid.p, B.cg, nlines, dz, B.twz, c.fft_tab[2].p, LPz);
     // y forward
     const int LPy = lines_per_block(c.plan[1], sizeof(C));
     const size_t smy = fft_smem(c.plan[1], sizeof(C), LPy);
     const dim3 gy((Kc + LPy - 1) / LPy, K0);
-    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(cg, Kc, dy, twy, c.fft_tab[1].p, LPy, ilog2(LPy), false);
+    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(B.cg, Kc, dy, B.twy, c.fft_tab[1].p, LPy, ilog2(LPy), false);
     // x forward + convolution + x inverse
     {
         const int LP = lines_per_block(c.plan[0], sizeof(C));
@@ -881,31 +882,240 @@ static void run_pme(Ctx& c, bool energy)
         cp.pa2 = M_PI * M_PI / (c.alpha * c.alpha);
         cp.reference = ref ? 1 : 0;
         if (energy)
-            k_fft_x_conv<R, true><<<gx, FFT_THREADS, sm, c.stream>>>(cg, K1, Kc, dx, twx, c.fft_tab[0].p, LP,
-                                                                     ilog2(LP), cp, infl, c.mvec[0].p, c.mvec[1].p,
+            k_fft_x_conv<R, true><<<gx, FFT_THREADS, sm, c.stream>>>(B.cg, K1, Kc, dx, B.twx, c.fft_tab[0].p, LP,
+                                                                     ilog2(LP), cp, B.infl, c.mvec[0].p, c.mvec[1].p,
                                                                      c.mvec[2].p, c.acc.p, c.status.p);
         else
-            k_fft_x_conv<R, false><<<gx, FFT_THREADS, sm, c.stream>>>(cg, K1, Kc, dx, twx, c.fft_tab[0].p, LP,
-                                                                      ilog2(LP), cp, infl, c.mvec[0].p, c.mvec[1].p,
+            k_fft_x_conv<R, false><<<gx, FFT_THREADS, sm, c.stream>>>(B.cg, K1, Kc, dx, B.twx, c.fft_tab[0].p, LP,
+                                                                      ilog2(LP), cp, B.infl, c.mvec[0].p, c.mvec[1].p,
                                                                       c.mvec[2].p, c.acc.p, c.status.p);
     }
     // y inverse
-    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(cg, Kc, dy, twy, c.fft_tab[1].p, LPy, ilog2(LPy), true);
+    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(B.cg, Kc, dy, B.twy, c.fft_tab[1].p, LPy, ilog2(LPy), true);
     // z inverse (half complex -> real)
-    k_fft_z_c2r<R><<<nbz, FFT_THREADS, smz, c.stream>>>(cg, rg, nlines, dz, twz, c.fft_tab[2].p, LPz);
+    k_fft_z_c2r<R><<<nbz, FFT_THREADS, smz, c.stream>>>(B.cg, B.rg, nlines, dz, B.twz, c.fft_tab[2].p, LPz);
+}
+
+template <typename R>
+static void run_pme(Ctx& c, bool energy)
+{
+    const bool ref = c.p.semantics == MDF_SEM_REFERENCE;
+    const PmeBufs<R> B(c);
+    const long long ntot = (long long)c.K[0] * c.K[1] * c.K[2];
+    MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
+    const int th = 256;
+    if (!ref) {
+        k_spread4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g,
+                                                                      c.qgrid.p, c.status.p);
+    } else {
+        k_spread_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, B.g, c.qgrid.p);
+    }
+    mark(c, "pme_spread");
+    conv_chain<R>(c, B, energy);
     mark(c, "pme_fft_conv");
     if (!ref) {
-        k_gather4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, g, rg,
-                                                                      c.f_slot.p, c.status.p);
+        k_gather4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g,
+                                                                      B.rg, c.f_slot.p, c.status.p);
     } else {
         c.forces_pme_ref.alloc(3 * (size_t)c.N);
-        k_gather_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, g,
-                                                                 reinterpret_cast<const double*>(rg),
+        k_gather_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, B.g,
+                                                                 reinterpret_cast<const double*>(B.rg),
                                                                  c.forces_pme_ref.p);
     }
     mark(c, "pme_gather");
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 7;   // spread, z, y, x+conv, y, z, gather
+}
+
+// ------------------------------------------------------------- adjoint
+// Reciprocal-space part of mdf_backward.  With E = 1/2 Q^T C Q (Q the charge
+// grid, C the convolution with the influence function), phi = C Q, F_a =
+// -q_a grad phi(x_a), v = dL/dF and gE = dL/dE, the derivative of
+// gE E + v.F with respect to q_a is
+//   gE phi(x_a) - v_a . grad phi(x_a) - theta_a^T C P,
+//   P = sum_b q_b (v_b . grad theta_b)   (a "dipole" grid).
+// C is symmetric, so C P is the same convolution chain applied to P.
+
+// Per slot: gE phi - v . grad phi at the atom, added to dq (fixed point).
+template <typename R>
+__global__ void k_adj_gather_phi(int nslots, const int* __restrict__ slot_atom, const double* __restrict__ xyz,
+                                 GridGeom g, const R* __restrict__ phi, const typename V4<R>::type* __restrict__ vs,
+                                 double gE, unsigned long long* __restrict__ dq, unsigned* st)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int a = slot_atom[s];
+    if (a < 0) return;
+    int base[3];
+    R th[3][4], dth[3][4];
+    for (int d = 0; d < 3; ++d) {
+        double u = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
+        if (!(u >= 0.0 && u <= (double)g.K[d])) {
+            status_set(st, ST_NONFINITE);
+            return;
+        }
+        if (u >= g.K[d]) u -= g.K[d];
+        const int b = min((int)floor(u), g.K[d] - 1);
+        base[d] = b;
+        bspline4<R>((R)(u - b), th[d], dth[d]);
+    }
+    R p = 0, gx = 0, gy = 0, gz = 0;
+    for (int i = 0; i < 4; ++i) {
+        int kx = base[0] - 1 + i;
+        kx += (kx < 0) ? g.K[0] : 0;
+        kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+        for (int j = 0; j < 4; ++j) {
+            int ky = base[1] - 1 + j;
+            ky += (ky < 0) ? g.K[1] : 0;
+            ky -= (ky >= g.K[1]) ? g.K[1] : 0;
+            const long long row = ((long long)kx * g.K[1] + ky) * g.K[2];
+            R sz = 0, dz = 0;
+            for (int k = 0; k < 4; ++k) {
+                int kz = base[2] - 1 + k;
+                kz += (kz < 0) ? g.K[2] : 0;
+                kz -= (kz >= g.K[2]) ? g.K[2] : 0;
+                const R v = phi[row + kz];
+                sz += th[2][k] * v;
+                dz += dth[2][k] * v;
+            }
+            p += th[0][i] * th[1][j] * sz;
+            gx += dth[0][i] * th[1][j] * sz;
+            gy += th[0][i] * dth[1][j] * sz;
+            gz += th[0][i] * th[1][j] * dz;
+        }
+    }
+    const typename V4<R>::type v = vs[s];
+    const double val = gE * (double)p - ((double)v.x * (double)(gx * (R)g.scale[0]) +
+                                         (double)v.y * (double)(gy * (R)g.scale[1]) +
+                                         (double)v.z * (double)(gz * (R)g.scale[2]));
+    fx_add(dq + s, val, FORCE_SCALE, st);
+}
+
+// Per slot: spread q_a (v_a . grad theta_a) onto the fixed-point grid.
+template <typename R>
+__global__ void k_adj_spread_dipole(int nslots, const int* __restrict__ slot_atom, const double* __restrict__ xyz,
+                                    const double* __restrict__ q, GridGeom g,
+                                    const typename V4<R>::type* __restrict__ vs, unsigned long long* __restrict__ qgrid,
+                                    unsigned* st)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int a = slot_atom[s];
+    if (a < 0) return;
+    const double qa = q[a];
+    if (qa == 0.0) return;
+    int base[3];
+    R th[3][4], dth[3][4];
+    for (int d = 0; d < 3; ++d) {
+        double u = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
+        if (!(u >= 0.0 && u <= (double)g.K[d])) {
+            status_set(st, ST_NONFINITE);
+            return;
+        }
+        if (u >= g.K[d]) u -= g.K[d];
+        const int b = min((int)floor(u), g.K[d] - 1);
+        base[d] = b;
+        bspline4<R>((R)(u - b), th[d], dth[d]);
+    }
+    const typename V4<R>::type v = vs[s];
+    const R cx = (R)qa * v.x * (R)g.scale[0], cy = (R)qa * v.y * (R)g.scale[1], cz = (R)qa * v.z * (R)g.scale[2];
+    for (int i = 0; i < 4; ++i) {
+        int kx = base[0] - 1 + i;
+        kx += (kx < 0) ? g.K[0] : 0;
+        kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+        for (int j = 0; j < 4; ++j) {
+            int ky = base[1] - 1 + j;
+            ky += (ky < 0) ? g.K[1] : 0;
+            ky -= (ky >= g.K[1]) ? g.K[1] : 0;
+            const long long row = ((long long)kx * g.K[1] + ky) * g.K[2];
+            const R wx = cx * dth[0][i] * th[1][j], wy = cy * th[0][i] * dth[1][j], wz = cz * th[0][i] * th[1][j];
+            for (int k = 0; k < 4; ++k) {
+                int kz = base[2] - 1 + k;
+                kz += (kz < 0) ? g.K[2] : 0;
+                kz -= (kz >= g.K[2]) ? g.K[2] : 0;
+                const R val = (wx + wy) * th[2][k] + wz * dth[2][k];
+                atomicAdd(qgrid + row + kz, (unsigned long long)__double2ll_rn((double)val * GRID_SCALE));
+            }
+        }
+    }
+}
+
+// Per slot: -theta_a^T (C P), added to dq.
+template <typename R>
+__global__ void k_adj_gather_dipole(int nslots, const int* __restrict__ slot_atom, const double* __restrict__ xyz,
+                                    GridGeom g, const R* __restrict__ cp, unsigned long long* __restrict__ dq,
+                                    unsigned* st)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslots) return;
+    const int a = slot_atom[s];
+    if (a < 0) return;
+    int base[3];
+    R th[3][4];
+    for (int d = 0; d < 3; ++d) {
+        double u = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
+        if (!(u >= 0.0 && u <= (double)g.K[d])) {
+            status_set(st, ST_NONFINITE);
+            return;
+        }
+        if (u >= g.K[d]) u -= g.K[d];
+        const int b = min((int)floor(u), g.K[d] - 1);
+        base[d] = b;
+        bspline4<R>((R)(u - b), th[d], nullptr);
+    }
+    R p = 0;
+    for (int i = 0; i < 4; ++i) {
+        int kx = base[0] - 1 + i;
+        kx += (kx < 0) ? g.K[0] : 0;
+        kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+        for (int j = 0; j < 4; ++j) {
+            int ky = base[1] - 1 + j;
+            ky += (ky < 0) ? g.K[1] : 0;
+            ky -= (ky >= g.K[1]) ? g.K[1] : 0;
+            const long long row = ((long long)kx * g.K[1] + ky) * g.K[2];
+            R sz = 0;
+            for (int k = 0; k < 4; ++k) {
+                int kz = base[2] - 1 + k;
+                kz += (kz < 0) ? g.K[2] : 0;
+                kz -= (kz >= g.K[2]) ? g.K[2] : 0;
+                sz += th[2][k] * cp[row + kz];
+            }
+            p += th[0][i] * th[1][j] * sz;
+        }
+    }
+    fx_add(dq + s, -(double)p, FORCE_SCALE, st);
+}
+
+template <typename R>
+static void run_pme_adjoint(Ctx& c, double gE)
+{
+    const PmeBufs<R> B(c);
+    const typename V4<R>::type* vs;
+    if (sizeof(R) == 4) vs = reinterpret_cast<const typename V4<R>::type*>(c.adj_vs_f.p);
+    else vs = reinterpret_cast<const typename V4<R>::type*>(c.adj_vs_d.p);
+    const long long ntot = (long long)c.K[0] * c.K[1] * c.K[2];
+    const int th = 256, nb = grid_blocks(c.n_slots, th);
+    // phi = C Q
+    MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
+    k_spread4<R><<<nb, th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g, c.qgrid.p, c.status.p);
+    conv_chain<R>(c, B, false);
+    k_adj_gather_phi<R><<<nb, th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, B.g, B.rg, vs, gE,
+                                                 c.adj_dq_slot.p, c.status.p);
+    // C P
+    MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
+    k_adj_spread_dipole<R><<<nb, th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g, vs, c.qgrid.p,
+                                                    c.status.p);
+    conv_chain<R>(c, B, false);
+    k_adj_gather_dipole<R><<<nb, th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, B.g, B.rg, c.adj_dq_slot.p,
+                                                    c.status.p);
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 14;
+}
+
+void pme_adjoint(Ctx& c, double gE, double)
+{
+    if (c.p.precision == MDF_PREC_MIXED) run_pme_adjoint<float>(c, gE);
+    else run_pme_adjoint<double>(c, gE);
 }
 
 void launch_pme(Ctx& c, bool energy)

@@ -21,7 +21,8 @@ EXPORTS = [
     "mdf_set_positions", "mdf_set_positions_device", "mdf_set_box", "mdf_build_pairlist", "mdf_compute",
     "mdf_compute_async", "mdf_fetch", "mdf_forces_device", "mdf_get_pme_forces", "mdf_set_stream",
     "mdf_pairlist_info", "mdf_enable_timing", "mdf_kernel_times", "mdf_cmap_coefficients",
-    "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_compute_bonded_noalloc",
+    "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
+    "mdf_backward",
 ]
 
 
@@ -68,6 +69,8 @@ def library(path=None):
     lib.mdf_kernel_launches.argtypes = [C.c_void_p]
     lib.mdf_kernel_launches.restype = C.c_int64
     lib.mdf_probe_fma_tflops.argtypes = [C.c_int, C.c_int, dp]
+    lib.mdf_set_parameters.argtypes = [C.c_void_p, dp, dp, dp]
+    lib.mdf_backward.argtypes = [C.c_void_p, dp, C.c_double, dp, dp, dp]
     lib.mdf_compute_bonded_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(abi.mdf_energies)]
     _LIB = lib
     return lib
@@ -108,6 +111,7 @@ class Engine:
         self.lib = library()
         self.flat = flat
         self.natoms = flat.natoms
+        self.n_ljpair = int(len(flat.lj_a))
         p = default_params()
         p.semantics, p.precision = int(semantics), int(precision)
         for k in range(3):
@@ -202,6 +206,29 @@ class Engine:
 
     def forces_device(self, ptr):
         self._check(self.lib.mdf_forces_device(self.h, C.c_void_p(ptr)), "forces_device")
+
+    def set_parameters(self, charge=None, lj_a=None, lj_b=None):
+        """Replace charges and/or the LJ A/B table (None keeps the current values)."""
+        def p(a):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            self._keep.append(a)
+            return a.ctypes.data_as(C.POINTER(C.c_double))
+        self._keep = []
+        self._check(self.lib.mdf_set_parameters(self.h, p(charge), p(lj_a), p(lj_b)), "set_parameters")
+
+    def backward(self, dL_dF, dL_dE):
+        """dL/dq [N], dL/dA [n_ljpair], dL/dB [n_ljpair] for dL/dF [N, 3] and dL/dE."""
+        g = None if dL_dF is None else np.ascontiguousarray(dL_dF, dtype=np.float64).reshape(-1)
+        dq = np.zeros(self.natoms)
+        dA = np.zeros(self.n_ljpair)
+        dB = np.zeros(self.n_ljpair)
+        dp_ = C.POINTER(C.c_double)
+        self._check(self.lib.mdf_backward(self.h, None if g is None else g.ctypes.data_as(dp_), float(dL_dE),
+                                          dq.ctypes.data_as(dp_), dA.ctypes.data_as(dp_), dB.ctypes.data_as(dp_)),
+                    "backward")
+        return dq, dA, dB
 
     def bonded_noalloc(self, forces_ptr, energy=True):
         """Bonded terms only, with the library's static scratch (no device

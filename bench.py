@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--profile", metavar="CONFIG", default=None,
                     help="profiling run: build CONFIG (tiny, small, c0, c1, c4), run --warmup + --steps "
                          "evaluations, print the per-phase times and exit (for ncu)")
@@ -191,6 +192,40 @@ def run_reference_arm(args, rank):
             "reference_breakdown_s": {k2: r[k2] for k2 in ("s_pme_chain", "s_list_energies", "s_calculate_forces",
                                                           "s_pairlist")}}
     print(json.dumps(line), flush=True)
+
+
+def adjoint_cost(dev, reps=10):
+    """c2 workload: the c0 system (28,227 atoms, PME 72^3), loss = mean |F - F_t|^2
+    + 1e-3 E_total.  Wall time of one forward evaluation (mdf_compute, energies
+    and forces to host) against one mdf_backward (dL/dq, dL/dA, dL/dB to host),
+    both synchronous calls through the C ABI, FP64 and mixed."""
+    from md_b200 import abi, engine, synth, topology
+    s = synth.make_config("c0")
+    flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    out = {"workload": "c2: c0 system, %d atoms, %d charges + 2 x %d LJ coefficients" % (
+        s.natoms, s.natoms, len(flat.lj_a))}
+    for name, prec in (("fp64", abi.MDF_PREC_FP64), ("mixed", abi.MDF_PREC_MIXED)):
+        eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=prec, ewald_tol=1e-5,
+                            grid=synth.GRIDS["c0"], device=dev)
+        eng.set_positions(s.coords)
+        eng.build_pairlist()
+        E, F = eng.compute()
+        Ft = F + np.random.default_rng(5).normal(0.0, 0.5, F.shape)
+        gF, gE = 2.0 * (F - Ft) / F.shape[0], 1e-3
+        for _ in range(3):
+            eng.compute()
+            eng.backward(gF, gE)
+        tf = tb = 0.0
+        for _ in range(reps):
+            a = time.perf_counter()
+            eng.compute()
+            tf += time.perf_counter() - a
+            a = time.perf_counter()
+            eng.backward(gF, gE)
+            tb += time.perf_counter() - a
+        eng.close()
+        out[name] = {"forward_ms": tf / reps * 1e3, "backward_ms": tb / reps * 1e3, "backward_over_forward": tb / tf}
+    return out
 
 
 def main():
@@ -340,6 +375,10 @@ def main():
         except Exception as e:  # the baseline is reported, never required
             cpu = {"value": None, "unit": "evals/s", "cores": 1, "kind": "reference", "sample": "failed: %s" % e}
 
+    adj = None
+    if rank == 0 and ws == 1 and not args.no_adjoint:
+        adj = adjoint_cost(dev)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
@@ -364,6 +403,7 @@ def main():
             "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": 3 * s.natoms * 8,
                     "d2h_bytes_per_step": 3 * s.natoms * 8 + 26 * 8},
             "fp64": fp64,
+            "adjoint": adj,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),

@@ -148,7 +148,12 @@ typedef struct {
      * prune_every = 0 disables pruning. */
     int32_t prune_every;
     double prune_margin;
-    int32_t reserved[4];
+    /* Launch shapes (results do not depend on them; mdf_batch_autotune picks
+     * them): warps per block of the pair kernel (2, 4 or 8; 0 = 8) and the
+     * most FFT lines per block (1, 2 or 4; 0 = 4). */
+    int32_t pair_warps;
+    int32_t fft_lines;
+    int32_t reserved[2];
 } mdf_params;
 
 /* Flags for mdf_compute. */
@@ -240,6 +245,43 @@ int mdf_set_parameters(mdf_ctx *ctx, const double *charge, const double *lj_a, c
  * bonded terms are constants here.  REFERENCE semantics return
  * MDF_ERR_UNSUPPORTED (their forces are not the gradient of their energy). */
 int mdf_backward(mdf_ctx *ctx, const double *dL_dF, double dL_dE, double *dL_dq, double *dL_dA, double *dL_dB);
+
+/* ---------------------------------------------------------------------------
+ * Batches: many independent PHYSICAL systems (uneven atom counts, boxes and
+ * PME grids) evaluated by one CUDA graph launch.  Positions and forces are
+ * the systems' 3N arrays concatenated in system order.  Each system keeps
+ * its own pairlist (built at the positions of mdf_batch_build_pairlists, or
+ * at the first compute); evaluate within the skin of those positions, or
+ * rebuild.  Not thread-safe; one batch per host thread. */
+typedef struct mdf_batch mdf_batch;
+
+typedef struct {
+    int32_t pair_warps;   /* chosen launch shapes (see mdf_params) */
+    int32_t fft_lines;
+    int32_t prune_every;
+    int32_t n_tried;      /* candidates timed */
+    double best_ms;       /* one batch evaluation with the chosen shapes */
+    double default_ms;    /* ... with the shapes the batch was created with */
+} mdf_tune_report;
+
+int mdf_batch_create(int nsys, const mdf_topology *const *topos, const mdf_params *params, mdf_batch **out);
+void mdf_batch_destroy(mdf_batch *b);
+const char *mdf_batch_last_error(const mdf_batch *b);
+/* Systems, total atoms, kernels in one graph launch (-1 before the first capture). */
+int mdf_batch_info(const mdf_batch *b, int64_t *n_systems, int64_t *total_atoms, int64_t *graph_kernels);
+/* Host positions [3 * total atoms]; copied at the call, uploaded inside the graph. */
+int mdf_batch_set_positions(mdf_batch *b, const double *xyz);
+int mdf_batch_build_pairlists(mdf_batch *b);
+/* One batch evaluation; forces [3 * total atoms] and energies [nsys] to host
+ * (either may be NULL).  Returns after the evaluation. */
+int mdf_batch_compute(mdf_batch *b, uint32_t flags, double *forces, mdf_energies *energies);
+/* The same split in two: launch (ordered after `stream` if non-NULL, and
+ * `stream` after it) and fetch (waits, then copies out). */
+int mdf_batch_launch(mdf_batch *b, uint32_t flags, void *stream);
+int mdf_batch_fetch(mdf_batch *b, uint32_t flags, double *forces, mdf_energies *energies);
+/* Time every candidate launch shape on this batch (reps graph launches each)
+ * and keep the fastest.  report may be NULL. */
+int mdf_batch_autotune(mdf_batch *b, int reps, mdf_tune_report *report);
 
 /* No counterpart in the reference.
  *

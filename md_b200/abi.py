@@ -55,5 +55,12 @@ class mdf_params(C.Structure):
         ("cutoff", C.c_double), ("skin", C.c_double), ("switch_radius", C.c_double),
         ("ewald_tol", C.c_double), ("ewald_alpha", C.c_double), ("grid", C.c_int32 * 3),
         ("pme_order", C.c_int32), ("coulomb_const", C.c_double), ("device", C.c_int32),
-        ("prune_every", C.c_int32), ("prune_margin", C.c_double), ("reserved", C.c_int32 * 4),
+        ("prune_every", C.c_int32), ("prune_margin", C.c_double), ("pair_warps", C.c_int32),
+        ("fft_lines", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
+
+
+class mdf_tune_report(C.Structure):
+    _fields_ = [("pair_warps", C.c_int32), ("fft_lines", C.c_int32), ("prune_every", C.c_int32),
+                ("n_tried", C.c_int32), ("best_ms", C.c_double), ("default_ms", C.c_double)]
+

@@ -244,7 +244,7 @@ void upload_topology(Ctx& c, const mdf_topology* t)
     MDF_CUDA_TRY(cudaStreamSynchronize(s));
 }
 
-static void eval_async_impl(Ctx& c, uint32_t flags)
+void eval_async_impl(Ctx& c, uint32_t flags)
 {
     if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
     if (!c.have_list) build_pairlist(c);
@@ -318,13 +318,48 @@ static void eval_async(Ctx& c, uint32_t flags)
     }
 }
 
+// Energies of the last finished evaluation from the host copy of its scalar
+// block (written by k_finalize into mapped host memory).
+void host_energies(const Ctx& c, uint32_t flags, mdf_energies* e_out)
+{
+    memset(e_out, 0, sizeof(*e_out));
+    if (!(flags & MDF_COMPUTE_ENERGY)) return;
+    for (int k = 0; k < MDF_E_COUNT; ++k) e_out->e[k] = (double)(long long)c.h_scal[k] * ENERGY_ISCALE;
+    e_out->e[MDF_E_EE_SELF] += c.e_self;
+    const bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
+    if (phys) {
+        const double V = c.box[0] * c.box[1] * c.box[2];
+        e_out->e[MDF_E_EE_RECIP] += -c.p.coulomb_const * M_PI * c.q_total * c.q_total / (2.0 * V * c.alpha * c.alpha);
+        const int vmap[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+        for (int k = 0; k < 9; ++k) e_out->virial[k] = (double)(long long)c.h_scal[ACC_VIR + vmap[k]] * ENERGY_ISCALE;
+        double tot = 0;
+        const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
+                             MDF_E_VDW, MDF_E_VDW14, MDF_E_EE_DIRECT, MDF_E_EE14, MDF_E_EE_EXCL,
+                             MDF_E_EE_SELF, MDF_E_EE_RECIP};
+        for (int k : terms) tot += e_out->e[k];
+        e_out->total = tot;
+    } else {
+        double tot = 0;
+        const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
+                             MDF_E_VDW, MDF_E_EE};
+        for (int k : terms) tot += e_out->e[k];
+        e_out->total = tot;
+    }
+}
+
+// Status bits of the last finished evaluation, as an exception.
+void check_host_status(const Ctx& c)
+{
+    const unsigned st = (unsigned)c.h_scal[NUM_ACC + 1];
+    if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite force or energy contribution");
+    if (st & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "fixed-point accumulator range exceeded");
+}
+
 static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
 {
     if (!c.pending) throw ApiError(MDF_ERR_STATE, "no evaluation to fetch");
     MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    unsigned st = (unsigned)c.h_scal[NUM_ACC + 1];
-    if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite force or energy contribution");
-    if (st & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "fixed-point accumulator range exceeded");
+    check_host_status(c);
     if (c.timing) {
         c.tlast.clear();
         for (int i = 1; i < c.nev; ++i) {
@@ -333,34 +368,7 @@ static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
             c.tlast.emplace_back(c.evname[i], ms);
         }
     }
-    if (e_out) {
-        memset(e_out, 0, sizeof(*e_out));
-        if (c.pending_flags & MDF_COMPUTE_ENERGY) {
-            for (int k = 0; k < MDF_E_COUNT; ++k) e_out->e[k] = (double)(long long)c.h_scal[k] * ENERGY_ISCALE;
-            e_out->e[MDF_E_EE_SELF] += c.e_self;
-            bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
-            if (phys) {
-                double V = c.box[0] * c.box[1] * c.box[2];
-                e_out->e[MDF_E_EE_RECIP] +=
-                    -c.p.coulomb_const * M_PI * c.q_total * c.q_total / (2.0 * V * c.alpha * c.alpha);
-                const int vmap[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-                for (int k = 0; k < 9; ++k)
-                    e_out->virial[k] = (double)(long long)c.h_scal[ACC_VIR + vmap[k]] * ENERGY_ISCALE;
-                double tot = 0;
-                const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
-                                     MDF_E_VDW, MDF_E_VDW14, MDF_E_EE_DIRECT, MDF_E_EE14, MDF_E_EE_EXCL,
-                                     MDF_E_EE_SELF, MDF_E_EE_RECIP};
-                for (int k : terms) tot += e_out->e[k];
-                e_out->total = tot;
-            } else {
-                double tot = 0;
-                const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
-                                     MDF_E_VDW, MDF_E_EE};
-                for (int k : terms) tot += e_out->e[k];
-                e_out->total = tot;
-            }
-        }
-    }
+    if (e_out) host_energies(c, c.pending_flags, e_out);
     if (forces_out)
         MDF_CUDA_TRY(cudaMemcpy(forces_out, c.forces_out.p, sizeof(double) * 3 * (size_t)c.N, cudaMemcpyDeviceToHost));
 }

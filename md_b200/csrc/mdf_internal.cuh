@@ -253,6 +253,9 @@ void setup_pme(Ctx& c);
 void launch_pme(Ctx& c, bool energy);
 void launch_finalize(Ctx& c, double* d_forces, bool pme_ref);
 void mark(Ctx& c, const char* name);
+void eval_async_impl(Ctx& c, uint32_t flags);
+void host_energies(const Ctx& c, uint32_t flags, mdf_energies* e_out);
+void check_host_status(const Ctx& c);
 
 // simple device-wide exclusive scan of ints (n up to a few million)
 void exclusive_scan_int(const int* d_in, int* d_out, int n, int* d_total_out, cudaStream_t s);

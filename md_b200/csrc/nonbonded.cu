@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
     __shared__ V4t sx[NB_WARPS][4][CLUSTER + 1];
     __shared__ int stj[NB_WARPS][4][CLUSTER];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int w = blockIdx.x * NB_WARPS + wib;
+    const int w = blockIdx.x * (blockDim.x >> 5) + wib;
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
 
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
     __syncthreads();
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int w = blockIdx.x * NB_WARPS + wib;
+    const int w = blockIdx.x * (blockDim.x >> 5) + wib;
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
     const float rc2 = (float)P.rc2, rsw = (float)P.rsw, inv_sw = (float)P.inv_sw, alpha = (float)P.alpha;
@@ -515,6 +515,13 @@ NBParams make_params(const Ctx& c)
     return P;
 }
 
+// Warps per block of the pair kernels: mdf_params.pair_warps (2, 4 or 8; 0 = 8).
+static int pair_warps(const Ctx& c)
+{
+    const int w = c.p.pair_warps;
+    return (w == 2 || w == 4 || w == 8) ? w : NB_WARPS;
+}
+
 // Atom pairs within the cutoff are counted by the first evaluation after a
 // pairlist build only (the count costs instructions in the pair loop).
 static bool begin_pair_count(Ctx& c)
@@ -530,17 +537,18 @@ template <typename R, int SEM>
 static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, const typename V2<R>::type* lj)
 {
     NBParams P = make_params(c);
-    int nb = grid_blocks(c.n_clusters, NB_WARPS);
+    const int wpb = pair_warps(c);
+    int nb = grid_blocks(c.n_clusters, wpb);
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
     const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     const int count = begin_pair_count(c) ? 1 : 0;
     if (energy)
-        k_pairs<R, SEM, true><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
+        k_pairs<R, SEM, true><<<nb, 32 * wpb, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
                                                                lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
                                                                c.npairs_dev.p, count, c.status.p);
     else
-        k_pairs<R, SEM, false><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
+        k_pairs<R, SEM, false><<<nb, 32 * wpb, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
                                                                 lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
                                                                 c.npairs_dev.p, count, c.status.p);
     MDF_CUDA_TRY(cudaGetLastError());
@@ -566,13 +574,14 @@ static void launch_pairs_f32(Ctx& c, bool energy)
 {
     NBParams P = make_params(c);
     ShiftTable sh = make_shift_table(c);
-    int nb = grid_blocks(c.n_clusters, NB_WARPS);
+    const int wpb = pair_warps(c);
+    int nb = grid_blocks(c.n_clusters, wpb);
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
     const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     const bool count = begin_pair_count(c);
 #define MDF_PF32(E, S, K)                                                                                           \
-    k_pairs_f32<E, S, K><<<nb, NB_THREADS, 0, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p,            \
+    k_pairs_f32<E, S, K><<<nb, 32 * wpb, 0, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p,            \
                                                           c.centerf.p, c.ljAB_f.p, P, sh, c.f_slot.p, c.n_slots,   \
                                                           c.acc.p, c.npairs_dev.p, c.status.p)
 #define MDF_PF32_K(E, S) \

@@ -680,10 +680,12 @@ static double cardinal_bspline(int n, double x)
     return (x * cardinal_bspline(n - 1, x) + (n - x) * cardinal_bspline(n - 1, x - 1.0)) / (n - 1);
 }
 
-// lines per block (power of two dividing FFT_THREADS) within 46 KB of shared memory
-static int lines_per_block(const FFTPlan1D& p, size_t csize)
+// lines per block (power of two dividing FFT_THREADS) within 46 KB of shared
+// memory, at most cap (mdf_params.fft_lines: 1, 2 or 4; 0 = 4)
+static int lines_per_block(const FFTPlan1D& p, size_t csize, int cap = 4)
 {
-    for (int lp = 4; lp >= 1; lp >>= 1) {
+    const int top = (cap == 1 || cap == 2) ? cap : 4;
+    for (int lp = top; lp >= 1; lp >>= 1) {
         size_t bytes = csize * ((size_t)p.n + 2 * (size_t)lp * p.n) + sizeof(int2) * (size_t)p.ntab;
         if (bytes <= 46 * 1024) return lp;
     }
@@ -862,19 +864,19 @@ static void conv_chain(Ctx& c, const PmeBufs<R>& B, bool energy)
     const int K0 = c.K[0], K1 = c.K[1], K2 = c.K[2], Kc = K2 / 2 + 1;
     const FFTDesc dx = to_desc(c.plan[0]), dy = to_desc(c.plan[1]), dz = to_desc(c.plan[2]);
     // z forward (real -> half complex)
-    const int LPz = lines_per_block(c.plan[2], sizeof(C));
+    const int LPz = lines_per_block(c.plan[2], sizeof(C), c.p.fft_lines);
     const size_t smz = fft_smem(c.plan[2], sizeof(C), LPz);
     const int nlines = K0 * K1;
     const int nbz = (nlines + 2 * LPz - 1) / (2 * LPz);
     k_fft_z_r2c<R><<<nbz, FFT_THREADS, smz, c.stream>>>(c.qgrid.p, B.cg, nlines, dz, B.twz, c.fft_tab[2].p, LPz);
     // y forward
-    const int LPy = lines_per_block(c.plan[1], sizeof(C));
+    const int LPy = lines_per_block(c.plan[1], sizeof(C), c.p.fft_lines);
     const size_t smy = fft_smem(c.plan[1], sizeof(C), LPy);
     const dim3 gy((Kc + LPy - 1) / LPy, K0);
     k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(B.cg, Kc, dy, B.twy, c.fft_tab[1].p, LPy, ilog2(LPy), false);
     // x forward + convolution + x inverse
     {
-        const int LP = lines_per_block(c.plan[0], sizeof(C));
+        const int LP = lines_per_block(c.plan[0], sizeof(C), c.p.fft_lines);
         const size_t sm = fft_smem(c.plan[0], sizeof(C), LP);
         const dim3 gx((Kc + LP - 1) / LP, K1);
         ConvParams cp;

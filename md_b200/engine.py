@@ -22,7 +22,9 @@ EXPORTS = [
     "mdf_compute_async", "mdf_fetch", "mdf_forces_device", "mdf_get_pme_forces", "mdf_set_stream",
     "mdf_pairlist_info", "mdf_enable_timing", "mdf_kernel_times", "mdf_cmap_coefficients",
     "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
-    "mdf_backward",
+    "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
+    "mdf_batch_set_positions", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
+    "mdf_batch_fetch", "mdf_batch_autotune",
 ]
 
 
@@ -71,6 +73,20 @@ def library(path=None):
     lib.mdf_probe_fma_tflops.argtypes = [C.c_int, C.c_int, dp]
     lib.mdf_set_parameters.argtypes = [C.c_void_p, dp, dp, dp]
     lib.mdf_backward.argtypes = [C.c_void_p, dp, C.c_double, dp, dp, dp]
+    vp = C.c_void_p
+    lib.mdf_batch_create.argtypes = [C.c_int, C.POINTER(C.POINTER(abi.mdf_topology)), C.POINTER(abi.mdf_params),
+                                     C.POINTER(vp)]
+    lib.mdf_batch_destroy.argtypes = [vp]
+    lib.mdf_batch_destroy.restype = None
+    lib.mdf_batch_last_error.argtypes = [vp]
+    lib.mdf_batch_last_error.restype = C.c_char_p
+    lib.mdf_batch_info.argtypes = [vp] + [C.POINTER(C.c_int64)] * 3
+    lib.mdf_batch_set_positions.argtypes = [vp, dp]
+    lib.mdf_batch_build_pairlists.argtypes = [vp]
+    lib.mdf_batch_compute.argtypes = [vp, C.c_uint32, dp, C.POINTER(abi.mdf_energies)]
+    lib.mdf_batch_launch.argtypes = [vp, C.c_uint32, vp]
+    lib.mdf_batch_fetch.argtypes = [vp, C.c_uint32, dp, C.POINTER(abi.mdf_energies)]
+    lib.mdf_batch_autotune.argtypes = [vp, C.c_int, C.POINTER(abi.mdf_tune_report)]
     lib.mdf_compute_bonded_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(abi.mdf_energies)]
     _LIB = lib
     return lib
@@ -258,3 +274,93 @@ class Engine:
         ms = (C.c_float * 32)()
         n = self.lib.mdf_kernel_times(self.h, names, ms, 32)
         return [(names[i].decode(), ms[i]) for i in range(n)]
+
+
+class Batch:
+    """Many independent PHYSICAL systems evaluated by one CUDA graph launch
+    (mdf_batch_*).  flats / boxes / grids: one per system."""
+
+    def __init__(self, flats, boxes, grids, precision=abi.MDF_PREC_MIXED, cutoff=9.0, skin=2.0, switch_radius=8.0,
+                 ewald_tol=1e-5, device=0, prune_every=1):
+        self.lib = library()
+        self.flats = list(flats)
+        n = len(self.flats)
+        self.natoms = [f.natoms for f in self.flats]
+        self.offsets = np.concatenate([[0], np.cumsum(self.natoms)])
+        tops = (C.POINTER(abi.mdf_topology) * n)(*[C.pointer(f.struct()) for f in self.flats])
+        params = (abi.mdf_params * n)()
+        for k in range(n):
+            p = default_params()
+            p.semantics, p.precision = abi.MDF_SEM_PHYSICAL, int(precision)
+            for d in range(3):
+                p.box[d] = float(boxes[k][d])
+                p.grid[d] = int(grids[k][d])
+            p.cutoff, p.skin, p.switch_radius = float(cutoff), float(skin), float(switch_radius)
+            p.ewald_tol, p.device = float(ewald_tol), int(device)
+            p.prune_every = int(prune_every)
+            params[k] = p
+        self._tops, self._params = tops, params
+        h = C.c_void_p()
+        rc = self.lib.mdf_batch_create(n, tops, params, C.byref(h))
+        if rc != 0:
+            raise MDFError(rc, "batch_create: %s" % self.lib.mdf_last_error(None).decode())
+        self.h = h
+        self.n = n
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise MDFError(rc, "%s: %s" % (what, self.lib.mdf_batch_last_error(self.h).decode()))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mdf_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_positions(self, coords_list):
+        x = np.ascontiguousarray(np.concatenate([np.asarray(c, float).reshape(-1) for c in coords_list]))
+        self._check(self.lib.mdf_batch_set_positions(self.h, x.ctypes.data_as(C.POINTER(C.c_double))), "set_positions")
+
+    def build_pairlists(self):
+        self._check(self.lib.mdf_batch_build_pairlists(self.h), "build_pairlists")
+
+    def compute(self, energy=True, forces=True):
+        """Per system: (energies dict or None, forces [n_k, 3] or None)."""
+        flags = (abi.MDF_COMPUTE_ENERGY if energy else 0) | (abi.MDF_COMPUTE_FORCES if forces else 0)
+        F = np.zeros(3 * int(self.offsets[-1])) if forces else None
+        E = (abi.mdf_energies * self.n)() if energy else None
+        self._check(self.lib.mdf_batch_compute(self.h, flags, F.ctypes.data_as(C.POINTER(C.c_double))
+                                               if forces else None, E), "compute")
+        out = []
+        for k in range(self.n):
+            e = E[k].as_dict() if energy else None
+            f = F[3 * self.offsets[k]:3 * self.offsets[k + 1]].reshape(-1, 3) if forces else None
+            out.append((e, f))
+        return out
+
+    def launch(self, energy=True, stream_ptr=None):
+        flags = abi.MDF_COMPUTE_FORCES | (abi.MDF_COMPUTE_ENERGY if energy else 0)
+        self._check(self.lib.mdf_batch_launch(self.h, flags, C.c_void_p(stream_ptr) if stream_ptr else None),
+                    "launch")
+
+    def fetch_into(self, forces_ptr, energy=True):
+        flags = abi.MDF_COMPUTE_FORCES | (abi.MDF_COMPUTE_ENERGY if energy else 0)
+        self._check(self.lib.mdf_batch_fetch(self.h, flags, C.cast(forces_ptr, C.POINTER(C.c_double))
+                                             if forces_ptr else None, None), "fetch")
+
+    def autotune(self, reps=5):
+        r = abi.mdf_tune_report()
+        self._check(self.lib.mdf_batch_autotune(self.h, int(reps), C.byref(r)), "autotune")
+        return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every, n_tried=r.n_tried,
+                    best_ms=r.best_ms, default_ms=r.default_ms)
+
+    def info(self):
+        a, b, c = C.c_int64(), C.c_int64(), C.c_int64()
+        self._check(self.lib.mdf_batch_info(self.h, C.byref(a), C.byref(b), C.byref(c)), "info")
+        return dict(n_systems=a.value, total_atoms=b.value, graph_kernels=c.value)
+

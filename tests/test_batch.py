@@ -1,0 +1,102 @@
+"""Batched evaluation (mdf_batch_*): uneven independent systems in one CUDA
+graph launch must give exactly the single-system results (same kernels,
+fixed-point sums) across graph replays and position updates.  After
+autotuning the launch shapes the forces are still bit-identical (each pair
+force is converted to fixed point on its own); energies, summed in FP64 per
+block before their fixed-point conversion, may move in the last bits
+(1e-12 relative + 1e-8 absolute).  The FP64 batch matches the oracle."""
+import numpy as np
+import pytest
+
+from md_b200 import abi, engine, synth
+from oracle import oracle as O
+from tests import helpers as H
+
+pytestmark = pytest.mark.gpu
+PHYS, FP64, MIXED = abi.MDF_SEM_PHYSICAL, abi.MDF_PREC_FP64, abi.MDF_PREC_MIXED
+TERMS = ["bond", "angle", "dihedral", "ub", "improper", "cmap", "vdw", "vdw14", "ee_direct", "ee14", "ee_excl",
+         "ee_self", "ee_recip", "total"]
+KW = dict(cutoff=9.0, skin=2.0, switch_radius=8.0, ewald_tol=1e-5)
+
+_SYS = None
+
+
+def systems():
+    global _SYS
+    if _SYS is None:
+        _SYS = synth.make_batch(n_systems=5, seed=77)
+    return _SYS
+
+
+def _flats(ss):
+    return [H.flat(s, PHYS, engine.cmap_coefficients) for s in ss]
+
+
+def _singles(ss, flats, prec, coords=None):
+    out = []
+    for k, (s, f) in enumerate(zip(ss, flats)):
+        eng = engine.Engine(f, s.box, semantics=PHYS, precision=prec, grid=s.meta["grid"], **KW)
+        eng.set_positions(s.coords)
+        eng.build_pairlist()
+        if coords is not None:
+            eng.set_positions(coords[k])
+        out.append(eng.compute())
+        eng.close()
+    return out
+
+
+def _same(res, ref, etol=0.0):
+    for (E, F), (E1, F1) in zip(res, ref):
+        assert np.array_equal(F, F1)
+        for t in TERMS:
+            # etol > 0: rounding of the per-block FP64 sums (relative) and their
+            # fixed-point conversion (2^-32 per block, absolute)
+            assert abs(E[t] - E1[t]) <= etol * abs(E1[t]) + (1e-8 if etol else 0.0), (t, E[t], E1[t])
+
+
+@pytest.mark.parametrize("prec", [MIXED, FP64])
+def test_batch_equals_single_systems(prec):
+    ss = systems()
+    flats = _flats(ss)
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=prec, **KW)
+    b.set_positions([s.coords for s in ss])
+    res = b.compute()
+    ref = _singles(ss, flats, prec)
+    _same(res, ref)
+    _same(b.compute(), ref)           # a graph replay
+    info = b.info()
+    assert info["n_systems"] == len(ss) and info["graph_kernels"] > len(ss)
+    b.close()
+
+
+def test_batch_autotune_keeps_results_and_follows_positions():
+    ss = systems()
+    flats = _flats(ss)
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
+    b.set_positions([s.coords for s in ss])
+    ref = _singles(ss, flats, MIXED)
+    rep = b.autotune(reps=2)
+    assert rep["n_tried"] == 18 and rep["best_ms"] > 0
+    assert rep["pair_warps"] in (2, 4, 8) and rep["fft_lines"] in (1, 2, 4) and rep["prune_every"] in (0, 1)
+    _same(b.compute(), ref, 1e-12)
+    # moved positions (within the skin): the graph uploads them at every launch
+    rng = np.random.default_rng(3)
+    moved = [s.coords + rng.uniform(-0.2, 0.2, s.coords.shape) for s in ss]
+    b.set_positions(moved)
+    _same(b.compute(), _singles(ss, flats, MIXED, coords=moved), 1e-12)
+    b.close()
+
+
+def test_fp64_batch_matches_oracle():
+    ss = systems()[:2]
+    flats = _flats(ss)
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=FP64, **KW)
+    b.set_positions([s.coords for s in ss])
+    res = b.compute()
+    for (E, F), s, f in zip(res, ss, flats):
+        p = O.make_params(PHYS, s.box, s.meta["grid"], H.alpha_for(1e-5, 9.0), H.KC, cutoff=9.0, switch=8.0)
+        e2, f2, _, _, _ = O.evaluate(f, p, s.coords)
+        assert H.frel(F, f2) < 1e-9
+        for t in TERMS[:-1]:
+            assert abs(E[t] - e2[abi.E_INDEX[t]]) <= 1e-9 * max(1.0, abs(e2[abi.E_INDEX[t]])), t
+    b.close()

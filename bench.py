@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--profile", metavar="CONFIG", default=None,
                     help="profiling run: build CONFIG (tiny, small, c0, c1, c4), run --warmup + --steps "
                          "evaluations, print the per-phase times and exit (for ncu)")
@@ -228,6 +229,69 @@ def adjoint_cost(dev, reps=10):
     return out
 
 
+def _batch_member(k):
+    from md_b200 import abi, engine, synth, topology
+    sysm = synth.make_batch_member(k)
+    flat = topology.flatten(sysm, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    return sysm, flat
+
+
+def make_batch_workload(n=256):
+    """c3's 256 uneven systems, generated in spawned worker processes."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    with cf.ProcessPoolExecutor(max_workers=min(8, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_batch_member, range(n)))
+
+
+def batch_bench(dev, members, stream, steps=20):
+    """c3: 256 uneven systems (25-40 A boxes, 1.5k-6k atoms, PME 24^3-40^3,
+    cutoff 9 A), mixed precision, one CUDA graph launch per batch evaluation,
+    launch shapes autotuned.  Device time per graph launch (CUDA events on the
+    stream the graph is ordered on; the graph includes the host<->device copies
+    of all positions and forces through pinned buffers) and the wall time of
+    set_positions + compute through the C ABI."""
+    import torch
+    from md_b200 import abi, engine
+    ss = [m[0] for m in members]
+    flats = [m[1] for m in members]
+    b = engine.Batch(flats, [x.box for x in ss], [x.meta["grid"] for x in ss], precision=abi.MDF_PREC_MIXED,
+                     cutoff=9.0, skin=2.0, switch_radius=8.0, ewald_tol=1e-5, device=dev)
+    b.set_positions([x.coords for x in ss])
+    t0 = time.perf_counter()
+    b.build_pairlists()
+    t_build = time.perf_counter() - t0
+    tune = b.autotune(reps=3)
+    for _ in range(3):
+        b.launch(stream_ptr=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    for k in range(steps):
+        ev[k][0].record(stream)
+        b.launch(stream_ptr=stream.cuda_stream)
+        ev[k][1].record(stream)
+    torch.cuda.synchronize(dev)
+    ms = float(np.mean([a.elapsed_time(c) for a, c in ev]))
+    pos = [x.coords for x in ss]
+    e2e_t = 0.0
+    for _ in range(max(5, steps // 2)):
+        a = time.perf_counter()
+        b.set_positions(pos)
+        b.compute(energy=True, forces=True)
+        e2e_t += time.perf_counter() - a
+    e2e_ms = e2e_t / max(5, steps // 2) * 1e3
+    info = b.info()
+    natoms = [x.natoms for x in ss]
+    b.close()
+    return {"workload": "c3: %d systems, %d-%d atoms (%d total), boxes 25-40 A, PME 24^3-40^3, cutoff 9 A, "
+                        "mixed precision, one CUDA graph launch per evaluation" % (len(ss), min(natoms),
+                                                                                   max(natoms), sum(natoms)),
+            "frames_per_s": len(ss) / (ms * 1e-3), "ms_per_batch": ms,
+            "e2e_frames_per_s": len(ss) / (e2e_ms * 1e-3), "e2e_ms_per_batch": e2e_ms,
+            "atoms_per_s": sum(natoms) / (ms * 1e-3), "graph_kernels": info["graph_kernels"],
+            "pairlist_build_s": t_build, "autotune": tune}
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
@@ -237,6 +301,9 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, rank)
         return
+    batch_members = None
+    if rank == 0 and ws == 1 and not args.no_batch:
+        batch_members = make_batch_workload()
     import torch
     import torch.distributed as dist
     from md_b200 import abi, engine
@@ -378,6 +445,9 @@ def main():
     adj = None
     if rank == 0 and ws == 1 and not args.no_adjoint:
         adj = adjoint_cost(dev)
+    batched = None
+    if batch_members is not None:
+        batched = batch_bench(dev, batch_members, stream)
 
     if rank == 0:
         line = {
@@ -404,6 +474,7 @@ def main():
                     "d2h_bytes_per_step": 3 * s.natoms * 8 + 26 * 8},
             "fp64": fp64,
             "adjoint": adj,
+            "batched": batched,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),

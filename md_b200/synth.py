@@ -188,6 +188,15 @@ class _Hash:
         return out
 
 
+def _chain_clear(pos, box, dmin):
+    """No two chain atoms more than three bonds apart closer than dmin (min image)."""
+    from scipy.spatial import cKDTree
+    w = pos - box * np.floor(pos / box)
+    w = np.minimum(w, np.nextafter(box, 0))
+    pairs = cKDTree(w, boxsize=box).query_pairs(dmin, output_type="ndarray")
+    return not np.any(np.abs(pairs[:, 0] - pairs[:, 1]) > 3) if len(pairs) else True
+
+
 def _place_next(a, b, c, r, theta, phi):
     """Position d with |cd|=r, angle(b,c,d)=theta, dihedral(a,b,c,d)=phi."""
     bc = c - b
@@ -208,13 +217,16 @@ def _place_next(a, b, c, r, theta, phi):
 # --------------------------------------------------------------------------
 
 def make_system(name, box, n_waters, n_residues, seed, atoms_per_residue=10,
-                n_chain_types=40, sentinels=False, water_first=False):
+                n_chain_types=40, sentinels=False, water_first=False, min_contact=0.0):
     """Build one seeded system.
 
     box: cubic edge (float) or 3-tuple.  ``sentinels`` appends a zero-force-
     constant tuple to every term list the reference's loaders truncate
     (``src/AmberTopology/CreateBondedFromParsed.cpp:11,74,100,126,152,178,220,262``),
     so that reference-semantics and physical-semantics term sets coincide.
+    ``min_contact`` > 0 rejects chain positions closer than that to any earlier
+    chain atom more than three bonds away (used by the batch systems, whose
+    small boxes crowd the walk).
     """
     rng = np.random.default_rng(seed)
     box = np.array([box] * 3 if np.isscalar(box) else box, dtype=np.float64)
@@ -233,39 +245,50 @@ def make_system(name, box, n_waters, n_residues, seed, atoms_per_residue=10,
     chain_pos = np.zeros((n_chain, 3))
     chain_bond_type = rng.integers(0, n_bond_types_chain, max(n_chain - 1, 0))
     chain_angle_type = rng.integers(0, n_angle_types_chain, max(n_chain - 2, 0))
-    if n_chain > 0:
-        hsh = _Hash(box, 3.0)
-        center = box / 2.0
-        start = center + rng.uniform(-1, 1, 3)
-        chain_pos[0] = start
-        hsh.add(chain_pos[0], 0)
-        for i in range(1, n_chain):
-            r = bond_r0_c[chain_bond_type[i - 1]] * (1.0 + rng.normal(0, 0.02))
-            best, best_score = None, -1e9
-            fallback = None
-            for attempt in range(60):
-                if i == 1:
-                    v = rng.normal(size=3); v /= np.linalg.norm(v)
-                    cand = chain_pos[0] + r * v
-                else:
-                    th = angle_t0_c[chain_angle_type[i - 2]] + rng.normal(0, 0.03)
-                    ph = rng.uniform(-math.pi, math.pi)
-                    a = chain_pos[i - 3] if i >= 3 else chain_pos[i - 2] + np.array([0.3, 0.7, 0.1])
-                    cand = _place_next(a, chain_pos[i - 2], chain_pos[i - 1], r, th, ph)
-                if np.any(np.abs(cand - center) > 0.62 * box):
-                    fallback = cand
-                    continue
-                near = [t for t in hsh.near(cand, 2.7) if t < i - 3]
-                if not near:
-                    best = cand
+    for _retry in range(50 if min_contact > 0 else 1):
+        walk_ok = True
+        if n_chain > 0:
+            hsh = _Hash(box, 3.0)
+            center = box / 2.0
+            start = center + rng.uniform(-1, 1, 3)
+            chain_pos[0] = start
+            hsh.add(chain_pos[0], 0)
+            for i in range(1, n_chain):
+                r = bond_r0_c[chain_bond_type[i - 1]] * (1.0 + rng.normal(0, 0.02))
+                best, best_score = None, -1e9
+                fallback = None
+                for attempt in range(400 if min_contact > 0 else 60):
+                    if i == 1:
+                        v = rng.normal(size=3); v /= np.linalg.norm(v)
+                        cand = chain_pos[0] + r * v
+                    else:
+                        th = angle_t0_c[chain_angle_type[i - 2]] + rng.normal(0, 0.03)
+                        ph = rng.uniform(-math.pi, math.pi)
+                        a = chain_pos[i - 3] if i >= 3 else chain_pos[i - 2] + np.array([0.3, 0.7, 0.1])
+                        cand = _place_next(a, chain_pos[i - 2], chain_pos[i - 1], r, th, ph)
+                    if np.any(np.abs(cand - center) > 0.62 * box):
+                        fallback = cand
+                        continue
+                    if min_contact > 0 and [t for t in hsh.near(cand, min_contact) if t < i - 3]:
+                        continue
+                    near = [t for t in hsh.near(cand, 2.7) if t < i - 3]
+                    if not near:
+                        best = cand
+                        break
+                    score = -len(near)
+                    if score > best_score or best is None:
+                        best, best_score = cand, score
+                if best is None:
+                    best = fallback
+                if best is None:        # crowded: start the walk again
+                    walk_ok = False
                     break
-                score = -len(near)
-                if score > best_score or best is None:
-                    best, best_score = cand, score
-            if best is None:
-                best = fallback
-            chain_pos[i] = best
-            hsh.add(best, i)
+                chain_pos[i] = best
+                hsh.add(best, i)
+        if walk_ok and (min_contact <= 0 or n_chain == 0 or _chain_clear(chain_pos, box, min_contact)):
+            break
+    else:
+        raise RuntimeError("chain walk found no clash-free path for %s" % name)
 
     # ---------------- waters on a jittered lattice
     nl = int(math.ceil(n_waters ** (1.0 / 3.0) - 1e-9)) if n_waters > 0 else 0
@@ -540,20 +563,30 @@ def smooth_grid_size(L, spacing=1.0):
         n += 1
 
 
-def make_batch(n_systems=256, seed=1003):
-    """Uneven independent systems: edge U(25,40) A, 10-30-residue chain."""
+def _batch_dims(n_systems, seed):
     rng = np.random.default_rng(seed)
     out = []
-    for s in range(n_systems):
+    for _ in range(n_systems):
         L = float(rng.uniform(25.0, 40.0))
         nres = int(rng.integers(10, 31))
-        # water count for roughly 0.1 atoms / A^3 minus the chain share
-        nw = max(10, int(0.1 * L ** 3 / 3.0) - nres * 10 // 3)
-        sysm = make_system("batch%03d" % s, L, nw, nres, seed * 1000 + s)
-        g = smooth_grid_size(sysm.box[0], 1.0)
-        sysm.meta["grid"] = (g, g, g)
-        out.append(sysm)
+        out.append((L, nres))
     return out
+
+
+def make_batch_member(k, n_systems=256, seed=1003):
+    """System k of make_batch(n_systems, seed), built on its own."""
+    L, nres = _batch_dims(n_systems, seed)[k]
+    # water count for roughly 0.1 atoms / A^3 minus the chain share
+    nw = max(10, int(0.1 * L ** 3 / 3.0) - nres * 10 // 3)
+    sysm = make_system("batch%03d" % k, L, nw, nres, seed * 1000 + k, min_contact=2.0)
+    g = smooth_grid_size(sysm.box[0], 1.0)
+    sysm.meta["grid"] = (g, g, g)
+    return sysm
+
+
+def make_batch(n_systems=256, seed=1003):
+    """Uneven independent systems: edge U(25,40) A, 10-30-residue chain."""
+    return [make_batch_member(k, n_systems, seed) for k in range(n_systems)]
 
 
 # --------------------------------------------------------------------------

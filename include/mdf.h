@@ -224,6 +224,12 @@ int mdf_kernel_times(mdf_ctx *ctx, const char **names, float *ms, int max_entrie
  * energy grids [nsets][res*res], the reference's table build
  * (src/AmberTopology/CreateNonBondedFromParsed.cpp:46-117). */
 int mdf_cmap_coefficients(int nsets, int res, const double *grids, double *coeff);
+/* Host-only utility, PHYSICAL semantics: the same table layout from C1
+ * bicubic Hermite patches (corner values, periodic-cubic-spline first
+ * derivatives and cross derivative, in grid-index units).  The reference's
+ * patches match the grid at cell corners but not along cell edges, so its
+ * CMAP energy jumps when a torsion crosses a grid line. */
+int mdf_cmap_coefficients_spline(int nsets, int res, const double *grids, double *coeff);
 
 /* Diagnostic: measured FMA throughput of the device's CUDA cores in TFLOP/s
  * (an FMA counts 2), precision MDF_PREC_MIXED for FP32, MDF_PREC_FP64 for

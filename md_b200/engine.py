@@ -24,7 +24,7 @@ EXPORTS = [
     "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
-    "mdf_batch_fetch", "mdf_batch_autotune",
+    "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
 ]
 
 
@@ -68,6 +68,7 @@ def library(path=None):
     lib.mdf_enable_timing.argtypes = [C.c_void_p, C.c_int]
     lib.mdf_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.c_int]
     lib.mdf_cmap_coefficients.argtypes = [C.c_int, C.c_int, dp, dp]
+    lib.mdf_cmap_coefficients_spline.argtypes = [C.c_int, C.c_int, dp, dp]
     lib.mdf_kernel_launches.argtypes = [C.c_void_p]
     lib.mdf_kernel_launches.restype = C.c_int64
     lib.mdf_probe_fma_tflops.argtypes = [C.c_int, C.c_int, dp]
@@ -90,6 +91,17 @@ def library(path=None):
     lib.mdf_compute_bonded_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(abi.mdf_energies)]
     _LIB = lib
     return lib
+
+
+def cmap_coefficients_spline(nsets, res, grids):
+    """C1 periodic-spline bicubic CMAP table (PHYSICAL semantics), host only."""
+    g = np.ascontiguousarray(grids, dtype=np.float64)
+    out = np.zeros(nsets * res * res * 16)
+    rc = library().mdf_cmap_coefficients_spline(nsets, res, g.ctypes.data_as(C.POINTER(C.c_double)),
+                                                out.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise MDFError(rc, "mdf_cmap_coefficients_spline")
+    return out
 
 
 def cmap_coefficients(nsets, res, grids):

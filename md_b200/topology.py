@@ -84,7 +84,12 @@ def _f64(a):
 def flatten(sysm, semantics, cmap_coeff_fn):
     """SynthSystem (or any object with the same prmtop fields) -> FlatTopology.
 
-    cmap_coeff_fn(nsets, res, grids[nsets, res*res]) -> coeff[nsets*res*res*16].
+    cmap_coeff_fn(nsets, res, grids[nsets, res*res]) -> coeff[nsets*res*res*16]
+    builds the REFERENCE CMAP table (the reference's 16x16-matrix patches).
+    PHYSICAL semantics always use the C1 spline table of
+    mdf_cmap_coefficients_spline instead: the reference's patches do not meet
+    along the cell edges, so their energy jumps as a torsion crosses a grid
+    line and dynamics cannot conserve energy.
     """
     ref = semantics == abi.MDF_SEM_REFERENCE
 
@@ -101,7 +106,12 @@ def flatten(sysm, semantics, cmap_coeff_fn):
 
     res = int(sysm.cmap_res[0]) if len(sysm.cmap_res) else 24
     nsets = int(sysm.cmap_grids.shape[0])
-    coeff = _f64(cmap_coeff_fn(nsets, res, np.ascontiguousarray(sysm.cmap_grids, dtype=np.float64)))
+    grids = np.ascontiguousarray(sysm.cmap_grids, dtype=np.float64)
+    if ref:
+        coeff = _f64(cmap_coeff_fn(nsets, res, grids))
+    else:
+        from . import engine
+        coeff = _f64(engine.cmap_coefficients_spline(nsets, res, grids))
 
     if ref:
         excl = np.zeros(0, np.int32)

@@ -80,3 +80,30 @@ def test_invalid_topology_rejected_before_device_work():
     with pytest.raises(engine.MDFError) as e:
         engine.Engine(flat, s.box)
     assert e.value.status in (1, 2)
+
+
+def test_cmap_spline_table_is_c1_and_interpolates():
+    """PHYSICAL CMAP table: patches meet with equal value and slope along every
+    cell edge (the reference's do not), hit the grid at the corners, and
+    interpolate a smooth periodic surface to 1e-3."""
+    res = 24
+    ph = np.arange(res) * 2 * np.pi / res
+    grid = 2 * np.cos(ph)[:, None] * np.sin(2 * ph)[None, :] + np.cos(ph[:, None] + ph[None, :])
+    C = engine.cmap_coefficients_spline(1, res, grid.reshape(1, -1)).reshape(res, res, 4, 4)
+    R = engine.cmap_coefficients(1, res, grid.reshape(1, -1)).reshape(res, res, 4, 4)
+    p = lambda t: np.array([1, t, t * t, t ** 3])
+    d = lambda t: np.array([0, 1, 2 * t, 3 * t * t])
+    e_ref = e_edge = e_slope = e_corner = e_int = 0.0
+    for i in range(res):
+        for j in range(res):
+            e_corner = max(e_corner, abs(p(0) @ C[i, j] @ p(0) - grid[i, j]))
+            for v in (0.0, 0.4, 0.8):
+                a, b = C[i, j], C[(i + 1) % res, j]
+                e_edge = max(e_edge, abs(p(1) @ a @ p(v) - p(0) @ b @ p(v)))
+                e_slope = max(e_slope, abs(d(1) @ a @ p(v) - d(0) @ b @ p(v)))
+                e_ref = max(e_ref, abs(p(1) @ R[i, j] @ p(v) - p(0) @ R[(i + 1) % res, j] @ p(v)))
+            x, y = (i + 0.5) * 2 * np.pi / res, (j + 0.5) * 2 * np.pi / res
+            e_int = max(e_int, abs(p(0.5) @ C[i, j] @ p(0.5) - (2 * np.cos(x) * np.sin(2 * y) + np.cos(x + y))))
+    assert e_edge < 1e-12 and e_slope < 1e-12 and e_corner < 1e-12
+    assert e_int < 1e-3
+    assert e_ref > 0.1      # the reference's table is discontinuous along cell edges

@@ -253,6 +253,49 @@ int mdf_set_parameters(mdf_ctx *ctx, const double *charge, const double *lj_a, c
 int mdf_backward(mdf_ctx *ctx, const double *dL_dF, double dL_dE, double *dL_dq, double *dL_dA, double *dL_dB);
 
 /* ---------------------------------------------------------------------------
+ * Dynamics and minimisation (PHYSICAL semantics).  Units: A, A/ps, amu,
+ * kcal/mol.  The reference has neither (apps/main.cpp stops after one
+ * evaluation); its intended consumer of calculate_forces is a minimiser
+ * (include/System/System.h:84,113) and its list rebuild test is
+ * ljpairs_needs_rebuild (src/System/NonBondedUtils.cpp:87-100). */
+typedef struct {
+    int32_t iterations;
+    int32_t rebuilds;
+    double e_initial, e_final;   /* total potential energy, kcal/mol */
+    double fmax_final;           /* largest force component at the end */
+} mdf_min_report;
+/* Steepest descent at the current positions, largest move per iteration
+ * adaptive up to max_step (A); stops at max |F| <= fmax_tol (kcal/mol/A) or
+ * after max_iter iterations.  The positions stay on the device
+ * (mdf_md_state reads them); call mdf_md_init afterwards to start dynamics. */
+int mdf_minimize(mdf_ctx *ctx, int32_t max_iter, double fmax_tol, double max_step, mdf_min_report *report);
+
+typedef struct {
+    int64_t steps;        /* steps done */
+    int64_t rebuilds;     /* list builds during the run */
+    int64_t samples;      /* energy samples (one per chunk) */
+    double wall_s;        /* host wall time of the run */
+    double pe_first, ke_first;   /* potential / kinetic energy after the first chunk */
+    double pe_last, ke_last;     /* ... after the last chunk */
+} mdf_md_report;
+/* masses [natoms] (amu); velocities [3N] (A/ps), or NULL to draw them from a
+ * Maxwell-Boltzmann distribution at temperature (K) with the given seed
+ * (centre-of-mass motion removed).  Builds the list and computes the forces. */
+int mdf_md_init(mdf_ctx *ctx, const double *masses, const double *velocities, double temperature, uint64_t seed);
+/* Velocity-Verlet NVE steps in CUDA-graph chunks of `chunk` steps (0 = 10).
+ * The pairlist is rebuilt every rebuild_every steps, or with rebuild_every = 0
+ * when the largest displacement since the last build, plus twice what the
+ * fastest atom covers in a chunk, would pass half the skin; a displacement
+ * past half the skin between builds is an error.  samples (may be NULL)
+ * receives up to cap rows (t ps, potential, kinetic), one per chunk. */
+int mdf_md_run(mdf_ctx *ctx, int64_t nsteps, double dt_ps, int32_t chunk, int32_t rebuild_every, double *samples,
+               int64_t cap, mdf_md_report *report);
+/* Current positions and velocities to host ([3N] each; either may be NULL). */
+int mdf_md_state(mdf_ctx *ctx, double *xyz, double *velocities);
+/* Amber ASCII restart (positions, velocities, box) of the current state. */
+int mdf_md_write_rst7(mdf_ctx *ctx, const char *path, const char *title, double time_ps);
+
+/* ---------------------------------------------------------------------------
  * Batches: many independent PHYSICAL systems (uneven atom counts, boxes and
  * PME grids) evaluated by one CUDA graph launch.  Positions and forces are
  * the systems' 3N arrays concatenated in system order.  Each system keeps

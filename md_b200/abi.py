@@ -64,3 +64,14 @@ class mdf_tune_report(C.Structure):
     _fields_ = [("pair_warps", C.c_int32), ("fft_lines", C.c_int32), ("prune_every", C.c_int32),
                 ("n_tried", C.c_int32), ("best_ms", C.c_double), ("default_ms", C.c_double)]
 
+
+class mdf_md_report(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("rebuilds", C.c_int64), ("samples", C.c_int64), ("wall_s", C.c_double),
+                ("pe_first", C.c_double), ("ke_first", C.c_double), ("pe_last", C.c_double),
+                ("ke_last", C.c_double)]
+
+
+class mdf_min_report(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("rebuilds", C.c_int32), ("e_initial", C.c_double),
+                ("e_final", C.c_double), ("fmax_final", C.c_double)]
+

@@ -518,6 +518,10 @@ void mdf_destroy(mdf_ctx* ctx)
         c.tw_d[d].release(); c.tw_f[d].release(); c.fft_tab[d].release(); c.mvec[d].release();
     }
     if (c.h_scal) cudaFreeHost(c.h_scal);
+    if (c.md_exec) cudaGraphExecDestroy(c.md_exec);
+    if (c.md_graph) cudaGraphDestroy(c.md_graph);
+    if (c.md_host) cudaFreeHost(c.md_host);
+    c.md_v.release(); c.md_invm.release(); c.md_xref.release(); c.min_x.release(); c.min_f.release();
     if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
     if (c.side) cudaStreamDestroy(c.side);
     if (c.ev_fork) cudaEventDestroy(c.ev_fork);
@@ -706,6 +710,52 @@ int mdf_backward(mdf_ctx* ctx, const double* dL_dF, double dL_dE, double* dL_dq,
         Ctx& c = ctx->c;
         MDF_CUDA_TRY(cudaSetDevice(c.device));
         backward(c, dL_dF, dL_dE, dL_dq, dL_dA, dL_dB);
+    });
+}
+
+int mdf_minimize(mdf_ctx* ctx, int32_t max_iter, double fmax_tol, double max_step, mdf_min_report* report)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        minimize(ctx->c, max_iter, fmax_tol, max_step, report);
+    });
+}
+
+int mdf_md_init(mdf_ctx* ctx, const double* masses, const double* velocities, double temperature, uint64_t seed)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        md_init(ctx->c, masses, velocities, temperature, seed);
+    });
+}
+
+int mdf_md_run(mdf_ctx* ctx, int64_t nsteps, double dt_ps, int32_t chunk, int32_t rebuild_every, double* samples,
+               int64_t cap, mdf_md_report* report)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        md_run(ctx->c, nsteps, dt_ps, chunk, rebuild_every, samples, cap, report);
+    });
+}
+
+int mdf_md_state(mdf_ctx* ctx, double* xyz, double* velocities)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        md_state(ctx->c, xyz, velocities);
+    });
+}
+
+int mdf_md_write_rst7(mdf_ctx* ctx, const char* path, const char* title, double time_ps)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        md_write_rst7(ctx->c, path, title, time_ps);
     });
 }
 

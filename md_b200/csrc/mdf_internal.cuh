@@ -223,6 +223,20 @@ struct Ctx {
     DevBuf<double> adj_dab;              // [2 n_ljpair] dL/dA | dL/dB
     DevBuf<double> adj_dq;               // [N] dL/dq out
 
+    // dynamics and minimiser (md.cu)
+    DevBuf<double> md_v;                 // [3N] velocities, A/ps
+    DevBuf<double> md_invm;              // [N] 418.4 / mass (0 = frozen)
+    DevBuf<double> md_xref;              // [3N] positions at the last list build
+    DevBuf<double> min_x, min_f;         // minimiser: positions and forces before the trial move
+    unsigned long long* md_host = nullptr;   // mapped words (see md.cu)
+    unsigned long long* md_dev = nullptr;
+    unsigned* md_dev_st = nullptr;
+    bool md_ready = false;
+    cudaGraph_t md_graph = nullptr;
+    cudaGraphExec_t md_exec = nullptr;
+    int md_graph_steps = 0;
+    double md_graph_dt = 0.0;
+
     // timing
     bool timing = false;
     std::vector<cudaEvent_t> evpool;          // reused timing events
@@ -240,6 +254,12 @@ struct Ctx {
 void upload_topology(Ctx& c, const mdf_topology* t);
 void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b);
 void set_charge_constants(Ctx& c, const double* charge);
+void md_init(Ctx& c, const double* masses, const double* vel, double temperature, uint64_t seed);
+void md_run(Ctx& c, long long nsteps, double dt, int chunk, int rebuild_every, double* samples, long long cap,
+            mdf_md_report* rep);
+void md_state(Ctx& c, double* xyz, double* vel);
+void md_write_rst7(Ctx& c, const char* path, const char* title, double time_ps);
+void minimize(Ctx& c, int max_iter, double fmax_tol, double max_step, mdf_min_report* rep);
 void backward(Ctx& c, const double* dL_dF, double dL_dE, double* dL_dq, double* dL_dA, double* dL_dB);
 void pme_adjoint(Ctx& c, double gE, double vscale);
 void build_pairlist(Ctx& c);

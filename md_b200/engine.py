@@ -25,6 +25,7 @@ EXPORTS = [
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
+    "mdf_minimize", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
 
@@ -74,6 +75,12 @@ def library(path=None):
     lib.mdf_probe_fma_tflops.argtypes = [C.c_int, C.c_int, dp]
     lib.mdf_set_parameters.argtypes = [C.c_void_p, dp, dp, dp]
     lib.mdf_backward.argtypes = [C.c_void_p, dp, C.c_double, dp, dp, dp]
+    lib.mdf_minimize.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.mdf_min_report)]
+    lib.mdf_md_init.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_uint64]
+    lib.mdf_md_run.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_int32, C.c_int32, dp, C.c_int64,
+                               C.POINTER(abi.mdf_md_report)]
+    lib.mdf_md_state.argtypes = [C.c_void_p, dp, dp]
+    lib.mdf_md_write_rst7.argtypes = [C.c_void_p, C.c_char_p, C.c_char_p, C.c_double]
     vp = C.c_void_p
     lib.mdf_batch_create.argtypes = [C.c_int, C.POINTER(C.POINTER(abi.mdf_topology)), C.POINTER(abi.mdf_params),
                                      C.POINTER(vp)]
@@ -257,6 +264,44 @@ class Engine:
                                           dq.ctypes.data_as(dp_), dA.ctypes.data_as(dp_), dB.ctypes.data_as(dp_)),
                     "backward")
         return dq, dA, dB
+
+    def minimize(self, max_iter=200, fmax_tol=10.0, max_step=0.1):
+        """Steepest descent at the current positions; returns the report dict."""
+        r = abi.mdf_min_report()
+        self._check(self.lib.mdf_minimize(self.h, int(max_iter), float(fmax_tol), float(max_step), C.byref(r)),
+                    "minimize")
+        return {k: getattr(r, k) for k, _ in abi.mdf_min_report._fields_}
+
+    def md_init(self, masses, velocities=None, temperature=300.0, seed=1):
+        """Start dynamics: masses [N] amu, velocities [N, 3] A/ps or Maxwell at temperature."""
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float64).reshape(-1)
+        dp_ = C.POINTER(C.c_double)
+        self._check(self.lib.mdf_md_init(self.h, m.ctypes.data_as(dp_), None if v is None else v.ctypes.data_as(dp_),
+                                         float(temperature), int(seed)), "md_init")
+
+    def md_run(self, nsteps, dt_ps, chunk=10, rebuild_every=0):
+        """Velocity-Verlet steps; returns (report dict, samples [n, 3]: t ps, PE, KE)."""
+        ch = max(int(chunk), 1)
+        cap = (int(nsteps) + ch - 1) // ch + 1
+        samp = np.zeros((cap, 3))
+        r = abi.mdf_md_report()
+        self._check(self.lib.mdf_md_run(self.h, int(nsteps), float(dt_ps), int(chunk), int(rebuild_every),
+                                        samp.ctypes.data_as(C.POINTER(C.c_double)), cap, C.byref(r)), "md_run")
+        rep = {k: getattr(r, k) for k, _ in abi.mdf_md_report._fields_}
+        return rep, samp[:min(int(r.samples), cap)]
+
+    def md_state(self, velocities=True):
+        x = np.zeros((self.natoms, 3))
+        v = np.zeros((self.natoms, 3)) if velocities else None
+        dp_ = C.POINTER(C.c_double)
+        self._check(self.lib.mdf_md_state(self.h, x.ctypes.data_as(dp_), v.ctypes.data_as(dp_) if velocities else None),
+                    "md_state")
+        return x, v
+
+    def write_rst7(self, path, title="md_b200 restart", time_ps=0.0):
+        self._check(self.lib.mdf_md_write_rst7(self.h, str(path).encode(), title.encode(), float(time_ps)),
+                    "write_rst7")
 
     def bonded_noalloc(self, forces_ptr, energy=True):
         """Bonded terms only, with the library's static scratch (no device

@@ -521,7 +521,7 @@ void mdf_destroy(mdf_ctx* ctx)
     if (c.md_exec) cudaGraphExecDestroy(c.md_exec);
     if (c.md_graph) cudaGraphDestroy(c.md_graph);
     if (c.md_host) cudaFreeHost(c.md_host);
-    c.md_v.release(); c.md_invm.release(); c.md_xref.release(); c.min_x.release(); c.min_f.release();
+    c.md_v.release(); c.md_invm.release(); c.md_xref.release(); c.min_x.release(); c.min_f.release(); c.md_words.release();
     if (c.stream && c.own_stream) cudaStreamDestroy(c.stream);
     if (c.side) cudaStreamDestroy(c.side);
     if (c.ev_fork) cudaEventDestroy(c.ev_fork);

@@ -33,9 +33,26 @@ constexpr double MD_ACCEL = 418.4;          // (kcal/mol/A)/amu -> A/ps^2
 constexpr double KB_KCAL = 0.0019872041;    // kcal/mol/K
 constexpr double AMBER_VEL = 20.455;        // A/ps per Amber velocity unit
 
-// mapped host words: kinetic energy (fixed point) | max displacement^2 bits |
-// status | max |F| bits (minimiser) | max speed^2 bits
+// Reduction words: kinetic energy (fixed point) | max displacement^2 bits |
+// status | max |F| bits (minimiser) | max speed^2 bits.  Kernels reduce into
+// device memory (every warp adds or takes a maximum); one small kernel then
+// publishes the words to mapped host memory for the host to read after the
+// stream is synchronised.  (Atomics straight into mapped host memory would
+// cross the host link once per warp.)
 constexpr int MD_WORDS = 5;
+
+__global__ void k_md_publish(const unsigned long long* __restrict__ src, unsigned long long* __restrict__ dst)
+{
+    const int i = threadIdx.x;
+    if (i < MD_WORDS) dst[i] = src[i];
+}
+
+// Zero the words whose bit is set in mask.
+__global__ void k_md_reset(unsigned long long* __restrict__ w, unsigned mask)
+{
+    const int i = threadIdx.x;
+    if (i < MD_WORDS && ((mask >> i) & 1u)) w[i] = 0ull;
+}
 
 static double bits_to_double(unsigned long long u)
 {
@@ -104,8 +121,11 @@ static void md_words(Ctx& c)
 {
     if (!c.md_host) {
         MDF_CUDA_TRY(cudaHostAlloc((void**)&c.md_host, sizeof(unsigned long long) * MD_WORDS, cudaHostAllocMapped));
-        MDF_CUDA_TRY(cudaHostGetDevicePointer((void**)&c.md_dev, c.md_host, 0));
+        MDF_CUDA_TRY(cudaHostGetDevicePointer((void**)&c.md_hmap, c.md_host, 0));
         memset(c.md_host, 0, sizeof(unsigned long long) * MD_WORDS);
+        c.md_words.alloc(MD_WORDS);
+        MDF_CUDA_TRY(cudaMemsetAsync(c.md_words.p, 0, sizeof(unsigned long long) * MD_WORDS, c.stream));
+        c.md_dev = c.md_words.p;
         c.md_dev_st = reinterpret_cast<unsigned*>(c.md_dev + 2);
     }
 }
@@ -127,6 +147,7 @@ static void md_capture(Ctx& c, int steps, double dt)
     c.timing = false;   // no per-phase events inside a captured chunk
     MDF_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
+        k_md_reset<<<1, 32, 0, s>>>(c.md_dev, (1u << 0) | (1u << 2) | (1u << 4));
         for (int k = 0; k < steps; ++k) {
             const bool last = k == steps - 1;
             k_md_kick_drift<<<grid_blocks(3LL * c.N, th), th, 0, s>>>(c.N, c.xyz.p, c.md_v.p, c.forces_out.p,
@@ -136,6 +157,7 @@ static void md_capture(Ctx& c, int steps, double dt)
                                                           last ? c.md_dev : nullptr, c.md_dev + 4, c.md_dev_st);
             k_md_displacement<<<grid_blocks(c.N, th), th, 0, s>>>(c.N, c.xyz.p, c.md_xref.p, c.md_dev + 1);
         }
+        k_md_publish<<<1, 32, 0, s>>>(c.md_dev, c.md_hmap);
         MDF_CUDA_TRY(cudaGetLastError());
     } catch (...) {
         c.timing = timing;
@@ -159,6 +181,8 @@ static void md_rebuild(Ctx& c)
     // forces at the current positions for the first half kick; also clears
     // the accumulators and counts pairs outside any capture
     eval_async_impl(c, MDF_COMPUTE_FORCES);
+    k_md_reset<<<1, 32, 0, c.stream>>>(c.md_dev, 1u << 1);   // displacement since this build
+    MDF_CUDA_TRY(cudaGetLastError());
     MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
     check_host_status(c);
     c.md_host[1] = 0;
@@ -203,6 +227,7 @@ void md_init(Ctx& c, const double* masses, const double* vel, double temperature
     c.md_v.upload(v.data(), v.size(), c.stream);
     c.md_xref.alloc(3 * (size_t)c.N);
     md_words(c);
+    MDF_CUDA_TRY(cudaMemsetAsync(c.md_words.p, 0, sizeof(unsigned long long) * MD_WORDS, c.stream));
     memset(c.md_host, 0, sizeof(unsigned long long) * MD_WORDS);
     double vmax2 = 3.0 * v2;   // bound until the first chunk has measured it
     memcpy(&c.md_host[4], &vmax2, sizeof(double));
@@ -234,9 +259,6 @@ void md_run(Ctx& c, long long nsteps, double dt, int chunk, int rebuild_every, d
             ++r.rebuilds;
         }
         if (!c.md_exec || c.md_graph_steps != steps || c.md_graph_dt != dt) md_capture(c, steps, dt);
-        c.md_host[0] = 0;   // kinetic energy of this chunk's last step
-        c.md_host[2] = 0;
-        c.md_host[4] = 0;
         MDF_CUDA_TRY(cudaGraphLaunch(c.md_exec, c.stream));
         MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
         check_host_status(c);
@@ -302,9 +324,10 @@ void minimize(Ctx& c, int max_iter, double fmax_tol, double max_step, mdf_min_re
     c.min_x.alloc(n3);
     c.min_f.alloc(n3);
     auto evaluate = [&](double& e, double& fmax) {
-        c.md_host[3] = 0;
+        k_md_reset<<<1, 32, 0, s>>>(c.md_dev, 1u << 3);
         eval_async_impl(c, MDF_COMPUTE_ENERGY | MDF_COMPUTE_FORCES);
         k_min_fmax<<<grid_blocks(n3, th), th, 0, s>>>((int)n3, c.forces_out.p, c.md_dev + 3);
+        k_md_publish<<<1, 32, 0, s>>>(c.md_dev, c.md_hmap);
         MDF_CUDA_TRY(cudaGetLastError());
         MDF_CUDA_TRY(cudaStreamSynchronize(s));
         check_host_status(c);

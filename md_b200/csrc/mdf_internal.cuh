@@ -228,8 +228,10 @@ struct Ctx {
     DevBuf<double> md_invm;              // [N] 418.4 / mass (0 = frozen)
     DevBuf<double> md_xref;              // [3N] positions at the last list build
     DevBuf<double> min_x, min_f;         // minimiser: positions and forces before the trial move
-    unsigned long long* md_host = nullptr;   // mapped words (see md.cu)
-    unsigned long long* md_dev = nullptr;
+    unsigned long long* md_host = nullptr;   // mapped host copy of the reduction words (see md.cu)
+    unsigned long long* md_hmap = nullptr;   // its device address
+    DevBuf<unsigned long long> md_words; // the reduction words in device memory
+    unsigned long long* md_dev = nullptr;    // = md_words.p
     unsigned* md_dev_st = nullptr;
     bool md_ready = false;
     cudaGraph_t md_graph = nullptr;

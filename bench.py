@@ -61,6 +61,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-md", action="store_true")
     ap.add_argument("--profile", metavar="CONFIG", default=None,
                     help="profiling run: build CONFIG (tiny, small, c0, c1, c4), run --warmup + --steps "
                          "evaluations, print the per-phase times and exit (for ncu)")
@@ -226,6 +227,50 @@ def adjoint_cost(dev, reps=10):
             tb += time.perf_counter() - a
         eng.close()
         out[name] = {"forward_ms": tf / reps * 1e3, "backward_ms": tb / reps * 1e3, "backward_over_forward": tb / tf}
+    return out
+
+
+def md_bench(dev, steps=1000, equil=200):
+    """c4: 215 A box of 320,000 flexible waters (960,000 atoms), PME 216^3,
+    cutoff 10 A + 2 A skin, velocity-Verlet NVE at 0.5 fs from 300 K Maxwell
+    velocities (seeded), pairlist rebuilt every 10 steps.  The lattice start is
+    first relaxed by the steepest-descent minimiser (the same positions feed
+    both precisions), then `equil` steps are run before the measured `steps`.
+    Steps/s is the host wall time of mdf_md_run (graph chunks of 10 steps,
+    list rebuilds and the per-chunk energy read-back included); the energy
+    drift is last minus first sample of the total energy over the measured
+    steps, mixed against FP64 from the same start."""
+    from md_b200 import abi, engine, synth, topology
+    s = synth.make_config("c4")
+    flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    kw = dict(semantics=abi.MDF_SEM_PHYSICAL, ewald_tol=1e-5, grid=synth.GRIDS["c4"], device=dev)
+    eng = engine.Engine(flat, s.box, precision=abi.MDF_PREC_MIXED, **kw)
+    eng.set_positions(s.coords)
+    eng.build_pairlist()
+    mrep = eng.minimize(max_iter=300, fmax_tol=10.0)
+    x0, _ = eng.md_state(velocities=False)
+    out = {"workload": "c4: %d atoms (320,000 flexible waters), 215 A box, PME 216^3, cutoff 10 A, skin 2 A, "
+                       "dt 0.5 fs, NVE, list rebuilt every 10 steps, %d measured steps after %d equilibration "
+                       "steps" % (s.natoms, steps, equil),
+           "minimiser": mrep}
+    for name, prec in (("mixed", abi.MDF_PREC_MIXED), ("fp64", abi.MDF_PREC_FP64)):
+        if prec != abi.MDF_PREC_MIXED:
+            eng.close()
+            eng = engine.Engine(flat, s.box, precision=prec, **kw)
+            eng.set_positions(x0)
+            eng.build_pairlist()
+        eng.md_init(s.mass, temperature=300.0, seed=1234)
+        eng.md_run(equil, 0.0005, chunk=10, rebuild_every=10)
+        rep, samp = eng.md_run(steps, 0.0005, chunk=10, rebuild_every=10)
+        tot = samp[:, 1] + samp[:, 2]
+        ke = float(samp[:, 2].mean())
+        out[name] = {"steps_per_s": rep["steps"] / rep["wall_s"], "ms_per_step": rep["wall_s"] / rep["steps"] * 1e3,
+                     "rebuilds": rep["rebuilds"], "e_total_first": float(tot[0]), "e_total_last": float(tot[-1]),
+                     "drift": float(tot[-1] - tot[0]), "drift_over_ke": float((tot[-1] - tot[0]) / ke),
+                     "e_total_std": float(tot.std()), "mean_ke": ke,
+                     "temperature_k": 2.0 * ke / (3.0 * s.natoms * 0.0019872041)}
+    eng.close()
+    out["mixed_over_fp64_speed"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
     return out
 
 
@@ -448,6 +493,9 @@ def main():
     batched = None
     if batch_members is not None:
         batched = batch_bench(dev, batch_members, stream)
+    dynamics = None
+    if rank == 0 and ws == 1 and not args.no_md:
+        dynamics = md_bench(dev)
 
     if rank == 0:
         line = {
@@ -475,6 +523,7 @@ def main():
             "fp64": fp64,
             "adjoint": adj,
             "batched": batched,
+            "dynamics": dynamics,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),

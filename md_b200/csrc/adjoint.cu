@@ -355,13 +355,26 @@ void backward(Ctx& c, const double* dL_dF, double dL_dE, double* dL_dq, double* 
                                                                       c.adj_vs_d.p);
     }
     const NBParams P = make_params(c);
+    // the reciprocal-space part runs on the side stream, concurrently with
+    // the pair adjoint (both only add into the fixed-point dq accumulators)
+    MDF_CUDA_TRY(cudaEventRecord(c.ev_fork, s));
+    MDF_CUDA_TRY(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
+    c.stream = c.side;
+    try {
+        pme_adjoint(c, gE, 1.0);
+    } catch (...) {
+        c.stream = s;
+        throw;
+    }
+    c.stream = s;
+    MDF_CUDA_TRY(cudaEventRecord(c.ev_join, c.side));
     if (mixed) launch_adj_pairs<float>(c, P, gE);
     else launch_adj_pairs<double>(c, P, gE);
     if (c.n_excl + c.n_14 > 0)
         k_adj_pairs_fp64<<<grid_blocks(c.n_excl + c.n_14, th), th, 0, s>>>(
             c.n_excl, c.excl_pairs.p, c.n_14, c.pairs14.p, c.p14_scale.p, c.xyz.p, c.q.p, c.adj_v.p, P, gE,
             c.adj_dq_atom.p, c.status.p);
-    pme_adjoint(c, gE, 1.0);
+    MDF_CUDA_TRY(cudaStreamWaitEvent(s, c.ev_join, 0));
     // d/dq_a of gE (E_self + E_net): -2 k alpha/sqrt(pi) q_a and -k pi Q / (V alpha^2)
     const double V = c.box[0] * c.box[1] * c.box[2];
     const double self_coef = gE * (-2.0 * c.p.coulomb_const * c.alpha / std::sqrt(M_PI));

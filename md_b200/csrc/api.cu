@@ -260,10 +260,10 @@ void eval_async_impl(Ctx& c, uint32_t flags)
         MDF_CUDA_TRY(cudaMemsetAsync(c.scal.p, 0, sizeof(unsigned long long) * NUM_SCAL, s));
         c.need_clear = false;
     }
-    // The PME chain only reads positions and charges and adds into the
-    // fixed-point accumulators, so it runs on the side stream while the main
-    // stream packs, prunes and runs the pair, exclusion and bonded kernels; the
-    // main stream waits for it before k_finalize.  With timing enabled every
+    // The exclusion, 1-4, bonded and PME kernels only read positions and
+    // charges and add into the fixed-point accumulators, so they run on the
+    // side stream while the main stream packs, prunes and runs the pair
+    // kernel; the main stream waits for them before k_finalize.  With timing enabled every
     // kernel runs on the main stream so the per-phase times are separable.
     const bool want_pme = phys || (flags & MDF_COMPUTE_PME_REFERENCE);
     const bool overlap = want_pme && !c.timing;
@@ -272,6 +272,8 @@ void eval_async_impl(Ctx& c, uint32_t flags)
         MDF_CUDA_TRY(cudaStreamWaitEvent(c.side, c.ev_fork, 0));
         c.stream = c.side;
         try {
+            launch_exclusions(c, energy);
+            launch_bonded(c, energy);
             launch_pme(c, energy);
         } catch (...) {
             c.stream = s;
@@ -293,10 +295,12 @@ void eval_async_impl(Ctx& c, uint32_t flags)
     }
     launch_nonbonded(c, energy);
     mark(c, "pairs");
-    launch_exclusions(c, energy);
-    mark(c, "excl_14");
-    launch_bonded(c, energy);
-    mark(c, "bonded");
+    if (!overlap) {
+        launch_exclusions(c, energy);
+        mark(c, "excl_14");
+        launch_bonded(c, energy);
+        mark(c, "bonded");
+    }
     if (want_pme && !overlap) {
         launch_pme(c, energy);
         c.have_pme_ref = !phys;

@@ -15,6 +15,8 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 REPO = os.path.dirname(PKG)
 LIB = os.path.join(PKG, "libmdf.so")
+HOST = os.path.join(PKG, "host")
+CLI = os.path.join(PKG, "mdb200")
 BUILD = os.path.join(PKG, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -28,7 +30,8 @@ def sources():
 
 def _digest():
     h = hashlib.sha256()
-    for p in sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [os.path.join(REPO, "include", "mdf.h")]:
+    for p in sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [os.path.join(REPO, "include", "mdf.h")] + \
+            sorted(glob.glob(os.path.join(HOST, "*.?pp"))):
         with open(p, "rb") as f:
             h.update(p.encode())
             h.update(f.read())
@@ -57,9 +60,22 @@ def build(force=False, verbose=False, jobs=8):
     out = subprocess.run(link, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("link failed:\n" + out.stdout + out.stderr)
+    build_host()
     with open(stamp, "w") as f:
         f.write(dig)
     return LIB
+
+
+def build_host():
+    """The C++ host (md_b200/host): prmtop/rst7 reader, mdb200::System and the
+    mdb200 command line, linked against libmdf.so (rpath to this directory)."""
+    srcs = sorted(glob.glob(os.path.join(HOST, "*.cpp")))
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(REPO, "include"), "-o", CLI] + srcs + \
+          ["-L" + PKG, "-lmdf", "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64", "-lcudart"]
+    out = subprocess.run(cmd, capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("host build failed:\n" + " ".join(cmd) + "\n" + out.stdout + out.stderr)
+    return CLI
 
 
 def _drain(procs, verbose):

@@ -1,0 +1,75 @@
+"""The C++ host (md_b200/host): the Amber prmtop/rst7 reader and the
+flattening with the REFERENCE/PHYSICAL switch produce exactly the arrays of the
+Python host (md_b200/topology.py) on the same files; and the mdb200 command
+line, the reference's `./md <prmtop> <coords>` on the GPU, prints the
+reference's own energies (golden O1 fixture) for the same files."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from md_b200 import abi, build, engine, synth
+from tests import helpers as H
+
+CLI = build.CLI
+ARRAYS = {"charge": np.float64, "type": np.int32, "nb_index": np.int32, "lj_a": np.float64, "lj_b": np.float64,
+          "lj14_a": np.float64, "lj14_b": np.float64, "bond_atoms": np.int32, "bond_k": np.float64,
+          "bond_r0": np.float64, "ub_atoms": np.int32, "ub_k": np.float64, "ub_r0": np.float64,
+          "angle_atoms": np.int32, "angle_k": np.float64, "angle_theta0": np.float64,
+          "dihedral_atoms": np.int32, "dihedral_k": np.float64, "dihedral_n": np.float64,
+          "dihedral_phase": np.float64, "improper_atoms": np.int32, "improper_k": np.float64,
+          "improper_phase": np.float64, "cmap_atoms": np.int32, "cmap_set": np.int32, "cmap_coeff": np.float64,
+          "excl_pairs": np.int32, "pairs14": np.int32, "scee14": np.float64, "scnb14": np.float64}
+
+
+def _files(cfg, sentinels, tmp_path):
+    s = H.system(cfg, sentinels)
+    return s, synth.write_files(s, str(tmp_path), stem=cfg)
+
+
+@pytest.mark.parametrize("cfg,sent", [("tiny", False), ("tiny", True), ("small", False)])
+@pytest.mark.parametrize("sem", [abi.MDF_SEM_REFERENCE, abi.MDF_SEM_PHYSICAL])
+def test_cpp_reader_matches_python_flatten(cfg, sent, sem, tmp_path):
+    engine.library()   # builds libmdf.so and the mdb200 command line
+    s, (prm, rst) = _files(cfg, sent, tmp_path)
+    out = tmp_path / "dump"
+    out.mkdir()
+    args = [CLI, prm, rst, "--dump-topology", str(out)] + (["--physical"] if sem == abi.MDF_SEM_PHYSICAL else [])
+    subprocess.run(args, check=True, capture_output=True)
+    flat = H.flat(s, sem, engine.cmap_coefficients)
+    for name, dt in ARRAYS.items():
+        got = np.fromfile(out / (name + ".bin"), dtype=dt)
+        want = np.asarray(getattr(flat, name)).reshape(-1).astype(dt)
+        assert got.shape == want.shape, (name, got.shape, want.shape)
+        assert np.array_equal(got, want), name
+
+
+def _energies(text):
+    out = {}
+    for key, label in (("bond", "Bond:"), ("angle", "Angle:"), ("dihedral", "CosineDihedral:"),
+                       ("ub", "Urey-Bradley:"), ("improper", "Impropers:"), ("cmap", "CMAP energy:"),
+                       ("vdw", "VDW:"), ("ee", "EE:"), ("ee_pairlist", "EE pairlist:"),
+                       ("ee_cutoff", "EE_energy_pairlist_cutoff_"), ("ee_direct", "EE_energy_pairlist_ewald_direct_"),
+                       ("ee_self", "EE_energy_pairlist_ewald_self_")):
+        m = re.search(r"^" + re.escape(label) + r"\s*(\S+)", text, re.M)
+        out[key] = float(m.group(1))
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["tiny", "tiny_sentinel"])
+def test_cli_prints_the_references_energies(case, tmp_path):
+    g = H.golden(case)
+    m = g["meta"]
+    s, (prm, rst) = _files(m["config"], m["sentinels"], tmp_path)
+    fo = tmp_path / "forces.bin"
+    grid = [str(k) for k in m["grid"]]
+    r = subprocess.run([CLI, prm, rst, "--tol", str(m["tol"]), "--grid"] + grid + ["--forces-out", str(fo)],
+                       check=True, capture_output=True, text=True)
+    E = _energies(r.stdout)
+    for k, v in E.items():
+        assert H.rel(v, g["energies"][k]) < 1e-9, (k, v, g["energies"][k])
+    F = np.fromfile(fo, dtype=np.float64).reshape(-1, 3)
+    H.check_forces_vs_golden(F, g, 1e-9, "forces")

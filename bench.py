@@ -281,12 +281,24 @@ def _batch_member(k):
     return sysm, flat
 
 
-def make_batch_workload(n=256):
-    """c3's 256 uneven systems, generated in spawned worker processes."""
+def batch_share(rank, ws, n=256):
+    """This rank's systems of the c3 batch: a cost-balanced greedy partition
+    (md_b200.shard), the same on every rank."""
+    from md_b200 import shard, synth
+    costs = []
+    for L, nres in synth._batch_dims(n, 1003):
+        nat = 3 * max(10, int(0.1 * L ** 3 / 3.0) - nres * 10 // 3) + 10 * nres
+        g = synth.smooth_grid_size(L, 1.0)
+        costs.append(shard.system_cost(nat, (g, g, g)))
+    return shard.partition(costs, ws)[rank]
+
+
+def make_batch_workload(indices):
+    """The given systems of c3's 256, generated in spawned worker processes."""
     import concurrent.futures as cf
     import multiprocessing as mp
     with cf.ProcessPoolExecutor(max_workers=min(8, os.cpu_count() or 1), mp_context=mp.get_context("spawn")) as ex:
-        return list(ex.map(_batch_member, range(n)))
+        return list(ex.map(_batch_member, list(indices)))
 
 
 def batch_bench(dev, members, stream, steps=20):
@@ -347,8 +359,8 @@ def main():
         run_reference_arm(args, rank)
         return
     batch_members = None
-    if rank == 0 and ws == 1 and not args.no_batch:
-        batch_members = make_batch_workload()
+    if not args.no_batch:
+        batch_members = make_batch_workload(batch_share(rank, ws))
     import torch
     import torch.distributed as dist
     from md_b200 import abi, engine
@@ -493,6 +505,15 @@ def main():
     batched = None
     if batch_members is not None:
         batched = batch_bench(dev, batch_members, stream)
+        if ws > 1:
+            # systems are independent: each rank ran its share; the batch time is the slowest rank's
+            from md_b200 import shard
+            ms = shard.max_over_ranks(batched["ms_per_batch"], device=dev)
+            e2e_ms = shard.max_over_ranks(batched["e2e_ms_per_batch"], device=dev)
+            batched.update({"workload": "c3: 256 systems sharded over %d GPUs by estimated cost (this line: "
+                                        "all ranks, slowest rank's time)" % ws,
+                            "ms_per_batch": ms, "frames_per_s": 256 / (ms * 1e-3),
+                            "e2e_ms_per_batch": e2e_ms, "e2e_frames_per_s": 256 / (e2e_ms * 1e-3)})
     dynamics = None
     if rank == 0 and ws == 1 and not args.no_md:
         dynamics = md_bench(dev)

@@ -51,6 +51,11 @@ GRID = (100, 100, 100)
 FLOPS_PER_PAIR = 60.0
 
 
+# DRAM bytes (read + write) of one k_pairs_f32 launch at c1, from the ncu
+# capture summarised in profiles/kernels_c1_mixed.md
+PAIR_TRAFFIC_BYTES = 20.0e6
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -534,7 +539,9 @@ def main():
                        "prune": "every evaluation, exact (margin 0)",
                        "pairs_in_cutoff": info["pairs_in_cutoff"]},
             "roofline": {"kernel": "k_pairs (LJ + erfc Ewald pair kernel)", "bound": "fp32", "achieved": achieved,
-                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": PAIR_TRAFFIC_BYTES,
+                         "traffic_source": "dram__bytes read+write per launch, one ncu capture of the same "
+                                           "workload (profiles/kernels_c1_mixed.md); algorithmic ~18 MB",
                          "peak_source": "measured FP32 FMA throughput of this GPU (mdf_probe_fma_tflops)",
                          "work": "%g FP32 flops x %d pairs in cutoff per launch" % (FLOPS_PER_PAIR,
                                                                                   info["pairs_in_cutoff"])},

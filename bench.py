@@ -51,8 +51,8 @@ GRID = (100, 100, 100)
 FLOPS_PER_PAIR = 60.0
 
 
-# DRAM bytes (read + write) of one k_pairs_f32 launch at c1, from the ncu
-# capture summarised in profiles/kernels_c1_mixed.md
+# DRAM bytes (read + write) of one k_pairs_f32 launch at c1, from one ncu
+# capture of `bench.py --profile c1` (dram__bytes.sum.per_second x duration)
 PAIR_TRAFFIC_BYTES = 20.0e6
 
 
@@ -541,7 +541,7 @@ def main():
             "roofline": {"kernel": "k_pairs (LJ + erfc Ewald pair kernel)", "bound": "fp32", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": PAIR_TRAFFIC_BYTES,
                          "traffic_source": "dram__bytes read+write per launch, one ncu capture of the same "
-                                           "workload (profiles/kernels_c1_mixed.md); algorithmic ~18 MB",
+                                           "workload (bench.py --profile c1); algorithmic ~18 MB",
                          "peak_source": "measured FP32 FMA throughput of this GPU (mdf_probe_fma_tflops)",
                          "work": "%g FP32 flops x %d pairs in cutoff per launch" % (FLOPS_PER_PAIR,
                                                                                   info["pairs_in_cutoff"])},

@@ -201,6 +201,14 @@ int mdf_forces_device(mdf_ctx *ctx, double *d_forces_out);
  * the last evaluation that asked for MDF_COMPUTE_PME_REFERENCE. */
 int mdf_get_pme_forces(mdf_ctx *ctx, double *forces_out);
 
+/* Diagnostic: the PME mesh of the last evaluation.  grid_out (may be NULL)
+ * receives K0, K1, K2; charge_grid [K0*K1*K2] the spread charges Q (x-major,
+ * z fastest) and potential_grid [K0*K1*K2] the potential C*Q the gather reads
+ * (the hand-written FFT's convolution with the influence function, unscaled
+ * inverse transform), either may be NULL.  Lets a caller check the FFT chain
+ * against another FFT (the tests use cuFFT through torch.fft). */
+int mdf_pme_grids(mdf_ctx *ctx, int32_t grid_out[3], double *charge_grid, double *potential_grid);
+
 /* Use an existing CUDA stream (cudaStream_t passed as void*); NULL = the
  * context's own stream. */
 int mdf_set_stream(mdf_ctx *ctx, void *stream);

@@ -622,6 +622,35 @@ int mdf_forces_device(mdf_ctx* ctx, double* d_forces_out)
     });
 }
 
+int mdf_pme_grids(mdf_ctx* ctx, int32_t grid_out[3], double* charge_grid, double* potential_grid)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        if (grid_out)
+            for (int d = 0; d < 3; ++d) grid_out[d] = c.K[d];
+        if (!charge_grid && !potential_grid) return;
+        if (!c.pending) throw ApiError(MDF_ERR_STATE, "no evaluation yet");
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        const size_t n = (size_t)c.K[0] * c.K[1] * c.K[2];
+        if (charge_grid) {
+            std::vector<long long> q(n);
+            MDF_CUDA_TRY(cudaMemcpy(q.data(), c.qgrid.p, sizeof(long long) * n, cudaMemcpyDeviceToHost));
+            for (size_t i = 0; i < n; ++i) charge_grid[i] = (double)q[i] * GRID_ISCALE;
+        }
+        if (potential_grid) {
+            if (c.rgrid_f.p) {
+                std::vector<float> r(n);
+                MDF_CUDA_TRY(cudaMemcpy(r.data(), c.rgrid_f.p, sizeof(float) * n, cudaMemcpyDeviceToHost));
+                for (size_t i = 0; i < n; ++i) potential_grid[i] = r[i];
+            } else {
+                MDF_CUDA_TRY(cudaMemcpy(potential_grid, c.rgrid_d.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+            }
+        }
+    });
+}
+
 int mdf_get_pme_forces(mdf_ctx* ctx, double* forces_out)
 {
     if (!ctx || !forces_out) return MDF_ERR_INVALID;

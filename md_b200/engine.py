@@ -25,7 +25,7 @@ EXPORTS = [
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
-    "mdf_minimize", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
+    "mdf_pme_grids", "mdf_minimize", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
 
@@ -64,6 +64,7 @@ def library(path=None):
     lib.mdf_fetch.argtypes = [C.c_void_p, dp, C.POINTER(abi.mdf_energies)]
     lib.mdf_forces_device.argtypes = [C.c_void_p, C.c_void_p]
     lib.mdf_get_pme_forces.argtypes = [C.c_void_p, dp]
+    lib.mdf_pme_grids.argtypes = [C.c_void_p, C.POINTER(C.c_int32), dp, dp]
     lib.mdf_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     lib.mdf_pairlist_info.argtypes = [C.c_void_p] + [C.POINTER(C.c_int64)] * 4
     lib.mdf_enable_timing.argtypes = [C.c_void_p, C.c_int]
@@ -311,6 +312,17 @@ class Engine:
         self._check(self.lib.mdf_compute_bonded_noalloc(self.h, flags, C.c_void_p(forces_ptr or None), C.byref(e)),
                     "compute_bonded_noalloc")
         return e.as_dict() if energy else None
+
+    def pme_grids(self):
+        """(Q, C*Q) of the last evaluation, each [K0, K1, K2]."""
+        k = (C.c_int32 * 3)()
+        self._check(self.lib.mdf_pme_grids(self.h, k, None, None), "pme_grids")
+        K = tuple(k)
+        q = np.zeros(K)
+        p = np.zeros(K)
+        dp_ = C.POINTER(C.c_double)
+        self._check(self.lib.mdf_pme_grids(self.h, k, q.ctypes.data_as(dp_), p.ctypes.data_as(dp_)), "pme_grids")
+        return q, p
 
     def pme_forces(self):
         f = np.zeros((self.natoms, 3))

@@ -90,6 +90,7 @@ void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b)
     const int ntp = c.ntp;
     std::vector<double2> ab(ntp * ntp, make_double2(0, 0)), ab14(ntp * ntp, make_double2(0, 0));
     std::vector<float2> abf(ntp * ntp, make_float2(0, 0));
+    std::vector<float4> ab4(ntp * ntp, make_float4(0, 0, 0, 0));
     std::vector<int> valid(ntp * ntp, 0), idx(ntp * ntp, -1);
     for (int i = 0; i < c.ntypes; ++i)
         for (int j = 0; j < c.ntypes; ++j) {
@@ -98,12 +99,15 @@ void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b)
             const int tp = i * ntp + j;
             ab[tp] = make_double2(lj_a[nb - 1], lj_b[nb - 1]);
             abf[tp] = make_float2((float)lj_a[nb - 1], (float)lj_b[nb - 1]);
+            ab4[tp] = make_float4((float)lj_a[nb - 1], (float)lj_b[nb - 1], (float)(12.0 * lj_a[nb - 1]),
+                                  (float)(6.0 * lj_b[nb - 1]));
             ab14[tp] = make_double2(c.h_lj14a[nb - 1], c.h_lj14b[nb - 1]);
             valid[tp] = 1;
             idx[tp] = nb - 1;
         }
     c.ljAB.upload(ab.data(), ab.size(), s);
     c.ljAB_f.upload(abf.data(), abf.size(), s);
+    c.ljAB4_f.upload(ab4.data(), ab4.size(), s);
     c.lj14AB.upload(ab14.data(), ab14.size(), s);
     c.ljvalid.upload(valid.data(), valid.size(), s);
     c.nbidx.upload(idx.data(), idx.size(), s);
@@ -505,7 +509,7 @@ void mdf_destroy(mdf_ctx* ctx)
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto& e : c.evpool) cudaEventDestroy(e);
-    c.q.release(); c.type.release(); c.ljAB.release(); c.ljAB_f.release(); c.lj14AB.release(); c.ljvalid.release();
+    c.q.release(); c.type.release(); c.ljAB.release(); c.ljAB4_f.release(); c.ljAB_f.release(); c.lj14AB.release(); c.ljvalid.release();
     c.bond_atoms.release(); c.ub_atoms.release(); c.angle_atoms.release(); c.dih_atoms.release();
     c.imp_atoms.release(); c.cmap_atoms.release(); c.cmap_set.release(); c.bond_par.release(); c.ub_par.release();
     c.angle_par.release(); c.imp_par.release(); c.dih_par.release(); c.cmap_coeff.release();

@@ -122,6 +122,7 @@ struct Ctx {
     DevBuf<int> type;          // [N]
     DevBuf<double2> ljAB;      // [(ntypes+1)^2] pair table (A,B); last row/col = padding type
     DevBuf<float2> ljAB_f;
+    DevBuf<float4> ljAB4_f;        // (A, B, 12A, 6B) per type pair, FP32 pair kernel
     DevBuf<double2> lj14AB;    // same indexing, 1-4 tables
     DevBuf<int> ljvalid;       // [(ntypes+1)^2] nb != 0
     int ntp = 0;               // ntypes + 1 (padding type appended)

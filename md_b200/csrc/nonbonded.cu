@@ -241,25 +241,57 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
 //    bit t;
 //  * the pair arithmetic is branch-free (inactive pairs are selected out);
 //  * energies are summed in FP32 per entry and in FP64 across entries.
+// 2^x on the special-function unit (PTX ex2.approx.ftz: relative error ~2^-22).
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Constants of the FP32 pair kernel, folded on the host.
+struct PairConstF {
+    float rc2;
+    float kex;        // -alpha^2 log2(e): exp(-alpha^2 r^2) = 2^(kex r^2)
+    float pa;         // 0.3275911 alpha (A&S 7.1.26 argument)
+    float two_a_spi;  // 2 alpha / sqrt(pi)
+    float inv_sw, rsw_inv;          // 1/(rc - rsw), rsw/(rc - rsw)
+    float d30, d60;                 // -30, 60 times inv_sw (dS/dr = x^2 (d30 + x (d60 + x d30)))
+    float uc6, uc12, rcf, rc2f;     // force-shifted LJ
+};
+
+// The mixed-precision production kernel (PHYSICAL semantics).  Same warp
+// layout as k_pairs; differences that matter for speed and accuracy:
+//  * cluster centres lie on a 2^-k grid and are exact in FP32, so the centre
+//    difference is exact and the image offset enters as hi + lo: the pair
+//    vector carries ~1e-6 A rounding, not the 1e-5 A of raw FP32 coordinates;
+//  * the lane's row of the 8x8 mask is rotated once per entry so step t tests
+//    bit t;
+//  * the pair arithmetic is branch-free (inactive pairs are selected out at
+//    the end, so a masked pair at r = 0 only produces values that are dropped);
+//  * the LJ table holds (A, B, 12A, 6B) per type pair, in shared memory when it
+//    fits (lj_smem), and the Gaussian uses 2^(kex r^2) on the SFU;
+//  * energies are summed in FP32 per entry and in FP64 across entries.
 template <bool ENERGY, bool SWITCH, bool COUNT>
 __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
     int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
-    const int* __restrict__ stype, const float4* __restrict__ centerf, const float2* __restrict__ ljAB, NBParams P,
-    ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots, unsigned long long* __restrict__ acc,
-    unsigned long long* __restrict__ npairs, unsigned* st)
+    const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp,
+    int lj_smem, float kc, PairConstF K, ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots,
+    unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs, unsigned* st)
 {
+    extern __shared__ float4 s_lj[];
     __shared__ float4 sx[NB_WARPS][4][CLUSTER + 1];
     __shared__ int stj[NB_WARPS][4][CLUSTER];
     __shared__ float sh[27][6];
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
+    if (lj_smem)
+        for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj[k] = lj4[k];
     __syncthreads();
+    const float4* __restrict__ ljt = lj_smem ? s_lj : lj4;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int w = blockIdx.x * (blockDim.x >> 5) + wib;
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
-    const float rc2 = (float)P.rc2, rsw = (float)P.rsw, inv_sw = (float)P.inv_sw, alpha = (float)P.alpha;
-    const float two_a_spi = (float)(2.0 * P.alpha / 1.7724538509055160273);
-    const float uc6 = (float)P.ucut_pow6, uc12 = (float)P.ucut_pow12, rcf = (float)P.rc, rc2f = (float)P.rc2;
     double e_lj = 0, e_dir = 0;
     int npc = 0;
     float fix = 0.f, fiy = 0.f, fiz = 0.f;
@@ -268,9 +300,10 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
         const ILRange L = ilist[w];
         const int I = L.i;
         const float4 xi = xq[I * CLUSTER + ii];
-        const int trow = stype[I * CLUSTER + ii] * P.ntp;
+        const int trow = stype[I * CLUSTER + ii] * ntp;
         const float4 cI = centerf[I];
-        const float qik = (float)P.kc * xi.w;
+        const float qik = kc * xi.w;
+        const float qik2 = qik * K.two_a_spi;
         const int rot_src = (lane & ~7) | ((ii + 1) & 7);
         for (int b = 0; b < L.count; b += 4) {
             const int e = b + jslot;
@@ -297,40 +330,37 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
                 const int jj = (ii + t) & 7;
                 const float4 xj = sx[wib][jslot][jj];
                 const float dx = xix - xj.x, dy = xiy - xj.y, dz = xiz - xj.z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                const bool on = ((rot >> t) & 1u) && r2 <= rc2;
-                const float r2s = on ? r2 : 1.0f;
-                const float rinv = rsqrtf(r2s);
-                const float r = r2s * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
-                const float2 ab = __ldg(&ljAB[trow + stj[wib][jslot][jj]]);
-                float U = (ab.x * rinv6 - ab.y) * rinv6;
-                float G = (12.f * ab.x * rinv6 - 6.f * ab.y) * rinv6 * rinv2;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
+                const float rinv = rsqrtf(r2);
+                const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
+                const float4 ab = ljt[trow + stj[wib][jslot][jj]];      // A, B, 12A, 6B
+                float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
+                float G = (rinv6 * rinv2) * fmaf(ab.z, rinv6, -ab.w);
                 if (SWITCH) {
-                    const float x = fmaxf(0.f, (r - rsw) * inv_sw), x2 = x * x, x3 = x2 * x;
-                    const float S = 1.f + x3 * (-10.f + x * (15.f - 6.f * x));
-                    const float dS = x2 * (-30.f + x * (60.f - 30.f * x)) * inv_sw;
-                    G = S * G - U * dS * rinv;
+                    const float x = fmaxf(0.f, fmaf(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
+                    const float S = fmaf(x2 * x, fmaf(x, fmaf(x, -6.f, 15.f), -10.f), 1.f);
+                    const float dSr = x2 * fmaf(x, fmaf(x, K.d30, K.d60), K.d30) * rinv;   // dS/dr / r
+                    G = fmaf(S, G, -U * dSr);
                     U = U * S;
                 } else {
-                    const float uc = ab.x * uc12 - ab.y * uc6;
-                    const float gc = (12.f * ab.x * uc12 - 6.f * ab.y * uc6) / rc2f;
-                    U = U - uc + (r - rcf) * (gc * rcf);
-                    G = G - gc * rcf * rinv;
+                    const float uc = ab.x * K.uc12 - ab.y * K.uc6;
+                    const float gc = (ab.z * K.uc12 - ab.w * K.uc6) / K.rc2f;
+                    U = U - uc + (r - K.rcf) * (gc * K.rcf);
+                    G = G - gc * K.rcf * rinv;
                 }
-                const float qq = qik * xj.w;
-                const float ar = alpha * r;
-                const float ex = __expf(-ar * ar);
-                const float erfcv = erfc_as(__fdividef(1.0f, 1.0f + 0.3275911f * ar), ex);
-                const float ec = qq * erfcv * rinv;
-                float g = G + (ec + qq * two_a_spi * ex) * rinv2;
+                const float ex = ex2_approx(K.kex * r2);
+                const float erfcv = erfc_as(__fdividef(1.0f, fmaf(K.pa, r, 1.0f)), ex);
+                const float ec = (qik * xj.w) * erfcv * rinv;
+                float g = fmaf(fmaf(qik2 * xj.w, ex, ec), rinv2, G);
                 g = on ? g : 0.f;
                 if (ENERGY) {
                     el += on ? U : 0.f;
                     ed += on ? ec : 0.f;
                 }
                 if (COUNT) npc += on ? 1 : 0;
-                fix += g * dx; fiy += g * dy; fiz += g * dz;
-                fjx -= g * dx; fjy -= g * dy; fjz -= g * dz;
+                fix = fmaf(g, dx, fix); fiy = fmaf(g, dy, fiy); fiz = fmaf(g, dz, fiz);
+                fjx = fmaf(-g, dx, fjx); fjy = fmaf(-g, dy, fjy); fjz = fmaf(-g, dz, fjz);
                 fjx = __shfl_sync(FULL, fjx, rot_src);
                 fjy = __shfl_sync(FULL, fjy, rot_src);
                 fjz = __shfl_sync(FULL, fjz, rot_src);
@@ -574,16 +604,34 @@ static void launch_pairs_f32(Ctx& c, bool energy)
 {
     NBParams P = make_params(c);
     ShiftTable sh = make_shift_table(c);
+    PairConstF K;
+    K.rc2 = (float)P.rc2;
+    K.kex = (float)(-P.alpha * P.alpha * 1.4426950408889634074);
+    K.pa = (float)(0.3275911 * P.alpha);
+    K.two_a_spi = (float)(2.0 * P.alpha / 1.7724538509055160273);
+    K.inv_sw = (float)P.inv_sw;
+    K.rsw_inv = (float)(P.rsw * P.inv_sw);
+    K.d30 = (float)(-30.0 * P.inv_sw);
+    K.d60 = (float)(60.0 * P.inv_sw);
+    K.uc6 = (float)P.ucut_pow6;
+    K.uc12 = (float)P.ucut_pow12;
+    K.rcf = (float)P.rc;
+    K.rc2f = (float)P.rc2;
+    const int ntp2 = c.ntp * c.ntp;
+    const size_t lj_bytes = sizeof(float4) * (size_t)ntp2;
+    const int lj_smem = lj_bytes <= 40 * 1024 ? 1 : 0;
+    const size_t dyn = lj_smem ? lj_bytes : 0;
     const int wpb = pair_warps(c);
     int nb = grid_blocks(c.n_clusters, wpb);
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
     const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     const bool count = begin_pair_count(c);
-#define MDF_PF32(E, S, K)                                                                                           \
-    k_pairs_f32<E, S, K><<<nb, 32 * wpb, 0, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p,            \
-                                                          c.centerf.p, c.ljAB_f.p, P, sh, c.f_slot.p, c.n_slots,   \
-                                                          c.acc.p, c.npairs_dev.p, c.status.p)
+#define MDF_PF32(E, S, K_)                                                                                     \
+    k_pairs_f32<E, S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p,       \
+                                                           c.centerf.p, c.ljAB4_f.p, c.ntp, lj_smem,              \
+                                                           (float)P.kc, K, sh, c.f_slot.p, c.n_slots, c.acc.p,   \
+                                                           c.npairs_dev.p, c.status.p)
 #define MDF_PF32_K(E, S) \
     do { if (count) MDF_PF32(E, S, true); else MDF_PF32(E, S, false); } while (0)
     if (energy) {

@@ -138,13 +138,14 @@ static void md_drop_graph(Ctx& c)
     c.md_graph = nullptr;
 }
 
-static void md_capture(Ctx& c, int steps, double dt)
+// Record one chunk of `steps` steps into a new graph (not instantiated).
+static cudaGraph_t md_record(Ctx& c, int steps, double dt)
 {
-    md_drop_graph(c);
     cudaStream_t s = c.stream;
     const int th = 256;
     const bool timing = c.timing;
     c.timing = false;   // no per-phase events inside a captured chunk
+    cudaGraph_t g = nullptr;
     MDF_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     try {
         k_md_reset<<<1, 32, 0, s>>>(c.md_dev, (1u << 0) | (1u << 2) | (1u << 4));
@@ -161,32 +162,64 @@ static void md_capture(Ctx& c, int steps, double dt)
         MDF_CUDA_TRY(cudaGetLastError());
     } catch (...) {
         c.timing = timing;
-        cudaGraph_t g = nullptr;
         cudaStreamEndCapture(s, &g);
         if (g) cudaGraphDestroy(g);
         throw;
     }
     c.timing = timing;
-    MDF_CUDA_TRY(cudaStreamEndCapture(s, &c.md_graph));
+    MDF_CUDA_TRY(cudaStreamEndCapture(s, &g));
+    return g;
+}
+
+// A ready graph for `steps` steps: instantiate on first use; after a list
+// rebuild re-record and update the instantiated graph in place (same shape,
+// new sizes and pointers), instantiating afresh only if the update is refused.
+static void md_prepare(Ctx& c, int steps, double dt)
+{
+    if (c.md_exec && c.md_graph_steps == steps && c.md_graph_dt == dt && !c.md_stale) return;
+    cudaGraph_t g = md_record(c, steps, dt);
+    if (c.md_exec && c.md_graph_steps == steps && c.md_graph_dt == dt) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(c.md_exec, g, &info) == cudaSuccess) {
+            if (c.md_graph) cudaGraphDestroy(c.md_graph);
+            c.md_graph = g;
+            c.md_stale = false;
+            return;
+        }
+        (void)cudaGetLastError();   // the refusal is not an error here
+    }
+    md_drop_graph(c);
+    c.md_graph = g;
     MDF_CUDA_TRY(cudaGraphInstantiate(&c.md_exec, c.md_graph, 0));
     c.md_graph_steps = steps;
     c.md_graph_dt = dt;
+    c.md_stale = false;
 }
 
-static void md_rebuild(Ctx& c)
+// New pairlist at the current positions.  With need_forces the forces are
+// evaluated too (start of a run); otherwise the last chunk's forces, at these
+// same positions, stay in place for the next half kick.
+static void md_rebuild(Ctx& c, bool need_forces)
 {
     build_pairlist(c);
     MDF_CUDA_TRY(cudaMemcpyAsync(c.md_xref.p, c.xyz.p, sizeof(double) * 3 * (size_t)c.N, cudaMemcpyDeviceToDevice,
                                  c.stream));
-    // forces at the current positions for the first half kick; also clears
-    // the accumulators and counts pairs outside any capture
-    eval_async_impl(c, MDF_COMPUTE_FORCES);
+    if (need_forces) {
+        eval_async_impl(c, MDF_COMPUTE_FORCES);   // also clears the accumulators and counts pairs
+    } else {
+        // the slot layout changed: clear the accumulators here rather than in
+        // every replay of the next graph; pairs are not counted inside graphs
+        MDF_CUDA_TRY(cudaMemsetAsync(c.f_slot.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.n_slots, c.stream));
+        MDF_CUDA_TRY(cudaMemsetAsync(c.f_atom.p, 0, sizeof(unsigned long long) * 3 * (size_t)c.N, c.stream));
+        c.need_clear = false;
+        c.count_next = false;
+    }
     k_md_reset<<<1, 32, 0, c.stream>>>(c.md_dev, 1u << 1);   // displacement since this build
     MDF_CUDA_TRY(cudaGetLastError());
     MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    check_host_status(c);
+    if (need_forces) check_host_status(c);
     c.md_host[1] = 0;
-    md_drop_graph(c);
+    c.md_stale = true;
 }
 
 void md_init(Ctx& c, const double* masses, const double* vel, double temperature, uint64_t seed)
@@ -232,7 +265,8 @@ void md_init(Ctx& c, const double* masses, const double* vel, double temperature
     double vmax2 = 3.0 * v2;   // bound until the first chunk has measured it
     memcpy(&c.md_host[4], &vmax2, sizeof(double));
     c.md_ready = true;
-    md_rebuild(c);
+    md_drop_graph(c);
+    md_rebuild(c, true);
 }
 
 void md_run(Ctx& c, long long nsteps, double dt, int chunk, int rebuild_every, double* samples, long long cap,
@@ -254,11 +288,11 @@ void md_run(Ctx& c, long long nsteps, double dt, int chunk, int rebuild_every, d
         const double dnow = std::sqrt(bits_to_double(c.md_host[1]));
         const double reach = 2.0 * steps * dt * std::sqrt(bits_to_double(c.md_host[4]));
         if (due || dnow + reach > half_skin) {
-            md_rebuild(c);
+            md_rebuild(c, false);
             since_build = 0;
             ++r.rebuilds;
         }
-        if (!c.md_exec || c.md_graph_steps != steps || c.md_graph_dt != dt) md_capture(c, steps, dt);
+        md_prepare(c, steps, dt);
         MDF_CUDA_TRY(cudaGraphLaunch(c.md_exec, c.stream));
         MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
         check_host_status(c);

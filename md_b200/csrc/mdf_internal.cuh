@@ -239,6 +239,7 @@ struct Ctx {
     cudaGraphExec_t md_exec = nullptr;
     int md_graph_steps = 0;
     double md_graph_dt = 0.0;
+    bool md_stale = false;               // list rebuilt since the graph was recorded
 
     // timing
     bool timing = false;

@@ -14,6 +14,8 @@ E_INDEX = {n: i for i, n in enumerate(E_NAMES)}
 MDF_E_COUNT = len(E_NAMES)
 
 MDF_OK, MDF_ERR_INVALID, MDF_ERR_CUDA, MDF_ERR_CAPACITY = 0, 1, 2, 3
+MDF_ERR_NONFINITE, MDF_ERR_OVERFLOW, MDF_ERR_TIMEOUT, MDF_ERR_STATE = 4, 5, 6, 7
+MDF_ERR_NOMEM, MDF_ERR_UNSUPPORTED = 8, 9
 MDF_NOALLOC_MAX_ATOMS = 131072   # include/mdf.h: scratch limit of mdf_compute_bonded_noalloc
 MDF_COMPUTE_ENERGY = 1
 MDF_COMPUTE_FORCES = 2
@@ -56,7 +58,7 @@ class mdf_params(C.Structure):
         ("ewald_tol", C.c_double), ("ewald_alpha", C.c_double), ("grid", C.c_int32 * 3),
         ("pme_order", C.c_int32), ("coulomb_const", C.c_double), ("device", C.c_int32),
         ("prune_every", C.c_int32), ("prune_margin", C.c_double), ("pair_warps", C.c_int32),
-        ("fft_lines", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("fft_lines", C.c_int32), ("pme_tile", C.c_int32), ("reserved", C.c_int32 * 1),
     ]
 
 

@@ -153,14 +153,7 @@ typedef struct {
      * most FFT lines per block (1, 2 or 4; 0 = 4). */
     int32_t pair_warps;
     int32_t fft_lines;
-    /* PHYSICAL PME spread and gather: grid lines in y per block of the
-     * shared-memory tile kernels (1, 2, 4 or 8, halved while a tile exceeds
-     * 100 KB; 0 = 4), or -1 for the per-atom kernels with global atomics.
-     * The tile kernels find atoms through the pairlist's columns and need
-     * every atom within half the skin + 1 A of its position at the last
-     * build (else MDF_ERR_STATE); results do not depend on the choice. */
-    int32_t pme_tile;
-    int32_t reserved[1];
+    int32_t reserved[2];
 } mdf_params;
 
 /* Flags for mdf_compute. */

@@ -58,7 +58,7 @@ class mdf_params(C.Structure):
         ("ewald_tol", C.c_double), ("ewald_alpha", C.c_double), ("grid", C.c_int32 * 3),
         ("pme_order", C.c_int32), ("coulomb_const", C.c_double), ("device", C.c_int32),
         ("prune_every", C.c_int32), ("prune_margin", C.c_double), ("pair_warps", C.c_int32),
-        ("fft_lines", C.c_int32), ("pme_tile", C.c_int32), ("reserved", C.c_int32 * 1),
+        ("fft_lines", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 

@@ -359,9 +359,6 @@ void host_energies(const Ctx& c, uint32_t flags, mdf_energies* e_out)
 void check_host_status(const Ctx& c)
 {
     const unsigned st = (unsigned)c.h_scal[NUM_ACC + 1];
-    if (st & ST_STALE_LIST)   // first: a stale list is the cause of whatever else went wrong
-        throw ApiError(MDF_ERR_STATE, "an atom moved more than half the skin + 1 A since the pairlist was built; "
-                                      "rebuild it");
     if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite force or energy contribution");
     if (st & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "fixed-point accumulator range exceeded");
 }
@@ -474,7 +471,6 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         if (!(c.p.cutoff > 0) || c.p.skin < 0) throw ApiError(MDF_ERR_INVALID, "bad cutoff or skin");
         if (c.p.switch_radius > 0 && !(c.p.switch_radius < c.p.cutoff))
             throw ApiError(MDF_ERR_INVALID, "lj_switch must be < lj_cutoff");
-        if (c.p.pme_tile < -1 || c.p.pme_tile > 8) throw ApiError(MDF_ERR_INVALID, "pme_tile must be -1 .. 8");
         int ndev = 0;
         cudaError_t e = cudaGetDeviceCount(&ndev);
         if (e != cudaSuccess || ndev == 0) throw ApiError(MDF_ERR_CUDA, "no CUDA device available");

@@ -29,7 +29,6 @@ enum : unsigned {
     ST_CAPACITY_PAIRS = 4u,
     ST_CAPACITY_COLUMN = 8u,
     ST_BAD_INDEX = 16u,
-    ST_STALE_LIST = 32u,    // an atom left the reach of its pairlist column (tiled PME)
 };
 
 struct PairEntry {          // one cluster pair of the half list (16 B)

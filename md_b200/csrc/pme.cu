@@ -36,19 +36,6 @@ template <> struct CT<float> { using type = float2; };
 template <> struct CT<double> { using type = double2; };
 
 constexpr int FFT_THREADS = 128;
-constexpr int PME_TX = 8;   // grid lines in x per tile of the shared-memory spread and gather
-constexpr size_t PME_TILE_SMEM = 100 * 1024;   // largest tile (bytes of shared memory)
-
-// Grid lines in y per tile (0: the per-atom kernels): mdf_params.pme_tile
-// (0 = 4), halved while the tile of per_line bytes per grid line, with a
-// halo of `halo` lines in x and y, exceeds PME_TILE_SMEM.
-static int pme_tile_y(const Ctx& c, size_t per_line, int halo)
-{
-    if (c.p.pme_tile < 0) return 0;
-    int ty = c.p.pme_tile > 0 ? std::min(c.p.pme_tile, 8) : 4;
-    while (ty >= 1 && (size_t)(PME_TX + halo) * (ty + halo) * per_line > PME_TILE_SMEM) ty >>= 1;
-    return ty;
-}
 
 struct FFTDesc {
     int n;
@@ -520,207 +507,6 @@ __global__ void k_gather4(int nslots, const int* __restrict__ slot_atom, const d
     fx_add(fslot + 2 * nslots + s, -qr * gz * (R)g.scale[2], FORCE_SCALE, st);
 }
 
-// ------------------------------------------- tiled spread and gather
-// One block per tile of TX x TY grid lines (all of z).  The atoms that can
-// reach the tile are found through the pairlist's x-y columns (the columns
-// overlapping the tile's x-y extent widened by the stencil and by `margin`,
-// the drift allowed since the list was built; never more than every column
-// once).  The spread accumulates in a shared-memory tile (int64 fixed point,
-// so the sum is order-independent and identical to the per-atom spread) and
-// writes every grid point of the tile exactly once: no global atomics and no
-// clearing pass.  The gather loads the tile plus a one/two-point halo of the
-// potential into shared memory and handles the atoms whose base grid point
-// lies in the tile core.  The gather also checks every atom it scans against
-// its list column; an atom that moved too far since the list was built sets
-// ST_STALE_LIST (the evaluation fails instead of dropping a charge).
-struct TileCols {
-    int cx0, nx, cy0, ny;   // first column and column count per direction (wrapping)
-};
-
-__device__ __forceinline__ TileCols tile_columns(double xlo, double xhi, double ylo, double yhi, double Lx, double Ly,
-                                                 int ncx, int ncy)
-{
-    TileCols t;
-    const double wx = Lx / ncx, wy = Ly / ncy;
-    t.cx0 = (int)floor(xlo / wx);
-    t.nx = (int)floor(xhi / wx) - t.cx0 + 1;
-    if (t.nx >= ncx) { t.cx0 = 0; t.nx = ncx; }
-    t.cy0 = (int)floor(ylo / wy);
-    t.ny = (int)floor(yhi / wy) - t.cy0 + 1;
-    if (t.ny >= ncy) { t.cy0 = 0; t.ny = ncy; }
-    return t;
-}
-
-__device__ __forceinline__ int wrapi(int i, int n)
-{
-    i %= n;
-    return i < 0 ? i + n : i;
-}
-
-// Column c (of nc, width L/nc, periodic) overlaps [p - m, p + m].  Every
-// tile whose stencil an atom at p reaches scans the columns of that window
-// (the tile ranges are widened by `margin` > m), so an atom whose list column
-// passes this test is seen by every tile that needs it.
-__device__ __forceinline__ bool column_near(double p, double m, double L, int nc, int c)
-{
-    const double w = L / nc;
-    const int lo = (int)floor((p - m) / w), hi = (int)floor((p + m) / w);
-    return hi - lo + 1 >= nc || wrapi(c - lo, nc) <= hi - lo;
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256) k_spread_tiled(int TX, int TY, GridGeom g, int ncx, int ncy,
-                                                      const int* __restrict__ col_cstart,
-                                                      const int* __restrict__ slot_atom,
-                                                      const double* __restrict__ xyz, const double* __restrict__ q,
-                                                      double margin, unsigned long long* __restrict__ qgrid,
-                                                      unsigned* st)
-{
-    extern __shared__ unsigned long long tile[];   // [TX][TY][K2]
-    const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int ntile = TX * TY * K2;
-    for (int k = threadIdx.x; k < ntile; k += blockDim.x) tile[k] = 0ull;
-    const double hx = g.L[0] / K0, hy = g.L[1] / K1;
-    const TileCols tc = tile_columns((x0 - 2) * hx - margin, (x0 + TX + 1) * hx + margin, (y0 - 2) * hy - margin,
-                                     (y0 + TY + 1) * hy + margin, g.L[0], g.L[1], ncx, ncy);
-    __syncthreads();
-    for (int iy = 0; iy < tc.ny; ++iy)
-        for (int ix = 0; ix < tc.nx; ++ix) {
-            const int col = wrapi(tc.cx0 + ix, ncx) + ncx * wrapi(tc.cy0 + iy, ncy);
-            const int s1 = col_cstart[col + 1] * CLUSTER;
-            for (int s = col_cstart[col] * CLUSTER + threadIdx.x; s < s1; s += blockDim.x) {
-                const int a = slot_atom[s];
-                if (a < 0) continue;
-                const double qa = q[a];
-                if (qa == 0.0) continue;
-                int base[3];
-                double u[3];
-                bool bad = false;
-                for (int d = 0; d < 3; ++d) {
-                    u[d] = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
-                    if (!(u[d] >= 0.0 && u[d] <= (double)g.K[d])) bad = true;
-                }
-                if (bad) {
-                    status_set(st, ST_NONFINITE);
-                    continue;
-                }
-                int lx[4], ly[4];
-                bool anyx = false, anyy = false;
-                for (int d = 0; d < 3; ++d) {
-                    if (u[d] >= g.K[d]) u[d] -= g.K[d];
-                    base[d] = min((int)floor(u[d]), g.K[d] - 1);
-                }
-                for (int i = 0; i < 4; ++i) {
-                    lx[i] = wrapi(base[0] - 1 + i, K0) - x0;
-                    ly[i] = wrapi(base[1] - 1 + i, K1) - y0;
-                    anyx |= (lx[i] >= 0 && lx[i] < TX);
-                    anyy |= (ly[i] >= 0 && ly[i] < TY);
-                }
-                if (!anyx || !anyy) continue;
-                R th[3][4];
-                for (int d = 0; d < 3; ++d) bspline4<R>((R)(u[d] - base[d]), th[d], nullptr);
-                const R qr = (R)qa;
-                int kz[4];
-                for (int k = 0; k < 4; ++k) kz[k] = wrapi(base[2] - 1 + k, K2);
-                for (int i = 0; i < 4; ++i) {
-                    if (lx[i] < 0 || lx[i] >= TX) continue;
-                    for (int j = 0; j < 4; ++j) {
-                        if (ly[j] < 0 || ly[j] >= TY) continue;
-                        const R wxy = qr * th[0][i] * th[1][j];
-                        unsigned long long* row = tile + (lx[i] * TY + ly[j]) * K2;
-                        for (int k = 0; k < 4; ++k) {
-                            const R v = wxy * th[2][k];
-                            atomicAdd(row + kz[k], (unsigned long long)__double2ll_rn((double)v * GRID_SCALE));
-                        }
-                    }
-                }
-            }
-        }
-    __syncthreads();
-    for (int k = threadIdx.x; k < ntile; k += blockDim.x) {
-        const int line = k / K2, z = k - line * K2;
-        const int lxx = line / TY, lyy = line - lxx * TY;
-        const int gx = x0 + lxx, gy = y0 + lyy;
-        if (gx < K0 && gy < K1) qgrid[((long long)gx * K1 + gy) * K2 + z] = tile[k];
-    }
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256) k_gather_tiled(int TX, int TY, GridGeom g, int ncx, int ncy,
-                                                      const int* __restrict__ col_cstart,
-                                                      const int* __restrict__ slot_atom,
-                                                      const double* __restrict__ xyz, const double* __restrict__ q,
-                                                      double margin, const R* __restrict__ phi,
-                                                      unsigned long long* __restrict__ fslot, int nslots, unsigned* st)
-{
-    extern __shared__ __align__(16) unsigned char gsm[];
-    R* pt = reinterpret_cast<R*>(gsm);   // [TX+3][TY+3][K2]: grid lines x0-1 .. x0+TX+1
-    const int K0 = g.K[0], K1 = g.K[1], K2 = g.K[2];
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-    const int HX = TX + 3, HY = TY + 3;
-    for (int k = threadIdx.x; k < HX * HY * K2; k += blockDim.x) {
-        const int line = k / K2, z = k - line * K2;
-        const int hx = line / HY, hy = line - hx * HY;
-        const int gx = wrapi(x0 - 1 + hx, K0), gy = wrapi(y0 - 1 + hy, K1);
-        pt[k] = phi[((long long)gx * K1 + gy) * K2 + z];
-    }
-    const double hxs = g.L[0] / K0, hys = g.L[1] / K1;
-    const TileCols tc = tile_columns(x0 * hxs - margin, (x0 + TX) * hxs + margin, y0 * hys - margin,
-                                     (y0 + TY) * hys + margin, g.L[0], g.L[1], ncx, ncy);
-    __syncthreads();
-    for (int iy = 0; iy < tc.ny; ++iy)
-        for (int ix = 0; ix < tc.nx; ++ix) {
-            const int colx = wrapi(tc.cx0 + ix, ncx), coly = wrapi(tc.cy0 + iy, ncy);
-            const int col = colx + ncx * coly;
-            const int s1 = col_cstart[col + 1] * CLUSTER;
-            for (int s = col_cstart[col] * CLUSTER + threadIdx.x; s < s1; s += blockDim.x) {
-                const int a = slot_atom[s];
-                if (a < 0) continue;
-                const double qa = q[a];
-                if (qa == 0.0) continue;
-                double u[3], w[3];
-                int base[3];
-                bool bad = false;
-                for (int d = 0; d < 3; ++d) {
-                    w[d] = wrap_coord(xyz[3 * a + d], g.L[d]);
-                    u[d] = w[d] * g.scale[d];
-                    if (!(u[d] >= 0.0 && u[d] <= (double)g.K[d])) bad = true;
-                    if (u[d] >= g.K[d]) u[d] -= g.K[d];
-                    base[d] = min((int)floor(u[d]), g.K[d] - 1);
-                }
-                if (bad) continue;   // the spread reports it
-                if (!column_near(w[0], margin - 0.01, g.L[0], ncx, colx) ||
-                    !column_near(w[1], margin - 0.01, g.L[1], ncy, coly))
-                    status_set(st, ST_STALE_LIST);
-                const int cx = base[0] - x0, cy = base[1] - y0;
-                if (cx < 0 || cx >= TX || cy < 0 || cy >= TY) continue;   // another tile's atom
-                R th[3][4], dth[3][4];
-                for (int d = 0; d < 3; ++d) bspline4<R>((R)(u[d] - base[d]), th[d], dth[d]);
-                int kz[4];
-                for (int k = 0; k < 4; ++k) kz[k] = wrapi(base[2] - 1 + k, K2);
-                R gx = 0, gy = 0, gz = 0;
-                for (int i = 0; i < 4; ++i)
-                    for (int j = 0; j < 4; ++j) {
-                        const R* row = pt + ((cx + i) * HY + (cy + j)) * K2;   // grid line (base-1+i, base-1+j)
-                        R sz = 0, dz = 0;
-                        for (int k = 0; k < 4; ++k) {
-                            const R p = row[kz[k]];
-                            sz += th[2][k] * p;
-                            dz += dth[2][k] * p;
-                        }
-                        gx += dth[0][i] * th[1][j] * sz;
-                        gy += th[0][i] * dth[1][j] * sz;
-                        gz += th[0][i] * th[1][j] * dz;
-                    }
-                const R qr = (R)qa;
-                fx_add(fslot + s, -qr * gx * (R)g.scale[0], FORCE_SCALE, st);
-                fx_add(fslot + nslots + s, -qr * gy * (R)g.scale[1], FORCE_SCALE, st);
-                fx_add(fslot + 2 * nslots + s, -qr * gz * (R)g.scale[2], FORCE_SCALE, st);
-            }
-        }
-}
-
 // The reference's order-5 weights (src/System/PBC.cpp:329-356 for the spread,
 // :359-401 for the gather; the two differ in operation order).
 __host__ __device__ __forceinline__ void ref_w5_spread(double u, double th[5])
@@ -998,13 +784,6 @@ void setup_pme(Ctx& c)
             c.tw_d[d].upload(tw.data(), K, c.stream);
         }
     }
-    {
-        const int maxsm = (int)PME_TILE_SMEM;
-        MDF_CUDA_TRY(cudaFuncSetAttribute(k_spread_tiled<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
-        MDF_CUDA_TRY(cudaFuncSetAttribute(k_spread_tiled<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
-        MDF_CUDA_TRY(cudaFuncSetAttribute(k_gather_tiled<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
-        MDF_CUDA_TRY(cudaFuncSetAttribute(k_gather_tiled<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm));
-    }
     // influence function, laid out [ky][kz][kx] (the x pass reads lines along kx)
     std::vector<double> infl((size_t)K1 * Kc * K0);
     const double V = c.box[0] * c.box[1] * c.box[2];
@@ -1125,17 +904,9 @@ static void run_pme(Ctx& c, bool energy)
     const bool ref = c.p.semantics == MDF_SEM_REFERENCE;
     const PmeBufs<R> B(c);
     const long long ntot = (long long)c.K[0] * c.K[1] * c.K[2];
+    MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
     const int th = 256;
-    const double margin = 0.5 * c.p.skin + 1.0;   // drift allowed since the columns were built, and more
-    const int sty = ref ? 0 : pme_tile_y(c, sizeof(unsigned long long) * (size_t)c.K[2], 0);
-    const bool tiled = sty > 0 && c.have_list;
-    if (!tiled) MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
-    if (tiled) {
-        const dim3 grid((c.K[0] + PME_TX - 1) / PME_TX, (c.K[1] + sty - 1) / sty);
-        const size_t sm = sizeof(unsigned long long) * PME_TX * sty * c.K[2];
-        k_spread_tiled<R><<<grid, th, sm, c.stream>>>(PME_TX, sty, B.g, c.ncol_x, c.ncol_y, c.col_cstart.p,
-                                                      c.slot_atom.p, c.xyz.p, c.q.p, margin, c.qgrid.p, c.status.p);
-    } else if (!ref) {
+    if (!ref) {
         k_spread4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g,
                                                                       c.qgrid.p, c.status.p);
     } else {
@@ -1144,14 +915,7 @@ static void run_pme(Ctx& c, bool energy)
     mark(c, "pme_spread");
     conv_chain<R>(c, B, energy);
     mark(c, "pme_fft_conv");
-    const int gty = ref ? 0 : pme_tile_y(c, sizeof(R) * (size_t)c.K[2], 3);
-    if (!ref && gty > 0 && c.have_list) {
-        const dim3 grid((c.K[0] + PME_TX - 1) / PME_TX, (c.K[1] + gty - 1) / gty);
-        const size_t sm = sizeof(R) * (PME_TX + 3) * (gty + 3) * c.K[2];
-        k_gather_tiled<R><<<grid, th, sm, c.stream>>>(PME_TX, gty, B.g, c.ncol_x, c.ncol_y, c.col_cstart.p,
-                                                      c.slot_atom.p, c.xyz.p, c.q.p, margin, B.rg, c.f_slot.p,
-                                                      c.n_slots, c.status.p);
-    } else if (!ref) {
+    if (!ref) {
         k_gather4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g,
                                                                       B.rg, c.f_slot.p, c.status.p);
     } else {

@@ -143,7 +143,7 @@ class Engine:
 
     def __init__(self, flat, box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, cutoff=10.0,
                  skin=2.0, switch_radius=9.0, ewald_tol=1e-5, ewald_alpha=0.0, grid=(0, 0, 0), pme_order=4,
-                 device=0, prune_every=1, prune_margin=0.0, pme_tile=0):
+                 device=0, prune_every=1, prune_margin=0.0):
         self.lib = library()
         self.flat = flat
         self.natoms = flat.natoms
@@ -156,7 +156,6 @@ class Engine:
         p.cutoff, p.skin, p.switch_radius = float(cutoff), float(skin), float(switch_radius)
         p.ewald_tol, p.ewald_alpha, p.pme_order, p.device = float(ewald_tol), float(ewald_alpha), int(pme_order), int(device)
         p.prune_every, p.prune_margin = int(prune_every), float(prune_margin)
-        p.pme_tile = int(pme_tile)
         self.params = p
         h = C.c_void_p()
         rc = self.lib.mdf_create(C.byref(flat.struct()), C.byref(p), C.byref(h))

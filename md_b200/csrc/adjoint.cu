@@ -122,6 +122,21 @@ __global__ void __launch_bounds__(NB_THREADS) k_adj_pairs(
     V4t* wsv = sv + wib * 4 * CLUSTER;
     int* wst = stj + wib * 4 * CLUSTER;
     R dqi = 0;
+    // LJ parameter derivatives: a one-entry cache per lane (most pairs of a
+    // solvent share one type pair), flushed to the block sums when the type
+    // pair changes and at the end
+    int kcache = -1;
+    R ca = 0, cb = 0;
+    auto flush_lj = [&]() {
+        if (kcache < 0) return;
+        if (nlj > 0) {
+            atomicAdd(part + kcache, ca);
+            atomicAdd(part + nlj + kcache, cb);
+        } else {
+            atomicAdd(dab + kcache, (double)ca);
+            atomicAdd(dab + n_ljpair + kcache, (double)cb);
+        }
+    };
     if (w < nlist) {
         const ILRange L = ilist[w];
         const int I = L.i;
@@ -192,12 +207,14 @@ __global__ void __launch_bounds__(NB_THREADS) k_adj_pairs(
                             gB = gB - gcB * rcr * rinv;
                         }
                         const R da = gEr * eA + gA * wv, db = gEr * eB + gB * wv;
-                        if (nlj > 0) {
-                            atomicAdd(part + k, da);
-                            atomicAdd(part + nlj + k, db);
+                        if (k == kcache) {
+                            ca += da;
+                            cb += db;
                         } else {
-                            atomicAdd(dab + k, (double)da);
-                            atomicAdd(dab + n_ljpair + k, (double)db);
+                            flush_lj();
+                            kcache = k;
+                            ca = da;
+                            cb = db;
                         }
                     }
                 }
@@ -210,6 +227,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_adj_pairs(
         dqi += __shfl_xor_sync(FULL, dqi, 16);
         if (jslot == 0 && dqi != (R)0) fx_add(dq_slot + I * CLUSTER + ii, (double)dqi, FORCE_SCALE, st);
     }
+    flush_lj();
     if (nlj > 0) {
         __syncthreads();
         for (int k = threadIdx.x; k < 2 * nlj; k += blockDim.x) {

@@ -479,7 +479,15 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         MDF_CUDA_TRY(cudaSetDevice(c.device));
         MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         c.own_stream = true;
-        MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+        {
+            // The side stream (exclusions, 1-4, bonded, PME) gets the highest
+            // priority: its kernels are short and few-block, and scheduled
+            // first they finish inside the pair kernel instead of stretching
+            // its tail (c1 mixed: 0.364 vs 0.386 ms per evaluation).
+            int lo = 0, hi = 0;
+            MDF_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            MDF_CUDA_TRY(cudaStreamCreateWithPriority(&c.side, cudaStreamNonBlocking, hi));
+        }
         MDF_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming));
         MDF_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_join, cudaEventDisableTiming));
         MDF_CUDA_TRY(cudaHostAlloc((void**)&c.h_scal, sizeof(unsigned long long) * NUM_SCAL, cudaHostAllocMapped));

@@ -54,6 +54,20 @@ FLOPS_PER_PAIR = 60.0
 # DRAM bytes (read + write) of one k_pairs_f32 launch at c1, from one ncu
 # capture of `bench.py --profile c1` (dram__bytes.sum.per_second x duration)
 PAIR_TRAFFIC_BYTES = 20.0e6
+# algorithmic bytes of one k_pairs_f32 launch at c1: pruned list 13.6 MB + packed
+# positions/charges 1.6 + types 0.4 + fixed-point force read-modify-write 2.4
+PAIR_ALGO_BYTES = 18.0e6
+HBM_FALLBACK_GBS = 6650.0   # earlier copy-bandwidth measurement on B200, when no measured peak is at hand
+
+
+def hbm_peak_gbs():
+    """(peak GB/s, source): the measured copy bandwidth next to this script, else the fallback."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured copy bandwidth (MEASURED_PEAKS.json)"
+    except (OSError, ValueError, KeyError):
+        return HBM_FALLBACK_GBS, "fallback 6.65 TB/s"
 
 
 def parse():
@@ -546,6 +560,7 @@ def main():
 
     peak = engine.probe_fma_tflops(dev, abi.MDF_PREC_MIXED)
     achieved = FLOPS_PER_PAIR * info["pairs_in_cutoff"] / (pair_ms * 1e-3) / 1e12
+    hbm_gbs, hbm_src = hbm_peak_gbs()
     kernel_ms = {k: float(np.mean(v)) for k, v in ktimes.items()}
     fft_check = cufft_check(eng, dev, s, kernel_ms.get("pme_fft_conv"))
 
@@ -602,7 +617,11 @@ def main():
                                            "workload (bench.py --profile c1); algorithmic ~18 MB",
                          "peak_source": "measured FP32 FMA throughput of this GPU (mdf_probe_fma_tflops)",
                          "work": "%g FP32 flops x %d pairs in cutoff per launch" % (FLOPS_PER_PAIR,
-                                                                                  info["pairs_in_cutoff"])},
+                                                                                  info["pairs_in_cutoff"]),
+                         "hbm_view": {"achieved": PAIR_ALGO_BYTES / (pair_ms * 1e-3) / 1e9, "peak": hbm_gbs,
+                                      "unit": "GB/s", "frac": PAIR_ALGO_BYTES / (pair_ms * 1e-3) / 1e9 / hbm_gbs,
+                                      "peak_source": hbm_src,
+                                      "note": "the pair kernel is FP32-issue bound, not HBM bound"}},
             "kernel_ms": kernel_ms,
             "fft_vs_cufft": fft_check,
             "e2e": {"value": e2e, "unit": "evals/s", "h2d_bytes_per_step": 3 * s.natoms * 8,

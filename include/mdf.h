@@ -185,7 +185,8 @@ int mdf_set_box(mdf_ctx *ctx, const double box[3]);
  * setup_pairlists / build_lj_pairlist, src/System/NonBondedUtils.cpp:49-57,185-282). */
 int mdf_build_pairlist(mdf_ctx *ctx);
 
-/* One evaluation.  forces_out: host 3N doubles or NULL; e_out: host or NULL.
+/* One evaluation.  forces_out: host 3N doubles or NULL (its content is
+ * unspecified when the call fails); e_out: host or NULL.
  * Replaces calculate_forces() + calculate_energies() (+ the PME chain). */
 int mdf_compute(mdf_ctx *ctx, uint32_t flags, double *forces_out, mdf_energies *e_out);
 

@@ -617,9 +617,14 @@ int mdf_compute(mdf_ctx* ctx, uint32_t flags, double* forces_out, mdf_energies* 
 {
     if (!ctx) return MDF_ERR_INVALID;
     return guarded(ctx, [&] {
-        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
-        eval_async(ctx->c, flags);
-        fetch(ctx->c, forces_out, e_out);
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        eval_async(c, flags);
+        // the force copy joins the evaluation's stream: one synchronisation for both
+        if (forces_out)
+            MDF_CUDA_TRY(cudaMemcpyAsync(forces_out, c.forces_out.p, sizeof(double) * 3 * (size_t)c.N,
+                                         cudaMemcpyDeviceToHost, c.stream));
+        fetch(c, nullptr, e_out);
     });
 }
 

@@ -310,8 +310,12 @@ def md_bench(dev, steps=1000, equil=200):
     """c4: 215 A box of 320,000 flexible waters (960,000 atoms), PME 216^3,
     cutoff 10 A + 2 A skin, velocity-Verlet NVE at 0.5 fs from 300 K Maxwell
     velocities (seeded), pairlist rebuilt every 10 steps.  The lattice start is
-    first relaxed by the steepest-descent minimiser (the same positions feed
-    both precisions), then `equil` steps are run before the measured `steps`.
+    first relaxed by the L-BFGS minimiser (the same positions feed both
+    precisions), then `equil` steps are run before the measured `steps`.  The
+    PME spread and gather of this workload are timed alone (phase events) and
+    set against HBM with their algorithmic bytes: spread 16 B/atom + 8 B K^3
+    grid write + 8 B K^3 clear, gather 16 B/atom + 4 B K^3 potential read +
+    24 B/atom force read-modify-write.
     Steps/s is the host wall time of mdf_md_run (graph chunks of 10 steps,
     list rebuilds and the per-chunk energy read-back included); the energy
     drift is last minus first sample of the total energy over the measured
@@ -323,12 +327,34 @@ def md_bench(dev, steps=1000, equil=200):
     eng = engine.Engine(flat, s.box, precision=abi.MDF_PREC_MIXED, **kw)
     eng.set_positions(s.coords)
     eng.build_pairlist()
-    mrep = eng.minimize(max_iter=300, fmax_tol=10.0)
+    t0 = time.perf_counter()
+    mrep = eng.minimize(max_iter=300, fmax_tol=10.0, method="lbfgs")
+    mrep["method"] = "L-BFGS, 8 pairs"
+    mrep["wall_s"] = time.perf_counter() - t0
     x0, _ = eng.md_state(velocities=False)
+    # spread / gather alone at c4 (timing mode: one stream, phase events)
+    eng.enable_timing(True)
+    ph = {}
+    for _ in range(6):
+        eng.compute()
+        for name, ms in eng.kernel_times():
+            ph.setdefault(name, []).append(ms)
+    eng.enable_timing(False)
+    K3 = float(np.prod(synth.GRIDS["c4"]))
+    sp_ms, ga_ms = float(np.median(ph["pme_spread"][1:])), float(np.median(ph["pme_gather"][1:]))
+    sp_b, ga_b = 16.0 * s.natoms + 16.0 * K3, 40.0 * s.natoms + 4.0 * K3
+    hbm, hbm_src = hbm_peak_gbs()
+    pme = {"spread_ms": sp_ms, "gather_ms": ga_ms,
+           "spread_gbs": sp_b / (sp_ms * 1e-3) / 1e9, "gather_gbs": ga_b / (ga_ms * 1e-3) / 1e9,
+           "hbm_peak_gbs": hbm, "peak_source": hbm_src}
+    pme["spread_hbm_frac"] = pme["spread_gbs"] / hbm
+    pme["gather_hbm_frac"] = pme["gather_gbs"] / hbm
+    pme["note"] = ("the 80 MB int64 grid stays in L2: the spread is bound by L2 int64 atomic throughput "
+                   "(64 per atom), the gather by L1/L2 latency of its 64 loads per atom")
     out = {"workload": "c4: %d atoms (320,000 flexible waters), 215 A box, PME 216^3, cutoff 10 A, skin 2 A, "
                        "dt 0.5 fs, NVE, list rebuilt every 10 steps, %d measured steps after %d equilibration "
                        "steps" % (s.natoms, steps, equil),
-           "minimiser": mrep}
+           "minimiser": mrep, "pme_spread_gather": pme}
     for name, prec in (("mixed", abi.MDF_PREC_MIXED), ("fp64", abi.MDF_PREC_FP64)):
         if prec != abi.MDF_PREC_MIXED:
             eng.close()

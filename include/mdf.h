@@ -272,12 +272,20 @@ typedef struct {
     int32_t rebuilds;
     double e_initial, e_final;   /* total potential energy, kcal/mol */
     double fmax_final;           /* largest force component at the end */
+    int32_t evaluations;         /* energy + force evaluations, line-search trials included */
+    int32_t reserved;
 } mdf_min_report;
 /* Steepest descent at the current positions, largest move per iteration
  * adaptive up to max_step (A); stops at max |F| <= fmax_tol (kcal/mol/A) or
  * after max_iter iterations.  The positions stay on the device
  * (mdf_md_state reads them); call mdf_md_init afterwards to start dynamics. */
 int mdf_minimize(mdf_ctx *ctx, int32_t max_iter, double fmax_tol, double max_step, mdf_min_report *report);
+/* L-BFGS (two-loop recursion, Nocedal & Wright Algorithm 7.4, `history`
+ * pairs, 0 = 8) with a backtracking Armijo line search; no atom moves more
+ * than max_step (A) per iteration.  Same stopping rule, list handling and
+ * report as mdf_minimize; bit-reproducible run to run. */
+int mdf_minimize_lbfgs(mdf_ctx *ctx, int32_t max_iter, double fmax_tol, double max_step, int32_t history,
+                       mdf_min_report *report);
 
 typedef struct {
     int64_t steps;        /* steps done */

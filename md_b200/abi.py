@@ -75,5 +75,6 @@ class mdf_md_report(C.Structure):
 
 class mdf_min_report(C.Structure):
     _fields_ = [("iterations", C.c_int32), ("rebuilds", C.c_int32), ("e_initial", C.c_double),
-                ("e_final", C.c_double), ("fmax_final", C.c_double)]
+                ("e_final", C.c_double), ("fmax_final", C.c_double), ("evaluations", C.c_int32),
+                ("reserved", C.c_int32)]
 

@@ -772,6 +772,16 @@ int mdf_minimize(mdf_ctx* ctx, int32_t max_iter, double fmax_tol, double max_ste
     });
 }
 
+int mdf_minimize_lbfgs(mdf_ctx* ctx, int32_t max_iter, double fmax_tol, double max_step, int32_t history,
+                       mdf_min_report* report)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        minimize_lbfgs(ctx->c, max_iter, fmax_tol, max_step, history, report);
+    });
+}
+
 int mdf_md_init(mdf_ctx* ctx, const double* masses, const double* velocities, double temperature, uint64_t seed)
 {
     if (!ctx) return MDF_ERR_INVALID;

@@ -377,6 +377,7 @@ void minimize(Ctx& c, int max_iter, double fmax_tol, double max_step, mdf_min_re
     double e0, f0;
     evaluate(e0, f0);
     r.e_initial = e0;
+    r.evaluations = 1;
     int it = 0;
     for (; it < max_iter && f0 > fmax_tol; ++it) {
         if (moved + step > 0.25 * c.p.skin) {
@@ -384,6 +385,7 @@ void minimize(Ctx& c, int max_iter, double fmax_tol, double max_step, mdf_min_re
             ++r.rebuilds;
             moved = 0.0;
             evaluate(e0, f0);   // the same positions on the new list
+            ++r.evaluations;
         }
         MDF_CUDA_TRY(cudaMemcpyAsync(c.min_x.p, c.xyz.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
         MDF_CUDA_TRY(cudaMemcpyAsync(c.min_f.p, c.forces_out.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
@@ -391,6 +393,7 @@ void minimize(Ctx& c, int max_iter, double fmax_tol, double max_step, mdf_min_re
         MDF_CUDA_TRY(cudaGetLastError());
         double e1, f1;
         evaluate(e1, f1);
+        ++r.evaluations;
         if (e1 < e0) {
             moved += step;
             e0 = e1;
@@ -402,6 +405,270 @@ void minimize(Ctx& c, int max_iter, double fmax_tol, double max_step, mdf_min_re
             step *= 0.5;
             if (step < 1e-7) break;
         }
+    }
+    MDF_CUDA_TRY(cudaStreamSynchronize(s));
+    r.iterations = it;
+    r.e_final = e0;
+    r.fmax_final = f0;
+    c.md_ready = false;   // positions and list changed: dynamics restart from mdf_md_init
+    md_drop_graph(c);
+    if (rep) *rep = r;
+}
+
+// ------------------------------------------------------------- L-BFGS
+// Limited-memory BFGS (Nocedal & Wright, Numerical Optimization, 2nd ed.,
+// Algorithm 7.4 two-loop recursion and 7.5), the solver the reference names
+// as the consumer of calculate_forces (include/System/System.h:84,113).
+// Vectors live on the device; the recursion's scalars (alpha_i, beta,
+// gamma) stay in device memory between its kernels, so a direction costs no
+// host round trip.  Dot products are two-stage reductions with a fixed block
+// count and order: runs are bit-reproducible.  Line search: backtracking
+// from t = 1 (the step scaled so no atom moves more than max_step) with the
+// Armijo condition, c1 = 1e-4 (where the energy change is below its
+// resolution, a smaller largest force component decides).  A pair (s, y)
+// with s.y <= 0 is not stored.
+constexpr int LB_BLOCKS = 296;   // 2 x 148 SMs
+constexpr int LB_THREADS = 256;
+
+__global__ void __launch_bounds__(LB_THREADS) k_lb_dot_part(long long n, const double* __restrict__ a,
+                                                            const double* __restrict__ b, double* __restrict__ part)
+{
+    __shared__ double w[LB_THREADS / 32];
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        s = fma(a[i], b[i], s);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int k = 0; k < LB_THREADS / 32; ++k) t += w[k];
+        part[blockIdx.x] = t;
+    }
+}
+
+// out = (sum of the partials) * (mul ? *mul : 1), in a fixed order
+__global__ void k_lb_dot_final(int nb, const double* __restrict__ part, double* __restrict__ out,
+                               const double* __restrict__ mul)
+{
+    if (threadIdx.x != 0) return;
+    double t = 0.0;
+    for (int k = 0; k < nb; ++k) t += part[k];
+    *out = mul ? t * *mul : t;
+}
+
+__global__ void k_lb_set(long long n, double* __restrict__ out, const double* __restrict__ in, double scale)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = scale * in[i];
+}
+
+// y += sign * (*coef) * x
+__global__ void k_lb_axpy(long long n, double* __restrict__ y, const double* __restrict__ x,
+                          const double* __restrict__ coef, double sign)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = fma(sign * *coef, x[i], y[i]);
+}
+
+// r += (*a - *b) * s
+__global__ void k_lb_axpy_diff(long long n, double* __restrict__ r, const double* __restrict__ s,
+                               const double* __restrict__ a, const double* __restrict__ b)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] = fma(*a - *b, s[i], r[i]);
+}
+
+// r *= (*num) / (*den)
+__global__ void k_lb_scale(long long n, double* __restrict__ r, const double* __restrict__ num,
+                           const double* __restrict__ den)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) r[i] *= *num / *den;
+}
+
+// x = x0 - t r (r approximates H g, so -r is the descent direction)
+__global__ void k_lb_trial(long long n, double* __restrict__ x, const double* __restrict__ x0,
+                           const double* __restrict__ r, double t)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = fma(-t, r[i], x0[i]);
+}
+
+// s = x - x0, y = g - g0 = F0 - F
+__global__ void k_lb_pair(long long n, double* __restrict__ s, double* __restrict__ y, const double* __restrict__ x,
+                          const double* __restrict__ x0, const double* __restrict__ f, const double* __restrict__ f0)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        s[i] = x[i] - x0[i];
+        y[i] = f0[i] - f[i];
+    }
+}
+
+__global__ void k_lb_recip(const double* __restrict__ in, double* __restrict__ out) { *out = 1.0 / *in; }
+
+// largest per-atom norm of r (max of non-negative doubles through their bit patterns)
+__global__ void k_lb_atom_max(int N, const double* __restrict__ r, unsigned long long* __restrict__ out)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    double m = 0.0;
+    if (a < N) m = sqrt(r[3 * a] * r[3 * a] + r[3 * a + 1] * r[3 * a + 1] + r[3 * a + 2] * r[3 * a + 2]);
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+void minimize_lbfgs(Ctx& c, int max_iter, double fmax_tol, double max_step, int m, mdf_min_report* rep)
+{
+    if (c.p.semantics != MDF_SEM_PHYSICAL) throw ApiError(MDF_ERR_UNSUPPORTED, "the minimiser needs PHYSICAL semantics");
+    if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
+    if (m < 0 || m > 64) throw ApiError(MDF_ERR_INVALID, "history must be 0 (= 8) .. 64");
+    if (m == 0) m = 8;
+    if (!(max_step > 0.0)) max_step = 0.1;
+    cudaStream_t s = c.stream;
+    const int th = 256;
+    const long long n3 = 3LL * c.N;
+    const int nbv = grid_blocks(n3, th);
+    md_words(c);
+    c.min_x.alloc(n3);
+    c.min_f.alloc(n3);
+    c.lb_s.alloc((size_t)m * n3);
+    c.lb_y.alloc((size_t)m * n3);
+    c.lb_q.alloc(n3);
+    c.lb_part.alloc(LB_BLOCKS);
+    // scalars: alpha[m] | rho[m] | beta | sy | yy | gd | dmax bits
+    c.lb_scal.alloc(2 * m + 5);
+    double* alpha = c.lb_scal.p;
+    double* rho = alpha + m;
+    double* beta = rho + m;
+    double* sy = beta + 1;
+    double* yy = sy + 1;
+    double* gd = yy + 1;
+    unsigned long long* dmaxw = reinterpret_cast<unsigned long long*>(gd + 1);
+    auto dot = [&](const double* a, const double* b, double* out, const double* mul) {
+        k_lb_dot_part<<<LB_BLOCKS, LB_THREADS, 0, s>>>(n3, a, b, c.lb_part.p);
+        k_lb_dot_final<<<1, 32, 0, s>>>(LB_BLOCKS, c.lb_part.p, out, mul);
+    };
+    auto evaluate = [&](double& e, double& fmax) {
+        k_md_reset<<<1, 32, 0, s>>>(c.md_dev, 1u << 3);
+        eval_async_impl(c, MDF_COMPUTE_ENERGY | MDF_COMPUTE_FORCES);
+        k_min_fmax<<<grid_blocks(n3, th), th, 0, s>>>((int)n3, c.forces_out.p, c.md_dev + 3);
+        k_md_publish<<<1, 32, 0, s>>>(c.md_dev, c.md_hmap);
+        MDF_CUDA_TRY(cudaGetLastError());
+        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        check_host_status(c);
+        mdf_energies en;
+        host_energies(c, MDF_COMPUTE_ENERGY, &en);
+        e = en.total;
+        fmax = bits_to_double(c.md_host[3]);
+    };
+    auto read_scalars = [&](double& gdv, double& dmaxv) {
+        double h[2];
+        MDF_CUDA_TRY(cudaMemcpyAsync(h, gd, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        gdv = h[0];
+        unsigned long long u;
+        memcpy(&u, &h[1], sizeof(u));
+        dmaxv = bits_to_double(u);
+    };
+    mdf_min_report r;
+    memset(&r, 0, sizeof(r));
+    build_pairlist(c);
+    double e0, f0;
+    evaluate(e0, f0);
+    r.e_initial = e0;
+    r.evaluations = 1;
+    int head = 0, count = 0;   // ring of stored pairs: newest at (head - 1) mod m
+    double moved = 0.0;
+    int it = 0;
+    for (; it < max_iter && f0 > fmax_tol; ++it) {
+        if (moved + max_step > 0.25 * c.p.skin) {
+            build_pairlist(c);
+            ++r.rebuilds;
+            moved = 0.0;
+            evaluate(e0, f0);   // the same positions on the new list
+            ++r.evaluations;
+        }
+        // r = H g by the two-loop recursion, g = -F
+        double* q = c.lb_q.p;
+        k_lb_set<<<nbv, th, 0, s>>>(n3, q, c.forces_out.p, -1.0);
+        for (int k = 0; k < count; ++k) {
+            const int i = (head - 1 - k + m) % m;
+            dot(c.lb_s.p + (size_t)i * n3, q, alpha + i, rho + i);
+            k_lb_axpy<<<nbv, th, 0, s>>>(n3, q, c.lb_y.p + (size_t)i * n3, alpha + i, -1.0);
+        }
+        if (count > 0) k_lb_scale<<<nbv, th, 0, s>>>(n3, q, sy, yy);   // H0 = (s.y / y.y) I, newest pair
+        for (int k = count - 1; k >= 0; --k) {
+            const int i = (head - 1 - k + m) % m;
+            dot(c.lb_y.p + (size_t)i * n3, q, beta, rho + i);
+            k_lb_axpy_diff<<<nbv, th, 0, s>>>(n3, q, c.lb_s.p + (size_t)i * n3, alpha + i, beta);
+        }
+        // directional derivative g.d = F.r (d = -r) and the largest atom move of r
+        dot(c.forces_out.p, q, gd, nullptr);
+        MDF_CUDA_TRY(cudaMemsetAsync(dmaxw, 0, sizeof(unsigned long long), s));
+        k_lb_atom_max<<<grid_blocks(c.N, th), th, 0, s>>>(c.N, q, dmaxw);
+        MDF_CUDA_TRY(cudaGetLastError());
+        double gdv, dmax;
+        read_scalars(gdv, dmax);
+        if (!(gdv < 0.0) || !(dmax > 0.0)) {   // not a descent direction: drop the history, use -g
+            count = 0;
+            k_lb_set<<<nbv, th, 0, s>>>(n3, q, c.forces_out.p, -1.0);
+            dot(c.forces_out.p, q, gd, nullptr);
+            MDF_CUDA_TRY(cudaMemsetAsync(dmaxw, 0, sizeof(unsigned long long), s));
+            k_lb_atom_max<<<grid_blocks(c.N, th), th, 0, s>>>(c.N, q, dmaxw);
+            read_scalars(gdv, dmax);
+            if (!(gdv < 0.0) || !(dmax > 0.0)) break;   // zero gradient
+        }
+        // first step (no curvature yet): at most 0.01 A; afterwards the unit step, capped at max_step
+        double t = count > 0 ? std::min(1.0, max_step / dmax) : std::min(0.01, max_step) / dmax;
+        MDF_CUDA_TRY(cudaMemcpyAsync(c.min_x.p, c.xyz.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+        MDF_CUDA_TRY(cudaMemcpyAsync(c.min_f.p, c.forces_out.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+        bool accepted = false;
+        double e1 = e0, f1 = f0;
+        for (int ls = 0; ls < 30; ++ls) {
+            k_lb_trial<<<nbv, th, 0, s>>>(n3, c.xyz.p, c.min_x.p, q, t);
+            evaluate(e1, f1);
+            ++r.evaluations;
+            // Armijo; or, with the change at the energy's resolution (fixed-point
+            // sums), a smaller largest force
+            const bool flat = std::fabs(e1 - e0) <= 1e-9 * std::max(1.0, std::fabs(e0));
+            if (e1 <= e0 + 1e-4 * t * gdv || (flat && f1 < f0)) {
+                accepted = true;
+                break;
+            }
+            t *= 0.5;
+        }
+        if (!accepted) {   // restore; with no history left to drop, stop
+            MDF_CUDA_TRY(cudaMemcpyAsync(c.xyz.p, c.min_x.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, s));
+            MDF_CUDA_TRY(cudaMemcpyAsync(c.forces_out.p, c.min_f.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice,
+                                         s));
+            if (count == 0) break;
+            count = 0;
+            continue;
+        }
+        moved += t * dmax;
+        // the new pair (s, y), kept when s.y > 0
+        double* sn = c.lb_s.p + (size_t)head * n3;
+        double* yn = c.lb_y.p + (size_t)head * n3;
+        k_lb_pair<<<nbv, th, 0, s>>>(n3, sn, yn, c.xyz.p, c.min_x.p, c.forces_out.p, c.min_f.p);
+        // staging: alpha[head] and beta are rewritten by the next recursion anyway
+        double* sy_stage = alpha + head;
+        double* yy_stage = beta;
+        dot(sn, yn, sy_stage, nullptr);
+        dot(yn, yn, yy_stage, nullptr);
+        double syv = 0.0, yyv = 0.0;
+        MDF_CUDA_TRY(cudaMemcpyAsync(&syv, sy_stage, sizeof(double), cudaMemcpyDeviceToHost, s));
+        MDF_CUDA_TRY(cudaMemcpyAsync(&yyv, yy_stage, sizeof(double), cudaMemcpyDeviceToHost, s));
+        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        if (syv > 1e-12 * std::sqrt(yyv) && yyv > 0.0) {
+            MDF_CUDA_TRY(cudaMemcpyAsync(sy, sy_stage, sizeof(double), cudaMemcpyDeviceToDevice, s));
+            MDF_CUDA_TRY(cudaMemcpyAsync(yy, yy_stage, sizeof(double), cudaMemcpyDeviceToDevice, s));
+            k_lb_recip<<<1, 1, 0, s>>>(sy_stage, rho + head);
+            head = (head + 1) % m;
+            count = std::min(count + 1, m);
+        }
+        e0 = e1;
+        f0 = f1;
     }
     MDF_CUDA_TRY(cudaStreamSynchronize(s));
     r.iterations = it;

@@ -229,6 +229,8 @@ struct Ctx {
     DevBuf<double> md_invm;              // [N] 418.4 / mass (0 = frozen)
     DevBuf<double> md_xref;              // [3N] positions at the last list build
     DevBuf<double> min_x, min_f;         // minimiser: positions and forces before the trial move
+    DevBuf<double> lb_s, lb_y;           // L-BFGS history [m][3N] (position and gradient differences)
+    DevBuf<double> lb_q, lb_part, lb_scal;   // two-loop vector, dot partials, recursion scalars
     unsigned long long* md_host = nullptr;   // mapped host copy of the reduction words (see md.cu)
     unsigned long long* md_hmap = nullptr;   // its device address
     DevBuf<unsigned long long> md_words; // the reduction words in device memory
@@ -264,6 +266,7 @@ void md_run(Ctx& c, long long nsteps, double dt, int chunk, int rebuild_every, d
 void md_state(Ctx& c, double* xyz, double* vel);
 void md_write_rst7(Ctx& c, const char* path, const char* title, double time_ps);
 void minimize(Ctx& c, int max_iter, double fmax_tol, double max_step, mdf_min_report* rep);
+void minimize_lbfgs(Ctx& c, int max_iter, double fmax_tol, double max_step, int history, mdf_min_report* rep);
 void backward(Ctx& c, const double* dL_dF, double dL_dE, double* dL_dq, double* dL_dA, double* dL_dB);
 void pme_adjoint(Ctx& c, double gE, double vscale);
 void build_pairlist(Ctx& c);

@@ -25,7 +25,7 @@ EXPORTS = [
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
-    "mdf_pme_grids", "mdf_minimize", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
+    "mdf_pme_grids", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
 
@@ -77,6 +77,8 @@ def library(path=None):
     lib.mdf_set_parameters.argtypes = [C.c_void_p, dp, dp, dp]
     lib.mdf_backward.argtypes = [C.c_void_p, dp, C.c_double, dp, dp, dp]
     lib.mdf_minimize.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.mdf_min_report)]
+    lib.mdf_minimize_lbfgs.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32,
+                                       C.POINTER(abi.mdf_min_report)]
     lib.mdf_md_init.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_uint64]
     lib.mdf_md_run.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.c_int32, C.c_int32, dp, C.c_int64,
                                C.POINTER(abi.mdf_md_report)]
@@ -266,12 +268,20 @@ class Engine:
                     "backward")
         return dq, dA, dB
 
-    def minimize(self, max_iter=200, fmax_tol=10.0, max_step=0.1):
-        """Steepest descent at the current positions; returns the report dict."""
+    def minimize(self, max_iter=200, fmax_tol=10.0, max_step=0.1, method="sd", history=8):
+        """Minimise from the current positions: method "sd" (steepest descent,
+        mdf_minimize) or "lbfgs" (mdf_minimize_lbfgs with `history` pairs);
+        returns the report dict."""
         r = abi.mdf_min_report()
-        self._check(self.lib.mdf_minimize(self.h, int(max_iter), float(fmax_tol), float(max_step), C.byref(r)),
-                    "minimize")
-        return {k: getattr(r, k) for k, _ in abi.mdf_min_report._fields_}
+        if method == "lbfgs":
+            rc = self.lib.mdf_minimize_lbfgs(self.h, int(max_iter), float(fmax_tol), float(max_step), int(history),
+                                             C.byref(r))
+        elif method == "sd":
+            rc = self.lib.mdf_minimize(self.h, int(max_iter), float(fmax_tol), float(max_step), C.byref(r))
+        else:
+            raise ValueError("method must be 'sd' or 'lbfgs'")
+        self._check(rc, "minimize")
+        return {k: getattr(r, k) for k, _ in abi.mdf_min_report._fields_ if k != "reserved"}
 
     def md_init(self, masses, velocities=None, temperature=300.0, seed=1):
         """Start dynamics: masses [N] amu, velocities [N, 3] A/ps or Maxwell at temperature."""

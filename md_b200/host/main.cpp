@@ -98,10 +98,10 @@ int main(int argc, char* argv[])
         std::printf("nX: %d nY: %d nZ: %d\n", sys.mesh(0), sys.mesh(1), sys.mesh(2));
         if (min_iters > 0) {
             mdf_min_report r;
-            if (mdf_minimize(sys.context(), min_iters, 1.0, 0.1, &r) != MDF_OK)
+            if (mdf_minimize_lbfgs(sys.context(), min_iters, 1.0, 0.1, 8, &r) != MDF_OK)
                 throw std::runtime_error(mdf_last_error(sys.context()));
-            std::printf("minimised: %d iterations, E %.10g -> %.10g, max |F| %.6g\n", r.iterations, r.e_initial,
-                        r.e_final, r.fmax_final);
+            std::printf("minimised (L-BFGS): %d iterations, %d evaluations, E %.10g -> %.10g, max |F| %.6g\n",
+                        r.iterations, r.evaluations, r.e_initial, r.e_final, r.fmax_final);
         }
         if (md_steps > 0) {
             mdf_md_report r;

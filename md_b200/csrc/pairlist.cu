@@ -456,7 +456,6 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
     const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (I >= ncl) return;
-    const int slot = lane >> 3, jj = lane & 7;
     const unsigned below = (1u << lane) - 1u;
     const ILRange L = ilist[I];
     R ax[CLUSTER], ay[CLUSTER], az[CLUSTER], an[CLUSTER];   // -2 x_i and |x_i|^2
@@ -484,36 +483,32 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
         const float gy = fmaxf(0.f, fmaxf(jlo.y + oy - ihi.y, ilo.y - (jhi.y + oy)));
         const float gz = fmaxf(0.f, fmaxf(jlo.z + oz - ihi.z, ilo.z - (jhi.z + oz)));
         const bool cand = have && my.mask != 0ull && gx * gx + gy * gy + gz * gz < rcut2;
-        unsigned todo = __ballot_sync(0xffffffffu, cand);
-        unsigned keepmask = 0u;
-        while (todo) {
-            // this lane's candidate: the (slot+1)-th lowest pending entry
-            unsigned x = todo;
-            if (slot >= 1) x &= x - 1u;
-            if (slot >= 2) x &= x - 1u;
-            if (slot >= 3) x &= x - 1u;
-            const bool valid = x != 0u;
-            const int s = valid ? __ffs(x) - 1 : 0;
-            const int j = __shfl_sync(0xffffffffu, my.j, s);
-            const R px = (R)__shfl_sync(0xffffffffu, ox, s), py = (R)__shfl_sync(0xffffffffu, oy, s),
-                    pz = (R)__shfl_sync(0xffffffffu, oz, s);
-            const V4t vj = xq[j * CLUSTER + jj];
-            const R qx = vj.x + px, qy = vj.y + py, qz = vj.z + pz;
-            const R thr = rc2 - (qx * qx + qy * qy + qz * qz);
-            R m = fma(ax[0], qx, fma(ay[0], qy, fma(az[0], qz, an[0])));
+        // this lane's entry against all 64 atom pairs, U j atoms at a time
+        // (loads issued together), until one pair is in range (U = 4 measured
+        // no faster than 2)
+        constexpr int U = 2;
+        bool keep = false;
+        if (cand) {
+            const R px = (R)ox, py = (R)oy, pz = (R)oz;
+            const V4t* __restrict__ xj = xq + (size_t)my.j * CLUSTER;
+#pragma unroll 1
+            for (int j = 0; j < CLUSTER && !keep; j += U) {
+                V4t v[U];
 #pragma unroll
-            for (int ii = 1; ii < CLUSTER; ++ii) m = fmin(m, fma(ax[ii], qx, fma(ay[ii], qy, fma(az[ii], qz, an[ii]))));
-            const unsigned b = __ballot_sync(0xffffffffu, valid && m < thr);
-            // lane L's own entry, if pending and among the four: its rank is its slot
-            const unsigned rank = __popc(todo & below);
-            if (((todo >> lane) & 1u) && rank < 4u && ((b >> (8u * rank)) & 0xffu)) keepmask |= 1u << lane;
-            todo &= todo - 1u;
-            todo &= todo - 1u;
-            todo &= todo - 1u;
-            todo &= todo - 1u;
+                for (int u = 0; u < U; ++u) v[u] = xj[j + u];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const R qx = v[u].x + px, qy = v[u].y + py, qz = v[u].z + pz;
+                    const R thr = rc2 - (qx * qx + qy * qy + qz * qz);
+                    R m = fma(ax[0], qx, fma(ay[0], qy, fma(az[0], qz, an[0])));
+#pragma unroll
+                    for (int ii = 1; ii < CLUSTER; ++ii) m = fmin(m, fma(ax[ii], qx, fma(ay[ii], qy, fma(az[ii], qz, an[ii]))));
+                    keep = keep || m < thr;
+                }
+            }
         }
-        keepmask = __ballot_sync(0xffffffffu, (keepmask >> lane) & 1u);
-        if ((keepmask >> lane) & 1u) plist_in[L.start + kept + __popc(keepmask & below)] = my;
+        const unsigned keepmask = __ballot_sync(0xffffffffu, keep);
+        if (keep) plist_in[L.start + kept + __popc(keepmask & below)] = my;
         kept += __popc(keepmask);
     }
     if (lane == 0) {

@@ -153,8 +153,23 @@ typedef struct {
      * most FFT lines per block (1, 2 or 4; 0 = 4). */
     int32_t pair_warps;
     int32_t fft_lines;
-    int32_t reserved[2];
+    /* Work split over nranks contexts (one per GPU, PHYSICAL semantics; 0 or
+     * 1 = one context does everything).  Every rank holds all positions;
+     * rank r takes its share of the i clusters (prune + pair kernel), of the
+     * exclusion, 1-4 and bonded lists and of the PME spread and gather; the
+     * charge grid and the fixed-point force/energy accumulators are summed
+     * over the ranks through the mdf_set_allreduce callback, so every rank
+     * ends with the full forces and energies, bit-identical to one context. */
+    int32_t rank;
+    int32_t nranks;
 } mdf_params;
+
+/* Sum of `count` 64-bit integers at d_buf (device memory of the context's
+ * GPU) over all ranks, in place, ordered on `stream` (a cudaStream_t): work
+ * queued on the stream before the call must be in the sum, work queued after
+ * it must see the result.  Two's-complement wrap-around (an NCCL int64 sum,
+ * for instance).  Returns 0 on success. */
+typedef int (*mdf_allreduce_u64)(uint64_t *d_buf, int64_t count, void *stream, void *user);
 
 /* Flags for mdf_compute. */
 #define MDF_COMPUTE_ENERGY 1u
@@ -180,6 +195,12 @@ int mdf_set_positions(mdf_ctx *ctx, const double *xyz);
 /* Device positions, 3N doubles already on ctx's device. */
 int mdf_set_positions_device(mdf_ctx *ctx, const double *d_xyz);
 int mdf_set_box(mdf_ctx *ctx, const double box[3]);
+/* The collective a context with nranks > 1 sums through (required there;
+ * called twice per evaluation: the PME charge grid, then the force and
+ * energy accumulators).  Only mdf_compute / mdf_compute_async / mdf_fetch
+ * support nranks > 1; the other evaluation entry points return
+ * MDF_ERR_UNSUPPORTED. */
+int mdf_set_allreduce(mdf_ctx *ctx, mdf_allreduce_u64 fn, void *user);
 
 /* Cell sort + cluster-pair list with exclusion masks (replaces
  * setup_pairlists / build_lj_pairlist, src/System/NonBondedUtils.cpp:49-57,185-282). */

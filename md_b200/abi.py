@@ -21,6 +21,9 @@ MDF_COMPUTE_ENERGY = 1
 MDF_COMPUTE_FORCES = 2
 MDF_COMPUTE_PME_REFERENCE = 4
 
+# int (*)(uint64_t *d_buf, int64_t count, void *stream, void *user): the sum over ranks (mdf_set_allreduce)
+MDF_ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 
@@ -58,7 +61,7 @@ class mdf_params(C.Structure):
         ("ewald_tol", C.c_double), ("ewald_alpha", C.c_double), ("grid", C.c_int32 * 3),
         ("pme_order", C.c_int32), ("coulomb_const", C.c_double), ("device", C.c_int32),
         ("prune_every", C.c_int32), ("prune_margin", C.c_double), ("pair_warps", C.c_int32),
-        ("fft_lines", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("fft_lines", C.c_int32), ("rank", C.c_int32), ("nranks", C.c_int32),
     ]
 
 

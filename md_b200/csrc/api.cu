@@ -248,9 +248,18 @@ void upload_topology(Ctx& c, const mdf_topology* t)
     MDF_CUDA_TRY(cudaStreamSynchronize(s));
 }
 
+void allreduce_u64(Ctx& c, unsigned long long* d, long long n)
+{
+    if (!c.allreduce) throw ApiError(MDF_ERR_STATE, "nranks > 1 needs mdf_set_allreduce");
+    if (n <= 0) return;
+    if (c.allreduce(reinterpret_cast<uint64_t*>(d), (int64_t)n, (void*)c.stream, c.allreduce_user) != 0)
+        throw ApiError(MDF_ERR_CUDA, "the allreduce callback failed");
+}
+
 void eval_async_impl(Ctx& c, uint32_t flags)
 {
     if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
+    if (distributed(c) && !c.allreduce) throw ApiError(MDF_ERR_STATE, "nranks > 1 needs mdf_set_allreduce");
     if (!c.have_list) build_pairlist(c);
     cudaStream_t s = c.stream;
     bool energy = (flags & MDF_COMPUTE_ENERGY) != 0;
@@ -310,6 +319,15 @@ void eval_async_impl(Ctx& c, uint32_t flags)
         c.have_pme_ref = !phys;
     }
     if (overlap) MDF_CUDA_TRY(cudaStreamWaitEvent(s, c.ev_join, 0));
+    if (distributed(c)) {
+        // every rank's partial forces, energies, virial and pair count, summed
+        // (the status word stays per rank)
+        allreduce_u64(c, c.f_slot.p, 3LL * c.n_slots);
+        allreduce_u64(c, c.f_atom.p, 3LL * c.N);
+        allreduce_u64(c, c.scal.p, NUM_ACC + 1);
+        if (c.counting) allreduce_u64(c, c.npairs_dev.p, 1);
+    }
+    c.counting = false;
     launch_finalize(c, c.forces_out.p, false);
     mark(c, "finalize");
     c.pending = true;
@@ -469,6 +487,11 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         if (c.p.precision != MDF_PREC_FP64 && c.p.precision != MDF_PREC_MIXED)
             throw ApiError(MDF_ERR_INVALID, "unknown precision");
         if (!(c.p.cutoff > 0) || c.p.skin < 0) throw ApiError(MDF_ERR_INVALID, "bad cutoff or skin");
+        if (c.p.nranks < 0 || (c.p.nranks > 1 && (c.p.rank < 0 || c.p.rank >= c.p.nranks)) ||
+            (c.p.nranks <= 1 && c.p.rank != 0))
+            throw ApiError(MDF_ERR_INVALID, "rank must lie in [0, nranks)");
+        if (c.p.nranks > 1 && c.p.semantics != MDF_SEM_PHYSICAL)
+            throw ApiError(MDF_ERR_UNSUPPORTED, "the work split needs PHYSICAL semantics");
         if (c.p.switch_radius > 0 && !(c.p.switch_radius < c.p.cutoff))
             throw ApiError(MDF_ERR_INVALID, "lj_switch must be < lj_cutoff");
         int ndev = 0;
@@ -757,9 +780,19 @@ int mdf_backward(mdf_ctx* ctx, const double* dL_dF, double dL_dE, double* dL_dq,
 {
     if (!ctx) return MDF_ERR_INVALID;
     return guarded(ctx, [&] {
+        if (distributed(ctx->c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
         Ctx& c = ctx->c;
         MDF_CUDA_TRY(cudaSetDevice(c.device));
         backward(c, dL_dF, dL_dE, dL_dq, dL_dA, dL_dB);
+    });
+}
+
+int mdf_set_allreduce(mdf_ctx* ctx, mdf_allreduce_u64 fn, void* user)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        ctx->c.allreduce = fn;
+        ctx->c.allreduce_user = user;
     });
 }
 
@@ -767,6 +800,7 @@ int mdf_minimize(mdf_ctx* ctx, int32_t max_iter, double fmax_tol, double max_ste
 {
     if (!ctx) return MDF_ERR_INVALID;
     return guarded(ctx, [&] {
+        if (distributed(ctx->c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
         MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
         minimize(ctx->c, max_iter, fmax_tol, max_step, report);
     });
@@ -777,6 +811,7 @@ int mdf_minimize_lbfgs(mdf_ctx* ctx, int32_t max_iter, double fmax_tol, double m
 {
     if (!ctx) return MDF_ERR_INVALID;
     return guarded(ctx, [&] {
+        if (distributed(ctx->c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
         MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
         minimize_lbfgs(ctx->c, max_iter, fmax_tol, max_step, history, report);
     });
@@ -786,6 +821,7 @@ int mdf_md_init(mdf_ctx* ctx, const double* masses, const double* velocities, do
 {
     if (!ctx) return MDF_ERR_INVALID;
     return guarded(ctx, [&] {
+        if (distributed(ctx->c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
         MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
         md_init(ctx->c, masses, velocities, temperature, seed);
     });
@@ -796,6 +832,7 @@ int mdf_md_run(mdf_ctx* ctx, int64_t nsteps, double dt_ps, int32_t chunk, int32_
 {
     if (!ctx) return MDF_ERR_INVALID;
     return guarded(ctx, [&] {
+        if (distributed(ctx->c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
         MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
         md_run(ctx->c, nsteps, dt_ps, chunk, rebuild_every, samples, cap, report);
     });

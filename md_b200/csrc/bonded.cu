@@ -16,7 +16,8 @@
 namespace mdf {
 
 struct BondedArgs {
-    int n[6];        // bonds, ub, angles, dihedrals, impropers, cmaps
+    int n[6];        // end index per list: bonds, ub, angles, dihedrals, impropers, cmaps
+    int lo[6];       // first index per list (a rank's share starts there)
     int blk0[7];     // first block of each segment (prefix)
     const int *bond_atoms, *ub_atoms, *angle_atoms, *dih_atoms, *imp_atoms, *cmap_atoms, *cmap_set;
     const double2 *bond_par, *ub_par, *angle_par, *imp_par;
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs A, unsigned long long
     const double PI = 3.14159265358979323846;
     int seg = 0;
     while (seg < 5 && (int)blockIdx.x >= A.blk0[seg + 1]) ++seg;
-    int i = ((int)blockIdx.x - A.blk0[seg]) * blockDim.x + threadIdx.x;
+    int i = A.lo[seg] + ((int)blockIdx.x - A.blk0[seg]) * blockDim.x + threadIdx.x;
     const double* x = A.xyz;
     double e = 0.0;
     int eidx = MDF_E_BOND;
@@ -278,10 +279,16 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs A, unsigned long long
 void launch_bonded(Ctx& c, bool energy)
 {
     BondedArgs A;
-    A.n[0] = c.n_bonds; A.n[1] = c.n_ub; A.n[2] = c.n_angles; A.n[3] = c.n_dih; A.n[4] = c.n_imp; A.n[5] = c.n_cmap;
+    const int total[6] = {c.n_bonds, c.n_ub, c.n_angles, c.n_dih, c.n_imp, c.n_cmap};
     const int th = 256;
     A.blk0[0] = 0;
-    for (int s = 0; s < 6; ++s) A.blk0[s + 1] = A.blk0[s] + (A.n[s] + th - 1) / th;
+    for (int s = 0; s < 6; ++s) {   // this rank's share of each list
+        long long lo, hi;
+        rank_slice(c, total[s], lo, hi);
+        A.lo[s] = (int)lo;
+        A.n[s] = (int)hi;
+        A.blk0[s + 1] = A.blk0[s] + (int)((hi - lo + th - 1) / th);
+    }
     int nblk = A.blk0[6];
     if (nblk == 0) return;
     A.bond_atoms = c.bond_atoms.p; A.ub_atoms = c.ub_atoms.p; A.angle_atoms = c.angle_atoms.p;
@@ -309,6 +316,7 @@ void launch_bonded_into(Ctx& c, bool energy, unsigned long long* f, unsigned lon
 {
     BondedArgs A;
     A.n[0] = c.n_bonds; A.n[1] = c.n_ub; A.n[2] = c.n_angles; A.n[3] = c.n_dih; A.n[4] = c.n_imp; A.n[5] = c.n_cmap;
+    for (int s = 0; s < 6; ++s) A.lo[s] = 0;
     const int th = 256;
     A.blk0[0] = 0;
     for (int s = 0; s < 6; ++s) A.blk0[s + 1] = A.blk0[s] + (A.n[s] + th - 1) / th;

@@ -191,6 +191,7 @@ struct Ctx {
     DevBuf<unsigned long long> npairs_dev;   // [1] atom pairs within the cutoff (first evaluation after a build)
     bool count_next = false;             // the next evaluation counts them
     bool counted = false;                // npairs_dev holds a count for the current list
+    bool counting = false;               // this evaluation counts (its count is summed over ranks)
     DevView<unsigned> status;            // = (unsigned*)&scal[NUM_ACC + 1]
     DevBuf<double> forces_out;           // [3N]
     DevBuf<double> forces_pme_ref;       // [3N]
@@ -237,6 +238,8 @@ struct Ctx {
     unsigned long long* md_dev = nullptr;    // = md_words.p
     unsigned* md_dev_st = nullptr;
     bool md_ready = false;
+    mdf_allreduce_u64 allreduce = nullptr;   // sum over ranks (nranks > 1)
+    void* allreduce_user = nullptr;
     cudaGraph_t md_graph = nullptr;
     cudaGraphExec_t md_exec = nullptr;
     int md_graph_steps = 0;
@@ -288,6 +291,18 @@ void check_host_status(const Ctx& c);
 void exclusive_scan_int(const int* d_in, int* d_out, int n, int* d_total_out, cudaStream_t s);
 
 int grid_blocks(long long n, int threads);
+
+// This rank's share [lo, hi) of n items (the whole range with one rank).
+inline void rank_slice(const Ctx& c, long long n, long long& lo, long long& hi)
+{
+    const long long P = c.p.nranks > 1 ? c.p.nranks : 1, r = P > 1 ? c.p.rank : 0;
+    lo = n * r / P;
+    hi = n * (r + 1) / P;
+}
+inline bool distributed(const Ctx& c) { return c.p.nranks > 1; }
+inline bool rank0(const Ctx& c) { return !distributed(c) || c.p.rank == 0; }
+// In-place sum over the ranks through the registered collective, on c.stream.
+void allreduce_u64(Ctx& c, unsigned long long* d, long long n);
 
 }  // namespace mdf
 

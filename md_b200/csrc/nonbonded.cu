@@ -560,6 +560,7 @@ static bool begin_pair_count(Ctx& c)
     MDF_CUDA_TRY(cudaMemsetAsync(c.npairs_dev.p, 0, sizeof(unsigned long long), c.stream));
     c.count_next = false;
     c.counted = true;
+    c.counting = true;
     return true;
 }
 
@@ -568,17 +569,21 @@ static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, 
 {
     NBParams P = make_params(c);
     const int wpb = pair_warps(c);
-    int nb = grid_blocks(c.n_clusters, wpb);
+    long long lo, hi;
+    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    const int ncl = (int)(hi - lo);
+    if (ncl == 0) return;
+    int nb = grid_blocks(ncl, wpb);
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
-    const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
+    const ILRange* il = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     const int count = begin_pair_count(c) ? 1 : 0;
     if (energy)
-        k_pairs<R, SEM, true><<<nb, 32 * wpb, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
+        k_pairs<R, SEM, true><<<nb, 32 * wpb, 0, c.stream>>>(ncl, il, pl, xq, c.slot_type.p, c.center.p,
                                                                lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
                                                                c.npairs_dev.p, count, c.status.p);
     else
-        k_pairs<R, SEM, false><<<nb, 32 * wpb, 0, c.stream>>>(c.n_clusters, il, pl, xq, c.slot_type.p, c.center.p,
+        k_pairs<R, SEM, false><<<nb, 32 * wpb, 0, c.stream>>>(ncl, il, pl, xq, c.slot_type.p, c.center.p,
                                                                 lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
                                                                 c.npairs_dev.p, count, c.status.p);
     MDF_CUDA_TRY(cudaGetLastError());
@@ -622,13 +627,17 @@ static void launch_pairs_f32(Ctx& c, bool energy)
     const int lj_smem = lj_bytes <= 40 * 1024 ? 1 : 0;
     const size_t dyn = lj_smem ? lj_bytes : 0;
     const int wpb = pair_warps(c);
-    int nb = grid_blocks(c.n_clusters, wpb);
+    long long lo, hi;
+    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    const int ncl = (int)(hi - lo);
+    if (ncl == 0) return;
+    int nb = grid_blocks(ncl, wpb);
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
-    const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
+    const ILRange* il = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     const bool count = begin_pair_count(c);
 #define MDF_PF32(E, S, K_)                                                                                     \
-    k_pairs_f32<E, S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(c.n_clusters, il, pl, c.xq_f.p, c.slot_type.p,       \
+    k_pairs_f32<E, S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(ncl, il, pl, c.xq_f.p, c.slot_type.p,                \
                                                            c.centerf.p, c.ljAB4_f.p, c.ntp, lj_smem,              \
                                                            (float)P.kc, K, sh, c.f_slot.p, c.n_slots, c.acc.p,   \
                                                            c.npairs_dev.p, c.status.p)
@@ -663,20 +672,25 @@ void launch_exclusions(Ctx& c, bool energy)
     NBParams P = make_params(c);
     const int th = 256;
     bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
-    if (c.n_excl > 0) {
-        int nb = grid_blocks(c.n_excl, th);
+    long long e0, e1, p0, p1;   // this rank's exclusions and 1-4 pairs
+    rank_slice(c, c.n_excl, e0, e1);
+    rank_slice(c, c.n_14, p0, p1);
+    if (e1 > e0) {
+        const int ne = (int)(e1 - e0);
+        int nb = grid_blocks(ne, th);
 #define MDF_EXCL(S, E)                                                                                          \
-    k_exclusions<S, E><<<nb, th, 0, c.stream>>>(c.n_excl, c.excl_pairs.p, c.excl_is14.p, c.xyz.p, c.q.p, P, c.N, \
-                                                c.f_atom.p, c.acc.p, c.status.p)
+    k_exclusions<S, E><<<nb, th, 0, c.stream>>>(ne, c.excl_pairs.p + 2 * e0, c.excl_is14.p + e0, c.xyz.p, c.q.p, \
+                                                P, c.N, c.f_atom.p, c.acc.p, c.status.p)
         if (phys) { if (energy) MDF_EXCL(MDF_SEM_PHYSICAL, true); else MDF_EXCL(MDF_SEM_PHYSICAL, false); }
         else if (energy) MDF_EXCL(MDF_SEM_REFERENCE, true);
 #undef MDF_EXCL
         if (phys || energy) c.launches += 1;
     }
-    if (c.n_14 > 0) {
-        int nb = grid_blocks(c.n_14, th);
+    if (p1 > p0) {
+        const int n14 = (int)(p1 - p0);
+        int nb = grid_blocks(n14, th);
 #define MDF_P14(S, E)                                                                                             \
-    k_pairs14<S, E><<<nb, th, 0, c.stream>>>(c.n_14, c.pairs14.p, c.p14_scale.p, c.xyz.p, c.q.p, c.type.p,        \
+    k_pairs14<S, E><<<nb, th, 0, c.stream>>>(n14, c.pairs14.p + 2 * p0, c.p14_scale.p + p0, c.xyz.p, c.q.p, c.type.p, \
                                              c.lj14AB.p, c.ljvalid.p, P, c.N, c.f_atom.p, c.acc.p, c.status.p)
         if (phys) { if (energy) MDF_P14(MDF_SEM_PHYSICAL, true); else MDF_P14(MDF_SEM_PHYSICAL, false); }
         else { if (energy) MDF_P14(MDF_SEM_REFERENCE, true); else MDF_P14(MDF_SEM_REFERENCE, false); }

@@ -453,11 +453,12 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
     __shared__ float sh[27][6];
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
     __syncthreads();
-    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;   // index into this launch's ilist range
     const int lane = threadIdx.x & 31;
-    if (I >= ncl) return;
+    if (w >= ncl) return;
     const unsigned below = (1u << lane) - 1u;
-    const ILRange L = ilist[I];
+    const ILRange L = ilist[w];
+    const int I = L.i;
     R ax[CLUSTER], ay[CLUSTER], az[CLUSTER], an[CLUSTER];   // -2 x_i and |x_i|^2
 #pragma unroll
     for (int k = 0; k < CLUSTER; ++k) {
@@ -514,7 +515,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
     if (lane == 0) {
         ILRange r;
         r.i = I; r.start = L.start; r.count = kept; r.pad = 0;
-        ilist_in[I] = r;
+        ilist_in[w] = r;
         if (kept) atomicAdd(n_in, (unsigned long long)kept);
     }
 }
@@ -535,15 +536,20 @@ void prune_pairlist(Ctx& c)
         }
     }
     MDF_CUDA_TRY(cudaMemsetAsync(c.n_in.p, 0, sizeof(unsigned long long), c.stream));
-    int blocks = grid_blocks((long long)c.n_clusters * 32, th);
-    if (c.p.precision == MDF_PREC_MIXED)
-        k_prune<float><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_f.p, c.centerf.p,
-                                                   c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc), c.ilist_in.p,
-                                                   c.plist_in.p, c.n_in.p);
-    else
-        k_prune<double><<<blocks, th, 0, c.stream>>>(c.n_clusters, c.ilist.p, c.plist.p, c.xq_d.p, c.centerf.p,
-                                                    c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc), c.ilist_in.p,
-                                                    c.plist_in.p, c.n_in.p);
+    long long lo, hi;
+    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    const int ncl = (int)(hi - lo);
+    int blocks = grid_blocks((long long)ncl * 32, th);
+    if (ncl > 0) {
+        if (c.p.precision == MDF_PREC_MIXED)
+            k_prune<float><<<blocks, th, 0, c.stream>>>(ncl, c.ilist.p + lo, c.plist.p, c.xq_f.p, c.centerf.p,
+                                                       c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc),
+                                                       c.ilist_in.p + lo, c.plist_in.p, c.n_in.p);
+        else
+            k_prune<double><<<blocks, th, 0, c.stream>>>(ncl, c.ilist.p + lo, c.plist.p, c.xq_d.p, c.centerf.p,
+                                                        c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc),
+                                                        c.ilist_in.p + lo, c.plist_in.p, c.n_in.p);
+    }
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
     c.pruned_valid = true;

@@ -408,12 +408,12 @@ struct GridGeom {
 };
 
 template <typename R>
-__global__ void k_spread4(int nslots, const int* __restrict__ slot_atom, const double* __restrict__ xyz,
+__global__ void k_spread4(int s0, int s1, const int* __restrict__ slot_atom, const double* __restrict__ xyz,
                           const double* __restrict__ q, GridGeom g, unsigned long long* __restrict__ qgrid,
                           unsigned* st)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nslots) return;
+    int s = s0 + blockIdx.x * blockDim.x + threadIdx.x;   // slots [s0, s1)
+    if (s >= s1) return;
     int a = slot_atom[s];
     if (a < 0) return;
     double qa = q[a];
@@ -454,12 +454,12 @@ __global__ void k_spread4(int nslots, const int* __restrict__ slot_atom, const d
 }
 
 template <typename R>
-__global__ void k_gather4(int nslots, const int* __restrict__ slot_atom, const double* __restrict__ xyz,
-                          const double* __restrict__ q, GridGeom g, const R* __restrict__ phi,
-                          unsigned long long* __restrict__ fslot, unsigned* st)
+__global__ void k_gather4(int s0, int s1, int nslots, const int* __restrict__ slot_atom,
+                          const double* __restrict__ xyz, const double* __restrict__ q, GridGeom g,
+                          const R* __restrict__ phi, unsigned long long* __restrict__ fslot, unsigned* st)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nslots) return;
+    int s = s0 + blockIdx.x * blockDim.x + threadIdx.x;   // slots [s0, s1) of nslots
+    if (s >= s1) return;
     int a = slot_atom[s];
     if (a < 0) return;
     double qa = q[a];
@@ -906,18 +906,24 @@ static void run_pme(Ctx& c, bool energy)
     const long long ntot = (long long)c.K[0] * c.K[1] * c.K[2];
     MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
     const int th = 256;
+    long long s0, s1;
+    rank_slice(c, c.n_slots, s0, s1);   // this rank's slots (all of them with one rank)
     if (!ref) {
-        k_spread4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g,
-                                                                      c.qgrid.p, c.status.p);
+        if (s1 > s0)
+            k_spread4<R><<<grid_blocks(s1 - s0, th), th, 0, c.stream>>>((int)s0, (int)s1, c.slot_atom.p, c.xyz.p,
+                                                                       c.q.p, B.g, c.qgrid.p, c.status.p);
+        if (distributed(c)) allreduce_u64(c, c.qgrid.p, ntot);   // the whole charge grid on every rank
     } else {
         k_spread_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, B.g, c.qgrid.p);
     }
     mark(c, "pme_spread");
-    conv_chain<R>(c, B, energy);
+    conv_chain<R>(c, B, energy && rank0(c));   // reciprocal energy and virial counted once
     mark(c, "pme_fft_conv");
     if (!ref) {
-        k_gather4<R><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g,
-                                                                      B.rg, c.f_slot.p, c.status.p);
+        if (s1 > s0)
+            k_gather4<R><<<grid_blocks(s1 - s0, th), th, 0, c.stream>>>((int)s0, (int)s1, c.n_slots, c.slot_atom.p,
+                                                                       c.xyz.p, c.q.p, B.g, B.rg, c.f_slot.p,
+                                                                       c.status.p);
     } else {
         c.forces_pme_ref.alloc(3 * (size_t)c.N);
         k_gather_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, B.g,
@@ -1099,7 +1105,7 @@ static void run_pme_adjoint(Ctx& c, double gE)
     const int th = 256, nb = grid_blocks(c.n_slots, th);
     // phi = C Q
     MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
-    k_spread4<R><<<nb, th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g, c.qgrid.p, c.status.p);
+    k_spread4<R><<<nb, th, 0, c.stream>>>(0, c.n_slots, c.slot_atom.p, c.xyz.p, c.q.p, B.g, c.qgrid.p, c.status.p);
     conv_chain<R>(c, B, false);
     k_adj_gather_phi<R><<<nb, th, 0, c.stream>>>(c.n_slots, c.slot_atom.p, c.xyz.p, B.g, B.rg, vs, gE,
                                                  c.adj_dq_slot.p, c.status.p);

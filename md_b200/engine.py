@@ -25,7 +25,7 @@ EXPORTS = [
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
-    "mdf_pme_grids", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
+    "mdf_pme_grids", "mdf_set_allreduce", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
 
@@ -77,6 +77,7 @@ def library(path=None):
     lib.mdf_set_parameters.argtypes = [C.c_void_p, dp, dp, dp]
     lib.mdf_backward.argtypes = [C.c_void_p, dp, C.c_double, dp, dp, dp]
     lib.mdf_minimize.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.mdf_min_report)]
+    lib.mdf_set_allreduce.argtypes = [C.c_void_p, abi.MDF_ALLREDUCE_FN, C.c_void_p]
     lib.mdf_minimize_lbfgs.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32,
                                        C.POINTER(abi.mdf_min_report)]
     lib.mdf_md_init.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_uint64]
@@ -145,7 +146,7 @@ class Engine:
 
     def __init__(self, flat, box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, cutoff=10.0,
                  skin=2.0, switch_radius=9.0, ewald_tol=1e-5, ewald_alpha=0.0, grid=(0, 0, 0), pme_order=4,
-                 device=0, prune_every=1, prune_margin=0.0):
+                 device=0, prune_every=1, prune_margin=0.0, rank=0, nranks=1):
         self.lib = library()
         self.flat = flat
         self.natoms = flat.natoms
@@ -158,6 +159,7 @@ class Engine:
         p.cutoff, p.skin, p.switch_radius = float(cutoff), float(skin), float(switch_radius)
         p.ewald_tol, p.ewald_alpha, p.pme_order, p.device = float(ewald_tol), float(ewald_alpha), int(pme_order), int(device)
         p.prune_every, p.prune_margin = int(prune_every), float(prune_margin)
+        p.rank, p.nranks = int(rank), int(nranks)
         self.params = p
         h = C.c_void_p()
         rc = self.lib.mdf_create(C.byref(flat.struct()), C.byref(p), C.byref(h))
@@ -205,6 +207,14 @@ class Engine:
 
     def set_positions_device(self, ptr):
         self._check(self.lib.mdf_set_positions_device(self.h, C.c_void_p(ptr)), "set_positions_device")
+
+    def set_allreduce(self, fn):
+        """The sum over ranks for a split context (nranks > 1): fn(ptr, count,
+        stream, user) -> 0, summing `count` int64 at device pointer `ptr` in place,
+        ordered on the CUDA stream handle `stream` (md_b200.distributed builds
+        one from a torch.distributed group)."""
+        self._allreduce_cb = abi.MDF_ALLREDUCE_FN(fn)   # kept alive with the engine
+        self._check(self.lib.mdf_set_allreduce(self.h, self._allreduce_cb, None), "set_allreduce")
 
     def set_box(self, box):
         b = np.ascontiguousarray(box, dtype=np.float64)

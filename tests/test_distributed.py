@@ -1,0 +1,147 @@
+"""The split evaluation (mdf_params.rank / nranks, mdf_set_allreduce).
+
+CPU (gloo, 2 ranks): the collective callback of md_b200.distributed, called
+through a C function pointer as the library calls it, sums int64 buffers in
+place across the ranks, two's-complement wrap-around included.
+
+GPU (gloo, 2 and 3 ranks sharing cuda:0; the collectives run on the host,
+no kernel waits on another rank): every rank ends with forces identical bit
+for bit to one context evaluating everything, mixed and FP64, on the first
+evaluation after a list build (pair counting on) and the next; energies agree
+to 1e-12 relative + 1e-8 (per-block FP64 sums are rounded to the 2^-32
+fixed point before they are added, and the blocks differ) and the pair count
+is exact.  Contexts with
+nranks > 1 refuse to evaluate without a collective, and the entry points
+that do not support the split say so.
+"""
+import ctypes as C
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from md_b200 import abi
+
+
+def _port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _run(worker, world, *args, timeout=300):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _port()
+    procs = [ctx.Process(target=worker, args=(r, world, port, q) + args) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=timeout) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    return [res[r] for r in range(world)]
+
+
+def _init(rank, world, port):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    return dist
+
+
+def _cb_worker(rank, world, port, q):
+    from md_b200 import distributed
+    dist = _init(rank, world, port)
+    fn = abi.MDF_ALLREDUCE_FN(distributed.torch_allreduce(host=True))
+    buf = np.array([rank + 1, -(rank + 1) * 1000, 2 ** 62, 7], dtype=np.int64)
+    rc = fn(buf.ctypes.data, 4, None, None)   # as the library would call it
+    q.put((rank, (rc, buf.tolist())))
+    dist.destroy_process_group()
+
+
+def test_allreduce_callback_two_rank_gloo_cpu():
+    res = _run(_cb_worker, 2)
+    wrap = -2 ** 63   # 2^62 + 2^62 wraps like an int64 accumulator
+    for rc, vals in res:
+        assert rc == 0
+        assert vals == [3, -3000, wrap, 14]
+
+
+def _eval_worker(rank, world, port, q, cfg, prec):
+    from md_b200 import distributed, engine, synth
+    from tests import helpers as H
+    dist = _init(rank, world, port)
+    s = H.system(cfg)
+    flat = H.flat(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=prec, ewald_tol=1e-5,
+                        grid=synth.GRIDS[cfg], rank=rank, nranks=world)
+    eng.set_allreduce(distributed.torch_allreduce())
+    eng.set_positions(s.coords)
+    eng.build_pairlist()
+    out = []
+    for _ in range(2):
+        E, F = eng.compute()
+        out.append((E, F, eng.pairlist_info()["pairs_in_cutoff"]))
+    eng.close()
+    q.put((rank, out))
+    dist.destroy_process_group()
+
+
+def _single(cfg, prec):
+    from md_b200 import engine, synth
+    from tests import helpers as H
+    s = H.system(cfg)
+    flat = H.flat(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=prec, ewald_tol=1e-5,
+                        grid=synth.GRIDS[cfg])
+    eng.set_positions(s.coords)
+    eng.build_pairlist()
+    out = []
+    for _ in range(2):
+        E, F = eng.compute()
+        out.append((E, F, eng.pairlist_info()["pairs_in_cutoff"]))
+    eng.close()
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg,world,prec", [("small", 2, abi.MDF_PREC_MIXED), ("small", 3, abi.MDF_PREC_FP64),
+                                            ("c0", 2, abi.MDF_PREC_MIXED)])
+def test_split_evaluation_matches_one_context(cfg, world, prec):
+    res = _run(_eval_worker, world, cfg, prec)
+    ref = _single(cfg, prec)
+    for out in res:
+        for (E, F, npair), (E0, F0, np0) in zip(out, ref):
+            assert np.array_equal(F, F0)
+            assert npair == np0
+            for k in abi.E_NAMES + ["total"]:
+                assert abs(E[k] - E0[k]) <= 1e-12 * abs(E0[k]) + 1e-8, (k, E[k], E0[k])
+
+
+@pytest.mark.gpu
+def test_split_context_needs_a_collective_and_refuses_the_rest():
+    from md_b200 import engine, synth
+    from tests import helpers as H
+    s = H.system("tiny")
+    flat = H.flat(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED,
+                        grid=synth.GRIDS["tiny"], rank=1, nranks=2)
+    eng.set_positions(s.coords)
+    with pytest.raises(engine.MDFError) as ei:
+        eng.compute()
+    assert ei.value.status == abi.MDF_ERR_STATE
+    with pytest.raises(engine.MDFError) as ei:
+        eng.md_init(s.mass)
+    assert ei.value.status == abi.MDF_ERR_UNSUPPORTED
+    with pytest.raises(engine.MDFError) as ei:
+        eng.minimize(max_iter=1, method="lbfgs")
+    assert ei.value.status == abi.MDF_ERR_UNSUPPORTED
+    eng.close()
+    for rank, nranks, sem in ((2, 2, abi.MDF_SEM_PHYSICAL), (0, 2, abi.MDF_SEM_REFERENCE)):
+        with pytest.raises(engine.MDFError):
+            engine.Engine(flat, s.box, semantics=sem, precision=abi.MDF_PREC_FP64, grid=synth.GRIDS["tiny"],
+                          rank=rank, nranks=nranks)

@@ -81,6 +81,7 @@ def parse():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-md", action="store_true")
+    ap.add_argument("--no-split", action="store_true", help="skip the c4 evaluation split over the ranks (N > 1)")
     ap.add_argument("--profile", metavar="CONFIG", default=None,
                     help="profiling run: build CONFIG (tiny, small, c0, c1, c4), run --warmup + --steps "
                          "evaluations, print the per-phase times and exit (for ncu)")
@@ -348,6 +349,64 @@ def cufft_check(eng, dev, s, ours_ms, reps=20):
     ref = out.cpu().numpy().astype(np.float64) * (K[0] * K[1] * K[2])
     return {"grid": list(K), "ours_ms": ours_ms, "cufft_ms": a.elapsed_time(b) / reps,
             "rel_l2_diff": float(np.linalg.norm(P - ref) / np.linalg.norm(ref))}
+
+
+def split_bench(dev, ws, rank, cfg="c4", steps=20, warmup=3):
+    """c4 (960k atoms, PME 216^3; `cfg` another named workload) evaluated by all ranks together: each rank
+    takes its share of the pair, bonded and PME spread/gather work and the
+    int64 charge grid and accumulators are summed with NCCL all-reduces
+    (mdf_params.rank / nranks + mdf_set_allreduce).  Time: CUDA events on each
+    rank's stream around `steps` evaluations, max over ranks.  Rank 0 also
+    times one context doing the whole evaluation, for the speed-up."""
+    import torch
+    import torch.distributed as dist
+    from md_b200 import abi, distributed, engine, synth, topology
+    s = synth.make_config(cfg)
+    flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    kw = dict(semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, ewald_tol=1e-5,
+              grid=synth.GRIDS[cfg], device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def timed(eng, collective):
+        eng.set_stream(stream.cuda_stream)
+        eng.set_positions(s.coords)
+        eng.build_pairlist()
+        for _ in range(warmup):
+            eng.compute_async(energy=True)
+            eng.fetch(forces=False)
+        if collective:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(steps):
+            eng.compute_async(energy=True)
+            eng.fetch(forces=False)
+        b.record(stream)
+        torch.cuda.synchronize(dev)
+        t = a.elapsed_time(b) / 1e3
+        if collective:
+            tt = torch.tensor([t], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    eng = engine.Engine(flat, s.box, rank=rank, nranks=ws, **kw)
+    eng.set_allreduce(distributed.torch_allreduce())
+    t_split = timed(eng, True)
+    eng.close()
+    out = {"workload": "%s: %d atoms, PME %s, cutoff 10 A, mixed precision; one evaluation split over %d ranks "
+                       "(int64 all-reduce of the charge grid and the force/energy accumulators)"
+                       % (cfg, s.natoms, "x".join(map(str, synth.GRIDS[cfg])), ws),
+           "n_ranks": ws, "evals_per_s": steps / t_split, "ms_per_eval": t_split / steps * 1e3}
+    if rank == 0:
+        one = engine.Engine(flat, s.box, **kw)
+        t_one = timed(one, False)
+        one.close()
+        out["one_gpu_evals_per_s"] = steps / t_one
+        out["speedup"] = t_one / t_split
+    dist.barrier()
+    return out
 
 
 def md_bench(dev, steps=1000, equil=200):
@@ -665,6 +724,9 @@ def main():
     dynamics = None
     if rank == 0 and ws == 1 and not args.no_md:
         dynamics = md_bench(dev)
+    split = None
+    if ws > 1 and not args.no_split:
+        split = split_bench(dev, ws, rank)
 
     if rank == 0:
         line = {
@@ -700,6 +762,7 @@ def main():
             "adjoint": adj,
             "batched": batched,
             "dynamics": dynamics,
+            "c4_split": split,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),

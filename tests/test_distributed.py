@@ -145,3 +145,22 @@ def test_split_context_needs_a_collective_and_refuses_the_rest():
         with pytest.raises(engine.MDFError):
             engine.Engine(flat, s.box, semantics=sem, precision=abi.MDF_PREC_FP64, grid=synth.GRIDS["tiny"],
                           rank=rank, nranks=nranks)
+
+
+def _bench_worker(rank, world, port, q):
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    dist = _init(rank, world, port)
+    out = bench.split_bench(0, world, rank, cfg="small", steps=3, warmup=1)
+    q.put((rank, out))
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_bench_split_line_runs():
+    """bench.py's split measurement (run by the driver at N > 1 with NCCL)
+    end to end with 2 gloo ranks on one GPU and a small workload."""
+    res = _run(_bench_worker, 2)
+    assert res[0]["n_ranks"] == 2 and res[0]["evals_per_s"] > 0 and res[0]["speedup"] > 0
+    assert "speedup" not in res[1]

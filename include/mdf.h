@@ -358,6 +358,13 @@ const char *mdf_batch_last_error(const mdf_batch *b);
 int mdf_batch_info(const mdf_batch *b, int64_t *n_systems, int64_t *total_atoms, int64_t *graph_kernels);
 /* Host positions [3 * total atoms]; copied at the call, uploaded inside the graph. */
 int mdf_batch_set_positions(mdf_batch *b, const double *xyz);
+/* The batch's own pinned host buffers ([3 * total atoms] each, system order):
+ * the graph copies positions from the first and forces into the second, so a
+ * caller that writes positions there (and passes that pointer to
+ * mdf_batch_set_positions) and reads forces there (forces = NULL in
+ * mdf_batch_compute / mdf_batch_fetch) moves no extra host copy.  Valid until
+ * mdf_batch_destroy. */
+int mdf_batch_host_buffers(mdf_batch *b, double **positions, double **forces);
 int mdf_batch_build_pairlists(mdf_batch *b);
 /* One batch evaluation; forces [3 * total atoms] and energies [nsys] to host
  * (either may be NULL).  Returns after the evaluation. */

@@ -282,9 +282,17 @@ int mdf_batch_set_positions(mdf_batch* b, const double* xyz)
 {
     if (!b || !xyz) return MDF_ERR_INVALID;
     return batch_guard(b, [&] {
-        memcpy(b->h_pos, xyz, sizeof(double) * b->total);
+        if (xyz != b->h_pos) memcpy(b->h_pos, xyz, sizeof(double) * b->total);   // own buffer: written in place
         b->have_positions = true;
     });
+}
+
+int mdf_batch_host_buffers(mdf_batch* b, double** positions, double** forces)
+{
+    if (!b) return MDF_ERR_INVALID;
+    if (positions) *positions = b->h_pos;
+    if (forces) *forces = b->h_forces;
+    return MDF_OK;
 }
 
 int mdf_batch_build_pairlists(mdf_batch* b)

@@ -484,32 +484,69 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
         const float gy = fmaxf(0.f, fmaxf(jlo.y + oy - ihi.y, ilo.y - (jhi.y + oy)));
         const float gz = fmaxf(0.f, fmaxf(jlo.z + oz - ihi.z, ilo.z - (jhi.z + oz)));
         const bool cand = have && my.mask != 0ull && gx * gx + gy * gy + gz * gz < rcut2;
-        // this lane's entry against all 64 atom pairs, U j atoms at a time
-        // (loads issued together), until one pair is in range (U = 4 measured
-        // no faster than 2)
-        constexpr int U = 2;
-        bool keep = false;
-        if (cand) {
-            const R px = (R)ox, py = (R)oy, pz = (R)oz;
-            const V4t* __restrict__ xj = xq + (size_t)my.j * CLUSTER;
+        unsigned keepmask;
+        if constexpr (sizeof(R) == 4) {
+            // FP32: this lane's entry against all 64 atom pairs, two j atoms at
+            // a time (loads issued together), until one pair is in range
+            bool keep = false;
+            if (cand) {
+                const R px = (R)ox, py = (R)oy, pz = (R)oz;
+                const V4t* __restrict__ xj = xq + (size_t)my.j * CLUSTER;
 #pragma unroll 1
-            for (int j = 0; j < CLUSTER && !keep; j += U) {
-                V4t v[U];
+                for (int j = 0; j < CLUSTER && !keep; j += 2) {
+                    V4t v[2];
+                    v[0] = xj[j];
+                    v[1] = xj[j + 1];
 #pragma unroll
-                for (int u = 0; u < U; ++u) v[u] = xj[j + u];
+                    for (int u = 0; u < 2; ++u) {
+                        const R qx = v[u].x + px, qy = v[u].y + py, qz = v[u].z + pz;
+                        const R thr = rc2 - (qx * qx + qy * qy + qz * qz);
+                        R m = fma(ax[0], qx, fma(ay[0], qy, fma(az[0], qz, an[0])));
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const R qx = v[u].x + px, qy = v[u].y + py, qz = v[u].z + pz;
-                    const R thr = rc2 - (qx * qx + qy * qy + qz * qz);
-                    R m = fma(ax[0], qx, fma(ay[0], qy, fma(az[0], qz, an[0])));
-#pragma unroll
-                    for (int ii = 1; ii < CLUSTER; ++ii) m = fmin(m, fma(ax[ii], qx, fma(ay[ii], qy, fma(az[ii], qz, an[ii]))));
-                    keep = keep || m < thr;
+                        for (int ii = 1; ii < CLUSTER; ++ii)
+                            m = fmin(m, fma(ax[ii], qx, fma(ay[ii], qy, fma(az[ii], qz, an[ii]))));
+                        keep = keep || m < thr;
+                    }
                 }
             }
+            keepmask = __ballot_sync(0xffffffffu, keep);
+        } else {
+            // FP64 (half-rate arithmetic: idle lanes cost more than bookkeeping):
+            // the pending candidates four at a time, eight lanes (one j atom
+            // each) per candidate
+            const int slot = lane >> 3, jj = lane & 7;
+            unsigned todo = __ballot_sync(0xffffffffu, cand);
+            unsigned mine = 0u;
+            while (todo) {
+                // this lane's candidate: the (slot+1)-th lowest pending entry
+                unsigned x = todo;
+                if (slot >= 1) x &= x - 1u;
+                if (slot >= 2) x &= x - 1u;
+                if (slot >= 3) x &= x - 1u;
+                const bool valid = x != 0u;
+                const int sl = valid ? __ffs(x) - 1 : 0;
+                const int j = __shfl_sync(0xffffffffu, my.j, sl);
+                const R px = (R)__shfl_sync(0xffffffffu, ox, sl), py = (R)__shfl_sync(0xffffffffu, oy, sl),
+                        pz = (R)__shfl_sync(0xffffffffu, oz, sl);
+                const V4t vj = xq[j * CLUSTER + jj];
+                const R qx = vj.x + px, qy = vj.y + py, qz = vj.z + pz;
+                const R thr = rc2 - (qx * qx + qy * qy + qz * qz);
+                R m = fma(ax[0], qx, fma(ay[0], qy, fma(az[0], qz, an[0])));
+#pragma unroll
+                for (int ii = 1; ii < CLUSTER; ++ii)
+                    m = fmin(m, fma(ax[ii], qx, fma(ay[ii], qy, fma(az[ii], qz, an[ii]))));
+                const unsigned bal = __ballot_sync(0xffffffffu, valid && m < thr);
+                // lane L's own entry, if pending and among the four: its rank is its slot
+                const unsigned rank = __popc(todo & below);
+                if (((todo >> lane) & 1u) && rank < 4u && ((bal >> (8u * rank)) & 0xffu)) mine = 1u;
+                todo &= todo - 1u;
+                todo &= todo - 1u;
+                todo &= todo - 1u;
+                todo &= todo - 1u;
+            }
+            keepmask = __ballot_sync(0xffffffffu, mine != 0u);
         }
-        const unsigned keepmask = __ballot_sync(0xffffffffu, keep);
-        if (keep) plist_in[L.start + kept + __popc(keepmask & below)] = my;
+        if ((keepmask >> lane) & 1u) plist_in[L.start + kept + __popc(keepmask & below)] = my;
         kept += __popc(keepmask);
     }
     if (lane == 0) {

@@ -23,7 +23,7 @@ EXPORTS = [
     "mdf_pairlist_info", "mdf_enable_timing", "mdf_kernel_times", "mdf_cmap_coefficients",
     "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
-    "mdf_batch_set_positions", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
+    "mdf_batch_set_positions", "mdf_batch_host_buffers", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
     "mdf_pme_grids", "mdf_set_allreduce", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
@@ -94,6 +94,7 @@ def library(path=None):
     lib.mdf_batch_last_error.restype = C.c_char_p
     lib.mdf_batch_info.argtypes = [vp] + [C.POINTER(C.c_int64)] * 3
     lib.mdf_batch_set_positions.argtypes = [vp, dp]
+    lib.mdf_batch_host_buffers.argtypes = [vp, C.POINTER(dp), C.POINTER(dp)]
     lib.mdf_batch_build_pairlists.argtypes = [vp]
     lib.mdf_batch_compute.argtypes = [vp, C.c_uint32, dp, C.POINTER(abi.mdf_energies)]
     lib.mdf_batch_launch.argtypes = [vp, C.c_uint32, vp]
@@ -411,20 +412,43 @@ class Batch:
         except Exception:
             pass
 
-    def set_positions(self, coords_list):
-        x = np.ascontiguousarray(np.concatenate([np.asarray(c, float).reshape(-1) for c in coords_list]))
+    def host_buffers(self):
+        """(positions, forces): numpy [total atoms, 3] views of the batch's pinned
+        host buffers (mdf_batch_host_buffers).  Positions written into the first
+        and passed to set_positions, and forces read from the second after
+        compute(copy_forces=False), move no extra host copy."""
+        dp_ = C.POINTER(C.c_double)
+        p, f = dp_(), dp_()
+        self._check(self.lib.mdf_batch_host_buffers(self.h, C.byref(p), C.byref(f)), "host_buffers")
+        n = int(self.offsets[-1])
+        return (np.ctypeslib.as_array(p, shape=(n, 3)), np.ctypeslib.as_array(f, shape=(n, 3)))
+
+    def set_positions(self, coords):
+        """coords: a list of [n_k, 3] arrays, one per system, or one [total, 3]
+        array (the positions view of host_buffers() is used in place)."""
+        if isinstance(coords, np.ndarray) and coords.dtype == np.float64 and coords.flags.c_contiguous \
+                and coords.size == 3 * int(self.offsets[-1]):
+            x = coords
+        else:
+            x = np.ascontiguousarray(np.concatenate([np.asarray(c, float).reshape(-1) for c in coords]))
         self._check(self.lib.mdf_batch_set_positions(self.h, x.ctypes.data_as(C.POINTER(C.c_double))), "set_positions")
 
     def build_pairlists(self):
         self._check(self.lib.mdf_batch_build_pairlists(self.h), "build_pairlists")
 
-    def compute(self, energy=True, forces=True):
-        """Per system: (energies dict or None, forces [n_k, 3] or None)."""
+    def compute(self, energy=True, forces=True, copy_forces=True):
+        """Per system: (energies dict or None, forces [n_k, 3] or None).  With
+        copy_forces=False the forces are views of the pinned host buffer (valid
+        until the next evaluation)."""
         flags = (abi.MDF_COMPUTE_ENERGY if energy else 0) | (abi.MDF_COMPUTE_FORCES if forces else 0)
-        F = np.zeros(3 * int(self.offsets[-1])) if forces else None
+        if forces and not copy_forces:
+            F = self.host_buffers()[1].reshape(-1)
+            fptr = None
+        else:
+            F = np.zeros(3 * int(self.offsets[-1])) if forces else None
+            fptr = F.ctypes.data_as(C.POINTER(C.c_double)) if forces else None
         E = (abi.mdf_energies * self.n)() if energy else None
-        self._check(self.lib.mdf_batch_compute(self.h, flags, F.ctypes.data_as(C.POINTER(C.c_double))
-                                               if forces else None, E), "compute")
+        self._check(self.lib.mdf_batch_compute(self.h, flags, fptr, E), "compute")
         out = []
         for k in range(self.n):
             e = E[k].as_dict() if energy else None

@@ -69,6 +69,27 @@ def test_batch_equals_single_systems(prec):
     b.close()
 
 
+def test_batch_pinned_host_buffers_in_place():
+    """Positions written into the batch's pinned buffer and forces read from
+    its pinned force buffer give the same results as the copying calls."""
+    ss = systems()
+    flats = _flats(ss)
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
+    pos, frc = b.host_buffers()
+    pos[:] = np.concatenate([s.coords for s in ss])
+    b.set_positions(pos)
+    res = b.compute(copy_forces=False)
+    ref = _singles(ss, flats, MIXED)
+    _same(res, ref, 1e-12)
+    assert np.shares_memory(res[0][1], frc)
+    rng = np.random.default_rng(4)
+    pos += rng.uniform(-0.1, 0.1, pos.shape)          # new frame written in place
+    moved = [pos[b.offsets[k]:b.offsets[k + 1]].copy() for k in range(len(ss))]
+    b.set_positions(pos)
+    _same(b.compute(copy_forces=False), _singles(ss, flats, MIXED, coords=moved), 1e-12)
+    b.close()
+
+
 def test_batch_autotune_keeps_results_and_follows_positions():
     ss = systems()
     flats = _flats(ss)

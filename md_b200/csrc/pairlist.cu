@@ -632,14 +632,14 @@ void build_pairlist(Ctx& c)
     for (int attempt = 0; attempt < 6; ++attempt) {
         c.ncol_x = std::max(1, (int)std::floor(c.box[0] / side));
         c.ncol_y = std::max(1, (int)std::floor(c.box[1] / side));
-        double wx = c.box[0] / c.ncol_x, wy = c.box[1] / c.ncol_y;
-        int Rx = (int)std::floor(rlist / wx) + 1, Ry = (int)std::floor(rlist / wy) + 1;
-        if (Rx >= c.ncol_x || Ry >= c.ncol_y) {
-            // columns too wide for the one-image search: use more, thinner columns
-            side *= 0.75;
-            if (attempt == 5) throw ApiError(MDF_ERR_INVALID, "box too small for the list cutoff");
-            continue;
-        }
+        // The one-image search visits the +-R columns around a column (R =
+        // floor(rlist / width) + 1), which must be distinct: R < columns.
+        // Sparse systems start from wide columns; add columns until it holds.
+        auto reach = [&](double L, int nc) { return (int)std::floor(rlist / (L / nc)) + 1; };
+        while (reach(c.box[0], c.ncol_x) >= c.ncol_x && c.ncol_x < 4096) ++c.ncol_x;
+        while (reach(c.box[1], c.ncol_y) >= c.ncol_y && c.ncol_y < 4096) ++c.ncol_y;
+        const int Rx = reach(c.box[0], c.ncol_x), Ry = reach(c.box[1], c.ncol_y);
+        if (Rx >= c.ncol_x || Ry >= c.ncol_y) throw ApiError(MDF_ERR_INVALID, "box too small for the list cutoff");
         c.ncols = c.ncol_x * c.ncol_y;
         c.col_count.alloc(c.ncols + 1);
         c.col_start.alloc(c.ncols + 1);

@@ -240,3 +240,36 @@ def test_prune_interval_with_margin_tracks_moving_atoms():
         assert H.frel(Fa, Fb) < 1e-12, step
         x = x + rng.uniform(-0.1, 0.1, x.shape)
     a.close(); b.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+@pytest.mark.parametrize("n,charged", [(1, True), (2, True), (2, False), (9, True), (17, False)])
+def test_few_atoms_match_o2(n, charged, prec):
+    """Ragged sizes: one atom (a lone cluster, only self and net-charge
+    reciprocal terms), one pair, one full cluster plus one, two clusters
+    plus one; charged and neutral LJ-only atoms (the PME chain on an empty
+    charge grid)."""
+    rng = np.random.default_rng(100 + n)
+    box = np.full(3, 24.0)
+    x = rng.uniform(0.0, 24.0, (n, 3))
+    while n > 1 and min(np.linalg.norm(((x[i] - x[j] + 12) % 24) - 12) for i in range(n)
+                        for j in range(i)) < 2.5:
+        x = rng.uniform(0.0, 24.0, (n, 3))
+    q = rng.normal(0.0, 0.5, n) if charged else np.zeros(n)
+    flat = H.simple_flat(q, lj_a=[6.0e5], lj_b=[600.0])
+    eng = engine.Engine(flat, box, semantics=PHYS, precision=prec, ewald_tol=1e-5, grid=(24, 24, 24))
+    eng.set_positions(x)
+    E, F = eng.compute()
+    p = O.make_params(PHYS, box, (24, 24, 24), H.alpha_for(1e-5), H.KC)
+    e2, f2, _, _, np2 = O.evaluate(flat, p, x)
+    # mixed: largest component error against the largest force, with a floor
+    # of 1e-5 kcal/mol/A (FP32 grid noise; a lone charge feels only the
+    # ~4e-3 discretisation force of the mesh)
+    tol, floor = (1e-9, 1e-9) if prec == FP64 else (5e-5, 1e-5)
+    scale = max(np.abs(f2).max(), 1e-12)
+    assert np.abs(F - f2).max() <= tol * scale + floor, (np.abs(F - f2).max(), scale)
+    for k in ("vdw", "ee_direct", "ee_self", "ee_recip"):
+        ref = e2[abi.E_INDEX[k]]
+        assert abs(E[k] - ref) <= tol * max(abs(ref), 1.0), (k, E[k], ref)
+    assert eng.pairlist_info()["pairs_in_cutoff"] == np2
+    eng.close()

@@ -280,8 +280,11 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
     unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs, unsigned* st)
 {
     extern __shared__ float4 s_lj[];
-    __shared__ float4 sx[NB_WARPS][4][CLUSTER + 1];
-    __shared__ int stj[NB_WARPS][4][CLUSTER];
+    // each staged j cluster is stored twice in a row, so the atom a lane meets
+    // at step t, (ii + t) mod 8, sits at the compile-time offset t from the
+    // lane's own slot: no index arithmetic in the pair loop
+    __shared__ float4 sx[NB_WARPS][4][2 * CLUSTER];
+    __shared__ int stj[NB_WARPS][4][2 * CLUSTER];
     __shared__ float sh[27][6];
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
     if (lj_smem)
@@ -314,8 +317,12 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
                 pe.j = I; pe.shift = 13; pe.mask = 0ull;
             }
             const int J = pe.j;
-            sx[wib][jslot][ii] = xq[J * CLUSTER + ii];
-            stj[wib][jslot][ii] = stype[J * CLUSTER + ii];
+            const float4 xjj = xq[J * CLUSTER + ii];
+            const int tjj = stype[J * CLUSTER + ii];
+            sx[wib][jslot][ii] = xjj;
+            sx[wib][jslot][ii + CLUSTER] = xjj;
+            stj[wib][jslot][ii] = tjj;
+            stj[wib][jslot][ii + CLUSTER] = tjj;
             const float4 cJ = centerf[J];
             const float* s6 = sh[pe.shift];
             const float xix = xi.x + (((cI.x - cJ.x) - s6[0]) - s6[3]);
@@ -325,16 +332,17 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
             const unsigned rot = ((rowm >> ii) | (rowm << (8 - ii))) & 0xffu;
             __syncwarp();
             float fjx = 0.f, fjy = 0.f, fjz = 0.f, el = 0.f, ed = 0.f;
+            const float4* __restrict__ sxl = &sx[wib][jslot][ii];
+            const int* __restrict__ stl = &stj[wib][jslot][ii];
 #pragma unroll
             for (int t = 0; t < CLUSTER; ++t) {
-                const int jj = (ii + t) & 7;
-                const float4 xj = sx[wib][jslot][jj];
+                const float4 xj = sxl[t];
                 const float dx = xix - xj.x, dy = xiy - xj.y, dz = xiz - xj.z;
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
                 const float rinv = rsqrtf(r2);
                 const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
-                const float4 ab = ljt[trow + stj[wib][jslot][jj]];      // A, B, 12A, 6B
+                const float4 ab = ljt[trow + stl[t]];      // A, B, 12A, 6B
                 float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
                 float G = (rinv6 * rinv2) * fmaf(ab.z, rinv6, -ab.w);
                 if (SWITCH) {

@@ -376,6 +376,12 @@ int mdf_batch_fetch(mdf_batch *b, uint32_t flags, double *forces, mdf_energies *
 /* Time every candidate launch shape on this batch (reps graph launches each)
  * and keep the fastest.  report may be NULL. */
 int mdf_batch_autotune(mdf_batch *b, int reps, mdf_tune_report *report);
+/* The same for one context: pair_warps {2, 4, 8} x fft_lines {1, 2, 4} x
+ * prune_every {0, 1} at the current positions (reps energy + force
+ * evaluations each, CUDA events on the context's stream); the fastest stays
+ * in the context's parameters.  Forces do not depend on the choice.  Not
+ * available with nranks > 1. */
+int mdf_autotune(mdf_ctx *ctx, int reps, mdf_tune_report *report);
 
 /* No counterpart in the reference.
  *

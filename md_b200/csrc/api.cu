@@ -787,6 +787,84 @@ int mdf_backward(mdf_ctx* ctx, const double* dL_dF, double dL_dE, double* dL_dq,
     });
 }
 
+int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        Ctx& c = ctx->c;
+        MDF_CUDA_TRY(cudaSetDevice(c.device));
+        if (distributed(c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
+        if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
+        if (!c.have_list) build_pairlist(c);
+        const int R = reps > 0 ? reps : 5;
+        const uint32_t flags = MDF_COMPUTE_ENERGY | MDF_COMPUTE_FORCES;
+        const int warps[3] = {2, 4, 8}, lines[3] = {1, 2, 4}, prune[2] = {0, 1};
+        const bool timing = c.timing;
+        c.timing = false;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        try {
+            MDF_CUDA_TRY(cudaEventCreate(&e0));
+            MDF_CUDA_TRY(cudaEventCreate(&e1));
+            auto apply = [&](int w, int l, int p) {
+                c.p.pair_warps = w;
+                c.p.fft_lines = l;
+                if (c.p.prune_every != p) {
+                    c.p.prune_every = p;
+                    c.pruned_valid = false;
+                    c.since_prune = 0;
+                }
+            };
+            auto time_it = [&]() {
+                eval_async(c, flags);   // untimed: first use of this shape
+                MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+                check_host_status(c);
+                MDF_CUDA_TRY(cudaEventRecord(e0, c.stream));
+                for (int r = 0; r < R; ++r) eval_async(c, flags);
+                MDF_CUDA_TRY(cudaEventRecord(e1, c.stream));
+                MDF_CUDA_TRY(cudaEventSynchronize(e1));
+                check_host_status(c);
+                float ms = 0;
+                MDF_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+                return (double)ms / R;
+            };
+            const int w0 = c.p.pair_warps, l0 = c.p.fft_lines, p0 = c.p.prune_every;
+            const double t_default = time_it();
+            double best = t_default;
+            int bw = w0, bl = l0, bp = p0, tried = 0;
+            for (int p : prune)
+                for (int w : warps)
+                    for (int l : lines) {
+                        apply(w, l, p);
+                        const double t = time_it();
+                        ++tried;
+                        if (t < best) {
+                            best = t;
+                            bw = w; bl = l; bp = p;
+                        }
+                    }
+            apply(bw, bl, bp);
+            if (rep) {
+                rep->pair_warps = bw;
+                rep->fft_lines = bl;
+                rep->prune_every = bp;
+                rep->n_tried = tried;
+                rep->best_ms = best;
+                rep->default_ms = t_default;
+            }
+        } catch (...) {
+            c.timing = timing;
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            throw;
+        }
+        c.timing = timing;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        c.pending = false;
+        c.md_stale = true;   // a recorded dynamics graph holds the old shapes
+    });
+}
+
 int mdf_set_allreduce(mdf_ctx* ctx, mdf_allreduce_u64 fn, void* user)
 {
     if (!ctx) return MDF_ERR_INVALID;

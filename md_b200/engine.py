@@ -25,7 +25,7 @@ EXPORTS = [
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_host_buffers", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
-    "mdf_pme_grids", "mdf_set_allreduce", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
+    "mdf_pme_grids", "mdf_set_allreduce", "mdf_autotune", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
 
@@ -77,6 +77,7 @@ def library(path=None):
     lib.mdf_set_parameters.argtypes = [C.c_void_p, dp, dp, dp]
     lib.mdf_backward.argtypes = [C.c_void_p, dp, C.c_double, dp, dp, dp]
     lib.mdf_minimize.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.mdf_min_report)]
+    lib.mdf_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(abi.mdf_tune_report)]
     lib.mdf_set_allreduce.argtypes = [C.c_void_p, abi.MDF_ALLREDUCE_FN, C.c_void_p]
     lib.mdf_minimize_lbfgs.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32,
                                        C.POINTER(abi.mdf_min_report)]
@@ -208,6 +209,13 @@ class Engine:
 
     def set_positions_device(self, ptr):
         self._check(self.lib.mdf_set_positions_device(self.h, C.c_void_p(ptr)), "set_positions_device")
+
+    def autotune(self, reps=5):
+        """mdf_autotune: the fastest launch shapes for this context (kept)."""
+        r = abi.mdf_tune_report()
+        self._check(self.lib.mdf_autotune(self.h, int(reps), C.byref(r)), "autotune")
+        return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every, n_tried=r.n_tried,
+                    best_ms=r.best_ms, default_ms=r.default_ms)
 
     def set_allreduce(self, fn):
         """The sum over ranks for a split context (nranks > 1): fn(ptr, count,

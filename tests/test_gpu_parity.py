@@ -273,3 +273,20 @@ def test_few_atoms_match_o2(n, charged, prec):
         assert abs(E[k] - ref) <= tol * max(abs(ref), 1.0), (k, E[k], ref)
     assert eng.pairlist_info()["pairs_in_cutoff"] == np2
     eng.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_autotune_keeps_forces_and_reports(prec):
+    """mdf_autotune tries 18 launch shapes and keeps the fastest; forces are
+    the same bit for bit before and after, energies to 1e-12 + 2^-32 per
+    block (per-block sums)."""
+    s = H.system("small")
+    eng, _ = make_engine(s, PHYS, prec, synth.GRIDS["small"])
+    E0, F0 = eng.compute()
+    rep = eng.autotune(reps=2)
+    assert rep["n_tried"] == 18 and rep["best_ms"] > 0 and rep["best_ms"] <= rep["default_ms"]
+    assert rep["pair_warps"] in (2, 4, 8) and rep["fft_lines"] in (1, 2, 4) and rep["prune_every"] in (0, 1)
+    E1, F1 = eng.compute()
+    assert np.array_equal(F0, F1)
+    assert abs(E1["total"] - E0["total"]) <= 1e-12 * abs(E0["total"]) + 1e-8
+    eng.close()

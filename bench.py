@@ -466,14 +466,15 @@ def md_bench(dev, steps=1000, equil=200):
             eng.build_pairlist()
         eng.md_init(s.mass, temperature=300.0, seed=1234)
         eng.md_run(equil, 0.0005, chunk=10, rebuild_every=10)
-        rep, samp = eng.md_run(steps, 0.0005, chunk=10, rebuild_every=10)
+        with ClockSampler(dev) as clk:
+            rep, samp = eng.md_run(steps, 0.0005, chunk=10, rebuild_every=10)
         tot = samp[:, 1] + samp[:, 2]
         ke = float(samp[:, 2].mean())
         out[name] = {"steps_per_s": rep["steps"] / rep["wall_s"], "ms_per_step": rep["wall_s"] / rep["steps"] * 1e3,
                      "rebuilds": rep["rebuilds"], "e_total_first": float(tot[0]), "e_total_last": float(tot[-1]),
                      "drift": float(tot[-1] - tot[0]), "drift_over_ke": float((tot[-1] - tot[0]) / ke),
                      "e_total_std": float(tot.std()), "mean_ke": ke,
-                     "temperature_k": 2.0 * ke / (3.0 * s.natoms * 0.0019872041)}
+                     "temperature_k": 2.0 * ke / (3.0 * s.natoms * 0.0019872041), "clocks": clk.summary()}
     eng.close()
     out["mixed_over_fp64_speed"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
     return out

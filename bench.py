@@ -474,7 +474,9 @@ def md_bench(dev, steps=1000, equil=200):
                      "rebuilds": rep["rebuilds"], "e_total_first": float(tot[0]), "e_total_last": float(tot[-1]),
                      "drift": float(tot[-1] - tot[0]), "drift_over_ke": float((tot[-1] - tot[0]) / ke),
                      "e_total_std": float(tot.std()), "mean_ke": ke,
-                     "temperature_k": 2.0 * ke / (3.0 * s.natoms * 0.0019872041), "clocks": clk.summary()}
+                     "temperature_k": 2.0 * ke / (3.0 * s.natoms * 0.0019872041), "clocks": clk.summary(),
+                     "host_s": {"rebuild": rep["rebuild_s"], "graph_record": rep["record_s"],
+                                "graph_wait": rep["wait_s"], "total": rep["wall_s"]}}
     eng.close()
     out["mixed_over_fp64_speed"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
     return out

@@ -315,6 +315,9 @@ typedef struct {
     double wall_s;        /* host wall time of the run */
     double pe_first, ke_first;   /* potential / kinetic energy after the first chunk */
     double pe_last, ke_last;     /* ... after the last chunk */
+    double rebuild_s;     /* host wall time in list rebuilds */
+    double record_s;      /* host wall time recording / updating the chunk graphs */
+    double wait_s;        /* host wall time waiting for the chunk graphs to finish */
 } mdf_md_report;
 /* masses [natoms] (amu); velocities [3N] (A/ps), or NULL to draw them from a
  * Maxwell-Boltzmann distribution at temperature (K) with the given seed

@@ -73,7 +73,7 @@ class mdf_tune_report(C.Structure):
 class mdf_md_report(C.Structure):
     _fields_ = [("steps", C.c_int64), ("rebuilds", C.c_int64), ("samples", C.c_int64), ("wall_s", C.c_double),
                 ("pe_first", C.c_double), ("ke_first", C.c_double), ("pe_last", C.c_double),
-                ("ke_last", C.c_double)]
+                ("ke_last", C.c_double), ("rebuild_s", C.c_double), ("record_s", C.c_double), ("wait_s", C.c_double)]
 
 
 class mdf_min_report(C.Structure):

@@ -287,14 +287,22 @@ void md_run(Ctx& c, long long nsteps, double dt, int chunk, int rebuild_every, d
         // twice that as headroom below half the skin
         const double dnow = std::sqrt(bits_to_double(c.md_host[1]));
         const double reach = 2.0 * steps * dt * std::sqrt(bits_to_double(c.md_host[4]));
+        using clk = std::chrono::steady_clock;
+        const auto ta = clk::now();
         if (due || dnow + reach > half_skin) {
             md_rebuild(c, false);
             since_build = 0;
             ++r.rebuilds;
         }
+        const auto tb = clk::now();
         md_prepare(c, steps, dt);
+        const auto tc = clk::now();
         MDF_CUDA_TRY(cudaGraphLaunch(c.md_exec, c.stream));
         MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+        const auto td = clk::now();
+        r.rebuild_s += std::chrono::duration<double>(tb - ta).count();
+        r.record_s += std::chrono::duration<double>(tc - tb).count();
+        r.wait_s += std::chrono::duration<double>(td - tc).count();
         check_host_status(c);
         if ((unsigned)c.md_host[2] & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "kinetic energy out of range");
         done += steps;

@@ -71,6 +71,10 @@ struct DevBuf {
     size_t n = 0;
     void alloc(size_t count) {
         if (count <= n && p) return;
+        // a buffer that has to grow (pair lists, slots after a rebuild) gets
+        // 1/8 headroom, so lists that creep up between rebuilds do not pay a
+        // cudaFree + cudaMalloc at every build
+        if (p) count += count / 8;
         release();
         size_t bytes = count * sizeof(T);
         if (bytes == 0) bytes = sizeof(T);

@@ -290,3 +290,46 @@ def test_autotune_keeps_forces_and_reports(prec):
     assert np.array_equal(F0, F1)
     assert abs(E1["total"] - E0["total"]) <= 1e-12 * abs(E0["total"]) + 1e-8
     eng.close()
+
+
+@pytest.mark.parametrize("case", ["tiny", "tiny_sentinel", "small"])
+def test_reference_mixed_matches_reference_cpu(case):
+    """REFERENCE semantics in mixed precision (FP32 pair arithmetic, the
+    reference's order-5 PME chain in FP32) against the unmodified reference:
+    forces to 1e-5 rms relative, every continuous energy term to 1e-5
+    relative (absolute floor 1e-4 kcal/mol for terms near zero).  The plain
+    Coulomb sums truncated at r = rc ("ee", "ee_pairlist") jump by k q q / rc
+    when a pair crosses the cutoff, and FP32 rounding of r^2 moves pairs that
+    lie within ~1e-6 A of it across: those two are held to 1e-3."""
+    g = H.golden(case)
+    m = g["meta"]
+    s = H.system(m["config"], m["sentinels"])
+    eng, _ = make_engine(s, REF, MIXED, m["grid"])
+    E, F = eng.compute()
+    for k in E_REF_TERMS:
+        ref = g["energies"][k]
+        tol = 1e-3 if k in ("ee", "ee_pairlist") else 1e-5
+        assert abs(E[k] - ref) <= tol * abs(ref) + 1e-4, (k, E[k], ref)
+    H.check_forces_vs_golden(F, g, 1e-5, "forces")
+    eng.close()
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_box_change_equals_fresh_context(prec):
+    """mdf_set_box with scaled positions gives the forces a context created
+    at the new box gives, bit for bit (PME tables, shifts and list rebuilt)."""
+    s = H.system("small")
+    grid = synth.GRIDS["small"]
+    eng, flat = make_engine(s, PHYS, prec, grid)
+    eng.compute()
+    f = 1.03
+    box2, x2 = np.asarray(s.box) * f, s.coords * f
+    eng.set_box(box2)
+    eng.set_positions(x2)
+    E1, F1 = eng.compute()
+    e2 = engine.Engine(flat, box2, semantics=PHYS, precision=prec, ewald_tol=1e-5, grid=grid)
+    e2.set_positions(x2)
+    E2, F2 = e2.compute()
+    assert np.array_equal(F1, F2)
+    assert abs(E1["total"] - E2["total"]) <= 1e-12 * abs(E2["total"]) + 1e-8
+    eng.close(); e2.close()

@@ -107,3 +107,24 @@ def test_cmap_spline_table_is_c1_and_interpolates():
     assert e_edge < 1e-12 and e_slope < 1e-12 and e_corner < 1e-12
     assert e_int < 1e-3
     assert e_ref > 0.1      # the reference's table is discontinuous along cell edges
+
+
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c++", "c++11")])
+def test_header_is_plain_c_and_cxx(lang, std, tmp_path):
+    """include/mdf.h compiles warning-free as C99 and as C++11 (the C ABI a
+    C, Fortran-interop or older C++ caller binds), and the struct sizes the C
+    compiler sees match the ctypes mirror."""
+    import subprocess
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    src = tmp_path / "probe.c"
+    src.write_text('#include <stdio.h>\n#include "mdf.h"\n'
+                   'int main(void) { printf("%zu %zu %zu %zu\\n", sizeof(mdf_params), sizeof(mdf_energies), '
+                   'sizeof(mdf_md_report), sizeof(mdf_min_report)); return 0; }\n')
+    exe = tmp_path / "probe"
+    cc = "gcc" if lang == "c" else "g++"
+    r = subprocess.run([cc, "-x", lang, "-std=" + std, "-Wall", "-Wextra", "-Werror", "-I" + inc, str(src), "-o",
+                        str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert sizes == [C.sizeof(abi.mdf_params), C.sizeof(abi.mdf_energies), C.sizeof(abi.mdf_md_report),
+                     C.sizeof(abi.mdf_min_report)]

@@ -118,8 +118,9 @@ def test_header_is_plain_c_and_cxx(lang, std, tmp_path):
     inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
     src = tmp_path / "probe.c"
     src.write_text('#include <stdio.h>\n#include "mdf.h"\n'
-                   'int main(void) { printf("%zu %zu %zu %zu\\n", sizeof(mdf_params), sizeof(mdf_energies), '
-                   'sizeof(mdf_md_report), sizeof(mdf_min_report)); return 0; }\n')
+                   'int main(void) { printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(mdf_params), sizeof(mdf_energies), '
+                   'sizeof(mdf_md_report), sizeof(mdf_min_report), sizeof(mdf_topology), sizeof(mdf_tune_report));'
+                   ' return 0; }\n')
     exe = tmp_path / "probe"
     cc = "gcc" if lang == "c" else "g++"
     r = subprocess.run([cc, "-x", lang, "-std=" + std, "-Wall", "-Wextra", "-Werror", "-I" + inc, str(src), "-o",
@@ -127,4 +128,4 @@ def test_header_is_plain_c_and_cxx(lang, std, tmp_path):
     assert r.returncode == 0, r.stderr
     sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
     assert sizes == [C.sizeof(abi.mdf_params), C.sizeof(abi.mdf_energies), C.sizeof(abi.mdf_md_report),
-                     C.sizeof(abi.mdf_min_report)]
+                     C.sizeof(abi.mdf_min_report), C.sizeof(abi.mdf_topology), C.sizeof(abi.mdf_tune_report)]

@@ -40,8 +40,6 @@ def _bonded_only(flat):
 @pytest.mark.parametrize("prec", [abi.MDF_PREC_FP64, abi.MDF_PREC_MIXED])
 def test_noalloc_bonded_matches_compute(sem, prec):
     import torch
-    if sem == abi.MDF_SEM_REFERENCE and prec == abi.MDF_PREC_MIXED:
-        pytest.skip("REFERENCE semantics run in FP64 only")
     s = H.system("tiny")
     flat = H.flat(s, sem, engine.cmap_coefficients)
     full = _engine(flat, s, sem, prec)

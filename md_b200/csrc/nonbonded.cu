@@ -249,6 +249,24 @@ __device__ __forceinline__ float ex2_approx(float x)
     return y;
 }
 
+// 1/sqrt(x) and 1/x on the special-function unit with denormal inputs flushed
+// (PTX rsqrt.approx.ftz / rcp.approx.ftz): the library forms also handle
+// denormal arguments, which a pair distance or 1 + p r never is, at the cost
+// of extra instructions in the pair loop.
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rcp_ftz(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Constants of the FP32 pair kernel, folded on the host.
 struct PairConstF {
     float rc2;
@@ -340,7 +358,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
                 const float dx = xix - xj.x, dy = xiy - xj.y, dz = xiz - xj.z;
                 const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
                 const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
-                const float rinv = rsqrtf(r2);
+                const float rinv = rsqrt_ftz(r2);
                 const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
                 const float4 ab = ljt[trow + stl[t]];      // A, B, 12A, 6B
                 float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
@@ -358,7 +376,7 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
                     G = G - gc * K.rcf * rinv;
                 }
                 const float ex = ex2_approx(K.kex * r2);
-                const float erfcv = erfc_as(__fdividef(1.0f, fmaf(K.pa, r, 1.0f)), ex);
+                const float erfcv = erfc_as(rcp_ftz(fmaf(K.pa, r, 1.0f)), ex);
                 const float ec = (qik * xj.w) * erfcv * rinv;
                 float g = fmaf(fmaf(qik2 * xj.w, ex, ec), rinv2, G);
                 g = on ? g : 0.f;

@@ -72,14 +72,14 @@ template <> struct Frame<double> {
 };
 
 template <typename R> __device__ __forceinline__ R rsqrt_r(R x);
-template <> __device__ __forceinline__ float rsqrt_r<float>(float x) { return rsqrtf(x); }
+template <> __device__ __forceinline__ float rsqrt_r<float>(float x) { return rsqrt_ftz(x); }
 template <> __device__ __forceinline__ double rsqrt_r<double>(double x) { return 1.0 / sqrt(x); }
 
 template <typename R> __device__ __forceinline__ void erfc_exp(R ar, R& erfcv, R& ex);
 template <> __device__ __forceinline__ void erfc_exp<float>(float ar, float& erfcv, float& ex)
 {
-    ex = __expf(-ar * ar);
-    erfcv = erfc_as(__fdividef(1.0f, 1.0f + 0.3275911f * ar), ex);
+    ex = ex2_approx(-1.4426950408889634f * ar * ar);
+    erfcv = erfc_as(rcp_ftz(1.0f + 0.3275911f * ar), ex);
 }
 template <> __device__ __forceinline__ void erfc_exp<double>(double ar, double& erfcv, double& ex)
 {

@@ -21,6 +21,32 @@ struct NBParams {
     double ucut_pow6, ucut_pow12;   // rc^-6, rc^-12 (force-shift LJ)
 };
 
+// 2^x on the special-function unit (PTX ex2.approx.ftz: relative error ~2^-22).
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// 1/sqrt(x) and 1/x on the special-function unit with denormal inputs flushed
+// (PTX rsqrt.approx.ftz / rcp.approx.ftz): the library forms also handle
+// denormal arguments, which a pair distance or 1 + p r never is, at the cost
+// of extra instructions in the pair loop.
+__device__ __forceinline__ float rsqrt_ftz(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rcp_ftz(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Abramowitz & Stegun 7.1.26 (Hastings): erfc(x) ~ t (a1 + t (a2 + ...)) e^{-x^2},
 // t = 1 / (1 + p x), |error| <= 1.5e-7.  Used by the FP32 pair kernel only.
 __device__ __forceinline__ float erfc_as(float t, float ex)

@@ -241,32 +241,6 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
 //    bit t;
 //  * the pair arithmetic is branch-free (inactive pairs are selected out);
 //  * energies are summed in FP32 per entry and in FP64 across entries.
-// 2^x on the special-function unit (PTX ex2.approx.ftz: relative error ~2^-22).
-__device__ __forceinline__ float ex2_approx(float x)
-{
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// 1/sqrt(x) and 1/x on the special-function unit with denormal inputs flushed
-// (PTX rsqrt.approx.ftz / rcp.approx.ftz): the library forms also handle
-// denormal arguments, which a pair distance or 1 + p r never is, at the cost
-// of extra instructions in the pair loop.
-__device__ __forceinline__ float rsqrt_ftz(float x)
-{
-    float y;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-__device__ __forceinline__ float rcp_ftz(float x)
-{
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
 // Constants of the FP32 pair kernel, folded on the host.
 struct PairConstF {
     float rc2;

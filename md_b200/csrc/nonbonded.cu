@@ -265,7 +265,10 @@ struct PairConstF {
 //    fits (lj_smem), and the Gaussian uses 2^(kex r^2) on the SFU;
 //  * energies are summed in FP32 per entry and in FP64 across entries.
 template <bool ENERGY, bool SWITCH, bool COUNT>
-__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(
+// Without energies the kernel fits 64 registers with no spills and four blocks
+// per SM (dynamics steps: +4%); with energies a 64-register cap spills and is
+// slower, so those keep three.
+__global__ void __launch_bounds__(NB_THREADS, ENERGY ? 3 : 4) k_pairs_f32(
     int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
     const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp,
     int lj_smem, float kc, PairConstF K, ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots,

@@ -265,10 +265,7 @@ struct PairConstF {
 //    fits (lj_smem), and the Gaussian uses 2^(kex r^2) on the SFU;
 //  * energies are summed in FP32 per entry and in FP64 across entries.
 template <bool ENERGY, bool SWITCH, bool COUNT>
-// Without energies the kernel fits 64 registers with no spills and four blocks
-// per SM (dynamics steps: +4%); with energies a 64-register cap spills and is
-// slower, so those keep three.
-__global__ void __launch_bounds__(NB_THREADS, ENERGY ? 3 : 4) k_pairs_f32(
+__device__ __forceinline__ void pairs_f32_body(
     int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
     const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp,
     int lj_smem, float kc, PairConstF K, ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots,
@@ -400,6 +397,31 @@ __global__ void __launch_bounds__(NB_THREADS, ENERGY ? 3 : 4) k_pairs_f32(
         if (lane == 0 && np) atomicAdd(npairs, (unsigned long long)np);
     }
 }
+
+#define MDF_PF32_PARAMS                                                                                        \
+    int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq, \
+        const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp, \
+        int lj_smem, float kc, PairConstF K, ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots,   \
+        unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs, unsigned* st
+#define MDF_PF32_ARGS nlist, ilist, plist, xq, stype, centerf, lj4, ntp, lj_smem, kc, K, shifts, fslot, nslots, acc, npairs, st
+
+// With energies: the compiler's own register choice (72, three blocks per SM;
+// a 64-register cap spills and is slower).
+template <bool SWITCH, bool COUNT>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(MDF_PF32_PARAMS)
+{
+    pairs_f32_body<true, SWITCH, COUNT>(MDF_PF32_ARGS);
+}
+
+// Forces only (every dynamics step but the last of a chunk): 64 registers
+// with no spills, four blocks per SM (+4% dynamics steps/s).
+template <bool SWITCH, bool COUNT>
+__global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force(MDF_PF32_PARAMS)
+{
+    pairs_f32_body<false, SWITCH, COUNT>(MDF_PF32_ARGS);
+}
+#undef MDF_PF32_PARAMS
+#undef MDF_PF32_ARGS
 
 // --------------------------------------------------------------- FP64 pairs
 __device__ __forceinline__ void pair_vec(const double* __restrict__ xyz, int a, int b, const NBParams& P,
@@ -640,10 +662,18 @@ static void launch_pairs_f32(Ctx& c, bool energy)
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     const bool count = begin_pair_count(c);
 #define MDF_PF32(E, S, K_)                                                                                     \
-    k_pairs_f32<E, S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(ncl, il, pl, c.xq_f.p, c.slot_type.p,                \
-                                                           c.centerf.p, c.ljAB4_f.p, c.ntp, lj_smem,              \
-                                                           (float)P.kc, K, sh, c.f_slot.p, c.n_slots, c.acc.p,   \
-                                                           c.npairs_dev.p, c.status.p)
+    do {                                                                                                       \
+        if (E)                                                                                                 \
+            k_pairs_f32<S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(ncl, il, pl, c.xq_f.p, c.slot_type.p,            \
+                                                                c.centerf.p, c.ljAB4_f.p, c.ntp, lj_smem,          \
+                                                                (float)P.kc, K, sh, c.f_slot.p, c.n_slots,       \
+                                                                c.acc.p, c.npairs_dev.p, c.status.p);            \
+        else                                                                                                   \
+            k_pairs_f32_force<S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(ncl, il, pl, c.xq_f.p, c.slot_type.p,      \
+                                                                      c.centerf.p, c.ljAB4_f.p, c.ntp, lj_smem,    \
+                                                                      (float)P.kc, K, sh, c.f_slot.p, c.n_slots, \
+                                                                      c.acc.p, c.npairs_dev.p, c.status.p);      \
+    } while (0)
 #define MDF_PF32_K(E, S) \
     do { if (count) MDF_PF32(E, S, true); else MDF_PF32(E, S, false); } while (0)
     if (energy) {

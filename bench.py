@@ -24,9 +24,20 @@ cpu_baseline / --impl reference
            C++) on the same system: PME chain + list energies +
            calculate_forces per step
 
+Launch shapes come from mdf_autotune before anything is timed.  The line also
+carries: fp64 (the same system in FP64, the mixed/FP64 ratio and the per-term
+errors), adjoint (c2: backward / forward cost), batched (c3: 256 systems per
+graph launch, device and end-to-end frames/s), dynamics (c4: L-BFGS
+minimisation, NVE steps/s and energy drift, mixed and FP64, with clocks and
+the host time split; PME spread/gather alone against HBM), clocks (NVML
+during the timed region) and gpu_launches.
+
 Multi-GPU (torchrun): each rank evaluates its own replica of the system (no
 data-path collective: a single 100k-atom system is not sharded), timings are
-max-reduced over ranks and value is the whole-job rate (weak scaling).
+max-reduced over ranks and value is the whole-job rate (weak scaling).  The
+c3 batch is sharded over the ranks by estimated cost, and c4_split times one
+c4 evaluation split over all ranks (int64 NCCL all-reduces through
+mdf_set_allreduce) against one GPU.
 """
 from __future__ import annotations
 

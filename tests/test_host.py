@@ -73,3 +73,25 @@ def test_cli_prints_the_references_energies(case, tmp_path):
         assert H.rel(v, g["energies"][k]) < 1e-9, (k, v, g["energies"][k])
     F = np.fromfile(fo, dtype=np.float64).reshape(-1, 3)
     H.check_forces_vs_golden(F, g, 1e-9, "forces")
+
+
+@pytest.mark.gpu
+def test_cli_minimise_and_dynamics(tmp_path):
+    """The command line's --minimize (L-BFGS) lowers the energy, and --md runs
+    velocity Verlet and writes a restart the reader takes back (PHYSICAL,
+    mixed)."""
+    import re
+    s, (prm, rst) = _files("tiny", False, tmp_path)
+    out = tmp_path / "out.rst7"
+    r = subprocess.run([CLI, prm, rst, "--physical", "--mixed", "--grid", "24", "24", "24", "--minimize", "50",
+                        "--md", "100", "0.0005", "--rst7-out", str(out)], check=True, capture_output=True, text=True)
+    m = re.search(r"minimised \(L-BFGS\): (\d+) iterations, (\d+) evaluations, E (\S+) -> (\S+),", r.stdout)
+    assert m, r.stdout
+    assert int(m.group(1)) > 0 and int(m.group(2)) > int(m.group(1))
+    assert float(m.group(4)) < float(m.group(3))
+    d = re.search(r"dynamics: (\d+) steps", r.stdout)
+    assert d and int(d.group(1)) == 100, r.stdout
+    lines = out.read_text().splitlines()   # title; atom count + time; fixed 12-column fields
+    assert int(lines[1][:6]) == s.natoms
+    vals = np.array([float(t[i:i + 12]) for t in lines[2:] for i in range(0, len(t), 12)])
+    assert vals.size == 6 * s.natoms + 6 and np.isfinite(vals).all()

@@ -3,7 +3,7 @@
 Run in a container that has the reference sources (it builds oracle/_ref/
 o1_harness from them):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   # default: every case
 
 For every case it writes tests/golden/<case>/:
   meta.json          generator config, sha256 of the written prmtop/rst7 text,
@@ -39,6 +39,7 @@ CASES = [
     ("tiny_sentinel", "tiny", True, True, True),
     ("small", "small", False, False, True),
     ("c0", "c0", False, False, False),
+    ("c1", "c1", False, False, False),
 ]
 DIGEST_ATOMS = 256
 
@@ -53,9 +54,11 @@ def digest_indices(n):
     return np.concatenate([np.arange(min(DIGEST_ATOMS, n)), rng.choice(n, size=min(DIGEST_ATOMS, n), replace=False)])
 
 
-def main():
+def main(only=()):
     O.build()
     for name, cfg, sent, keep, full in CASES:
+        if only and name not in only:
+            continue
         out = os.path.join(HERE, name)
         os.makedirs(out, exist_ok=True)
         s = synth.make_config(cfg, sentinels=sent)
@@ -86,4 +89,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

@@ -14,6 +14,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 KC = synth.KC
 
 _SYS_CACHE = {}
+_O2_CACHE = {}
 
 
 def alpha_for(tol, cutoff=10.0):
@@ -42,6 +43,17 @@ def system(cfg, sentinels=False):
     if key not in _SYS_CACHE:
         _SYS_CACHE[key] = synth.make_config(cfg, sentinels=sentinels)
     return _SYS_CACHE[key]
+
+
+def o2_physical(cfg, flat_phys):
+    """O2 PHYSICAL evaluation of a named workload at its grid, Ewald tol 1e-5
+    (cached: several tests compare against the same oracle result)."""
+    if cfg not in _O2_CACHE:
+        from oracle import oracle as O
+        s = system(cfg)
+        p = O.make_params(abi.MDF_SEM_PHYSICAL, s.box, synth.GRIDS[cfg], alpha_for(1e-5), KC)
+        _O2_CACHE[cfg] = O.evaluate(flat_phys, p, s.coords)
+    return _O2_CACHE[cfg]
 
 
 def files_sha(sysm):

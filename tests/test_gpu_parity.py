@@ -35,7 +35,7 @@ def make_engine(s, sem, prec, grid, tol=1e-5, **kw):
     return eng, flat
 
 
-@pytest.mark.parametrize("case", ["tiny", "tiny_sentinel", "small", "c0"])
+@pytest.mark.parametrize("case", ["tiny", "tiny_sentinel", "small", "c0", "c1"])
 def test_reference_fp64_matches_reference_cpu(case):
     g = H.golden(case)
     m = g["meta"]
@@ -49,14 +49,15 @@ def test_reference_fp64_matches_reference_cpu(case):
     eng.close()
 
 
-@pytest.mark.parametrize("cfg", ["tiny", "small", "c0"])
+@pytest.mark.parametrize("cfg", ["tiny", "small", "c0", "c1"])
 def test_physical_fp64_matches_o2(cfg):
+    """The FP64 GPU path (the denominator of the mixed/FP64 ratio) against O2,
+    up to the 100k-atom workload the ratio is quoted on."""
     s = H.system(cfg)
     grid = synth.GRIDS[cfg]
     eng, flat = make_engine(s, PHYS, FP64, grid)
     E, F = eng.compute()
-    p = O.make_params(PHYS, s.box, grid, H.alpha_for(1e-5), H.KC)
-    e2, f2, vir2, _, np2 = O.evaluate(flat, p, s.coords)
+    e2, f2, vir2, _, np2 = H.o2_physical(cfg, flat)
     for k in E_PHYS_TERMS:
         ref = e2[abi.E_INDEX[k]]
         assert abs(E[k] - ref) <= 1e-9 * max(abs(ref), 1.0), (k, E[k], ref)
@@ -72,8 +73,7 @@ def test_mixed_precision_force_error_below_1e5(cfg):
     grid = synth.GRIDS[cfg]
     eng, flat = make_engine(s, PHYS, MIXED, grid)
     E, F = eng.compute()
-    p = O.make_params(PHYS, s.box, grid, H.alpha_for(1e-5), H.KC)
-    e2, f2, _, _, _ = O.evaluate(flat, p, s.coords)
+    e2, f2, _, _, _ = H.o2_physical(cfg, flat)
     err = H.frel(F, f2)
     assert err <= 1e-5, err
     tot2 = sum(e2[abi.E_INDEX[k]] for k in E_PHYS_TERMS)
@@ -333,3 +333,27 @@ def test_box_change_equals_fresh_context(prec):
     assert np.array_equal(F1, F2)
     assert abs(E1["total"] - E2["total"]) <= 1e-12 * abs(E2["total"]) + 1e-8
     eng.close(); e2.close()
+
+
+def test_c4_960k_atoms_fp64_and_mixed_match_o2():
+    """The dynamics workload (215 A box, 320,000 flexible waters, 960,000 atoms,
+    PME 216^3) at its starting positions: the FP64 GPU path against O2 at
+    1e-9, the mixed path against O2 at <= 1e-5 rms relative force error and
+    1e-6 relative total energy, and mixed against FP64 on the GPU."""
+    s = H.system("c4")
+    grid = synth.GRIDS["c4"]
+    e64, flat = make_engine(s, PHYS, FP64, grid)
+    E64, F64 = e64.compute()
+    e64.close()
+    emx, _ = make_engine(s, PHYS, MIXED, grid)
+    Emx, Fmx = emx.compute()
+    emx.close()
+    e2, f2, _, _, _ = H.o2_physical("c4", flat)
+    assert H.frel(F64, f2) < 1e-9, H.frel(F64, f2)
+    for k in E_PHYS_TERMS:
+        ref = e2[abi.E_INDEX[k]]
+        assert abs(E64[k] - ref) <= 1e-9 * max(abs(ref), 1.0), (k, E64[k], ref)
+    assert H.frel(Fmx, f2) <= 1e-5, H.frel(Fmx, f2)
+    assert H.frel(Fmx, F64) <= 1e-5, H.frel(Fmx, F64)
+    tot2 = sum(e2[abi.E_INDEX[k]] for k in E_PHYS_TERMS)
+    assert H.rel(Emx["total"], tot2) < 1e-6

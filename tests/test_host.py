@@ -95,3 +95,24 @@ def test_cli_minimise_and_dynamics(tmp_path):
     assert int(lines[1][:6]) == s.natoms
     vals = np.array([float(t[i:i + 12]) for t in lines[2:] for i in range(0, len(t), 12)])
     assert vals.size == 6 * s.natoms + 6 and np.isfinite(vals).all()
+
+
+def test_cpp_reader_at_960k_atoms(tmp_path):
+    """The dynamics workload (320,000 flexible waters, 960,000 atoms) written as
+    prmtop/rst7 (~100 MB + 35 MB) and read back by the C++ reader: the same
+    PHYSICAL arrays as the Python host, and the read + flatten within a few
+    seconds (mdb200 times and prints both; about 1.1 s on one core here)."""
+    engine.library()
+    s, (prm, rst) = _files("c4", False, tmp_path)
+    out = tmp_path / "dump"
+    out.mkdir()
+    r = subprocess.run([CLI, prm, rst, "--physical", "--dump-topology", str(out)], check=True, capture_output=True,
+                       text=True)
+    m = re.search(r"read (\d+) atoms in (\S+) s, flattened in (\S+) s", r.stdout)
+    assert m and int(m.group(1)) == s.natoms, r.stdout
+    assert float(m.group(2)) + float(m.group(3)) < 10.0, r.stdout
+    flat = H.flat(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    for name in ("charge", "type", "bond_atoms", "bond_k", "angle_atoms", "angle_theta0", "excl_pairs"):
+        got = np.fromfile(out / (name + ".bin"), dtype=ARRAYS[name])
+        want = np.asarray(getattr(flat, name)).reshape(-1).astype(ARRAYS[name])
+        assert np.array_equal(got, want), name

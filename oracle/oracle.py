@@ -19,7 +19,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(REF_DIR, "liboracle.so")
 O1 = os.path.join(REF_DIR, "o1_harness")
-REFERENCE_SRC = "/root/reference"
+REF_ON_MDF = os.path.join(REF_DIR, "ref_on_mdf")
+# reference checkout the O1 recipe compiles: $MD_REFERENCE, else the default location
+REFERENCE_SRC = os.environ.get("MD_REFERENCE", "/root/reference")
 
 _lib = None
 
@@ -36,7 +38,11 @@ def build(quiet=True):
     targets = ["_ref/liboracle.so"]
     if os.path.isdir(REFERENCE_SRC):
         targets.append("_ref/o1_harness")
-    out = subprocess.run(["make", "-s", "-j8"] + targets, cwd=HERE, capture_output=True, text=True)
+        # the reference's own System on libmdf (needs libmdf.so built first)
+        if os.path.exists(os.path.join(os.path.dirname(HERE), "md_b200", "libmdf.so")):
+            targets.append("_ref/ref_on_mdf")
+    out = subprocess.run(["make", "-s", "-j8", "REF=" + REFERENCE_SRC] + targets, cwd=HERE, capture_output=True,
+                         text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
 
@@ -164,6 +170,29 @@ def read_o1(outdir):
         p = os.path.join(outdir, g + ".bin")
         if os.path.exists(p):
             res[g] = np.fromfile(p, dtype=np.float64)
+    return res
+
+
+def run_ref_on_mdf(prmtop, rst7, grid, tol=1e-5, repeat=1, precision="fp64"):
+    """The reference's own System with calculate_energies / calculate_forces
+    on libmdf (oracle/binding): energies and forces in the O1 harness format."""
+    if not os.path.exists(REF_ON_MDF):
+        raise FileNotFoundError("ref_on_mdf not built (needs the reference sources and libmdf.so)")
+    outdir = tempfile.mkdtemp(prefix="refmdf_")
+    cmd = [REF_ON_MDF, prmtop, rst7, outdir, "--tol", repr(tol), "--grid"] + [str(g) for g in grid] + \
+          ["--repeat", str(repeat)]
+    env = dict(os.environ, MD_MDF_PRECISION=precision)
+    r = subprocess.run(cmd, capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        raise RuntimeError("ref_on_mdf failed (%d): %s" % (r.returncode, r.stderr[-2000:]))
+    res = {"energies": {}}
+    with open(os.path.join(outdir, "energies.txt")) as f:
+        for line in f:
+            k, v = line.split()
+            res["energies"][k] = float(v)
+    res["forces"] = np.fromfile(os.path.join(outdir, "forces.bin"), dtype=np.float64).reshape(-1, 3)
+    import shutil
+    shutil.rmtree(outdir, ignore_errors=True)
     return res
 
 

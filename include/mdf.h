@@ -265,6 +265,13 @@ int mdf_cmap_coefficients_spline(int nsets, int res, const double *grids, double
  * (an FMA counts 2), precision MDF_PREC_MIXED for FP32, MDF_PREC_FP64 for
  * FP64.  The roofline denominator of the FP32-pipe-bound pair kernel. */
 int mdf_probe_fma_tflops(int device, int precision, double *tflops);
+/* Diagnostic: measured rate of int64 reductions (atomic adds) per second
+ * into an L2-resident buffer of `words` 64-bit words on the device.
+ * pattern 0 = four consecutive words per thread at scattered 32-byte rows
+ * (the PME charge spread's access), 1 = 32 consecutive words per warp (the
+ * most favourable form).  The roofline denominator of the charge spread,
+ * whose fixed-point grid stays in L2. */
+int mdf_probe_l2_reductions(int device, int64_t words, int pattern, double *per_s);
 
 /* Replace the per-atom charges (internal unit, [natoms]) and/or the LJ A/B
  * coefficients ([n_ljpair], indexed by NONBONDED_PARM_INDEX - 1) of the
@@ -402,9 +409,14 @@ int mdf_autotune(mdf_ctx *ctx, int reps, mdf_tune_report *report);
  *
  * The first call on a device looks up the static array's device address
  * (cudaGetSymbolAddress) and keeps it; make that first call before any
- * stream capture.  The array is shared by every context on the device, so
- * calls that overlap in time (other threads, other streams) race and corrupt
- * each other's results: serialise them. */
+ * stream capture.  The address is kept while any context lives on that
+ * device; destroying the device's last context forgets it, so a caller that
+ * resets the device (cudaDeviceReset) after destroying its contexts gets a
+ * fresh lookup on the next first call.  The array is shared by every context
+ * on the device, so calls that overlap in time (other threads, other streams)
+ * race and corrupt each other's results: serialise them.  A context with
+ * nranks > 1 gets MDF_ERR_UNSUPPORTED (the bonded lists are not split over
+ * the ranks here). */
 #define MDF_NOALLOC_MAX_ATOMS 131072
 int mdf_compute_bonded_noalloc(mdf_ctx *ctx, uint32_t flags, double *d_forces, mdf_energies *energies);
 

@@ -6,11 +6,14 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <set>
 #include <string>
 #include <utility>
 #include <vector>
 
+#include "kargs.cuh"
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
 
@@ -41,11 +44,15 @@ void mark(Ctx& c, const char* name)
 // Forces out in atom order, and every accumulator cleared for the next
 // evaluation (read-and-clear: an evaluation needs no memsets).  The scalar
 // block was copied to the host before this kernel runs.
-__global__ void k_finalize(int N, int nslots, unsigned long long* __restrict__ fatom,
-                           unsigned long long* __restrict__ fslot, const int* __restrict__ atom_slot,
-                           double* __restrict__ out, unsigned long long* __restrict__ scal,
-                           unsigned long long* __restrict__ host_scal)
+__device__ __forceinline__ void finalize_dev(const FinalizeArgs& A)
 {
+    const int N = A.N, nslots = A.nslots;
+    unsigned long long* __restrict__ fatom = A.fatom;
+    unsigned long long* __restrict__ fslot = A.fslot;
+    const int* __restrict__ atom_slot = A.atom_slot;
+    double* __restrict__ out = A.out;
+    unsigned long long* __restrict__ scal = A.scal;
+    unsigned long long* __restrict__ host_scal = A.host_scal;
     int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a < NUM_SCAL) {
         host_scal[a] = scal[a];   // mapped pinned memory: no copy-engine round trip
@@ -67,12 +74,46 @@ __global__ void k_finalize(int N, int nslots, unsigned long long* __restrict__ f
     for (int k = 0; k < 3; ++k) out[3 * a + k] = (double)v[k] * FORCE_ISCALE;
 }
 
+__global__ void k_finalize(FinalizeArgs A)
+{
+    finalize_dev(A);
+}
+
+__global__ void k_finalize_multi(const FinalizeArgs* __restrict__ As)
+{
+    const FinalizeArgs& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    finalize_dev(A);
+}
+
+FinalizeArgs make_finalize_args(const Ctx& c, double* d_forces)
+{
+    FinalizeArgs A;
+    A.gx = grid_blocks(std::max(c.N, NUM_SCAL), 256);
+    A.gy = 1;
+    A.N = c.N;
+    A.nslots = c.n_slots;
+    A.fatom = c.f_atom.p;
+    A.fslot = c.f_slot.p;
+    A.atom_slot = c.atom_slot.p;
+    A.out = d_forces;
+    A.scal = c.scal.p;
+    A.host_scal = c.d_hscal;
+    return A;
+}
+
 void launch_finalize(Ctx& c, double* d_forces, bool)
 {
-    k_finalize<<<grid_blocks(std::max(c.N, NUM_SCAL), 256), 256, 0, c.stream>>>(
-        c.N, c.n_slots, c.f_atom.p, c.f_slot.p, c.atom_slot.p, d_forces, c.scal.p, c.d_hscal);
+    const FinalizeArgs A = make_finalize_args(c, d_forces);
+    k_finalize<<<grid_of(A), 256, 0, c.stream>>>(A);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
+}
+
+void launch_finalize_multi(const FinalizeArgs* d_args, int nsys, int gx, cudaStream_t s)
+{
+    k_finalize_multi<<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    MDF_CUDA_TRY(cudaGetLastError());
 }
 
 static void check_index(const int32_t* a, long long n, int N, const char* what)
@@ -427,6 +468,11 @@ static int guarded(mdf_ctx* ctx, F&& f)
 
 static thread_local std::string g_create_error;
 
+// Live contexts per device; when the last one on a device is destroyed the
+// no-allocation entry point forgets that device's scratch address.
+static std::mutex g_live_mutex;
+static std::map<int, int> g_live;
+
 extern "C" {
 
 void mdf_params_default(mdf_params* p)
@@ -529,6 +575,11 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         mdf_destroy(ctx);
         return rc;
     }
+    {
+        std::lock_guard<std::mutex> lock(g_live_mutex);
+        ++g_live[ctx->c.device];
+        ctx->c.counted_live = true;
+    }
     *out = ctx;
     return MDF_OK;
 }
@@ -537,6 +588,10 @@ void mdf_destroy(mdf_ctx* ctx)
 {
     if (!ctx) return;
     Ctx& c = ctx->c;
+    if (c.counted_live) {
+        std::lock_guard<std::mutex> lock(g_live_mutex);
+        if (--g_live[c.device] == 0) noalloc_forget_device(c.device);
+    }
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto& e : c.evpool) cudaEventDestroy(e);
@@ -548,7 +603,7 @@ void mdf_destroy(mdf_ctx* ctx)
     c.xyz.release(); c.atom_col.release(); c.col_count.release(); c.col_start.release(); c.col_cstart.release();
     c.col_atoms.release(); c.slot_atom.release(); c.atom_slot.release(); c.slot_type.release(); c.center.release(); c.centerf.release();
     c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
-    c.ilist.release(); c.icount.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
+    c.ilist.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
     c.plist_in.release(); c.ilist_in.release(); c.n_in.release(); c.cur_lo.release(); c.cur_hi.release();
     c.f_atom.release(); c.scal.release(); c.npairs_dev.release(); c.forces_out.release(); c.forces_pme_ref.release();
     c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
@@ -557,6 +612,8 @@ void mdf_destroy(mdf_ctx* ctx)
         c.tw_d[d].release(); c.tw_f[d].release(); c.fft_tab[d].release(); c.mvec[d].release();
     }
     if (c.h_scal) cudaFreeHost(c.h_scal);
+    if (c.h_build) cudaFreeHost(c.h_build);
+    c.d_build.release();
     if (c.md_exec) cudaGraphExecDestroy(c.md_exec);
     if (c.md_graph) cudaGraphDestroy(c.md_graph);
     if (c.md_host) cudaFreeHost(c.md_host);

@@ -20,8 +20,10 @@
 #include <algorithm>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
+#include "kargs.cuh"
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
 
@@ -50,6 +52,14 @@ struct mdf_batch {
     DevBuf<double*> d_xyz_ptr, d_f_ptr;
     DevBuf<long long> d_off;
     std::string last_error;
+    // one launch per kernel for all systems (uniform launch parameters), or
+    // every system's own kernel chain in the graph
+    bool multi = false;
+    cudaStream_t side = nullptr;         // PME, bonded, exclusions: concurrent with pack/prune/pairs
+    cudaEvent_t ev_fork2 = nullptr, ev_join2 = nullptr;
+    // per-kernel argument arrays of the multi form (rebuilt before each capture)
+    DevBuf<unsigned char> args;          // one allocation, the arrays below point into it
+    size_t args_cap = 0;
 };
 
 namespace {
@@ -129,12 +139,240 @@ void enqueue(mdf_batch* b, uint32_t flags)
     b->graph_kernels = k0 + 2;
 }
 
+// ----------------------------------------------------------- multi form
+// Every kernel of an evaluation is launched once for all systems (grid z =
+// system, each block reads its system's arguments from device memory), so a
+// batch evaluation is ~17 graph nodes whatever the number of systems.  It
+// needs the launch-selecting parameters to agree across systems: precision,
+// LJ switch on or off, pruning on or off, pair-kernel warps and FFT lines.
+bool uniform_launches(const mdf_batch* b)
+{
+    const mdf_params& p0 = b->sys[0]->c.p;
+    for (const mdf_ctx* x : b->sys) {
+        const mdf_params& p = x->c.p;
+        if (p.precision != p0.precision || (p.switch_radius > 0) != (p0.switch_radius > 0) ||
+            (p.prune_every > 0) != (p0.prune_every > 0) || p.pair_warps != p0.pair_warps ||
+            p.fft_lines != p0.fft_lines || p.nranks > 1)
+            return false;
+    }
+    return true;
+}
+
+// Host-built argument arrays of one batch evaluation, copied to the device
+// before capture; the captured launches read them at every replay.
+template <typename R>
+struct MultiArgs {
+    std::vector<PackArgs<R>> pack;
+    std::vector<PruneArgs<R>> prune;
+    std::vector<PairF32Args> pf32;
+    std::vector<PairArgs<R>> p64;
+    std::vector<ExclArgs> excl;
+    std::vector<Pair14Args> p14;
+    std::vector<BondedArgs> bonded;
+    std::vector<ZeroArgs> zero;
+    std::vector<SpreadArgs> spread;
+    std::vector<FFTZArgs<R>> zf, zi;
+    std::vector<FFTYArgs<R>> yf, yi;
+    std::vector<FFTXArgs<R>> x;
+    std::vector<GatherArgs<R>> gather;
+    std::vector<FinalizeArgs> fin;
+    FFTChainMax fm{};
+    int gx_pack = 0, gx_prune = 0, gx_pairs = 0, gx_excl = 0, gx_14 = 0, gx_bonded = 0, gx_zero = 0, gx_spread = 0,
+        gx_gather = 0, gx_fin = 0;
+    size_t dyn_pairs = 0;
+    int threads = 256;
+    bool prune_on = false, use_switch = false, energy = false;
+};
+
+template <typename R>
+struct MultiDev {
+    const PackArgs<R>* pack;
+    const PruneArgs<R>* prune;
+    const PairF32Args* pf32;
+    const PairArgs<R>* p64;
+    const ExclArgs* excl;
+    const Pair14Args* p14;
+    const BondedArgs* bonded;
+    const ZeroArgs* zero;
+    const SpreadArgs* spread;
+    FFTChainDev<R> fft;
+    const GatherArgs<R>* gather;
+    const FinalizeArgs* fin;
+};
+
+template <typename T>
+size_t arr_bytes(const std::vector<T>& v)
+{
+    return (v.size() * sizeof(T) + 255) & ~(size_t)255;
+}
+
+// Build every system's arguments into M and copy them into b->args
+// (synchronously, outside any capture); returns the device arrays.  (The
+// prune kernel's kept-entry counter is not cleared per evaluation here: a
+// batch does not report it.)
+template <typename R>
+MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
+{
+    const int n = b->nsys;
+    const bool energy = (flags & MDF_COMPUTE_ENERGY) != 0;
+    M.energy = energy;
+    const Ctx& c0 = b->sys[0]->c;
+    M.prune_on = c0.p.prune_every > 0;
+    M.use_switch = c0.p.switch_radius > 0;
+    M.threads = pair_threads(c0);
+    for (int s = 0; s < n; ++s) {
+        Ctx& c = b->sys[s]->c;
+        if (M.prune_on) c.pruned_valid = true;   // the captured chain prunes before the pair kernel
+        M.pack.push_back(make_pack_args<R>(c));
+        M.prune.push_back(make_prune_args<R>(c));
+        if (sizeof(R) == 4) {
+            size_t dyn = 0;
+            M.pf32.push_back(make_pair_f32_args(c, &dyn));
+            M.dyn_pairs = std::max(M.dyn_pairs, dyn);
+        } else {
+            M.p64.push_back(make_pair_args<R>(c, false));
+        }
+        M.excl.push_back(make_excl_args(c));
+        M.p14.push_back(make_pair14_args(c));
+        M.bonded.push_back(make_bonded_args(c, false, c.f_atom.p, c.acc.p, c.status.p));
+        const long long ntot = (long long)c.K[0] * c.K[1] * c.K[2];
+        ZeroArgs z;
+        z.gx = grid_blocks(ntot, 256 * 8);
+        z.gy = 1;
+        z.p = c.qgrid.p;
+        z.n = ntot;
+        M.zero.push_back(z);
+        M.spread.push_back(make_spread_args(c));
+        const FFTChain<R> F = make_fft_chain<R>(c, energy);
+        M.zf.push_back(F.zf);
+        M.yf.push_back(F.yf);
+        M.x.push_back(F.x);
+        M.yi.push_back(F.yi);
+        M.zi.push_back(F.zi);
+        M.fm.zx = std::max(M.fm.zx, F.zf.gx);
+        M.fm.yx = std::max(M.fm.yx, F.yf.gx);
+        M.fm.yy = std::max(M.fm.yy, F.yf.gy);
+        M.fm.xx = std::max(M.fm.xx, F.x.gx);
+        M.fm.xy = std::max(M.fm.xy, F.x.gy);
+        M.fm.smz = std::max(M.fm.smz, F.smz);
+        M.fm.smy = std::max(M.fm.smy, F.smy);
+        M.fm.smx = std::max(M.fm.smx, F.smx);
+        M.gather.push_back(make_gather_args<R>(c));
+        // forces straight into the batch's concatenated device buffer
+        M.fin.push_back(make_finalize_args(c, b->d_forces.p + b->off[s]));
+    }
+    auto gmax = [](const auto& v) {
+        int g = 0;
+        for (const auto& a : v) g = std::max(g, a.gx);
+        return g;
+    };
+    M.gx_pack = gmax(M.pack);
+    M.gx_prune = gmax(M.prune);
+    M.gx_pairs = sizeof(R) == 4 ? gmax(M.pf32) : gmax(M.p64);
+    M.gx_excl = gmax(M.excl);
+    M.gx_14 = gmax(M.p14);
+    M.gx_bonded = gmax(M.bonded);
+    M.gx_zero = gmax(M.zero);
+    M.gx_spread = gmax(M.spread);
+    M.gx_gather = gmax(M.gather);
+    M.gx_fin = gmax(M.fin);
+    // one device allocation for every array
+    const size_t total = arr_bytes(M.pack) + arr_bytes(M.prune) + arr_bytes(M.pf32) + arr_bytes(M.p64) +
+                         arr_bytes(M.excl) + arr_bytes(M.p14) + arr_bytes(M.bonded) + arr_bytes(M.zero) +
+                         arr_bytes(M.spread) + arr_bytes(M.zf) + arr_bytes(M.yf) + arr_bytes(M.x) +
+                         arr_bytes(M.yi) + arr_bytes(M.zi) + arr_bytes(M.gather) + arr_bytes(M.fin);
+    std::vector<unsigned char> host(total);
+    b->args.alloc(total);
+    size_t off = 0;
+    MultiDev<R> D;
+    auto put = [&](const auto& v, auto*& dptr) {
+        using T = typename std::decay_t<decltype(v)>::value_type;
+        if (!v.empty()) memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
+        dptr = reinterpret_cast<T*>(b->args.p + off);
+        off += arr_bytes(v);
+    };
+    put(M.pack, D.pack);
+    put(M.prune, D.prune);
+    put(M.pf32, D.pf32);
+    put(M.p64, D.p64);
+    put(M.excl, D.excl);
+    put(M.p14, D.p14);
+    put(M.bonded, D.bonded);
+    put(M.zero, D.zero);
+    put(M.spread, D.spread);
+    put(M.zf, D.fft.zf);
+    put(M.yf, D.fft.yf);
+    put(M.x, D.fft.x);
+    put(M.yi, D.fft.yi);
+    put(M.zi, D.fft.zi);
+    put(M.gather, D.gather);
+    put(M.fin, D.fin);
+    MDF_CUDA_TRY(cudaMemcpyAsync(b->args.p, host.data(), total, cudaMemcpyHostToDevice, b->main));
+    MDF_CUDA_TRY(cudaStreamSynchronize(b->main));
+    return D;
+}
+
+template <typename R>
+void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D)
+{
+    const int n = b->nsys, th = 256;
+    const dim3 grid((unsigned)((b->max_len + th - 1) / th), (unsigned)n);
+    MDF_CUDA_TRY(cudaMemcpyAsync(b->d_pos.p, b->h_pos, sizeof(double) * b->total, cudaMemcpyHostToDevice, b->main));
+    k_batch_scatter<<<grid, th, 0, b->main>>>(b->d_off.p, b->d_pos.p, b->d_xyz_ptr.p);
+    MDF_CUDA_TRY(cudaGetLastError());
+    long long k = 2;   // scatter + finalize
+    // side stream: exclusions, 1-4, bonded terms, PME (they only read positions
+    // and charges and add into the fixed-point accumulators)
+    MDF_CUDA_TRY(cudaEventRecord(b->ev_fork2, b->main));
+    MDF_CUDA_TRY(cudaStreamWaitEvent(b->side, b->ev_fork2, 0));
+    launch_exclusions_multi(D.excl, M.gx_excl, D.p14, M.gx_14, n, M.energy, b->side);
+    k += (M.gx_excl > 0) + (M.gx_14 > 0);
+    launch_bonded_multi(D.bonded, n, M.gx_bonded, M.energy, b->side);
+    k += M.gx_bonded > 0;
+    launch_pme_multi<R>(D.zero, M.gx_zero, D.spread, M.gx_spread, D.fft, M.fm, D.gather, M.gx_gather, n, M.energy,
+                        b->side);
+    k += 8;   // grid clear, spread, five FFT passes, gather
+    MDF_CUDA_TRY(cudaEventRecord(b->ev_join2, b->side));
+    // main stream: pack, prune, pair kernel
+    launch_pack_multi<R>(D.pack, n, M.gx_pack, b->main);
+    ++k;
+    if (M.prune_on) {
+        launch_prune_multi<R>(D.prune, n, M.gx_prune, b->main);
+        ++k;
+    }
+    if (M.gx_pairs > 0) {
+        if (sizeof(R) == 4)
+            launch_pairs_f32_multi(D.pf32, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, b->main);
+        else
+            launch_pairs_multi_fp64(reinterpret_cast<const PairArgs<double>*>(D.p64), n, M.gx_pairs, M.threads,
+                                    M.energy, b->main);
+        ++k;
+    }
+    MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, b->ev_join2, 0));
+    launch_finalize_multi(D.fin, n, M.gx_fin, b->main);
+    MDF_CUDA_TRY(cudaMemcpyAsync(b->h_forces, b->d_forces.p, sizeof(double) * b->total, cudaMemcpyDeviceToHost,
+                                 b->main));
+    b->graph_kernels = k;
+}
+
 void capture(mdf_batch* b, uint32_t flags)
 {
     drop_graph(b);
+    b->multi = uniform_launches(b);
+    const bool fp32 = b->sys[0]->c.p.precision == MDF_PREC_MIXED;
+    MultiArgs<float> Mf;
+    MultiArgs<double> Md;
+    MultiDev<float> Df{};
+    MultiDev<double> Dd{};
+    if (b->multi) {
+        if (fp32) Df = prepare_multi<float>(b, flags, Mf);
+        else Dd = prepare_multi<double>(b, flags, Md);
+    }
     MDF_CUDA_TRY(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
     try {
-        enqueue(b, flags);
+        if (!b->multi) enqueue(b, flags);
+        else if (fp32) enqueue_multi<float>(b, Mf, Df);
+        else enqueue_multi<double>(b, Md, Dd);
     } catch (...) {
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(b->main, &g);
@@ -216,6 +454,13 @@ int mdf_batch_create(int nsys, const mdf_topology* const* topos, const mdf_param
         MDF_CUDA_TRY(cudaSetDevice(b->device));
         MDF_CUDA_TRY(cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking));
         MDF_CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+        {
+            int lo = 0, hi = 0;   // the short PME / bonded kernels first (as in one context)
+            MDF_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+            MDF_CUDA_TRY(cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, hi));
+        }
+        MDF_CUDA_TRY(cudaEventCreateWithFlags(&b->ev_fork2, cudaEventDisableTiming));
+        MDF_CUDA_TRY(cudaEventCreateWithFlags(&b->ev_join2, cudaEventDisableTiming));
         b->join.assign(nsys, nullptr);
         for (int s = 0; s < nsys; ++s) MDF_CUDA_TRY(cudaEventCreateWithFlags(&b->join[s], cudaEventDisableTiming));
         MDF_CUDA_TRY(cudaHostAlloc((void**)&b->h_pos, sizeof(double) * b->total, cudaHostAllocDefault));
@@ -260,6 +505,10 @@ void mdf_batch_destroy(mdf_batch* b)
     for (cudaEvent_t e : b->join)
         if (e) cudaEventDestroy(e);
     if (b->fork) cudaEventDestroy(b->fork);
+    if (b->ev_fork2) cudaEventDestroy(b->ev_fork2);
+    if (b->ev_join2) cudaEventDestroy(b->ev_join2);
+    if (b->side) cudaStreamDestroy(b->side);
+    b->args.release();
     if (b->main) cudaStreamDestroy(b->main);
     delete b;
 }

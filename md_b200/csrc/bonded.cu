@@ -10,23 +10,12 @@
 // improper difference into (-pi, pi].
 #include <cmath>
 
+#include "kargs.cuh"
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
 
 namespace mdf {
 
-struct BondedArgs {
-    int n[6];        // end index per list: bonds, ub, angles, dihedrals, impropers, cmaps
-    int lo[6];       // first index per list (a rank's share starts there)
-    int blk0[7];     // first block of each segment (prefix)
-    const int *bond_atoms, *ub_atoms, *angle_atoms, *dih_atoms, *imp_atoms, *cmap_atoms, *cmap_set;
-    const double2 *bond_par, *ub_par, *angle_par, *imp_par;
-    const double* dih_par;
-    const double* cmap_coeff;
-    int cmap_res;
-    const double* xyz;
-    int N;
-};
 
 __device__ __forceinline__ void ld3(const double* x, int a, double p[3])
 {
@@ -135,9 +124,11 @@ __device__ void cmap_eval(const double* __restrict__ coeff, int res, int set, do
 }
 
 template <bool PHYS, bool ENERGY>
-__global__ void __launch_bounds__(256) k_bonded(BondedArgs A, unsigned long long* __restrict__ f,
-                                                unsigned long long* __restrict__ acc, unsigned* st)
+__device__ __forceinline__ void bonded_dev(const BondedArgs& A)
 {
+    unsigned long long* __restrict__ f = A.f;
+    unsigned long long* __restrict__ acc = A.acc;
+    unsigned* st = A.st;
     const double PI = 3.14159265358979323846;
     int seg = 0;
     while (seg < 5 && (int)blockIdx.x >= A.blk0[seg + 1]) ++seg;
@@ -276,21 +267,37 @@ __global__ void __launch_bounds__(256) k_bonded(BondedArgs A, unsigned long long
     }
 }
 
-void launch_bonded(Ctx& c, bool energy)
+template <bool PHYS, bool ENERGY>
+__global__ void __launch_bounds__(256) k_bonded(BondedArgs A)
+{
+    bonded_dev<PHYS, ENERGY>(A);
+}
+
+template <bool PHYS, bool ENERGY>
+__global__ void __launch_bounds__(256) k_bonded_multi(const BondedArgs* __restrict__ As)
+{
+    const BondedArgs& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    bonded_dev<PHYS, ENERGY>(A);
+}
+
+// The six term lists in one launch: this rank's share of each (all of them
+// with one rank, or with whole = true), accumulated into f / acc / st.
+BondedArgs make_bonded_args(const Ctx& c, bool whole, unsigned long long* f, unsigned long long* acc, unsigned* st)
 {
     BondedArgs A;
     const int total[6] = {c.n_bonds, c.n_ub, c.n_angles, c.n_dih, c.n_imp, c.n_cmap};
     const int th = 256;
     A.blk0[0] = 0;
-    for (int s = 0; s < 6; ++s) {   // this rank's share of each list
-        long long lo, hi;
-        rank_slice(c, total[s], lo, hi);
+    for (int s = 0; s < 6; ++s) {
+        long long lo = 0, hi = total[s];
+        if (!whole) rank_slice(c, total[s], lo, hi);
         A.lo[s] = (int)lo;
         A.n[s] = (int)hi;
         A.blk0[s + 1] = A.blk0[s] + (int)((hi - lo + th - 1) / th);
     }
-    int nblk = A.blk0[6];
-    if (nblk == 0) return;
+    A.gx = A.blk0[6];
+    A.gy = 1;
     A.bond_atoms = c.bond_atoms.p; A.ub_atoms = c.ub_atoms.p; A.angle_atoms = c.angle_atoms.p;
     A.dih_atoms = c.dih_atoms.p; A.imp_atoms = c.imp_atoms.p; A.cmap_atoms = c.cmap_atoms.p;
     A.cmap_set = c.cmap_set.p;
@@ -298,44 +305,44 @@ void launch_bonded(Ctx& c, bool energy)
     A.dih_par = c.dih_par.p; A.cmap_coeff = c.cmap_coeff.p; A.cmap_res = c.cmap_res;
     A.xyz = c.xyz.p;
     A.N = c.N;
-    bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
-    if (phys) {
-        if (energy) k_bonded<true, true><<<nblk, th, 0, c.stream>>>(A, c.f_atom.p, c.acc.p, c.status.p);
-        else k_bonded<true, false><<<nblk, th, 0, c.stream>>>(A, c.f_atom.p, c.acc.p, c.status.p);
+    A.f = f;
+    A.acc = acc;
+    A.st = st;
+    return A;
+}
+
+static void launch_bonded_args(const Ctx& c, const BondedArgs& A, bool energy)
+{
+    if (A.gx == 0) return;
+    const int th = 256;
+    if (c.p.semantics == MDF_SEM_PHYSICAL) {
+        if (energy) k_bonded<true, true><<<grid_of(A), th, 0, c.stream>>>(A);
+        else k_bonded<true, false><<<grid_of(A), th, 0, c.stream>>>(A);
     } else {
-        if (energy) k_bonded<false, true><<<nblk, th, 0, c.stream>>>(A, c.f_atom.p, c.acc.p, c.status.p);
-        else k_bonded<false, false><<<nblk, th, 0, c.stream>>>(A, c.f_atom.p, c.acc.p, c.status.p);
+        if (energy) k_bonded<false, true><<<grid_of(A), th, 0, c.stream>>>(A);
+        else k_bonded<false, false><<<grid_of(A), th, 0, c.stream>>>(A);
     }
     MDF_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_bonded(Ctx& c, bool energy)
+{
+    const BondedArgs A = make_bonded_args(c, false, c.f_atom.p, c.acc.p, c.status.p);
+    if (A.gx == 0) return;
+    launch_bonded_args(c, A, energy);
     c.launches += 1;
 }
 
-// The same kernel with caller-supplied accumulators: f [3 * N] fixed-point
-// forces (SoA x|y|z), acc the energy words, st the status word.
 void launch_bonded_into(Ctx& c, bool energy, unsigned long long* f, unsigned long long* acc, unsigned* st)
 {
-    BondedArgs A;
-    A.n[0] = c.n_bonds; A.n[1] = c.n_ub; A.n[2] = c.n_angles; A.n[3] = c.n_dih; A.n[4] = c.n_imp; A.n[5] = c.n_cmap;
-    for (int s = 0; s < 6; ++s) A.lo[s] = 0;
-    const int th = 256;
-    A.blk0[0] = 0;
-    for (int s = 0; s < 6; ++s) A.blk0[s + 1] = A.blk0[s] + (A.n[s] + th - 1) / th;
-    const int nblk = A.blk0[6];
-    if (nblk == 0) return;
-    A.bond_atoms = c.bond_atoms.p; A.ub_atoms = c.ub_atoms.p; A.angle_atoms = c.angle_atoms.p;
-    A.dih_atoms = c.dih_atoms.p; A.imp_atoms = c.imp_atoms.p; A.cmap_atoms = c.cmap_atoms.p;
-    A.cmap_set = c.cmap_set.p;
-    A.bond_par = c.bond_par.p; A.ub_par = c.ub_par.p; A.angle_par = c.angle_par.p; A.imp_par = c.imp_par.p;
-    A.dih_par = c.dih_par.p; A.cmap_coeff = c.cmap_coeff.p; A.cmap_res = c.cmap_res;
-    A.xyz = c.xyz.p;
-    A.N = c.N;
-    if (c.p.semantics == MDF_SEM_PHYSICAL) {
-        if (energy) k_bonded<true, true><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
-        else k_bonded<true, false><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
-    } else {
-        if (energy) k_bonded<false, true><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
-        else k_bonded<false, false><<<nblk, th, 0, c.stream>>>(A, f, acc, st);
-    }
+    launch_bonded_args(c, make_bonded_args(c, true, f, acc, st), energy);
+}
+
+void launch_bonded_multi(const BondedArgs* d_args, int nsys, int gx, bool energy, cudaStream_t s)
+{
+    if (gx == 0) return;
+    if (energy) k_bonded_multi<true, true><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    else k_bonded_multi<true, false><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
     MDF_CUDA_TRY(cudaGetLastError());
 }
 

@@ -174,7 +174,6 @@ struct Ctx {
     DevBuf<double4> xq_d;          // [n_slots] (FP64)
     DevBuf<int> cluster_col;       // [n_clusters]
     DevBuf<ILRange> ilist;         // [n_clusters]
-    DevBuf<int> icount;            // [n_clusters + 1]
     DevBuf<PairEntry> plist;       // [cap] outer list (cutoff + skin)
     long long n_entries = 0;
     DevBuf<PairEntry> plist_in;    // pruned list the pair kernel walks (same offsets as plist)
@@ -183,6 +182,8 @@ struct Ctx {
     int since_prune = 0;
     bool pruned_valid = false;
     DevBuf<int> scan_tmp;
+    DevBuf<int> d_build;           // [4] list entries claimed by the search
+    int* h_build = nullptr;        // pinned: cluster count, entry count, status of the last build
 
     // accumulators.  The force accumulators are cleared by the kernel that
     // reads them (k_finalize); the scalar block is copied to the host and then
@@ -258,6 +259,8 @@ struct Ctx {
     std::vector<std::pair<const char*, float>> tlast;
     long long launches = 0;                   // kernels launched by evaluations
 
+    bool counted_live = false;           // counted in the per-device live-context table
+
     // last evaluation bookkeeping
     bool pending = false;
     uint32_t pending_flags = 0;
@@ -290,9 +293,7 @@ void mark(Ctx& c, const char* name);
 void eval_async_impl(Ctx& c, uint32_t flags);
 void host_energies(const Ctx& c, uint32_t flags, mdf_energies* e_out);
 void check_host_status(const Ctx& c);
-
-// simple device-wide exclusive scan of ints (n up to a few million)
-void exclusive_scan_int(const int* d_in, int* d_out, int n, int* d_total_out, cudaStream_t s);
+void noalloc_forget_device(int device);
 
 int grid_blocks(long long n, int threads);
 

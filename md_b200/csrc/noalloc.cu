@@ -55,9 +55,22 @@ __global__ void k_noalloc_forces(int N, const unsigned long long* __restrict__ f
     for (int k = 0; k < 3; ++k) out[3 * a + k] = (double)(long long)f[(size_t)k * N + a] * FORCE_ISCALE;
 }
 
+// Forget the cached address of a device whose last context is gone: a caller
+// may reset the device (cudaDeviceReset) before creating new contexts, and the
+// module - with the array - is then loaded again, possibly elsewhere.
+void noalloc_forget_device(int device)
+{
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES) return;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    g_noalloc_ptr[device] = nullptr;
+}
+
 static void bonded_noalloc(Ctx& c, uint32_t flags, double* d_forces, mdf_energies* e_out)
 {
     if (!c.have_positions) throw ApiError(MDF_ERR_STATE, "positions not set");
+    // the bonded lists are not split over ranks here: a rank's context would
+    // return the whole bonded set, unlike mdf_compute
+    if (distributed(c)) throw ApiError(MDF_ERR_UNSUPPORTED, "mdf_compute_bonded_noalloc: not available with nranks > 1");
     if (c.N > NOALLOC_MAX_ATOMS)
         throw ApiError(MDF_ERR_INVALID, "mdf_compute_bonded_noalloc: " + std::to_string(c.N) +
                                             " atoms exceed the static scratch limit of " +

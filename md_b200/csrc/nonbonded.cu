@@ -21,6 +21,7 @@
 // accumulators once per cluster pair.
 #include <cmath>
 
+#include "kargs.cuh"
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
 #include "nb_common.cuh"
@@ -28,13 +29,23 @@
 namespace mdf {
 
 template <typename R, int SEM, bool ENERGY>
-__global__ void __launch_bounds__(NB_THREADS) k_pairs(
-    int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist,
-    const typename V4<R>::type* __restrict__ xq, const int* __restrict__ stype, const double4* __restrict__ center,
-    const typename V2<R>::type* __restrict__ ljAB, const int* __restrict__ ljvalid, NBParams P,
-    unsigned long long* __restrict__ fslot, int nslots, unsigned long long* __restrict__ acc,
-    unsigned long long* __restrict__ npairs, int count, unsigned* st)
+__device__ __forceinline__ void pairs_dev(const PairArgs<R>& A)
 {
+    const int nlist = A.nlist;
+    const ILRange* __restrict__ ilist = A.ilist;
+    const PairEntry* __restrict__ plist = A.plist;
+    const typename V4<R>::type* __restrict__ xq = A.xq;
+    const int* __restrict__ stype = A.stype;
+    const double4* __restrict__ center = A.center;
+    const typename V2<R>::type* __restrict__ ljAB = A.ljAB;
+    const int* __restrict__ ljvalid = A.ljvalid;
+    const NBParams& P = A.P;
+    unsigned long long* __restrict__ fslot = A.fslot;
+    const int nslots = A.nslots;
+    unsigned long long* __restrict__ acc = A.acc;
+    unsigned long long* __restrict__ npairs = A.npairs;
+    const int count = A.count;
+    unsigned* st = A.st;
     using V4t = typename V4<R>::type;
     using V2t = typename V2<R>::type;
     __shared__ V4t sx[NB_WARPS][4][CLUSTER + 1];
@@ -229,6 +240,20 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
     }
 }
 
+template <typename R, int SEM, bool ENERGY>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs(PairArgs<R> A)
+{
+    pairs_dev<R, SEM, ENERGY>(A);
+}
+
+template <typename R, int SEM, bool ENERGY>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_multi(const PairArgs<R>* __restrict__ As)
+{
+    const PairArgs<R>& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs_dev<R, SEM, ENERGY>(A);
+}
+
 // ------------------------------------------------- FP32 PHYSICAL pair kernel
 // Periodic image offsets s*L of the 27 shift codes as an FP32 hi + lo pair.
 
@@ -241,16 +266,6 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs(
 //    bit t;
 //  * the pair arithmetic is branch-free (inactive pairs are selected out);
 //  * energies are summed in FP32 per entry and in FP64 across entries.
-// Constants of the FP32 pair kernel, folded on the host.
-struct PairConstF {
-    float rc2;
-    float kex;        // -alpha^2 log2(e): exp(-alpha^2 r^2) = 2^(kex r^2)
-    float pa;         // 0.3275911 alpha (A&S 7.1.26 argument)
-    float two_a_spi;  // 2 alpha / sqrt(pi)
-    float inv_sw, rsw_inv;          // 1/(rc - rsw), rsw/(rc - rsw)
-    float d30, d60;                 // -30, 60 times inv_sw (dS/dr = x^2 (d30 + x (d60 + x d30)))
-    float uc6, uc12, rcf, rc2f;     // force-shifted LJ
-};
 
 // The mixed-precision production kernel (PHYSICAL semantics).  Same warp
 // layout as k_pairs; differences that matter for speed and accuracy:
@@ -268,9 +283,10 @@ template <bool ENERGY, bool SWITCH, bool COUNT>
 __device__ __forceinline__ void pairs_f32_body(
     int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
     const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp,
-    int lj_smem, float kc, PairConstF K, ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots,
-    unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs, unsigned* st)
+    int lj_smem, float kc, const PairConstF& Kin, const ShiftTable& shifts, unsigned long long* __restrict__ fslot,
+    int nslots, unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs, unsigned* st)
 {
+    const PairConstF K = Kin;   // registers (the multi-system launch reads it from device memory)
     extern __shared__ float4 s_lj[];
     // each staged j cluster is stored twice in a row, so the atom a lane meets
     // at step t, (ii + t) mod 8, sits at the compile-time offset t from the
@@ -398,30 +414,44 @@ __device__ __forceinline__ void pairs_f32_body(
     }
 }
 
-#define MDF_PF32_PARAMS                                                                                        \
-    int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq, \
-        const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp, \
-        int lj_smem, float kc, PairConstF K, ShiftTable shifts, unsigned long long* __restrict__ fslot, int nslots,   \
-        unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs, unsigned* st
-#define MDF_PF32_ARGS nlist, ilist, plist, xq, stype, centerf, lj4, ntp, lj_smem, kc, K, shifts, fslot, nslots, acc, npairs, st
+#define MDF_PF32_UNPACK(A)                                                                                       \
+    A.nlist, A.ilist, A.plist, A.xq, A.stype, A.centerf, A.lj4, A.ntp, A.lj_smem, A.kc, A.K, A.shifts, A.fslot,      \
+        A.nslots, A.acc, A.npairs, A.st
 
 // With energies: the compiler's own register choice (72, three blocks per SM;
 // a 64-register cap spills and is slower).
 template <bool SWITCH, bool COUNT>
-__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(MDF_PF32_PARAMS)
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(PairF32Args A)
 {
-    pairs_f32_body<true, SWITCH, COUNT>(MDF_PF32_ARGS);
+    pairs_f32_body<true, SWITCH, COUNT>(MDF_PF32_UNPACK(A));
 }
 
 // Forces only (every dynamics step but the last of a chunk): 64 registers
 // with no spills, four blocks per SM (+4% dynamics steps/s).
 template <bool SWITCH, bool COUNT>
-__global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force(MDF_PF32_PARAMS)
+__global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force(PairF32Args A)
 {
-    pairs_f32_body<false, SWITCH, COUNT>(MDF_PF32_ARGS);
+    pairs_f32_body<false, SWITCH, COUNT>(MDF_PF32_UNPACK(A));
 }
-#undef MDF_PF32_PARAMS
-#undef MDF_PF32_ARGS
+
+// Many systems in one launch (blockIdx.z = system), with the same register
+// budgets as the one-system kernels above.
+template <bool SWITCH>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32_multi(const PairF32Args* __restrict__ As)
+{
+    const PairF32Args& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs_f32_body<true, SWITCH, false>(MDF_PF32_UNPACK(A));
+}
+
+template <bool SWITCH>
+__global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force_multi(const PairF32Args* __restrict__ As)
+{
+    const PairF32Args& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs_f32_body<false, SWITCH, false>(MDF_PF32_UNPACK(A));
+}
+#undef MDF_PF32_UNPACK
 
 // --------------------------------------------------------------- FP64 pairs
 __device__ __forceinline__ void pair_vec(const double* __restrict__ xyz, int a, int b, const NBParams& P,
@@ -446,10 +476,18 @@ __device__ __forceinline__ void add_pair_force(unsigned long long* f, int N, int
 // excluded pairs that are not 1-4 (src/System/NonBondedEnergy.cpp:271-304),
 // no force.
 template <int SEM, bool ENERGY>
-__global__ void k_exclusions(int n, const int* __restrict__ pairs, const int* __restrict__ is14,
-                             const double* __restrict__ xyz, const double* __restrict__ q, NBParams P, int N,
-                             unsigned long long* __restrict__ fatom, unsigned long long* __restrict__ acc, unsigned* st)
+__device__ __forceinline__ void exclusions_dev(const ExclArgs& A)
 {
+    const int n = A.n;
+    const int* __restrict__ pairs = A.pairs;
+    const int* __restrict__ is14 = A.is14;
+    const double* __restrict__ xyz = A.xyz;
+    const double* __restrict__ q = A.q;
+    const NBParams& P = A.P;
+    const int N = A.N;
+    unsigned long long* __restrict__ fatom = A.fatom;
+    unsigned long long* __restrict__ acc = A.acc;
+    unsigned* st = A.st;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     double e = 0.0;
     if (k < n && !(SEM == MDF_SEM_REFERENCE && is14[k])) {
@@ -477,11 +515,35 @@ __global__ void k_exclusions(int n, const int* __restrict__ pairs, const int* __
 // REFERENCE: the reference's is14 branches of the list loops (A14/B14 with the
 // switch, Coulomb / scee, and CalculateEnergyEwaldDirectTerm_14's erf(r)).
 template <int SEM, bool ENERGY>
-__global__ void k_pairs14(int n, const int* __restrict__ pairs, const double2* __restrict__ scale,
-                          const double* __restrict__ xyz, const double* __restrict__ q, const int* __restrict__ type,
-                          const double2* __restrict__ lj14, const int* __restrict__ ljvalid, NBParams P, int N,
-                          unsigned long long* __restrict__ fatom, unsigned long long* __restrict__ acc, unsigned* st)
+__global__ void k_exclusions(ExclArgs A)
 {
+    exclusions_dev<SEM, ENERGY>(A);
+}
+
+template <int SEM, bool ENERGY>
+__global__ void k_exclusions_multi(const ExclArgs* __restrict__ As)
+{
+    const ExclArgs& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    exclusions_dev<SEM, ENERGY>(A);
+}
+
+template <int SEM, bool ENERGY>
+__device__ __forceinline__ void pairs14_dev(const Pair14Args& A)
+{
+    const int n = A.n;
+    const int* __restrict__ pairs = A.pairs;
+    const double2* __restrict__ scale = A.scale;
+    const double* __restrict__ xyz = A.xyz;
+    const double* __restrict__ q = A.q;
+    const int* __restrict__ type = A.type;
+    const double2* __restrict__ lj14 = A.lj14;
+    const int* __restrict__ ljvalid = A.ljvalid;
+    const NBParams& P = A.P;
+    const int N = A.N;
+    unsigned long long* __restrict__ fatom = A.fatom;
+    unsigned long long* __restrict__ acc = A.acc;
+    unsigned* st = A.st;
     int k = blockIdx.x * blockDim.x + threadIdx.x;
     double ev = 0, ec = 0, eall = 0, epl = 0, ecut = 0, edir = 0;
     if (k < n) {
@@ -549,6 +611,20 @@ __global__ void k_pairs14(int n, const int* __restrict__ pairs, const double2* _
     }
 }
 
+template <int SEM, bool ENERGY>
+__global__ void k_pairs14(Pair14Args A)
+{
+    pairs14_dev<SEM, ENERGY>(A);
+}
+
+template <int SEM, bool ENERGY>
+__global__ void k_pairs14_multi(const Pair14Args* __restrict__ As)
+{
+    const Pair14Args& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs14_dev<SEM, ENERGY>(A);
+}
+
 // ------------------------------------------------------------------ host
 NBParams make_params(const Ctx& c)
 {
@@ -577,6 +653,11 @@ static int pair_warps(const Ctx& c)
     return (w == 2 || w == 4 || w == 8) ? w : NB_WARPS;
 }
 
+int pair_threads(const Ctx& c)
+{
+    return 32 * pair_warps(c);
+}
+
 // Atom pairs within the cutoff are counted by the first evaluation after a
 // pairlist build only (the count costs instructions in the pair loop).
 static bool begin_pair_count(Ctx& c)
@@ -589,30 +670,62 @@ static bool begin_pair_count(Ctx& c)
     return true;
 }
 
-template <typename R, int SEM>
-static void launch_pairs_t(Ctx& c, bool energy, const typename V4<R>::type* xq, const typename V2<R>::type* lj)
+// Pair-kernel arguments of this rank's i clusters.  With count set the kernel
+// counts the atom pairs inside the cutoff (first evaluation after a build).
+template <typename R>
+PairArgs<R> make_pair_args(const Ctx& c, bool count)
 {
-    NBParams P = make_params(c);
+    PairArgs<R> A;
+    A.P = make_params(c);
     const int wpb = pair_warps(c);
     long long lo, hi;
     rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
-    const int ncl = (int)(hi - lo);
-    if (ncl == 0) return;
-    int nb = grid_blocks(ncl, wpb);
+    A.nlist = (int)(hi - lo);
+    A.gx = grid_blocks(A.nlist, wpb);
+    A.gy = 1;
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
-    const ILRange* il = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
-    const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
-    const int count = begin_pair_count(c) ? 1 : 0;
-    if (energy)
-        k_pairs<R, SEM, true><<<nb, 32 * wpb, 0, c.stream>>>(ncl, il, pl, xq, c.slot_type.p, c.center.p,
-                                                               lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
-                                                               c.npairs_dev.p, count, c.status.p);
-    else
-        k_pairs<R, SEM, false><<<nb, 32 * wpb, 0, c.stream>>>(ncl, il, pl, xq, c.slot_type.p, c.center.p,
-                                                                lj, c.ljvalid.p, P, c.f_slot.p, c.n_slots, c.acc.p,
-                                                                c.npairs_dev.p, count, c.status.p);
+    A.ilist = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
+    A.plist = pruned ? c.plist_in.p : c.plist.p;
+    if (sizeof(R) == 4) {
+        A.xq = reinterpret_cast<const typename V4<R>::type*>(c.xq_f.p);
+        A.ljAB = reinterpret_cast<const typename V2<R>::type*>(c.ljAB_f.p);
+    } else {
+        A.xq = reinterpret_cast<const typename V4<R>::type*>(c.xq_d.p);
+        A.ljAB = reinterpret_cast<const typename V2<R>::type*>(c.ljAB.p);
+    }
+    A.stype = c.slot_type.p;
+    A.center = c.center.p;
+    A.ljvalid = c.ljvalid.p;
+    A.fslot = c.f_slot.p;
+    A.nslots = c.n_slots;
+    A.acc = c.acc.p;
+    A.npairs = c.npairs_dev.p;
+    A.count = count ? 1 : 0;
+    A.st = c.status.p;
+    return A;
+}
+template PairArgs<float> make_pair_args<float>(const Ctx&, bool);
+template PairArgs<double> make_pair_args<double>(const Ctx&, bool);
+
+template <typename R, int SEM>
+static void launch_pairs_t(Ctx& c, bool energy)
+{
+    const bool count = begin_pair_count(c);
+    const PairArgs<R> A = make_pair_args<R>(c, count);
+    if (A.nlist == 0) return;
+    const int th = 32 * pair_warps(c);
+    if (energy) k_pairs<R, SEM, true><<<grid_of(A), th, 0, c.stream>>>(A);
+    else k_pairs<R, SEM, false><<<grid_of(A), th, 0, c.stream>>>(A);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
+}
+
+void launch_pairs_multi_fp64(const PairArgs<double>* d_args, int nsys, int gx, int threads, bool energy,
+                             cudaStream_t s)
+{
+    if (energy) k_pairs_multi<double, MDF_SEM_PHYSICAL, true><<<dim3(gx, 1, nsys), threads, 0, s>>>(d_args);
+    else k_pairs_multi<double, MDF_SEM_PHYSICAL, false><<<dim3(gx, 1, nsys), threads, 0, s>>>(d_args);
+    MDF_CUDA_TRY(cudaGetLastError());
 }
 
 ShiftTable make_shift_table(const Ctx& c)
@@ -630,11 +743,15 @@ ShiftTable make_shift_table(const Ctx& c)
     return t;
 }
 
-static void launch_pairs_f32(Ctx& c, bool energy)
+// FP32 pair-kernel arguments (PHYSICAL) of this rank's i clusters; *dyn gets
+// the dynamic shared memory the LJ table needs (0 when it stays in global
+// memory).
+PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn)
 {
-    NBParams P = make_params(c);
-    ShiftTable sh = make_shift_table(c);
-    PairConstF K;
+    PairF32Args A;
+    const NBParams P = make_params(c);
+    A.shifts = make_shift_table(c);
+    PairConstF& K = A.K;
     K.rc2 = (float)P.rc2;
     K.kex = (float)(-P.alpha * P.alpha * 1.4426950408889634074);
     K.pa = (float)(0.3275911 * P.alpha);
@@ -649,42 +766,69 @@ static void launch_pairs_f32(Ctx& c, bool energy)
     K.rc2f = (float)P.rc2;
     const int ntp2 = c.ntp * c.ntp;
     const size_t lj_bytes = sizeof(float4) * (size_t)ntp2;
-    const int lj_smem = lj_bytes <= 40 * 1024 ? 1 : 0;
-    const size_t dyn = lj_smem ? lj_bytes : 0;
+    A.lj_smem = lj_bytes <= 40 * 1024 ? 1 : 0;
+    if (dyn) *dyn = A.lj_smem ? lj_bytes : 0;
     const int wpb = pair_warps(c);
     long long lo, hi;
     rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
-    const int ncl = (int)(hi - lo);
-    if (ncl == 0) return;
-    int nb = grid_blocks(ncl, wpb);
+    A.nlist = (int)(hi - lo);
+    A.gx = grid_blocks(A.nlist, wpb);
+    A.gy = 1;
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
-    const ILRange* il = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
-    const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
+    A.ilist = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
+    A.plist = pruned ? c.plist_in.p : c.plist.p;
+    A.xq = c.xq_f.p;
+    A.stype = c.slot_type.p;
+    A.centerf = c.centerf.p;
+    A.lj4 = c.ljAB4_f.p;
+    A.ntp = c.ntp;
+    A.kc = (float)P.kc;
+    A.fslot = c.f_slot.p;
+    A.nslots = c.n_slots;
+    A.acc = c.acc.p;
+    A.npairs = c.npairs_dev.p;
+    A.st = c.status.p;
+    return A;
+}
+
+static void launch_pairs_f32(Ctx& c, bool energy)
+{
     const bool count = begin_pair_count(c);
+    size_t dyn = 0;
+    const PairF32Args A = make_pair_f32_args(c, &dyn);
+    if (A.nlist == 0) return;
+    const int th = 32 * pair_warps(c);
+    const bool sw = c.p.switch_radius > 0.0;
 #define MDF_PF32(E, S, K_)                                                                                     \
     do {                                                                                                       \
-        if (E)                                                                                                 \
-            k_pairs_f32<S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(ncl, il, pl, c.xq_f.p, c.slot_type.p,            \
-                                                                c.centerf.p, c.ljAB4_f.p, c.ntp, lj_smem,          \
-                                                                (float)P.kc, K, sh, c.f_slot.p, c.n_slots,       \
-                                                                c.acc.p, c.npairs_dev.p, c.status.p);            \
-        else                                                                                                   \
-            k_pairs_f32_force<S, K_><<<nb, 32 * wpb, dyn, c.stream>>>(ncl, il, pl, c.xq_f.p, c.slot_type.p,      \
-                                                                      c.centerf.p, c.ljAB4_f.p, c.ntp, lj_smem,    \
-                                                                      (float)P.kc, K, sh, c.f_slot.p, c.n_slots, \
-                                                                      c.acc.p, c.npairs_dev.p, c.status.p);      \
+        if (E) k_pairs_f32<S, K_><<<grid_of(A), th, dyn, c.stream>>>(A);                                         \
+        else k_pairs_f32_force<S, K_><<<grid_of(A), th, dyn, c.stream>>>(A);                                     \
     } while (0)
 #define MDF_PF32_K(E, S) \
     do { if (count) MDF_PF32(E, S, true); else MDF_PF32(E, S, false); } while (0)
     if (energy) {
-        if (P.use_switch) MDF_PF32_K(true, true); else MDF_PF32_K(true, false);
+        if (sw) MDF_PF32_K(true, true); else MDF_PF32_K(true, false);
     } else {
-        if (P.use_switch) MDF_PF32_K(false, true); else MDF_PF32_K(false, false);
+        if (sw) MDF_PF32_K(false, true); else MDF_PF32_K(false, false);
     }
 #undef MDF_PF32_K
 #undef MDF_PF32
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
+}
+
+void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
+                            bool use_switch, cudaStream_t s)
+{
+    const dim3 g(gx, 1, nsys);
+    if (energy) {
+        if (use_switch) k_pairs_f32_multi<true><<<g, threads, dyn, s>>>(d_args);
+        else k_pairs_f32_multi<false><<<g, threads, dyn, s>>>(d_args);
+    } else {
+        if (use_switch) k_pairs_f32_force_multi<true><<<g, threads, dyn, s>>>(d_args);
+        else k_pairs_f32_force_multi<false><<<g, threads, dyn, s>>>(d_args);
+    }
+    MDF_CUDA_TRY(cudaGetLastError());
 }
 
 void launch_nonbonded(Ctx& c, bool energy)
@@ -693,42 +837,90 @@ void launch_nonbonded(Ctx& c, bool energy)
     bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
     if (c.p.precision == MDF_PREC_MIXED) {
         if (phys) launch_pairs_f32(c, energy);
-        else launch_pairs_t<float, MDF_SEM_REFERENCE>(c, energy, c.xq_f.p, c.ljAB_f.p);
+        else launch_pairs_t<float, MDF_SEM_REFERENCE>(c, energy);
     } else {
-        if (phys) launch_pairs_t<double, MDF_SEM_PHYSICAL>(c, energy, c.xq_d.p, c.ljAB.p);
-        else launch_pairs_t<double, MDF_SEM_REFERENCE>(c, energy, c.xq_d.p, c.ljAB.p);
+        if (phys) launch_pairs_t<double, MDF_SEM_PHYSICAL>(c, energy);
+        else launch_pairs_t<double, MDF_SEM_REFERENCE>(c, energy);
     }
+}
+
+// This rank's excluded pairs and 1-4 pairs.
+ExclArgs make_excl_args(const Ctx& c)
+{
+    ExclArgs A;
+    long long e0, e1;
+    rank_slice(c, c.n_excl, e0, e1);
+    A.n = (int)(e1 - e0);
+    A.gx = grid_blocks(A.n, 256);
+    A.gy = 1;
+    A.pairs = c.excl_pairs.p + 2 * e0;
+    A.is14 = c.excl_is14.p + e0;
+    A.xyz = c.xyz.p;
+    A.q = c.q.p;
+    A.P = make_params(c);
+    A.N = c.N;
+    A.fatom = c.f_atom.p;
+    A.acc = c.acc.p;
+    A.st = c.status.p;
+    return A;
+}
+
+Pair14Args make_pair14_args(const Ctx& c)
+{
+    Pair14Args A;
+    long long p0, p1;
+    rank_slice(c, c.n_14, p0, p1);
+    A.n = (int)(p1 - p0);
+    A.gx = grid_blocks(A.n, 256);
+    A.gy = 1;
+    A.pairs = c.pairs14.p + 2 * p0;
+    A.scale = c.p14_scale.p + p0;
+    A.xyz = c.xyz.p;
+    A.q = c.q.p;
+    A.type = c.type.p;
+    A.lj14 = c.lj14AB.p;
+    A.ljvalid = c.ljvalid.p;
+    A.P = make_params(c);
+    A.N = c.N;
+    A.fatom = c.f_atom.p;
+    A.acc = c.acc.p;
+    A.st = c.status.p;
+    return A;
 }
 
 void launch_exclusions(Ctx& c, bool energy)
 {
-    NBParams P = make_params(c);
     const int th = 256;
-    bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
-    long long e0, e1, p0, p1;   // this rank's exclusions and 1-4 pairs
-    rank_slice(c, c.n_excl, e0, e1);
-    rank_slice(c, c.n_14, p0, p1);
-    if (e1 > e0) {
-        const int ne = (int)(e1 - e0);
-        int nb = grid_blocks(ne, th);
-#define MDF_EXCL(S, E)                                                                                          \
-    k_exclusions<S, E><<<nb, th, 0, c.stream>>>(ne, c.excl_pairs.p + 2 * e0, c.excl_is14.p + e0, c.xyz.p, c.q.p, \
-                                                P, c.N, c.f_atom.p, c.acc.p, c.status.p)
+    const bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
+    const ExclArgs E = make_excl_args(c);
+    if (E.n > 0) {
+#define MDF_EXCL(S, EN) k_exclusions<S, EN><<<grid_of(E), th, 0, c.stream>>>(E)
         if (phys) { if (energy) MDF_EXCL(MDF_SEM_PHYSICAL, true); else MDF_EXCL(MDF_SEM_PHYSICAL, false); }
         else if (energy) MDF_EXCL(MDF_SEM_REFERENCE, true);
 #undef MDF_EXCL
         if (phys || energy) c.launches += 1;
     }
-    if (p1 > p0) {
-        const int n14 = (int)(p1 - p0);
-        int nb = grid_blocks(n14, th);
-#define MDF_P14(S, E)                                                                                             \
-    k_pairs14<S, E><<<nb, th, 0, c.stream>>>(n14, c.pairs14.p + 2 * p0, c.p14_scale.p + p0, c.xyz.p, c.q.p, c.type.p, \
-                                             c.lj14AB.p, c.ljvalid.p, P, c.N, c.f_atom.p, c.acc.p, c.status.p)
+    const Pair14Args P14 = make_pair14_args(c);
+    if (P14.n > 0) {
+#define MDF_P14(S, EN) k_pairs14<S, EN><<<grid_of(P14), th, 0, c.stream>>>(P14)
         if (phys) { if (energy) MDF_P14(MDF_SEM_PHYSICAL, true); else MDF_P14(MDF_SEM_PHYSICAL, false); }
         else { if (energy) MDF_P14(MDF_SEM_REFERENCE, true); else MDF_P14(MDF_SEM_REFERENCE, false); }
 #undef MDF_P14
         c.launches += 1;
+    }
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_exclusions_multi(const ExclArgs* d_excl, int gx_excl, const Pair14Args* d_14, int gx_14, int nsys,
+                             bool energy, cudaStream_t s)
+{
+    if (gx_excl > 0) {
+        if (energy) k_exclusions_multi<MDF_SEM_PHYSICAL, true><<<dim3(gx_excl, 1, nsys), 256, 0, s>>>(d_excl);
+        else k_exclusions_multi<MDF_SEM_PHYSICAL, false><<<dim3(gx_excl, 1, nsys), 256, 0, s>>>(d_excl);
+    }
+    if (gx_14 > 0) {
+        if (energy) k_pairs14_multi<MDF_SEM_PHYSICAL, true><<<dim3(gx_14, 1, nsys), 256, 0, s>>>(d_14);
+        else k_pairs14_multi<MDF_SEM_PHYSICAL, false><<<dim3(gx_14, 1, nsys), 256, 0, s>>>(d_14);
     }
     MDF_CUDA_TRY(cudaGetLastError());
 }

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "kargs.cuh"
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
 
@@ -23,37 +24,51 @@ int grid_blocks(long long n, int threads)
 }
 
 // ------------------------------------------------------------------ scan
-// Single-block exclusive scan; n up to a few million.
-__global__ void k_scan_1block(const int* __restrict__ in, int* __restrict__ out, int n, int* total)
-{
-    __shared__ int part[1024];
-    int tid = threadIdx.x;
-    int per = (n + blockDim.x - 1) / blockDim.x;
-    int b0 = tid * per, b1 = min(n, b0 + per);
-    int s = 0;
-    for (int i = b0; i < b1; ++i) s += in[i];
-    part[tid] = s;
-    __syncthreads();
-    // Hillis-Steele inclusive scan over the block partials
-    for (int o = 1; o < blockDim.x; o <<= 1) {
-        int v = tid >= o ? part[tid - o] : 0;
-        __syncthreads();
-        part[tid] += v;
-        __syncthreads();
-    }
-    int run = tid ? part[tid - 1] : 0;
-    for (int i = b0; i < b1; ++i) {
-        int v = in[i];
-        out[i] = run;
-        run += v;
-    }
-    if (tid == blockDim.x - 1 && total) *total = part[tid];
-}
+// Column table in one block: exclusive scans of the atom counts (col_start)
+// and of the cluster counts (col_cstart, ceil(count / 8) per column), and the
+// cluster total at col_cstart[ncols].  A column above COL_MAX atoms (the
+// in-block sort's limit) sets ST_CAPACITY_COLUMN.  ncols is at most a few
+// thousand, so each thread takes a contiguous chunk.
+constexpr int COL_MAX = 2048;   // atoms per column handled by the in-block sort
 
-void exclusive_scan_int(const int* d_in, int* d_out, int n, int* d_total_out, cudaStream_t s)
+__global__ void __launch_bounds__(1024) k_column_table(int ncols, const int* __restrict__ cnt,
+                                                       int* __restrict__ col_start, int* __restrict__ col_cstart,
+                                                       unsigned* st)
 {
-    k_scan_1block<<<1, 1024, 0, s>>>(d_in, d_out, n, d_total_out);
-    MDF_CUDA_TRY(cudaGetLastError());
+    __shared__ int part_a[1024], part_c[1024];
+    const int tid = threadIdx.x, per = (ncols + blockDim.x - 1) / blockDim.x;
+    const int b0 = min(ncols, tid * per), b1 = min(ncols, b0 + per);
+    int sa = 0, sc = 0;
+    bool over = false;
+    for (int i = b0; i < b1; ++i) {
+        const int n = cnt[i];
+        sa += n;
+        sc += (n + CLUSTER - 1) / CLUSTER;
+        over = over || n > COL_MAX;
+    }
+    if (over) status_set(st, ST_CAPACITY_COLUMN);
+    part_a[tid] = sa;
+    part_c[tid] = sc;
+    __syncthreads();
+    for (int o = 1; o < blockDim.x; o <<= 1) {   // Hillis-Steele inclusive scan of the partials
+        const int va = tid >= o ? part_a[tid - o] : 0, vc = tid >= o ? part_c[tid - o] : 0;
+        __syncthreads();
+        part_a[tid] += va;
+        part_c[tid] += vc;
+        __syncthreads();
+    }
+    int ra = tid ? part_a[tid - 1] : 0, rc = tid ? part_c[tid - 1] : 0;
+    for (int i = b0; i < b1; ++i) {
+        const int n = cnt[i];
+        col_start[i] = ra;
+        col_cstart[i] = rc;
+        ra += n;
+        rc += (n + CLUSTER - 1) / CLUSTER;
+    }
+    if (tid == blockDim.x - 1) {
+        col_start[ncols] = part_a[tid];
+        col_cstart[ncols] = part_c[tid];
+    }
 }
 
 // ------------------------------------------------------------- binning
@@ -77,12 +92,6 @@ __global__ void k_assign_columns(int N, const double* __restrict__ xyz, double L
     atomicAdd(&col_count[col], 1);
 }
 
-__global__ void k_clusters_per_column(int ncols, const int* __restrict__ cnt, int* __restrict__ ncl)
-{
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < ncols) ncl[c] = (cnt[c] + CLUSTER - 1) / CLUSTER;
-}
-
 __global__ void k_bucket(int N, const int* __restrict__ atom_col, const int* __restrict__ col_start,
                          int* __restrict__ col_fill, int* __restrict__ col_atoms)
 {
@@ -92,8 +101,6 @@ __global__ void k_bucket(int N, const int* __restrict__ atom_col, const int* __r
     int pos = col_start[col] + atomicAdd(&col_fill[col], 1);
     col_atoms[pos] = i;
 }
-
-constexpr int COL_MAX = 2048;   // atoms per column handled by the in-block sort
 
 // One block (1024 threads) per column: bitonic sort of (z, atom) keys, then
 // cut into clusters of 8.
@@ -108,11 +115,20 @@ __global__ void __launch_bounds__(1024) k_sort_columns(const double* __restrict_
     __shared__ unsigned long long key[COL_MAX];
     int col = blockIdx.x, tid = threadIdx.x;
     int n = col_count[col];
+    int s0 = col_start[col];
     if (n > COL_MAX) {
+        // The build restarts with thinner columns; until then this column's
+        // clusters are left empty and its atoms point at slot 0, so the
+        // kernels queued after this one only touch valid memory.
         if (tid == 0) status_set(st, ST_CAPACITY_COLUMN);
+        const int c0 = col_cstart[col], ncl = (n + CLUSTER - 1) / CLUSTER;
+        for (int k = tid; k < ncl * CLUSTER; k += blockDim.x) {
+            slot_atom[c0 * CLUSTER + k] = -1;
+            if ((k % CLUSTER) == 0) cluster_col[c0 + k / CLUSTER] = col;
+        }
+        for (int k = tid; k < n; k += blockDim.x) atom_slot[col_atoms[s0 + k]] = 0;
         return;
     }
-    int s0 = col_start[col];
     // pad to the next power of two >= n (at least 2)
     int m = 2;
     while (m < n) m <<= 1;
@@ -161,12 +177,15 @@ __global__ void __launch_bounds__(1024) k_sort_columns(const double* __restrict_
 
 // Cluster bounding boxes (wrapped coordinates) and centres; center.w = number
 // of real atoms in the cluster.
-__global__ void k_cluster_geom(int ncl, const double* __restrict__ xyz, double Lx, double Ly, double Lz,
-                               double quantum, const int* __restrict__ slot_atom, double4* __restrict__ center,
-                               float4* __restrict__ centerf, float4* __restrict__ bb_lo, float4* __restrict__ bb_hi)
+// Launched over the cluster capacity; the clusters the column table made
+// (*d_ncl) are the ones with work.
+__global__ void k_cluster_geom(const int* __restrict__ d_ncl, const double* __restrict__ xyz, double Lx, double Ly,
+                               double Lz, double quantum, const int* __restrict__ slot_atom,
+                               double4* __restrict__ center, float4* __restrict__ centerf, float4* __restrict__ bb_lo,
+                               float4* __restrict__ bb_hi)
 {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncl) return;
+    if (c >= *d_ncl) return;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     int nv = 0;
     for (int k = 0; k < CLUSTER; ++k) {
@@ -198,11 +217,18 @@ __global__ void k_cluster_geom(int ncl, const double* __restrict__ xyz, double L
 // Also the cluster's current bounding box in its own frame (FP32, rounded
 // outward) for the prune's box test.  blockDim.x must be a multiple of 32.
 template <typename R>
-__global__ void k_pack(int nslots, const double* __restrict__ xyz, const double* __restrict__ q,
-                       const int* __restrict__ slot_atom, const double4* __restrict__ center, double Lx, double Ly,
-                       double Lz, typename V4<R>::type* __restrict__ xq, float4* __restrict__ cur_lo,
-                       float4* __restrict__ cur_hi, unsigned* st)
+__device__ __forceinline__ void pack_dev(const PackArgs<R>& A)
 {
+    const int nslots = A.nslots;
+    const double* __restrict__ xyz = A.xyz;
+    const double* __restrict__ q = A.q;
+    const int* __restrict__ slot_atom = A.slot_atom;
+    const double4* __restrict__ center = A.center;
+    const double Lx = A.L[0], Ly = A.L[1], Lz = A.L[2];
+    typename V4<R>::type* __restrict__ xq = A.xq;
+    float4* __restrict__ cur_lo = A.cur_lo;
+    float4* __restrict__ cur_hi = A.cur_hi;
+    unsigned* st = A.st;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     const bool inside = s < nslots;
     const int a = inside ? slot_atom[s] : -1;
@@ -239,11 +265,25 @@ __global__ void k_pack(int nslots, const double* __restrict__ xyz, const double*
     }
 }
 
-__global__ void k_slot_type(int nslots, const int* __restrict__ slot_atom, const int* __restrict__ type, int pad_type,
-                            int* __restrict__ slot_type)
+template <typename R>
+__global__ void k_pack(PackArgs<R> A)
+{
+    pack_dev(A);
+}
+
+template <typename R>
+__global__ void k_pack_multi(const PackArgs<R>* __restrict__ As)
+{
+    const PackArgs<R>& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pack_dev(A);
+}
+
+__global__ void k_slot_type(const int* __restrict__ d_ncl, const int* __restrict__ slot_atom,
+                            const int* __restrict__ type, int pad_type, int* __restrict__ slot_type)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= nslots) return;
+    if (s >= *d_ncl * CLUSTER) return;
     int a = slot_atom[s];
     slot_type[s] = a < 0 ? pad_type : type[a];
 }
@@ -270,130 +310,137 @@ __device__ __forceinline__ unsigned long long entry_mask(int nvi, int nvj, bool 
     return m;
 }
 
-// One warp per i cluster.  FILL=false: count entries into icount[i];
-// FILL=true: write them at ilist[i].start (deterministic lane-major order).
-template <bool FILL>
-__global__ void __launch_bounds__(256) k_pair_search(int ncl, SearchGeom g, const int* __restrict__ cluster_col,
+// One warp per i cluster (launched over the cluster capacity; clusters at or
+// above *d_ncl return).  Two sweeps over the same candidates: the first counts
+// this lane's entries, then lane 0 claims the cluster's range of the list with
+// one atomicAdd on *d_total and the second sweep writes the entries there
+// after the lane-exclusive prefix.  The order inside an i cluster's range is
+// fixed (lane-major over the column/image candidates), so every evaluation
+// sums the same terms in the same order; only the ranges' positions in the
+// list depend on the order the warps ran in.  Entries past `cap` are counted
+// but not written (ST_CAPACITY_PAIRS: the host grows the list and searches
+// again).
+__global__ void __launch_bounds__(256) k_pair_search(const int* __restrict__ d_ncl, SearchGeom g,
+                                                     const int* __restrict__ cluster_col,
                                                      const int* __restrict__ col_cstart,
                                                      const float4* __restrict__ bb_lo, const float4* __restrict__ bb_hi,
-                                                     const double4* __restrict__ center, int* __restrict__ icount,
-                                                     const int* __restrict__ istart, PairEntry* __restrict__ out,
-                                                     long long cap, ILRange* __restrict__ ilist, unsigned* st)
+                                                     const double4* __restrict__ center, int* __restrict__ d_total,
+                                                     PairEntry* __restrict__ out, long long cap,
+                                                     ILRange* __restrict__ ilist, unsigned* st)
 {
-    int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    if (I >= ncl) return;
-    int col = cluster_col[I];
-    int cx = col % g.ncx, cy = col / g.ncx;
-    float4 lo = bb_lo[I], hi = bb_hi[I];
-    int nvi = (int)center[I].w;
-    int nxc = 2 * g.Rx + 1, nyc = 2 * g.Ry + 1;
-    int ncombo = nxc * nyc * 3;
-    float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (I >= *d_ncl) return;
+    const int col = cluster_col[I];
+    const int cx = col % g.ncx, cy = col / g.ncx;
+    const float4 lo = bb_lo[I], hi = bb_hi[I];
+    const int nvi = (int)center[I].w;
+    const int nxc = 2 * g.Rx + 1, nyc = 2 * g.Ry + 1;
+    const int ncombo = nxc * nyc * 3;
+    const float Lx = (float)g.L[0], Ly = (float)g.L[1], Lz = (float)g.L[2];
     int cnt = 0;
     long long base = 0;
-    // FILL runs two sweeps: count this lane's entries, then write them after
-    // the lane-exclusive prefix
-    for (int sweep = FILL ? 0 : 1; sweep < 2; ++sweep) {
-        if (FILL && sweep == 1) {
-            // lane-exclusive prefix
+    for (int sweep = 0; sweep < 2; ++sweep) {
+        if (sweep == 1) {
             int incl = cnt;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                int v = __shfl_up_sync(0xffffffffu, incl, o);
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += v;
             }
-            base = (long long)istart[I] + (incl - cnt);
-            if (lane == 31) {
+            const int tot = __shfl_sync(0xffffffffu, incl, 31);
+            int start = 0;
+            if (lane == 0) start = atomicAdd(d_total, tot);
+            start = __shfl_sync(0xffffffffu, start, 0);
+            if (lane == 0) {
                 ILRange r;
                 r.i = I;
-                r.start = istart[I];
-                r.count = incl;
+                r.start = start;
+                r.count = tot;
                 r.pad = 0;
                 ilist[I] = r;
+                if ((long long)start + tot > cap) status_set(st, ST_CAPACITY_PAIRS);
             }
+            base = (long long)start + (incl - cnt);
             cnt = 0;
         }
         for (int combo = lane; combo < ncombo; combo += 32) {
-            int szi = combo % 3;
-            int rest = combo / 3;
-            int dcx = rest % nxc - g.Rx;
-            int dcy = rest / nxc - g.Ry;
+            const int szi = combo % 3;
+            const int rest = combo / 3;
+            const int dcx = rest % nxc - g.Rx;
+            const int dcy = rest / nxc - g.Ry;
             int jx = cx + dcx, jy = cy + dcy;
-            int sx = jx < 0 ? -1 : (jx >= g.ncx ? 1 : 0);
-            int sy = jy < 0 ? -1 : (jy >= g.ncy ? 1 : 0);
+            const int sx = jx < 0 ? -1 : (jx >= g.ncx ? 1 : 0);
+            const int sy = jy < 0 ? -1 : (jy >= g.ncy ? 1 : 0);
             jx -= sx * g.ncx;
             jy -= sy * g.ncy;
-            int sz = szi - 1;
-            float cxl = (float)(jx * g.colw[0] + sx * g.L[0]), cxh = (float)((jx + 1) * g.colw[0] + sx * g.L[0]);
-            float cyl = (float)(jy * g.colw[1] + sy * g.L[1]), cyh = (float)((jy + 1) * g.colw[1] + sy * g.L[1]);
-            float gx = fmaxf(0.f, fmaxf(cxl - hi.x, lo.x - cxh));
-            float gy = fmaxf(0.f, fmaxf(cyl - hi.y, lo.y - cyh));
+            const int sz = szi - 1;
+            const float cxl = (float)(jx * g.colw[0] + sx * g.L[0]), cxh = (float)((jx + 1) * g.colw[0] + sx * g.L[0]);
+            const float cyl = (float)(jy * g.colw[1] + sy * g.L[1]), cyh = (float)((jy + 1) * g.colw[1] + sy * g.L[1]);
+            const float gx = fmaxf(0.f, fmaxf(cxl - hi.x, lo.x - cxh));
+            const float gy = fmaxf(0.f, fmaxf(cyl - hi.y, lo.y - cyh));
             if (gx * gx + gy * gy > g.rlist2) continue;
-            float zmin = lo.z - g.rlist - sz * Lz, zmax = hi.z + g.rlist - sz * Lz;
+            const float zmin = lo.z - g.rlist - sz * Lz, zmax = hi.z + g.rlist - sz * Lz;
             if (zmax < -1.0f || zmin > Lz + 1.0f) continue;
-            int jcol = jx + g.ncx * jy;
-            int c0 = col_cstart[jcol], c1 = col_cstart[jcol + 1];
+            const int jcol = jx + g.ncx * jy;
+            const int c0 = col_cstart[jcol], c1 = col_cstart[jcol + 1];
             // first cluster whose hi.z >= zmin
             int a = c0, b = c1;
             while (a < b) {
-                int mid = (a + b) >> 1;
+                const int mid = (a + b) >> 1;
                 if (bb_hi[mid].z < zmin) a = mid + 1;
                 else b = mid;
             }
             for (int J = a; J < c1; ++J) {
-                float4 jl = bb_lo[J], jh = bb_hi[J];
+                const float4 jl = bb_lo[J], jh = bb_hi[J];
                 if (jl.z > zmax) break;
-                float ox = sx * Lx, oy = sy * Ly, oz = sz * Lz;
-                float dx = fmaxf(0.f, fmaxf(jl.x + ox - hi.x, lo.x - (jh.x + ox)));
-                float dy = fmaxf(0.f, fmaxf(jl.y + oy - hi.y, lo.y - (jh.y + oy)));
-                float dz = fmaxf(0.f, fmaxf(jl.z + oz - hi.z, lo.z - (jh.z + oz)));
+                const float ox = sx * Lx, oy = sy * Ly, oz = sz * Lz;
+                const float dx = fmaxf(0.f, fmaxf(jl.x + ox - hi.x, lo.x - (jh.x + ox)));
+                const float dy = fmaxf(0.f, fmaxf(jl.y + oy - hi.y, lo.y - (jh.y + oy)));
+                const float dz = fmaxf(0.f, fmaxf(jl.z + oz - hi.z, lo.z - (jh.z + oz)));
                 if (dx * dx + dy * dy + dz * dz > g.rlist2) continue;
-                int code = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+                const int code = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
                 if (J < I || (J == I && code < 13)) continue;
-                if (FILL && sweep == 1) {
-                    long long pos = base + cnt;
+                if (sweep == 1) {
+                    const long long pos = base + cnt;
                     if (pos < cap) {
                         PairEntry e;
                         e.j = J;
                         e.shift = code;
                         e.mask = entry_mask(nvi, (int)center[J].w, J == I && code == 13);
                         out[pos] = e;
-                    } else {
-                        status_set(st, ST_CAPACITY_PAIRS);
                     }
                 }
                 ++cnt;
             }
         }
     }
-    if (!FILL) {
-        int tot = cnt;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-        if (lane == 0) icount[I] = tot;
-    }
 }
 
-// Clear the mask bit of every excluded pair in the entry that holds it.
+// Clear the mask bit of every excluded pair in the entry that holds it.  One
+// warp per excluded pair: the warp locates the (I, J, image) entry in I's
+// range 32 entries at a time (coalesced 16-byte loads) and one lane clears
+// the bit.
 __global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const int* __restrict__ atom_slot,
                                   const double* __restrict__ xyz, const double4* __restrict__ center, double Lx,
                                   double Ly, double Lz, const ILRange* __restrict__ ilist,
-                                  PairEntry* __restrict__ plist)
+                                  PairEntry* __restrict__ plist, long long cap)
 {
-    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (k >= nexcl) return;
-    int a = excl[2 * k], b = excl[2 * k + 1];
-    int sa = atom_slot[a], sb = atom_slot[b];
-    int Ia = sa / CLUSTER, la = sa % CLUSTER, Ib = sb / CLUSTER, lb = sb % CLUSTER;
-    double4 ca = center[Ia], cb = center[Ib];
+    const int a = excl[2 * k], b = excl[2 * k + 1];
+    const int sa = atom_slot[a], sb = atom_slot[b];
+    const int Ia = sa / CLUSTER, la = sa % CLUSTER, Ib = sb / CLUSTER, lb = sb % CLUSTER;
+    const double4 ca = center[Ia], cb = center[Ib];
     // list-geometry positions: centre + min-image offset
-    double pa[3] = {ca.x + min_image(xyz[3 * a] - ca.x, Lx), ca.y + min_image(xyz[3 * a + 1] - ca.y, Ly),
-                    ca.z + min_image(xyz[3 * a + 2] - ca.z, Lz)};
-    double pb[3] = {cb.x + min_image(xyz[3 * b] - cb.x, Lx), cb.y + min_image(xyz[3 * b + 1] - cb.y, Ly),
-                    cb.z + min_image(xyz[3 * b + 2] - cb.z, Lz)};
+    const double pa[3] = {ca.x + min_image(xyz[3 * a] - ca.x, Lx), ca.y + min_image(xyz[3 * a + 1] - ca.y, Ly),
+                          ca.z + min_image(xyz[3 * a + 2] - ca.z, Lz)};
+    const double pb[3] = {cb.x + min_image(xyz[3 * b] - cb.x, Lx), cb.y + min_image(xyz[3 * b + 1] - cb.y, Ly),
+                          cb.z + min_image(xyz[3 * b + 2] - cb.z, Lz)};
     // J atoms sit at p + s L in I's frame: s = round((p_I - p_J) / L)
-    int s[3] = {(int)round((pa[0] - pb[0]) / Lx), (int)round((pa[1] - pb[1]) / Ly), (int)round((pa[2] - pb[2]) / Lz)};
+    const int s[3] = {(int)round((pa[0] - pb[0]) / Lx), (int)round((pa[1] - pb[1]) / Ly),
+                      (int)round((pa[2] - pb[2]) / Lz)};
     if (s[0] < -1 || s[0] > 1 || s[1] < -1 || s[1] > 1 || s[2] < -1 || s[2] > 1) return;  // never listed
     int I, J, bit;
     int code = (s[0] + 1) + 3 * (s[1] + 1) + 9 * (s[2] + 1);
@@ -407,11 +454,15 @@ __global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const
         else if (code > 13) bit = la * 8 + lb;
         else { bit = lb * 8 + la; code = 26 - code; }
     }
-    ILRange r = ilist[I];
-    for (int e = r.start; e < r.start + r.count; ++e) {
-        if (plist[e].j == J && plist[e].shift == code) {
-            atomicAnd(&plist[e].mask, ~(1ull << bit));
-            break;
+    const ILRange r = ilist[I];
+    const long long end = min((long long)r.start + r.count, cap);
+    for (long long e0 = r.start; e0 < end; e0 += 32) {
+        const long long e = e0 + lane;
+        const bool hit = e < end && plist[e].j == J && plist[e].shift == code;
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (m) {
+            if (lane == __ffs(m) - 1) atomicAnd(&plist[e].mask, ~(1ull << bit));
+            return;
         }
     }
 }
@@ -425,10 +476,6 @@ __global__ void k_exclusion_masks(int nexcl, const int* __restrict__ excl, const
 // at the first unmasked pair inside rcut.  Kept entries are compacted, in
 // list order, into the same offsets of the pruned list.  Image offsets use the
 // exact-FP32 centres plus the hi/lo shift table.
-struct PruneShifts {
-    float v[27][6];
-};
-
 // Dynamic pruning: keep the outer-list entries that have at least one atom
 // pair within the prune radius at the current positions.  Warp per i cluster.
 // The warp loads 32 entries at once (one per lane), drops those whose current
@@ -443,12 +490,20 @@ struct PruneShifts {
 // Kept entries are written in order, packed from the i cluster's start offset
 // in the outer list.
 template <typename R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
-    int ncl, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist,
-    const typename V4<R>::type* __restrict__ xq, const float4* __restrict__ centerf,
-    const float4* __restrict__ cur_lo, const float4* __restrict__ cur_hi, PruneShifts shifts, float rcut2,
-    ILRange* __restrict__ ilist_in, PairEntry* __restrict__ plist_in, unsigned long long* __restrict__ n_in)
+__device__ __forceinline__ void prune_dev(const PruneArgs<R>& A)
 {
+    const int ncl = A.ncl;
+    const ILRange* __restrict__ ilist = A.ilist;
+    const PairEntry* __restrict__ plist = A.plist;
+    const typename V4<R>::type* __restrict__ xq = A.xq;
+    const float4* __restrict__ centerf = A.centerf;
+    const float4* __restrict__ cur_lo = A.cur_lo;
+    const float4* __restrict__ cur_hi = A.cur_hi;
+    const PruneShifts& shifts = A.shifts;
+    const float rcut2 = A.rcut2;
+    ILRange* __restrict__ ilist_in = A.ilist_in;
+    PairEntry* __restrict__ plist_in = A.plist_in;
+    unsigned long long* __restrict__ n_in = A.n_in;
     using V4t = typename V4<R>::type;
     __shared__ float sh[27][6];
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
@@ -557,35 +612,74 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(
     }
 }
 
-void prune_pairlist(Ctx& c)
+template <typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(PruneArgs<R> A)
 {
-    const int th = 256;
+    prune_dev(A);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune_multi(const PruneArgs<R>* __restrict__ As)
+{
+    const PruneArgs<R>& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    prune_dev(A);
+}
+
+// Prune arguments for this rank's i clusters (ncl = 0: nothing to do).
+template <typename R>
+PruneArgs<R> make_prune_args(const Ctx& c)
+{
+    PruneArgs<R> A;
     // a hair above the cutoff so working-precision rounding never drops a pair at r ~ rc
-    double rc = c.p.cutoff + std::max(0.0, c.p.prune_margin) + 0.02;
-    PruneShifts sh;
+    const double rc = c.p.cutoff + std::max(0.0, c.p.prune_margin) + 0.02;
     for (int code = 0; code < 27; ++code) {
         int sv[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
         for (int d = 0; d < 3; ++d) {
             double v = sv[d] * c.box[d];
             float hi = (float)v;
-            sh.v[code][d] = hi;
-            sh.v[code][3 + d] = (float)(v - (double)hi);
+            A.shifts.v[code][d] = hi;
+            A.shifts.v[code][3 + d] = (float)(v - (double)hi);
         }
     }
-    MDF_CUDA_TRY(cudaMemsetAsync(c.n_in.p, 0, sizeof(unsigned long long), c.stream));
     long long lo, hi;
     rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
-    const int ncl = (int)(hi - lo);
-    int blocks = grid_blocks((long long)ncl * 32, th);
-    if (ncl > 0) {
-        if (c.p.precision == MDF_PREC_MIXED)
-            k_prune<float><<<blocks, th, 0, c.stream>>>(ncl, c.ilist.p + lo, c.plist.p, c.xq_f.p, c.centerf.p,
-                                                       c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc),
-                                                       c.ilist_in.p + lo, c.plist_in.p, c.n_in.p);
-        else
-            k_prune<double><<<blocks, th, 0, c.stream>>>(ncl, c.ilist.p + lo, c.plist.p, c.xq_d.p, c.centerf.p,
-                                                        c.cur_lo.p, c.cur_hi.p, sh, (float)(rc * rc),
-                                                        c.ilist_in.p + lo, c.plist_in.p, c.n_in.p);
+    A.ncl = (int)(hi - lo);
+    A.gx = grid_blocks((long long)A.ncl * 32, 256);
+    A.gy = 1;
+    A.ilist = c.ilist.p + lo;
+    A.plist = c.plist.p;
+    A.xq = reinterpret_cast<const typename V4<R>::type*>(sizeof(R) == 4 ? (const void*)c.xq_f.p : (const void*)c.xq_d.p);
+    A.centerf = c.centerf.p;
+    A.cur_lo = c.cur_lo.p;
+    A.cur_hi = c.cur_hi.p;
+    A.rcut2 = (float)(rc * rc);
+    A.ilist_in = c.ilist_in.p + lo;
+    A.plist_in = c.plist_in.p;
+    A.n_in = c.n_in.p;
+    return A;
+}
+template PruneArgs<float> make_prune_args<float>(const Ctx&);
+template PruneArgs<double> make_prune_args<double>(const Ctx&);
+
+template <typename R>
+void launch_prune_multi(const PruneArgs<R>* d_args, int nsys, int gx, cudaStream_t s)
+{
+    k_prune_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+template void launch_prune_multi<float>(const PruneArgs<float>*, int, int, cudaStream_t);
+template void launch_prune_multi<double>(const PruneArgs<double>*, int, int, cudaStream_t);
+
+void prune_pairlist(Ctx& c)
+{
+    MDF_CUDA_TRY(cudaMemsetAsync(c.n_in.p, 0, sizeof(unsigned long long), c.stream));
+    if (c.p.precision == MDF_PREC_MIXED) {
+        const PruneArgs<float> A = make_prune_args<float>(c);
+        if (A.ncl > 0) k_prune<float><<<grid_of(A), 256, 0, c.stream>>>(A);
+    } else {
+        const PruneArgs<double> A = make_prune_args<double>(c);
+        if (A.ncl > 0) k_prune<double><<<grid_of(A), 256, 0, c.stream>>>(A);
     }
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
@@ -598,23 +692,57 @@ static double atom_density(const Ctx& c)
     return (double)c.N / (c.box[0] * c.box[1] * c.box[2]);
 }
 
+template <typename R>
+PackArgs<R> make_pack_args(const Ctx& c)
+{
+    PackArgs<R> A;
+    A.nslots = c.n_slots;
+    A.gx = grid_blocks(c.n_slots, 256);
+    A.gy = 1;
+    A.xyz = c.xyz.p;
+    A.q = c.q.p;
+    A.slot_atom = c.slot_atom.p;
+    A.center = c.center.p;
+    for (int d = 0; d < 3; ++d) A.L[d] = c.box[d];
+    A.xq = reinterpret_cast<typename V4<R>::type*>(sizeof(R) == 4 ? (void*)c.xq_f.p : (void*)c.xq_d.p);
+    A.cur_lo = c.cur_lo.p;
+    A.cur_hi = c.cur_hi.p;
+    A.st = c.status.p;
+    return A;
+}
+template PackArgs<float> make_pack_args<float>(const Ctx&);
+template PackArgs<double> make_pack_args<double>(const Ctx&);
+
+template <typename R>
+void launch_pack_multi(const PackArgs<R>* d_args, int nsys, int gx, cudaStream_t s)
+{
+    k_pack_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+template void launch_pack_multi<float>(const PackArgs<float>*, int, int, cudaStream_t);
+template void launch_pack_multi<double>(const PackArgs<double>*, int, int, cudaStream_t);
+
 void pack_positions(Ctx& c)
 {
-    int th = 256;
     if (c.p.precision == MDF_PREC_MIXED) {
-        k_pack<float><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.xyz.p, c.q.p, c.slot_atom.p,
-                                                                         c.center.p, c.box[0], c.box[1], c.box[2],
-                                                                         c.xq_f.p, c.cur_lo.p, c.cur_hi.p, c.status.p);
+        const PackArgs<float> A = make_pack_args<float>(c);
+        k_pack<float><<<grid_of(A), 256, 0, c.stream>>>(A);
     } else {
-        k_pack<double><<<grid_blocks(c.n_slots, th), th, 0, c.stream>>>(c.n_slots, c.xyz.p, c.q.p, c.slot_atom.p,
-                                                                          c.center.p, c.box[0], c.box[1], c.box[2],
-                                                                          c.xq_d.p, c.cur_lo.p, c.cur_hi.p,
-                                                                          c.status.p);
+        const PackArgs<double> A = make_pack_args<double>(c);
+        k_pack<double><<<grid_of(A), 256, 0, c.stream>>>(A);
     }
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
 }
 
+// The whole build is queued on the context's stream without a host round trip
+// in between: every buffer the build kernels write is sized from bounds known
+// on the host (clusters <= ceil(N/8) + columns; the list from a density
+// estimate or the last build), the kernels read the cluster count from the
+// device, and one synchronisation at the end returns the cluster and entry
+// counts with the status word.  A list that outgrew its capacity is grown and
+// searched again; a column above the sort's limit restarts with thinner
+// columns.
 void build_pairlist(Ctx& c)
 {
     c.npairs_dev.alloc(1);
@@ -622,12 +750,14 @@ void build_pairlist(Ctx& c)
     c.counted = false;
     cudaStream_t s = c.stream;
     const int th = 256;
-    double rlist = c.p.cutoff + c.p.skin;
+    const double rlist = c.p.cutoff + c.p.skin;
     for (int d = 0; d < 3; ++d)
         if (!(c.box[d] >= 2.0 * c.p.cutoff))
             throw ApiError(MDF_ERR_INVALID, "box edge shorter than twice the cutoff (minimum image undefined)");
+    if (!c.h_build) MDF_CUDA_TRY(cudaHostAlloc((void**)&c.h_build, 4 * sizeof(int), cudaHostAllocDefault));
+    c.d_build.alloc(4);
     // column cross-section ~ one cluster of atoms per column-height cube
-    double rho = atom_density(c);
+    const double rho = atom_density(c);
     double side = std::cbrt((double)CLUSTER / std::max(rho, 1e-6));
     for (int attempt = 0; attempt < 6; ++attempt) {
         c.ncol_x = std::max(1, (int)std::floor(c.box[0] / side));
@@ -641,6 +771,9 @@ void build_pairlist(Ctx& c)
         const int Rx = reach(c.box[0], c.ncol_x), Ry = reach(c.box[1], c.ncol_y);
         if (Rx >= c.ncol_x || Ry >= c.ncol_y) throw ApiError(MDF_ERR_INVALID, "box too small for the list cutoff");
         c.ncols = c.ncol_x * c.ncol_y;
+        // every column wastes at most one partly filled cluster
+        const long long ncl_cap = ((long long)c.N + CLUSTER - 1) / CLUSTER + c.ncols;
+        if (ncl_cap * CLUSTER > INT32_MAX / 3) throw ApiError(MDF_ERR_CAPACITY, "too many atoms for one context");
         c.col_count.alloc(c.ncols + 1);
         c.col_start.alloc(c.ncols + 1);
         c.col_cstart.alloc(c.ncols + 1);
@@ -648,54 +781,41 @@ void build_pairlist(Ctx& c)
         c.atom_col.alloc(c.N);
         c.col_atoms.alloc(c.N);
         c.atom_slot.alloc(c.N);
+        c.slot_atom.alloc(ncl_cap * CLUSTER);
+        c.slot_type.alloc(ncl_cap * CLUSTER);
+        c.cluster_col.alloc(ncl_cap);
+        c.center.alloc(ncl_cap);
+        c.centerf.alloc(ncl_cap);
+        c.bb_lo.alloc(ncl_cap);
+        c.bb_hi.alloc(ncl_cap);
+        c.ilist.alloc(ncl_cap);
+        if (!c.plist.p) {
+            // list estimate: half the clusters within rlist + one cluster extent, 30% over
+            const double ext = rlist + side;
+            const double per = 0.5 * (rho / CLUSTER) * (4.0 / 3.0) * M_PI * ext * ext * ext * 1.3;
+            c.plist.alloc((size_t)(ncl_cap * std::max(32.0, per)) + 1024);
+        }
+        {
+            // largest power-of-two quantum keeping every centre exact in FP32 (24-bit significand)
+            const double lmax = std::max(c.box[0], std::max(c.box[1], c.box[2]));
+            c.center_quantum = std::ldexp(1.0, (int)std::ceil(std::log2(lmax + 1.0)) - 24);
+        }
+        const int* d_ncl = c.col_cstart.p + c.ncols;   // cluster count, written by k_column_table
         MDF_CUDA_TRY(cudaMemsetAsync(c.col_count.p, 0, sizeof(int) * (c.ncols + 1), s));
+        MDF_CUDA_TRY(cudaMemsetAsync(c.scan_tmp.p, 0, sizeof(int) * (c.ncols + 1), s));
         MDF_CUDA_TRY(cudaMemsetAsync(c.status.p, 0, sizeof(unsigned), s));
         k_assign_columns<<<grid_blocks(c.N, th), th, 0, s>>>(c.N, c.xyz.p, c.box[0], c.box[1], c.ncol_x, c.ncol_y,
                                                              c.atom_col.p, c.col_count.p, c.status.p);
-        exclusive_scan_int(c.col_count.p, c.col_start.p, c.ncols + 1, nullptr, s);
-        k_clusters_per_column<<<grid_blocks(c.ncols + 1, th), th, 0, s>>>(c.ncols + 1, c.col_count.p, c.scan_tmp.p);
-        exclusive_scan_int(c.scan_tmp.p, c.col_cstart.p, c.ncols + 1, nullptr, s);
-        int ncl = 0;
-        MDF_CUDA_TRY(cudaMemcpyAsync(&ncl, c.col_cstart.p + c.ncols, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MDF_CUDA_TRY(cudaMemsetAsync(c.scan_tmp.p, 0, sizeof(int) * (c.ncols + 1), s));
+        k_column_table<<<1, 1024, 0, s>>>(c.ncols, c.col_count.p, c.col_start.p, c.col_cstart.p, c.status.p);
         k_bucket<<<grid_blocks(c.N, th), th, 0, s>>>(c.N, c.atom_col.p, c.col_start.p, c.scan_tmp.p, c.col_atoms.p);
-        MDF_CUDA_TRY(cudaStreamSynchronize(s));
-        c.n_clusters = ncl;
-        c.n_slots = ncl * CLUSTER;
-        c.slot_atom.alloc(c.n_slots);
-        c.cluster_col.alloc(ncl);
         k_sort_columns<<<c.ncols, 1024, 0, s>>>(c.xyz.p, c.box[2], c.col_count.p, c.col_start.p, c.col_cstart.p,
                                                 c.col_atoms.p, c.slot_atom.p, c.atom_slot.p, c.cluster_col.p,
                                                 c.status.p);
-        unsigned st = 0;
-        MDF_CUDA_TRY(cudaMemcpyAsync(&st, c.status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        MDF_CUDA_TRY(cudaStreamSynchronize(s));
-        if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite position");
-        if (st & ST_CAPACITY_COLUMN) {
-            side *= 0.7;   // too many atoms in a column: thinner columns
-            if (attempt == 5) throw ApiError(MDF_ERR_CAPACITY, "column too populated for the in-block sort");
-            continue;
-        }
-        // geometry
-        c.center.alloc(ncl);
-        c.bb_lo.alloc(ncl);
-        c.bb_hi.alloc(ncl);
-        c.cur_lo.alloc(ncl);
-        c.cur_hi.alloc(ncl);
-        c.centerf.alloc(ncl);
-        {
-            // largest power-of-two quantum keeping every centre exact in FP32 (24-bit significand)
-            double lmax = std::max(c.box[0], std::max(c.box[1], c.box[2]));
-            c.center_quantum = std::ldexp(1.0, (int)std::ceil(std::log2(lmax + 1.0)) - 24);
-        }
-        k_cluster_geom<<<grid_blocks(ncl, th), th, 0, s>>>(ncl, c.xyz.p, c.box[0], c.box[1], c.box[2],
-                                                           c.center_quantum, c.slot_atom.p, c.center.p, c.centerf.p,
-                                                           c.bb_lo.p, c.bb_hi.p);
-        c.slot_type.alloc(c.n_slots);
-        k_slot_type<<<grid_blocks(c.n_slots, th), th, 0, s>>>(c.n_slots, c.slot_atom.p, c.type.p, c.ntp - 1,
-                                                              c.slot_type.p);
-        if (c.p.precision == MDF_PREC_MIXED) c.xq_f.alloc(c.n_slots);
-        else c.xq_d.alloc(c.n_slots);
+        k_cluster_geom<<<grid_blocks(ncl_cap, th), th, 0, s>>>(d_ncl, c.xyz.p, c.box[0], c.box[1], c.box[2],
+                                                               c.center_quantum, c.slot_atom.p, c.center.p,
+                                                               c.centerf.p, c.bb_lo.p, c.bb_hi.p);
+        k_slot_type<<<grid_blocks(ncl_cap * CLUSTER, th), th, 0, s>>>(d_ncl, c.slot_atom.p, c.type.p, c.ntp - 1,
+                                                                      c.slot_type.p);
         MDF_CUDA_TRY(cudaGetLastError());
 
         SearchGeom g;
@@ -710,33 +830,47 @@ void build_pairlist(Ctx& c)
         // bounding boxes are rounded outward to float; pad the list radius a hair
         g.rlist = (float)(rlist * (1.0 + 1e-6));
         g.rlist2 = g.rlist * g.rlist;
-        c.icount.alloc(ncl + 1);
-        c.ilist.alloc(ncl);
-        MDF_CUDA_TRY(cudaMemsetAsync(c.icount.p, 0, sizeof(int) * (ncl + 1), s));
-        int wblocks = grid_blocks((long long)ncl * 32, th);
-        k_pair_search<false><<<wblocks, th, 0, s>>>(ncl, g, c.cluster_col.p, c.col_cstart.p, c.bb_lo.p, c.bb_hi.p,
-                                                    c.center.p, c.icount.p, nullptr, nullptr, 0, nullptr, c.status.p);
-        c.scan_tmp.alloc(ncl + 1);
-        exclusive_scan_int(c.icount.p, c.scan_tmp.p, ncl + 1, nullptr, s);
-        int total = 0;
-        MDF_CUDA_TRY(cudaMemcpyAsync(&total, c.scan_tmp.p + ncl, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MDF_CUDA_TRY(cudaStreamSynchronize(s));
-        c.n_entries = total;
-        c.plist.alloc((size_t)total + 1);
-        k_pair_search<true><<<wblocks, th, 0, s>>>(ncl, g, c.cluster_col.p, c.col_cstart.p, c.bb_lo.p, c.bb_hi.p,
-                                                   c.center.p, nullptr, c.scan_tmp.p, c.plist.p, total, c.ilist.p,
-                                                   c.status.p);
-        if (c.n_excl > 0)
-            k_exclusion_masks<<<grid_blocks(c.n_excl, th), th, 0, s>>>(c.n_excl, c.excl_pairs.p, c.atom_slot.p,
-                                                                      c.xyz.p, c.center.p, c.box[0], c.box[1],
-                                                                      c.box[2], c.ilist.p, c.plist.p);
-        MDF_CUDA_TRY(cudaGetLastError());
-        MDF_CUDA_TRY(cudaMemcpyAsync(&st, c.status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        MDF_CUDA_TRY(cudaStreamSynchronize(s));
+        unsigned st = 0;
+        for (int search = 0; search < 3; ++search) {
+            const long long cap = (long long)c.plist.n;
+            MDF_CUDA_TRY(cudaMemsetAsync(c.d_build.p, 0, sizeof(int) * 4, s));
+            k_pair_search<<<grid_blocks(ncl_cap * 32, th), th, 0, s>>>(d_ncl, g, c.cluster_col.p, c.col_cstart.p,
+                                                                       c.bb_lo.p, c.bb_hi.p, c.center.p, c.d_build.p,
+                                                                       c.plist.p, cap, c.ilist.p, c.status.p);
+            if (c.n_excl > 0)
+                k_exclusion_masks<<<grid_blocks((long long)c.n_excl * 32, th), th, 0, s>>>(
+                    c.n_excl, c.excl_pairs.p, c.atom_slot.p, c.xyz.p, c.center.p, c.box[0], c.box[1], c.box[2],
+                    c.ilist.p, c.plist.p, cap);
+            MDF_CUDA_TRY(cudaGetLastError());
+            MDF_CUDA_TRY(cudaMemcpyAsync(c.h_build, d_ncl, sizeof(int), cudaMemcpyDeviceToHost, s));
+            MDF_CUDA_TRY(cudaMemcpyAsync(c.h_build + 1, c.d_build.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+            MDF_CUDA_TRY(cudaMemcpyAsync(c.h_build + 2, c.status.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            MDF_CUDA_TRY(cudaStreamSynchronize(s));
+            st = (unsigned)c.h_build[2];
+            if (st & (ST_NONFINITE | ST_CAPACITY_COLUMN)) break;
+            if (!(st & ST_CAPACITY_PAIRS)) break;
+            // the list outgrew its buffer: grow to the count found (+1/8) and search again
+            c.plist.alloc((size_t)c.h_build[1] + 1);
+            MDF_CUDA_TRY(cudaMemsetAsync(c.status.p, 0, sizeof(unsigned), s));
+        }
+        if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite position");
+        if (st & ST_CAPACITY_COLUMN) {
+            side *= 0.7;   // too many atoms in a column: thinner columns
+            if (attempt == 5) throw ApiError(MDF_ERR_CAPACITY, "column too populated for the in-block sort");
+            continue;
+        }
         if (st & ST_CAPACITY_PAIRS) throw ApiError(MDF_ERR_CAPACITY, "pair list capacity exceeded");
+        const int ncl = c.h_build[0];
+        c.n_clusters = ncl;
+        c.n_slots = ncl * CLUSTER;
+        c.n_entries = c.h_build[1];
+        c.cur_lo.alloc(ncl);
+        c.cur_hi.alloc(ncl);
+        if (c.p.precision == MDF_PREC_MIXED) c.xq_f.alloc(c.n_slots);
+        else c.xq_d.alloc(c.n_slots);
         c.f_slot.alloc((size_t)3 * c.n_slots);
         c.need_clear = true;   // slot layout changed: clear the accumulators before the next evaluation
-        c.plist_in.alloc((size_t)total + 1);
+        c.plist_in.alloc(c.plist.n);
         c.ilist_in.alloc(ncl);
         c.n_in.alloc(1);
         c.pruned_valid = false;

@@ -26,6 +26,7 @@
 #include <cmath>
 #include <vector>
 
+#include "kargs.cuh"
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
 
@@ -37,14 +38,6 @@ template <> struct CT<double> { using type = double2; };
 
 constexpr int FFT_THREADS = 128;
 
-struct FFTDesc {
-    int n;
-    int nst;
-    int radix[12];
-    int ns[12];
-    int toff[12];
-    int ntab;
-};
 
 template <typename C>
 __device__ __forceinline__ C cmul(C a, C b)
@@ -214,11 +207,15 @@ __device__ __forceinline__ void fft_smem_setup(unsigned char* raw, const FFTDesc
 
 // ------------------------------------------------------------- z passes
 template <typename R>
-__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const unsigned long long* __restrict__ qgrid,
-                                                           typename CT<R>::type* __restrict__ cgrid, int nlines,
-                                                           FFTDesc dz, const typename CT<R>::type* __restrict__ twz,
-                                                           const int2* __restrict__ tabz, int LP)
+__device__ __forceinline__ void fft_z_r2c_dev(const FFTZArgs<R>& A)
 {
+    const unsigned long long* __restrict__ qgrid = A.qgrid;
+    typename CT<R>::type* __restrict__ cgrid = A.cgrid;
+    const int nlines = A.nlines;
+    const FFTDesc& dz = A.d;
+    const typename CT<R>::type* __restrict__ twz = A.tw;
+    const int2* __restrict__ tabz = A.tab;
+    const int LP = A.LP;
     using C = typename CT<R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw, *bufA, *bufB;
@@ -245,11 +242,15 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_r2c(const unsigned long l
 }
 
 template <typename R>
-__global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const typename CT<R>::type* __restrict__ cgrid,
-                                                           R* __restrict__ rgrid, int nlines, FFTDesc dz,
-                                                           const typename CT<R>::type* __restrict__ twz,
-                                                           const int2* __restrict__ tabz, int LP)
+__device__ __forceinline__ void fft_z_c2r_dev(const FFTZArgs<R>& A)
 {
+    const typename CT<R>::type* __restrict__ cgrid = A.cgrid;
+    R* __restrict__ rgrid = A.rgrid;
+    const int nlines = A.nlines;
+    const FFTDesc& dz = A.d;
+    const typename CT<R>::type* __restrict__ twz = A.tw;
+    const int2* __restrict__ tabz = A.tab;
+    const int LP = A.LP;
     using C = typename CT<R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw, *bufA, *bufB;
@@ -281,11 +282,15 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_z_c2r(const typename CT<R>:
 
 // ------------------------------------------------------------- y pass
 template <typename R>
-__global__ void __launch_bounds__(FFT_THREADS) k_fft_y(typename CT<R>::type* __restrict__ cgrid, int Kc, FFTDesc dy,
-                                                       const typename CT<R>::type* __restrict__ twy,
-                                                       const int2* __restrict__ taby, int LP, int lp_shift,
-                                                       bool inverse)
+__device__ __forceinline__ void fft_y_dev(const FFTYArgs<R>& A)
 {
+    typename CT<R>::type* __restrict__ cgrid = A.cgrid;
+    const int Kc = A.Kc;
+    const FFTDesc& dy = A.d;
+    const typename CT<R>::type* __restrict__ twy = A.tw;
+    const int2* __restrict__ taby = A.tab;
+    const int LP = A.LP, lp_shift = A.lp_shift;
+    const bool inverse = A.inverse != 0;
     using C = typename CT<R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw, *bufA, *bufB;
@@ -311,19 +316,23 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_y(typename CT<R>::type* __r
 }
 
 // ------------------------------------------- x pass + convolution + inverse
-struct ConvParams {
-    int K[3];
-    double pa2;       // pi^2 / alpha^2 (virial factor)
-    int reference;    // REFERENCE solve: no energy or virial
-};
 
 template <typename R, bool ENERGY>
-__global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv(
-    typename CT<R>::type* __restrict__ cgrid, int K1, int Kc, FFTDesc dx, const typename CT<R>::type* __restrict__ twx,
-    const int2* __restrict__ tabx, int LP, int lp_shift, ConvParams cp, const R* __restrict__ infl,
-    const double* __restrict__ mx, const double* __restrict__ my, const double* __restrict__ mz,
-    unsigned long long* __restrict__ acc, unsigned* st)
+__device__ __forceinline__ void fft_x_conv_dev(const FFTXArgs<R>& A)
 {
+    typename CT<R>::type* __restrict__ cgrid = A.cgrid;
+    const int K1 = A.K1, Kc = A.Kc;
+    const FFTDesc& dx = A.d;
+    const typename CT<R>::type* __restrict__ twx = A.tw;
+    const int2* __restrict__ tabx = A.tab;
+    const int LP = A.LP, lp_shift = A.lp_shift;
+    const ConvParams& cp = A.cp;
+    const R* __restrict__ infl = A.infl;
+    const double* __restrict__ mx = A.mx;
+    const double* __restrict__ my = A.my;
+    const double* __restrict__ mz = A.mz;
+    unsigned long long* __restrict__ acc = A.acc;
+    unsigned* st = A.st;
     using C = typename CT<R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *tw, *bufA, *bufB;
@@ -383,6 +392,40 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv(
     }
 }
 
+// One-system kernels (arguments by value) and their many-system forms
+// (blockIdx.z = system; blocks past the system's own grid return).
+#define MDF_FFT_KERNELS(NAME, DEV, ARGS, ...)                                                                   \
+    template <__VA_ARGS__>                                                                                    \
+    __global__ void __launch_bounds__(FFT_THREADS) NAME(ARGS A)                                               \
+    {                                                                                                         \
+        DEV(A);                                                                                               \
+    }                                                                                                         \
+    template <__VA_ARGS__>                                                                                    \
+    __global__ void __launch_bounds__(FFT_THREADS) NAME##_multi(const ARGS* __restrict__ As)                  \
+    {                                                                                                         \
+        const ARGS& A = As[blockIdx.z];                                                                       \
+        if ((int)blockIdx.x >= A.gx || (int)blockIdx.y >= A.gy) return;                                       \
+        DEV(A);                                                                                               \
+    }
+MDF_FFT_KERNELS(k_fft_z_r2c, fft_z_r2c_dev<R>, FFTZArgs<R>, typename R)
+MDF_FFT_KERNELS(k_fft_z_c2r, fft_z_c2r_dev<R>, FFTZArgs<R>, typename R)
+MDF_FFT_KERNELS(k_fft_y, fft_y_dev<R>, FFTYArgs<R>, typename R)
+#undef MDF_FFT_KERNELS
+
+template <typename R, bool ENERGY>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv(FFTXArgs<R> A)
+{
+    fft_x_conv_dev<R, ENERGY>(A);
+}
+
+template <typename R, bool ENERGY>
+__global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv_multi(const FFTXArgs<R>* __restrict__ As)
+{
+    const FFTXArgs<R>& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx || (int)blockIdx.y >= A.gy) return;
+    fft_x_conv_dev<R, ENERGY>(A);
+}
+
 // ------------------------------------------------------ spread / gather
 // Cardinal B-spline of order 4: th[j] = M4(w + 3 - j), placed at base-1+j.
 template <typename R>
@@ -401,11 +444,6 @@ __device__ __forceinline__ void bspline4(R w, R th[4], R dth[4])
     }
 }
 
-struct GridGeom {
-    int K[3];
-    double L[3];
-    double scale[3];   // K/L
-};
 
 template <typename R>
 __global__ void k_spread4(int s0, int s1, const int* __restrict__ slot_atom, const double* __restrict__ xyz,
@@ -453,11 +491,119 @@ __global__ void k_spread4(int s0, int s1, const int* __restrict__ slot_atom, con
     }
 }
 
+// One weight of the order-4 cardinal B-spline: th[j] of bspline4 for a single j.
 template <typename R>
-__global__ void k_gather4(int s0, int s1, int nslots, const int* __restrict__ slot_atom,
-                          const double* __restrict__ xyz, const double* __restrict__ q, GridGeom g,
-                          const R* __restrict__ phi, unsigned long long* __restrict__ fslot, unsigned* st)
+__device__ __forceinline__ R bspline4_one(R w, int j)
 {
+    const R w2 = w * w, w3 = w2 * w, om = (R)1 - w;
+    R v;
+    if (j == 0) v = om * om * om;
+    else if (j == 1) v = (R)3 * w3 - (R)6 * w2 + (R)4;
+    else if (j == 2) v = (R)-3 * w3 + (R)3 * w2 + (R)3 * w + (R)1;
+    else v = w3;
+    return v * (R)(1.0 / 6.0);
+}
+
+// Charge spread with 16 lanes per atom: lane (i, j) of the atom's 4 x 4 (x, y)
+// stencil rows adds the row's 4 consecutive z points, so each lane's four
+// int64 reductions fall in one 32-byte sector (two at the periodic z edge)
+// and the 16 lanes of an atom touch 16 distinct rows.  Against one thread per
+// atom (64 reductions scattered over 16 rows by one thread) this keeps more
+// reductions in flight per warp and spreads them over more L2 slices.  Each
+// lane computes only the weights it uses: theta_x[i], theta_y[j] and the four
+// theta_z.  The grid words are identical to the per-atom form's (the same
+// rounded fixed-point values, summed in any order).  Launched with a multiple
+// of 16 threads per block.
+template <typename R>
+__device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A)
+{
+    const int s0 = A.s0, s1 = A.s1;
+    const int* __restrict__ slot_atom = A.slot_atom;
+    const double* __restrict__ xyz = A.xyz;
+    const double* __restrict__ q = A.q;
+    const GridGeom& g = A.g;
+    unsigned long long* __restrict__ qgrid = A.qgrid;
+    unsigned* st = A.st;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = s0 + (int)(t >> 4);
+    const int row = (int)(t & 15), i = row >> 2, j = row & 3;
+    if (s >= s1) return;
+    const int a = slot_atom[s];
+    if (a < 0) return;
+    const double qa = q[a];
+    if (qa == 0.0) return;
+    int base[3];
+    R w[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double u = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
+        if (!(u >= 0.0 && u <= (double)g.K[d])) {   // non-finite position
+            if (row == 0) status_set(st, ST_NONFINITE);
+            return;
+        }
+        if (u >= g.K[d]) u -= g.K[d];
+        const int b = min((int)floor(u), g.K[d] - 1);
+        base[d] = b;
+        w[d] = (R)(u - b);
+    }
+    int kx = base[0] - 1 + i;
+    kx += (kx < 0) ? g.K[0] : 0;
+    kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+    int ky = base[1] - 1 + j;
+    ky += (ky < 0) ? g.K[1] : 0;
+    ky -= (ky >= g.K[1]) ? g.K[1] : 0;
+    const R wxy = (R)qa * bspline4_one<R>(w[0], i) * bspline4_one<R>(w[1], j);
+    R th[4];
+    bspline4<R>(w[2], th, nullptr);
+    unsigned long long* rowp = qgrid + ((long long)kx * g.K[1] + ky) * g.K[2];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int kz = base[2] - 1 + k;
+        kz += (kz < 0) ? g.K[2] : 0;
+        kz -= (kz >= g.K[2]) ? g.K[2] : 0;
+        const R v = wxy * th[k];
+        long long fx;
+        if (sizeof(R) == 4) fx = __float2ll_rn((float)v * 1099511627776.0f);   // exact 2^40 scaling
+        else fx = __double2ll_rn((double)v * GRID_SCALE);
+        atomicAdd(rowp + kz, (unsigned long long)fx);
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spread4_rows(SpreadArgs A)
+{
+    spread4_rows_dev<R>(A);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_spread4_rows_multi(const SpreadArgs* __restrict__ As)
+{
+    const SpreadArgs& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    spread4_rows_dev<R>(A);
+}
+
+// Clear many systems' charge grids in one launch.
+__global__ void k_zero_multi(const ZeroArgs* __restrict__ As)
+{
+    const ZeroArgs& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < A.n;
+         i += (long long)A.gx * blockDim.x)
+        A.p[i] = 0ull;
+}
+
+template <typename R>
+__device__ __forceinline__ void gather4_dev(const GatherArgs<R>& A)
+{
+    const int s0 = A.s0, s1 = A.s1, nslots = A.nslots;
+    const int* __restrict__ slot_atom = A.slot_atom;
+    const double* __restrict__ xyz = A.xyz;
+    const double* __restrict__ q = A.q;
+    const GridGeom& g = A.g;
+    const R* __restrict__ phi = A.phi;
+    unsigned long long* __restrict__ fslot = A.fslot;
+    unsigned* st = A.st;
     int s = s0 + blockIdx.x * blockDim.x + threadIdx.x;   // slots [s0, s1) of nslots
     if (s >= s1) return;
     int a = slot_atom[s];
@@ -505,6 +651,20 @@ __global__ void k_gather4(int s0, int s1, int nslots, const int* __restrict__ sl
     fx_add(fslot + s, -qr * gx * (R)g.scale[0], FORCE_SCALE, st);
     fx_add(fslot + nslots + s, -qr * gy * (R)g.scale[1], FORCE_SCALE, st);
     fx_add(fslot + 2 * nslots + s, -qr * gz * (R)g.scale[2], FORCE_SCALE, st);
+}
+
+template <typename R>
+__global__ void k_gather4(GatherArgs<R> A)
+{
+    gather4_dev<R>(A);
+}
+
+template <typename R>
+__global__ void k_gather4_multi(const GatherArgs<R>* __restrict__ As)
+{
+    const GatherArgs<R>& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    gather4_dev<R>(A);
 }
 
 // The reference's order-5 weights (src/System/PBC.cpp:329-356 for the spread,
@@ -854,49 +1014,150 @@ struct PmeBufs {
     }
 };
 
-// Fixed-point charge grid (c.qgrid) -> real potential grid: z, y, x + influence
-// function (+ energy and virial), y^-1, z^-1.  Five launches.
+// The five FFT launches of one chain (fixed-point charge grid c.qgrid -> real
+// potential grid): z, y, x + influence function (+ energy and virial), y^-1,
+// z^-1, with their dynamic shared memory.
 template <typename R>
-static void conv_chain(Ctx& c, const PmeBufs<R>& B, bool energy)
+FFTChain<R> make_fft_chain(const Ctx& c, bool energy)
 {
     using C = typename CT<R>::type;
+    const PmeBufs<R> B(const_cast<Ctx&>(c));
+    FFTChain<R> F;
     const bool ref = c.p.semantics == MDF_SEM_REFERENCE;
-    const int K0 = c.K[0], K1 = c.K[1], K2 = c.K[2], Kc = K2 / 2 + 1;
-    const FFTDesc dx = to_desc(c.plan[0]), dy = to_desc(c.plan[1]), dz = to_desc(c.plan[2]);
-    // z forward (real -> half complex)
+    const int K0 = c.K[0], K1 = c.K[1], Kc = c.K[2] / 2 + 1;
+    // z forward (real -> half complex) and z inverse share a geometry
     const int LPz = lines_per_block(c.plan[2], sizeof(C), c.p.fft_lines);
-    const size_t smz = fft_smem(c.plan[2], sizeof(C), LPz);
+    F.smz = fft_smem(c.plan[2], sizeof(C), LPz);
     const int nlines = K0 * K1;
-    const int nbz = (nlines + 2 * LPz - 1) / (2 * LPz);
-    k_fft_z_r2c<R><<<nbz, FFT_THREADS, smz, c.stream>>>(c.qgrid.p, B.cg, nlines, dz, B.twz, c.fft_tab[2].p, LPz);
-    // y forward
+    F.zf.gx = (nlines + 2 * LPz - 1) / (2 * LPz);
+    F.zf.gy = 1;
+    F.zf.qgrid = c.qgrid.p;
+    F.zf.cgrid = B.cg;
+    F.zf.rgrid = B.rg;
+    F.zf.nlines = nlines;
+    F.zf.d = to_desc(c.plan[2]);
+    F.zf.tw = B.twz;
+    F.zf.tab = c.fft_tab[2].p;
+    F.zf.LP = LPz;
+    F.zi = F.zf;
+    // y forward / inverse
     const int LPy = lines_per_block(c.plan[1], sizeof(C), c.p.fft_lines);
-    const size_t smy = fft_smem(c.plan[1], sizeof(C), LPy);
-    const dim3 gy((Kc + LPy - 1) / LPy, K0);
-    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(B.cg, Kc, dy, B.twy, c.fft_tab[1].p, LPy, ilog2(LPy), false);
+    F.smy = fft_smem(c.plan[1], sizeof(C), LPy);
+    F.yf.gx = (Kc + LPy - 1) / LPy;
+    F.yf.gy = K0;
+    F.yf.cgrid = B.cg;
+    F.yf.Kc = Kc;
+    F.yf.d = to_desc(c.plan[1]);
+    F.yf.tw = B.twy;
+    F.yf.tab = c.fft_tab[1].p;
+    F.yf.LP = LPy;
+    F.yf.lp_shift = ilog2(LPy);
+    F.yf.inverse = 0;
+    F.yi = F.yf;
+    F.yi.inverse = 1;
     // x forward + convolution + x inverse
-    {
-        const int LP = lines_per_block(c.plan[0], sizeof(C), c.p.fft_lines);
-        const size_t sm = fft_smem(c.plan[0], sizeof(C), LP);
-        const dim3 gx((Kc + LP - 1) / LP, K1);
-        ConvParams cp;
-        for (int d = 0; d < 3; ++d) cp.K[d] = c.K[d];
-        cp.pa2 = M_PI * M_PI / (c.alpha * c.alpha);
-        cp.reference = ref ? 1 : 0;
-        if (energy)
-            k_fft_x_conv<R, true><<<gx, FFT_THREADS, sm, c.stream>>>(B.cg, K1, Kc, dx, B.twx, c.fft_tab[0].p, LP,
-                                                                     ilog2(LP), cp, B.infl, c.mvec[0].p, c.mvec[1].p,
-                                                                     c.mvec[2].p, c.acc.p, c.status.p);
-        else
-            k_fft_x_conv<R, false><<<gx, FFT_THREADS, sm, c.stream>>>(B.cg, K1, Kc, dx, B.twx, c.fft_tab[0].p, LP,
-                                                                      ilog2(LP), cp, B.infl, c.mvec[0].p, c.mvec[1].p,
-                                                                      c.mvec[2].p, c.acc.p, c.status.p);
-    }
-    // y inverse
-    k_fft_y<R><<<gy, FFT_THREADS, smy, c.stream>>>(B.cg, Kc, dy, B.twy, c.fft_tab[1].p, LPy, ilog2(LPy), true);
-    // z inverse (half complex -> real)
-    k_fft_z_c2r<R><<<nbz, FFT_THREADS, smz, c.stream>>>(B.cg, B.rg, nlines, dz, B.twz, c.fft_tab[2].p, LPz);
+    const int LP = lines_per_block(c.plan[0], sizeof(C), c.p.fft_lines);
+    F.smx = fft_smem(c.plan[0], sizeof(C), LP);
+    F.x.gx = (Kc + LP - 1) / LP;
+    F.x.gy = K1;
+    F.x.cgrid = B.cg;
+    F.x.K1 = K1;
+    F.x.Kc = Kc;
+    F.x.d = to_desc(c.plan[0]);
+    F.x.tw = B.twx;
+    F.x.tab = c.fft_tab[0].p;
+    F.x.LP = LP;
+    F.x.lp_shift = ilog2(LP);
+    for (int d = 0; d < 3; ++d) F.x.cp.K[d] = c.K[d];
+    F.x.cp.pa2 = M_PI * M_PI / (c.alpha * c.alpha);
+    F.x.cp.reference = ref ? 1 : 0;
+    F.x.infl = B.infl;
+    F.x.mx = c.mvec[0].p;
+    F.x.my = c.mvec[1].p;
+    F.x.mz = c.mvec[2].p;
+    F.x.acc = c.acc.p;
+    F.x.st = c.status.p;
+    F.energy = energy;
+    return F;
 }
+template FFTChain<float> make_fft_chain<float>(const Ctx&, bool);
+template FFTChain<double> make_fft_chain<double>(const Ctx&, bool);
+
+template <typename R>
+static void conv_chain(Ctx& c, const PmeBufs<R>&, bool energy)
+{
+    const FFTChain<R> F = make_fft_chain<R>(c, energy);
+    k_fft_z_r2c<R><<<grid_of(F.zf), FFT_THREADS, F.smz, c.stream>>>(F.zf);
+    k_fft_y<R><<<grid_of(F.yf), FFT_THREADS, F.smy, c.stream>>>(F.yf);
+    if (energy) k_fft_x_conv<R, true><<<grid_of(F.x), FFT_THREADS, F.smx, c.stream>>>(F.x);
+    else k_fft_x_conv<R, false><<<grid_of(F.x), FFT_THREADS, F.smx, c.stream>>>(F.x);
+    k_fft_y<R><<<grid_of(F.yi), FFT_THREADS, F.smy, c.stream>>>(F.yi);
+    k_fft_z_c2r<R><<<grid_of(F.zi), FFT_THREADS, F.smz, c.stream>>>(F.zi);
+}
+
+// Many systems' FFT chains, one launch per pass (each struct array holds one
+// entry per system; grids and shared memory are the largest over systems).
+template <typename R>
+void launch_fft_chain_multi(const FFTChainDev<R>& D, int nsys, const FFTChainMax& M, bool energy, cudaStream_t s)
+{
+    k_fft_z_r2c_multi<R><<<dim3(M.zx, 1, nsys), FFT_THREADS, M.smz, s>>>(D.zf);
+    k_fft_y_multi<R><<<dim3(M.yx, M.yy, nsys), FFT_THREADS, M.smy, s>>>(D.yf);
+    if (energy) k_fft_x_conv_multi<R, true><<<dim3(M.xx, M.xy, nsys), FFT_THREADS, M.smx, s>>>(D.x);
+    else k_fft_x_conv_multi<R, false><<<dim3(M.xx, M.xy, nsys), FFT_THREADS, M.smx, s>>>(D.x);
+    k_fft_y_multi<R><<<dim3(M.yx, M.yy, nsys), FFT_THREADS, M.smy, s>>>(D.yi);
+    k_fft_z_c2r_multi<R><<<dim3(M.zx, 1, nsys), FFT_THREADS, M.smz, s>>>(D.zi);
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+template void launch_fft_chain_multi<float>(const FFTChainDev<float>&, int, const FFTChainMax&, bool, cudaStream_t);
+template void launch_fft_chain_multi<double>(const FFTChainDev<double>&, int, const FFTChainMax&, bool,
+                                             cudaStream_t);
+
+// Spread and gather arguments of this rank's slots (PHYSICAL, order 4).
+SpreadArgs make_spread_args(const Ctx& c)
+{
+    SpreadArgs A;
+    long long s0, s1;
+    rank_slice(c, c.n_slots, s0, s1);   // this rank's slots (all of them with one rank)
+    A.s0 = (int)s0;
+    A.s1 = (int)s1;
+    A.gx = grid_blocks(16 * (s1 - s0), 256);
+    A.gy = 1;
+    A.slot_atom = c.slot_atom.p;
+    A.xyz = c.xyz.p;
+    A.q = c.q.p;
+    for (int d = 0; d < 3; ++d) {
+        A.g.K[d] = c.K[d];
+        A.g.L[d] = c.box[d];
+        A.g.scale[d] = (double)c.K[d] / c.box[d];
+    }
+    A.qgrid = c.qgrid.p;
+    A.st = c.status.p;
+    return A;
+}
+
+template <typename R>
+GatherArgs<R> make_gather_args(const Ctx& c)
+{
+    GatherArgs<R> A;
+    const PmeBufs<R> B(const_cast<Ctx&>(c));
+    long long s0, s1;
+    rank_slice(c, c.n_slots, s0, s1);
+    A.s0 = (int)s0;
+    A.s1 = (int)s1;
+    A.nslots = c.n_slots;
+    A.gx = grid_blocks(s1 - s0, 256);
+    A.gy = 1;
+    A.slot_atom = c.slot_atom.p;
+    A.xyz = c.xyz.p;
+    A.q = c.q.p;
+    A.g = B.g;
+    A.phi = B.rg;
+    A.fslot = c.f_slot.p;
+    A.st = c.status.p;
+    return A;
+}
+template GatherArgs<float> make_gather_args<float>(const Ctx&);
+template GatherArgs<double> make_gather_args<double>(const Ctx&);
 
 template <typename R>
 static void run_pme(Ctx& c, bool energy)
@@ -906,12 +1167,9 @@ static void run_pme(Ctx& c, bool energy)
     const long long ntot = (long long)c.K[0] * c.K[1] * c.K[2];
     MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * ntot, c.stream));
     const int th = 256;
-    long long s0, s1;
-    rank_slice(c, c.n_slots, s0, s1);   // this rank's slots (all of them with one rank)
     if (!ref) {
-        if (s1 > s0)
-            k_spread4<R><<<grid_blocks(s1 - s0, th), th, 0, c.stream>>>((int)s0, (int)s1, c.slot_atom.p, c.xyz.p,
-                                                                       c.q.p, B.g, c.qgrid.p, c.status.p);
+        const SpreadArgs S = make_spread_args(c);
+        if (S.s1 > S.s0) k_spread4_rows<R><<<grid_of(S), th, 0, c.stream>>>(S);
         if (distributed(c)) allreduce_u64(c, c.qgrid.p, ntot);   // the whole charge grid on every rank
     } else {
         k_spread_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, B.g, c.qgrid.p);
@@ -920,10 +1178,8 @@ static void run_pme(Ctx& c, bool energy)
     conv_chain<R>(c, B, energy && rank0(c));   // reciprocal energy and virial counted once
     mark(c, "pme_fft_conv");
     if (!ref) {
-        if (s1 > s0)
-            k_gather4<R><<<grid_blocks(s1 - s0, th), th, 0, c.stream>>>((int)s0, (int)s1, c.n_slots, c.slot_atom.p,
-                                                                       c.xyz.p, c.q.p, B.g, B.rg, c.f_slot.p,
-                                                                       c.status.p);
+        const GatherArgs<R> G = make_gather_args<R>(c);
+        if (G.s1 > G.s0) k_gather4<R><<<grid_of(G), th, 0, c.stream>>>(G);
     } else {
         c.forces_pme_ref.alloc(3 * (size_t)c.N);
         k_gather_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, B.g,
@@ -934,6 +1190,24 @@ static void run_pme(Ctx& c, bool energy)
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 7;   // spread, z, y, x+conv, y, z, gather
 }
+
+// Many systems: clear the charge grids, spread, the FFT chain, gather.
+template <typename R>
+void launch_pme_multi(const ZeroArgs* d_zero, int zx, const SpreadArgs* d_spread, int sx, const FFTChainDev<R>& D,
+                      const FFTChainMax& M, const GatherArgs<R>* d_gather, int gx, int nsys, bool energy,
+                      cudaStream_t s)
+{
+    k_zero_multi<<<dim3(zx, 1, nsys), 256, 0, s>>>(d_zero);
+    k_spread4_rows_multi<R><<<dim3(sx, 1, nsys), 256, 0, s>>>(d_spread);
+    MDF_CUDA_TRY(cudaGetLastError());
+    launch_fft_chain_multi<R>(D, nsys, M, energy, s);
+    k_gather4_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_gather);
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+template void launch_pme_multi<float>(const ZeroArgs*, int, const SpreadArgs*, int, const FFTChainDev<float>&,
+                                      const FFTChainMax&, const GatherArgs<float>*, int, int, bool, cudaStream_t);
+template void launch_pme_multi<double>(const ZeroArgs*, int, const SpreadArgs*, int, const FFTChainDev<double>&,
+                                       const FFTChainMax&, const GatherArgs<double>*, int, int, bool, cudaStream_t);
 
 // ------------------------------------------------------------- adjoint
 // Reciprocal-space part of mdf_backward.  With E = 1/2 Q^T C Q (Q the charge

@@ -21,7 +21,7 @@ EXPORTS = [
     "mdf_set_positions", "mdf_set_positions_device", "mdf_set_box", "mdf_build_pairlist", "mdf_compute",
     "mdf_compute_async", "mdf_fetch", "mdf_forces_device", "mdf_get_pme_forces", "mdf_set_stream",
     "mdf_pairlist_info", "mdf_enable_timing", "mdf_kernel_times", "mdf_cmap_coefficients",
-    "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
+    "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_probe_l2_reductions", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_host_buffers", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
@@ -74,6 +74,7 @@ def library(path=None):
     lib.mdf_kernel_launches.argtypes = [C.c_void_p]
     lib.mdf_kernel_launches.restype = C.c_int64
     lib.mdf_probe_fma_tflops.argtypes = [C.c_int, C.c_int, dp]
+    lib.mdf_probe_l2_reductions.argtypes = [C.c_int, C.c_int64, C.c_int, dp]
     lib.mdf_set_parameters.argtypes = [C.c_void_p, dp, dp, dp]
     lib.mdf_backward.argtypes = [C.c_void_p, dp, C.c_double, dp, dp, dp]
     lib.mdf_minimize.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.mdf_min_report)]
@@ -134,6 +135,17 @@ def probe_fma_tflops(device=0, precision=abi.MDF_PREC_MIXED):
     rc = library().mdf_probe_fma_tflops(device, precision, C.byref(v))
     if rc != 0:
         raise MDFError(rc, "mdf_probe_fma_tflops")
+    return v.value
+
+
+def probe_l2_reductions(device=0, words=10077696, pattern=0):
+    """Measured int64 reductions per second into an L2-resident buffer of
+    `words` 64-bit words (default: the 216^3 PME grid); pattern 0 = the charge
+    spread's 32-byte rows, 1 = 256-byte warp runs."""
+    v = C.c_double(0)
+    rc = library().mdf_probe_l2_reductions(device, int(words), int(pattern), C.byref(v))
+    if rc != 0:
+        raise MDFError(rc, "mdf_probe_l2_reductions")
     return v.value
 
 

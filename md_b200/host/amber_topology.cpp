@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <fstream>
 #include <map>
 #include <set>
@@ -15,48 +16,128 @@ namespace mdb200 {
 
 namespace {
 
-// %FLAG name -> the section's lines (after its %FORMAT line)
-std::map<std::string, std::vector<std::string>> read_sections(const std::string& path)
+// The whole file in memory (NUL-terminated) and, per %FLAG name, the byte
+// range of its body.  Numbers are parsed in place: no per-line strings, no
+// stream objects (a 960,000-atom prmtop is ~100 MB).
+struct Sections {
+    std::string buf;
+    std::map<std::string, std::pair<size_t, size_t>> range;   // [begin, end) of the body
+    bool has(const std::string& name) const { return range.count(name) != 0; }
+};
+
+std::string slurp(const std::string& path, const char* what)
 {
-    std::ifstream f(path);
-    if (!f) throw std::runtime_error("cannot open prmtop " + path);
-    std::map<std::string, std::vector<std::string>> out;
-    std::string line, cur;
-    while (std::getline(f, line)) {
-        if (line.rfind("%FLAG", 0) == 0) {
-            std::istringstream ss(line.substr(5));
-            ss >> cur;
-            out[cur];
-        } else if (line.rfind("%FORMAT", 0) == 0 || line.rfind("%VERSION", 0) == 0 || line.rfind("%COMMENT", 0) == 0) {
-            continue;
-        } else if (!cur.empty()) {
-            out[cur].push_back(line);
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f) throw std::runtime_error(std::string("cannot open ") + what + " " + path);
+    std::string buf;
+    std::fseek(f, 0, SEEK_END);
+    const long n = std::ftell(f);
+    std::fseek(f, 0, SEEK_SET);
+    if (n > 0) {
+        buf.resize((size_t)n);
+        if (std::fread(&buf[0], 1, (size_t)n, f) != (size_t)n) {
+            std::fclose(f);
+            throw std::runtime_error(std::string("cannot read ") + what + " " + path);
         }
     }
-    return out;
+    std::fclose(f);
+    return buf;   // std::string keeps a NUL after the last byte
+}
+
+Sections read_sections(const std::string& path)
+{
+    Sections s;
+    s.buf = slurp(path, "prmtop");
+    const char* d = s.buf.data();
+    const size_t n = s.buf.size();
+    std::string cur;
+    size_t pos = 0;
+    while (pos < n) {
+        const char* nl = static_cast<const char*>(std::memchr(d + pos, '\n', n - pos));
+        const size_t end = nl ? (size_t)(nl - d) : n;
+        if (end - pos >= 5 && std::strncmp(d + pos, "%FLAG", 5) == 0) {
+            if (!cur.empty()) s.range[cur].second = pos;
+            size_t p = pos + 5;
+            while (p < end && (d[p] == ' ' || d[p] == '\t')) ++p;
+            size_t q = p;
+            while (q < end && d[q] != ' ' && d[q] != '\t' && d[q] != '\r') ++q;
+            cur.assign(d + p, q - p);
+            s.range[cur] = {end < n ? end + 1 : n, n};
+        }
+        pos = end + 1;
+    }
+    if (!cur.empty()) s.range[cur].second = n;
+    return s;
+}
+
+// Calls fn(token_start) for every whitespace-separated token of the section's
+// body, skipping its %FORMAT / %COMMENT lines.  Returns false if the section
+// is absent.
+template <typename Fn>
+bool for_each_token(const Sections& s, const std::string& name, Fn&& fn)
+{
+    auto it = s.range.find(name);
+    if (it == s.range.end()) return false;
+    const char* d = s.buf.data();
+    size_t p = it->second.first;
+    const size_t e = it->second.second;
+    bool line_start = true;
+    while (p < e) {
+        const char c = d[p];
+        if (c == '\n') {
+            line_start = true;
+            ++p;
+            continue;
+        }
+        if (line_start && c == '%') {   // %FORMAT / %COMMENT line
+            while (p < e && d[p] != '\n') ++p;
+            continue;
+        }
+        line_start = false;
+        if (c == ' ' || c == '\t' || c == '\r') {
+            ++p;
+            continue;
+        }
+        const size_t next = fn(d + p);
+        p += next;
+    }
+    return true;
 }
 
 template <typename T>
-std::vector<T> numbers(const std::map<std::string, std::vector<std::string>>& s, const std::string& name,
-                       bool required = true)
+std::vector<T> numbers(const Sections& s, const std::string& name, bool required = true)
 {
     std::vector<T> v;
-    auto it = s.find(name);
-    if (it == s.end()) {
-        if (required) throw std::runtime_error("prmtop section missing: " + name);
-        return v;
-    }
-    for (const std::string& line : it->second) {
-        std::istringstream ss(line);
-        std::string tok;
-        while (ss >> tok) {
-            char* end = nullptr;
-            const double x = std::strtod(tok.c_str(), &end);
-            if (end == tok.c_str()) throw std::runtime_error("bad number '" + tok + "' in " + name);
-            v.push_back(static_cast<T>(x));
+    const bool found = for_each_token(s, name, [&](const char* tok) -> size_t {
+        char* end = nullptr;
+        const double x = std::strtod(tok, &end);
+        if (end == tok) {
+            size_t k = 0;
+            while (tok[k] && tok[k] != ' ' && tok[k] != '\n') ++k;
+            throw std::runtime_error("bad number '" + std::string(tok, k) + "' in " + name);
         }
-    }
+        v.push_back(static_cast<T>(x));
+        return (size_t)(end - tok);
+    });
+    if (!found && required) throw std::runtime_error("prmtop section missing: " + name);
     return v;
+}
+
+// First line of a text section (the title).
+std::string first_line(const Sections& s, const std::string& name)
+{
+    auto it = s.range.find(name);
+    if (it == s.range.end()) return "";
+    const char* d = s.buf.data();
+    size_t p = it->second.first;
+    const size_t e = it->second.second;
+    while (p < e) {
+        const char* nl = static_cast<const char*>(std::memchr(d + p, '\n', e - p));
+        const size_t end = nl ? (size_t)(nl - d) : e;
+        if (d[p] != '%') return std::string(d + p, end - p);
+        p = end + 1;
+    }
+    return "";
 }
 
 void require(bool ok, const std::string& what)
@@ -68,20 +149,22 @@ void require(bool ok, const std::string& what)
 
 AmberTopology AmberTopology::read(const std::string& prmtop, const std::string& rst7)
 {
-    const auto s = read_sections(prmtop);
+    const Sections s = read_sections(prmtop);
     AmberTopology t;
-    if (s.count("TITLE") && !s.at("TITLE").empty()) t.title = s.at("TITLE")[0];
+    t.title = first_line(s, "TITLE");
     const auto ptr = numbers<long long>(s, "POINTERS");
     require(ptr.size() >= 2, "POINTERS too short");
     t.natoms = (int)ptr[0];
     t.ntypes = (int)ptr[1];
     const int N = t.natoms;
     // long double divide, as the reference does (TopologyParser.cpp:49-52)
-    for (const std::string& line : s.count("CHARGE") ? s.at("CHARGE") : std::vector<std::string>{}) {
-        std::istringstream ss(line);
-        std::string tok;
-        while (ss >> tok) t.charge.push_back((double)(std::strtold(tok.c_str(), nullptr) / 18.2206899283247L));
-    }
+    for_each_token(s, "CHARGE", [&](const char* tok) -> size_t {
+        char* end = nullptr;
+        const long double v = std::strtold(tok, &end);
+        if (end == tok) throw std::runtime_error("bad number in CHARGE");
+        t.charge.push_back((double)(v / 18.2206899283247L));
+        return (size_t)(end - tok);
+    });
     t.mass = numbers<double>(s, "MASS");
     for (int ty : numbers<int>(s, "ATOM_TYPE_INDEX")) t.type.push_back(ty - 1);
     t.nb_index = numbers<int>(s, "NONBONDED_PARM_INDEX");
@@ -201,24 +284,36 @@ AmberTopology AmberTopology::read(const std::string& prmtop, const std::string& 
 // fields six per line, then (velocities and) the box line.
 void AmberTopology::read_coordinates(const std::string& path)
 {
-    std::ifstream f(path);
-    if (!f) throw std::runtime_error("cannot open coordinates " + path);
-    std::string line;
-    std::getline(f, line);   // title
-    std::getline(f, line);
-    int n = 0;
-    {
-        std::istringstream ss(line);
-        ss >> n;
-    }
+    const std::string buf = slurp(path, "coordinates");
+    const char* d = buf.data();
+    const size_t nb = buf.size();
+    auto line_end = [&](size_t p) {
+        const char* nl = static_cast<const char*>(std::memchr(d + p, '\n', nb - p));
+        return nl ? (size_t)(nl - d) : nb;
+    };
+    size_t p = line_end(0) + 1;   // title
+    if (p > nb) throw std::runtime_error("rst7 too short");
+    const size_t e2 = line_end(p);
+    const int n = std::atoi(std::string(d + p, e2 - p).c_str());
     if (n != natoms) throw std::runtime_error("rst7 atom count differs from the prmtop");
     std::vector<double> vals;
-    while (std::getline(f, line)) {
-        for (size_t p = 0; p + 1 <= line.size(); p += 12) {
-            std::string fld = line.substr(p, 12);
-            if (fld.find_first_not_of(' ') == std::string::npos) continue;
-            vals.push_back(std::strtod(fld.c_str(), nullptr));
+    vals.reserve(3 * (size_t)n + 6);
+    p = e2 + 1;
+    while (p < nb) {
+        size_t e = line_end(p);
+        if (e > p && d[e - 1] == '\r') --e;
+        // fixed 12-character fields
+        for (size_t q = p; q < e; q += 12) {
+            char fld[13];
+            const size_t w = std::min<size_t>(12, e - q);
+            std::memcpy(fld, d + q, w);
+            fld[w] = 0;
+            size_t k = 0;
+            while (k < w && fld[k] == ' ') ++k;
+            if (k == w) continue;
+            vals.push_back(std::strtod(fld, nullptr));
         }
+        p = line_end(p) + 1;
     }
     if (vals.size() < 3 * (size_t)n) throw std::runtime_error("rst7 has too few coordinates");
     coords.assign(vals.begin(), vals.begin() + 3 * (size_t)n);
@@ -335,31 +430,49 @@ FlatTopology flatten(const AmberTopology& t, int semantics)
         }
     }
     if (!ref) {
-        std::set<std::pair<int, int>> ex, near;
-        auto key = [](int a, int b) { return std::make_pair(std::min(a, b), std::max(a, b)); };
+        // pairs as sorted 64-bit keys (min << 32 | max): the order of a set of
+        // pairs, built with one sort instead of a tree insert per pair
+        auto key = [](int a, int b) {
+            return ((unsigned long long)(unsigned)std::min(a, b) << 32) | (unsigned)std::max(a, b);
+        };
+        auto sort_unique = [](std::vector<unsigned long long>& v) {
+            std::sort(v.begin(), v.end());
+            v.erase(std::unique(v.begin(), v.end()), v.end());
+        };
+        std::vector<unsigned long long> ex, near;
         for (int i = 0; i < t.natoms; ++i)
-            for (int j : t.excluded[i]) ex.insert(key(i, j));
-        for (size_t k = 0; k < o.bond_atoms.size(); k += 2) near.insert(key(o.bond_atoms[k], o.bond_atoms[k + 1]));
-        for (size_t k = 0; k < o.angle_atoms.size(); k += 3)
-            near.insert(key(o.angle_atoms[k], o.angle_atoms[k + 2]));
-        std::map<std::pair<int, int>, std::pair<double, double>> p14;
+            for (int j : t.excluded[i]) ex.push_back(key(i, j));
+        for (size_t k = 0; k < o.bond_atoms.size(); k += 2) near.push_back(key(o.bond_atoms[k], o.bond_atoms[k + 1]));
+        for (size_t k = 0; k < o.angle_atoms.size(); k += 3) near.push_back(key(o.angle_atoms[k], o.angle_atoms[k + 2]));
+        sort_unique(near);
+        // 1-4 pairs with the largest SCEE / SCNB over the dihedrals that generate them
+        std::vector<std::pair<unsigned long long, std::pair<double, double>>> cand;
         for (const int* d : dkept) {
             if (d[5] || d[6]) continue;
             const auto kk = key(d[0], d[3]);
-            if (near.count(kk)) continue;
-            const double sc = t.scee.at(d[4]), sn = t.scnb.at(d[4]);
-            auto it = p14.find(kk);
-            if (it == p14.end()) p14[kk] = {sc, sn};
-            else it->second = {std::max(it->second.first, sc), std::max(it->second.second, sn)};
+            if (std::binary_search(near.begin(), near.end(), kk)) continue;
+            cand.push_back({kk, {t.scee.at(d[4]), t.scnb.at(d[4])}});
         }
-        for (const auto& kv : p14) ex.insert(kv.first);
-        for (const auto& e : ex) {
-            o.excl_pairs.push_back(e.first);
-            o.excl_pairs.push_back(e.second);
+        std::sort(cand.begin(), cand.end(),
+                  [](const auto& x, const auto& y) { return x.first < y.first; });
+        std::vector<std::pair<unsigned long long, std::pair<double, double>>> p14;
+        for (const auto& c : cand) {
+            if (!p14.empty() && p14.back().first == c.first)
+                p14.back().second = {std::max(p14.back().second.first, c.second.first),
+                                     std::max(p14.back().second.second, c.second.second)};
+            else
+                p14.push_back(c);
+        }
+        for (const auto& kv : p14) ex.push_back(kv.first);
+        sort_unique(ex);
+        o.excl_pairs.reserve(2 * ex.size());
+        for (unsigned long long e : ex) {
+            o.excl_pairs.push_back((int)(e >> 32));
+            o.excl_pairs.push_back((int)(e & 0xffffffffu));
         }
         for (const auto& kv : p14) {
-            o.pairs14.push_back(kv.first.first);
-            o.pairs14.push_back(kv.first.second);
+            o.pairs14.push_back((int)(kv.first >> 32));
+            o.pairs14.push_back((int)(kv.first & 0xffffffffu));
             o.scee14.push_back(kv.second.first);
             o.scnb14.push_back(kv.second.second);
         }

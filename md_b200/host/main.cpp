@@ -7,6 +7,7 @@
 //   mdb200 <prmtop> [coords] [--physical] [--mixed] [--tol T] [--grid NX NY NZ]
 //          [--device D] [--minimize ITERS] [--md STEPS DT_PS] [--rst7-out PATH]
 //          [--forces-out PATH] [--dump-topology DIR]
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -85,9 +86,15 @@ int main(int argc, char* argv[])
         else { usage(); return 1; }
     }
     try {
+        const auto t0 = std::chrono::steady_clock::now();
         AmberTopology top = AmberTopology::read(prmtop, coords);
+        const auto t1 = std::chrono::steady_clock::now();
         if (!dump_dir.empty()) {
-            dump_topology(flatten(top, sem), dump_dir);
+            const FlatTopology flat = flatten(top, sem);
+            const auto t2 = std::chrono::steady_clock::now();
+            std::printf("read %d atoms in %.3f s, flattened in %.3f s\n", top.natoms,
+                        std::chrono::duration<double>(t1 - t0).count(), std::chrono::duration<double>(t2 - t1).count());
+            dump_topology(flat, dump_dir);
             return 0;
         }
         std::vector<double> mass = top.mass;

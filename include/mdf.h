@@ -171,6 +171,22 @@ typedef struct {
  * for instance).  Returns 0 on success. */
 typedef int (*mdf_allreduce_u64)(uint64_t *d_buf, int64_t count, void *stream, void *user);
 
+/* The collectives of the distributed reciprocal space and force return
+ * (mdf_set_collectives), all on device memory of the context's GPU, ordered on
+ * `stream` like mdf_allreduce_u64, returning 0 on success:
+ *   reduce-scatter  send holds nranks blocks of `count` int64 words; rank r
+ *                   receives into recv the sum over ranks of block r
+ *                   (ncclReduceScatter, ncclInt64, ncclSum);
+ *   all-gather      rank r's `bytes` bytes of send land at recv + r * bytes on
+ *                   every rank (ncclAllGather);
+ *   all-to-all      send holds nranks blocks of `bytes` bytes, block k for rank
+ *                   k; recv block k comes from rank k (grouped ncclSend /
+ *                   ncclRecv). */
+typedef int (*mdf_reduce_scatter_u64)(const uint64_t *d_send, uint64_t *d_recv, int64_t count, void *stream,
+                                      void *user);
+typedef int (*mdf_allgather_bytes)(const void *d_send, void *d_recv, int64_t bytes, void *stream, void *user);
+typedef int (*mdf_alltoall_bytes)(const void *d_send, void *d_recv, int64_t bytes, void *stream, void *user);
+
 /* Flags for mdf_compute. */
 #define MDF_COMPUTE_ENERGY 1u
 #define MDF_COMPUTE_FORCES 2u
@@ -201,6 +217,20 @@ int mdf_set_box(mdf_ctx *ctx, const double box[3]);
  * support nranks > 1; the other evaluation entry points return
  * MDF_ERR_UNSUPPORTED. */
 int mdf_set_allreduce(mdf_ctx *ctx, mdf_allreduce_u64 fn, void *user);
+/* With nranks > 1, also register the collectives above (all three, or NULL
+ * to go back to the all-reduce form): the reciprocal space is then
+ * distributed as x-slabs of the PME grid - the charge grid is reduce-scattered
+ * (each rank receives its slab of planes), every rank runs the z and y
+ * passes of its slab, an all-to-all transposes to y-slabs for the x pass and
+ * the convolution (each rank its y-range, energy and virial included), a
+ * second all-to-all transposes back, and the potential slabs are all-gathered
+ * for the force gather - and the forces come back by a reduce-scatter of the
+ * fixed-point accumulators (each rank finalises its block of atom slots) and
+ * an all-gather of the finished forces.  Every rank still ends with all
+ * forces and energies, bit-identical to one context; the energy words and the
+ * pair count are still summed by the all-reduce. */
+int mdf_set_collectives(mdf_ctx *ctx, mdf_reduce_scatter_u64 reduce_scatter, mdf_allgather_bytes allgather,
+                        mdf_alltoall_bytes alltoall, void *user);
 
 /* Cell sort + cluster-pair list with exclusion masks (replaces
  * setup_pairlists / build_lj_pairlist, src/System/NonBondedUtils.cpp:49-57,185-282). */
@@ -216,6 +246,21 @@ int mdf_compute(mdf_ctx *ctx, uint32_t flags, double *forces_out, mdf_energies *
 int mdf_compute_async(mdf_ctx *ctx, uint32_t flags);
 /* Wait for the last async evaluation and copy its results (either may be NULL). */
 int mdf_fetch(mdf_ctx *ctx, double *forces_out, mdf_energies *e_out);
+/* Pipelined evaluations from and to host memory, two in flight: mdf_submit
+ * queues the copy of positions xyz (3N doubles, host) to the device on the
+ * context's copy stream, the evaluation on its stream and the copy of the
+ * forces back to forces_out (3N doubles, host, or NULL) on the copy stream,
+ * and returns at once; mdf_collect waits for the oldest submitted evaluation,
+ * checks its status and fills e_out (may be NULL).  The copies of one
+ * evaluation overlap the computation of the other, so a caller that submits
+ * evaluation k+1 before collecting k hides them.  xyz must stay unchanged and
+ * forces_out untouched until the evaluation is collected; pinned host memory
+ * (cudaHostAlloc) makes the copies asynchronous.  A third submit before a
+ * collect returns MDF_ERR_STATE.  The results equal mdf_compute's bit for
+ * bit; mdf_fetch does not see these evaluations.  Not available with
+ * nranks > 1. */
+int mdf_submit(mdf_ctx *ctx, uint32_t flags, const double *xyz, double *forces_out);
+int mdf_collect(mdf_ctx *ctx, mdf_energies *e_out);
 /* Device forces (3N doubles on ctx's device) of the last evaluation. */
 int mdf_forces_device(mdf_ctx *ctx, double *d_forces_out);
 

@@ -23,6 +23,10 @@ MDF_COMPUTE_PME_REFERENCE = 4
 
 # int (*)(uint64_t *d_buf, int64_t count, void *stream, void *user): the sum over ranks (mdf_set_allreduce)
 MDF_ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
+# (send, recv, count or bytes, stream, user) -> int: reduce-scatter, all-gather, all-to-all
+MDF_REDUCE_SCATTER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
+MDF_ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
+MDF_ALLTOALL_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p)
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)

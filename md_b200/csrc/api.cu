@@ -86,6 +86,86 @@ __global__ void k_finalize_multi(const FinalizeArgs* __restrict__ As)
     finalize_dev(A);
 }
 
+// Distributed force return.  Fold the per-atom accumulators into slot order
+// and lay the slots out as nranks blocks of Sb slots, [P][3][Sb], reading
+// and clearing both accumulators (padding slots past nslots are zero).
+__global__ void k_stage_forces(int N, int nslots, int Sb, int P, unsigned long long* __restrict__ fatom,
+                               unsigned long long* __restrict__ fslot, const int* __restrict__ slot_atom,
+                               unsigned long long* __restrict__ stage)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= P * Sb) return;
+    const int blk = s / Sb, sl = s - blk * Sb;
+    const int a = s < nslots ? slot_atom[s] : -1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        unsigned long long v = 0ull;
+        if (s < nslots) {
+            v = fslot[(long long)k * nslots + s];
+            fslot[(long long)k * nslots + s] = 0ull;
+            if (a >= 0) {
+                v += fatom[(long long)k * N + a];
+                fatom[(long long)k * N + a] = 0ull;
+            }
+        }
+        stage[((long long)blk * 3 + k) * Sb + sl] = v;
+    }
+}
+
+// This rank's block of summed slots -> FP64 forces [Sb][3]; also the scalar
+// block to the mapped host copy and cleared (as k_finalize does).
+__global__ void k_finish_block(int nslots, int Sb, int rank, const unsigned long long* __restrict__ mine,
+                               double* __restrict__ out, unsigned long long* __restrict__ scal,
+                               unsigned long long* __restrict__ host_scal)
+{
+    const int sl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sl < NUM_SCAL) {
+        host_scal[sl] = scal[sl];
+        scal[sl] = 0ull;
+    }
+    if (sl >= Sb) return;
+    const bool real = (long long)rank * Sb + sl < nslots;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        out[3 * sl + k] = real ? (double)(long long)mine[(long long)k * Sb + sl] * FORCE_ISCALE : 0.0;
+}
+
+// All ranks' finished slots [P Sb][3] -> forces in atom order.
+__global__ void k_slots_to_atoms(int N, const int* __restrict__ atom_slot, const double* __restrict__ all,
+                                 double* __restrict__ out)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a >= N) return;
+    const int s = atom_slot[a];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[3 * a + k] = all[3 * (long long)s + k];
+}
+
+static void finish_slab_forces(Ctx& c, double* d_forces)
+{
+    const int P = c.p.nranks, S = c.n_slots, Sb = (S + P - 1) / P;
+    c.f_stage.alloc((size_t)P * 3 * Sb);
+    c.f_mine.alloc((size_t)3 * Sb);
+    c.f_out_blk.alloc((size_t)3 * Sb);
+    c.f_out_all.alloc((size_t)3 * Sb * P);
+    k_stage_forces<<<grid_blocks((long long)P * Sb, 256), 256, 0, c.stream>>>(c.N, S, Sb, P, c.f_atom.p, c.f_slot.p,
+                                                                            c.slot_atom.p, c.f_stage.p);
+    MDF_CUDA_TRY(cudaGetLastError());
+    if (c.coll_rs(reinterpret_cast<const uint64_t*>(c.f_stage.p), reinterpret_cast<uint64_t*>(c.f_mine.p),
+                  (int64_t)3 * Sb, (void*)c.stream, c.coll_user) != 0)
+        throw ApiError(MDF_ERR_CUDA, "the reduce-scatter callback failed");
+    k_finish_block<<<grid_blocks(std::max(Sb, NUM_SCAL), 256), 256, 0, c.stream>>>(S, Sb, c.p.rank, c.f_mine.p,
+                                                                                  c.f_out_blk.p, c.scal.p,
+                                                                                  c.d_hscal);
+    MDF_CUDA_TRY(cudaGetLastError());
+    if (c.coll_ag(c.f_out_blk.p, c.f_out_all.p, (int64_t)(sizeof(double) * 3 * Sb), (void*)c.stream,
+                  c.coll_user) != 0)
+        throw ApiError(MDF_ERR_CUDA, "the all-gather callback failed");
+    k_slots_to_atoms<<<grid_blocks(c.N, 256), 256, 0, c.stream>>>(c.N, c.atom_slot.p, c.f_out_all.p, d_forces);
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 3;
+}
+
 FinalizeArgs make_finalize_args(const Ctx& c, double* d_forces)
 {
     FinalizeArgs A;
@@ -104,7 +184,9 @@ FinalizeArgs make_finalize_args(const Ctx& c, double* d_forces)
 
 void launch_finalize(Ctx& c, double* d_forces, bool)
 {
-    const FinalizeArgs A = make_finalize_args(c, d_forces);
+    if (c.fin_wait) MDF_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.fin_wait, 0));
+    FinalizeArgs A = make_finalize_args(c, c.fin_forces ? c.fin_forces : d_forces);
+    if (c.fin_hscal) A.host_scal = c.fin_hscal;
     k_finalize<<<grid_of(A), 256, 0, c.stream>>>(A);
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
@@ -132,6 +214,7 @@ void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b)
     std::vector<double2> ab(ntp * ntp, make_double2(0, 0)), ab14(ntp * ntp, make_double2(0, 0));
     std::vector<float2> abf(ntp * ntp, make_float2(0, 0));
     std::vector<float4> ab4(ntp * ntp, make_float4(0, 0, 0, 0));
+    std::vector<double4> ab4d(ntp * ntp, make_double4(0, 0, 0, 0));
     std::vector<int> valid(ntp * ntp, 0), idx(ntp * ntp, -1);
     for (int i = 0; i < c.ntypes; ++i)
         for (int j = 0; j < c.ntypes; ++j) {
@@ -142,6 +225,7 @@ void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b)
             abf[tp] = make_float2((float)lj_a[nb - 1], (float)lj_b[nb - 1]);
             ab4[tp] = make_float4((float)lj_a[nb - 1], (float)lj_b[nb - 1], (float)(12.0 * lj_a[nb - 1]),
                                   (float)(6.0 * lj_b[nb - 1]));
+            ab4d[tp] = make_double4(lj_a[nb - 1], lj_b[nb - 1], 12.0 * lj_a[nb - 1], 6.0 * lj_b[nb - 1]);
             ab14[tp] = make_double2(c.h_lj14a[nb - 1], c.h_lj14b[nb - 1]);
             valid[tp] = 1;
             idx[tp] = nb - 1;
@@ -149,6 +233,7 @@ void set_lj_tables(Ctx& c, const double* lj_a, const double* lj_b)
     c.ljAB.upload(ab.data(), ab.size(), s);
     c.ljAB_f.upload(abf.data(), abf.size(), s);
     c.ljAB4_f.upload(ab4.data(), ab4.size(), s);
+    c.ljAB4_d.upload(ab4d.data(), ab4d.size(), s);
     c.lj14AB.upload(ab14.data(), ab14.size(), s);
     c.ljvalid.upload(valid.data(), valid.size(), s);
     c.nbidx.upload(idx.data(), idx.size(), s);
@@ -360,6 +445,18 @@ void eval_async_impl(Ctx& c, uint32_t flags)
         c.have_pme_ref = !phys;
     }
     if (overlap) MDF_CUDA_TRY(cudaStreamWaitEvent(s, c.ev_join, 0));
+    if (slab_mode(c)) {
+        // energies, virial and pair count summed; the forces by reduce-scatter
+        // of the accumulators and all-gather of the finished forces
+        allreduce_u64(c, c.scal.p, NUM_ACC + 1);
+        if (c.counting) allreduce_u64(c, c.npairs_dev.p, 1);
+        c.counting = false;
+        finish_slab_forces(c, c.forces_out.p);
+        mark(c, "finalize");
+        c.pending = true;
+        c.pending_flags = flags;
+        return;
+    }
     if (distributed(c)) {
         // every rank's partial forces, energies, virial and pair count, summed
         // (the status word stays per rank)
@@ -389,16 +486,21 @@ static void eval_async(Ctx& c, uint32_t flags)
 // block (written by k_finalize into mapped host memory).
 void host_energies(const Ctx& c, uint32_t flags, mdf_energies* e_out)
 {
+    host_energies_from(c, c.h_scal, flags, e_out);
+}
+
+void host_energies_from(const Ctx& c, const unsigned long long* hs, uint32_t flags, mdf_energies* e_out)
+{
     memset(e_out, 0, sizeof(*e_out));
     if (!(flags & MDF_COMPUTE_ENERGY)) return;
-    for (int k = 0; k < MDF_E_COUNT; ++k) e_out->e[k] = (double)(long long)c.h_scal[k] * ENERGY_ISCALE;
+    for (int k = 0; k < MDF_E_COUNT; ++k) e_out->e[k] = (double)(long long)hs[k] * ENERGY_ISCALE;
     e_out->e[MDF_E_EE_SELF] += c.e_self;
     const bool phys = c.p.semantics == MDF_SEM_PHYSICAL;
     if (phys) {
         const double V = c.box[0] * c.box[1] * c.box[2];
         e_out->e[MDF_E_EE_RECIP] += -c.p.coulomb_const * M_PI * c.q_total * c.q_total / (2.0 * V * c.alpha * c.alpha);
         const int vmap[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
-        for (int k = 0; k < 9; ++k) e_out->virial[k] = (double)(long long)c.h_scal[ACC_VIR + vmap[k]] * ENERGY_ISCALE;
+        for (int k = 0; k < 9; ++k) e_out->virial[k] = (double)(long long)hs[ACC_VIR + vmap[k]] * ENERGY_ISCALE;
         double tot = 0;
         const int terms[] = {MDF_E_BOND, MDF_E_ANGLE, MDF_E_DIHEDRAL, MDF_E_UB, MDF_E_IMPROPER, MDF_E_CMAP,
                              MDF_E_VDW, MDF_E_VDW14, MDF_E_EE_DIRECT, MDF_E_EE14, MDF_E_EE_EXCL,
@@ -417,7 +519,12 @@ void host_energies(const Ctx& c, uint32_t flags, mdf_energies* e_out)
 // Status bits of the last finished evaluation, as an exception.
 void check_host_status(const Ctx& c)
 {
-    const unsigned st = (unsigned)c.h_scal[NUM_ACC + 1];
+    check_status_word(c.h_scal);
+}
+
+void check_status_word(const unsigned long long* hs)
+{
+    const unsigned st = (unsigned)hs[NUM_ACC + 1];
     if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite force or energy contribution");
     if (st & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "fixed-point accumulator range exceeded");
 }
@@ -438,6 +545,70 @@ static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
     if (e_out) host_energies(c, c.pending_flags, e_out);
     if (forces_out)
         MDF_CUDA_TRY(cudaMemcpy(forces_out, c.forces_out.p, sizeof(double) * 3 * (size_t)c.N, cudaMemcpyDeviceToHost));
+}
+
+// Pipelined evaluation: the positions go in on the copy stream (into the
+// stage's buffer, then one device copy on the evaluation stream), the
+// evaluation runs on the context's stream and writes the stage's forces and
+// scalar block, and the forces go out on the copy stream.  With two stages the
+// copies of one evaluation overlap the computation of the other.
+static void submit(Ctx& c, uint32_t flags, const double* xyz, double* forces_out)
+{
+    if (c.inflight >= 2) throw ApiError(MDF_ERR_STATE, "two evaluations in flight: collect one first");
+    if (distributed(c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
+    const size_t n3 = 3 * (size_t)c.N;
+    if (!c.copy) MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking));
+    Ctx::Stage& S = c.stage[c.stage_next];
+    if (!S.h_scal) {
+        MDF_CUDA_TRY(cudaHostAlloc((void**)&S.h_scal, sizeof(unsigned long long) * NUM_SCAL, cudaHostAllocMapped));
+        memset(S.h_scal, 0, sizeof(unsigned long long) * NUM_SCAL);
+        MDF_CUDA_TRY(cudaHostGetDevicePointer((void**)&S.d_hscal, S.h_scal, 0));
+        for (cudaEvent_t* e : {&S.h2d, &S.consumed, &S.done, &S.d2h})
+            MDF_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+    S.xyz.alloc(n3);
+    S.forces.alloc(n3);
+    // positions in: the stage buffer is free once the stage's last evaluation copied it
+    MDF_CUDA_TRY(cudaStreamWaitEvent(c.copy, S.consumed, 0));
+    MDF_CUDA_TRY(cudaMemcpyAsync(S.xyz.p, xyz, sizeof(double) * n3, cudaMemcpyHostToDevice, c.copy));
+    MDF_CUDA_TRY(cudaEventRecord(S.h2d, c.copy));
+    MDF_CUDA_TRY(cudaStreamWaitEvent(c.stream, S.h2d, 0));
+    MDF_CUDA_TRY(cudaMemcpyAsync(c.xyz.p, S.xyz.p, sizeof(double) * n3, cudaMemcpyDeviceToDevice, c.stream));
+    MDF_CUDA_TRY(cudaEventRecord(S.consumed, c.stream));
+    c.have_positions = true;
+    // the evaluation, finalising into the stage (after its last forces left)
+    c.fin_forces = S.forces.p;
+    c.fin_hscal = S.d_hscal;
+    c.fin_wait = S.d2h;
+    try {
+        eval_async_impl(c, flags);
+    } catch (...) {
+        c.fin_forces = nullptr; c.fin_hscal = nullptr; c.fin_wait = nullptr;
+        c.need_clear = true;
+        throw;
+    }
+    c.fin_forces = nullptr; c.fin_hscal = nullptr; c.fin_wait = nullptr;
+    c.pending = false;   // results belong to the stage, not to mdf_fetch
+    MDF_CUDA_TRY(cudaEventRecord(S.done, c.stream));
+    // forces out
+    MDF_CUDA_TRY(cudaStreamWaitEvent(c.copy, S.done, 0));
+    if (forces_out)
+        MDF_CUDA_TRY(cudaMemcpyAsync(forces_out, S.forces.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, c.copy));
+    MDF_CUDA_TRY(cudaEventRecord(S.d2h, c.copy));
+    S.flags = flags;
+    c.stage_next ^= 1;
+    ++c.inflight;
+}
+
+static void collect(Ctx& c, mdf_energies* e_out)
+{
+    if (c.inflight == 0) throw ApiError(MDF_ERR_STATE, "no submitted evaluation to collect");
+    Ctx::Stage& S = c.stage[c.stage_old];
+    c.stage_old ^= 1;
+    --c.inflight;
+    MDF_CUDA_TRY(cudaEventSynchronize(S.d2h));
+    check_status_word(S.h_scal);
+    if (e_out) host_energies_from(c, S.h_scal, S.flags, e_out);
 }
 
 }  // namespace mdf
@@ -595,7 +766,7 @@ void mdf_destroy(mdf_ctx* ctx)
     cudaSetDevice(c.device);
     if (c.stream) cudaStreamSynchronize(c.stream);
     for (auto& e : c.evpool) cudaEventDestroy(e);
-    c.q.release(); c.type.release(); c.ljAB.release(); c.ljAB4_f.release(); c.ljAB_f.release(); c.lj14AB.release(); c.ljvalid.release();
+    c.q.release(); c.type.release(); c.ljAB.release(); c.ljAB4_f.release(); c.ljAB4_d.release(); c.ljAB_f.release(); c.lj14AB.release(); c.ljvalid.release();
     c.bond_atoms.release(); c.ub_atoms.release(); c.angle_atoms.release(); c.dih_atoms.release();
     c.imp_atoms.release(); c.cmap_atoms.release(); c.cmap_set.release(); c.bond_par.release(); c.ub_par.release();
     c.angle_par.release(); c.imp_par.release(); c.dih_par.release(); c.cmap_coeff.release();
@@ -605,6 +776,8 @@ void mdf_destroy(mdf_ctx* ctx)
     c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
     c.ilist.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
     c.plist_in.release(); c.ilist_in.release(); c.n_in.release(); c.cur_lo.release(); c.cur_hi.release();
+    c.q_slab.release(); c.pme_slab.release(); c.pme_send.release(); c.pme_recv.release(); c.pme_rslab.release();
+    c.f_stage.release(); c.f_mine.release(); c.f_out_blk.release(); c.f_out_all.release();
     c.f_atom.release(); c.scal.release(); c.npairs_dev.release(); c.forces_out.release(); c.forces_pme_ref.release();
     c.qgrid.release(); c.cgrid_f.release(); c.cgrid_d.release(); c.rgrid_f.release();
     c.rgrid_d.release(); c.infl_f.release(); c.infl_d.release();
@@ -613,6 +786,17 @@ void mdf_destroy(mdf_ctx* ctx)
     }
     if (c.h_scal) cudaFreeHost(c.h_scal);
     if (c.h_build) cudaFreeHost(c.h_build);
+    for (auto& S : c.stage) {
+        if (S.h_scal) cudaFreeHost(S.h_scal);
+        for (cudaEvent_t e : {S.h2d, S.consumed, S.done, S.d2h})
+            if (e) cudaEventDestroy(e);
+        S.xyz.release();
+        S.forces.release();
+    }
+    if (c.copy) {
+        cudaStreamSynchronize(c.copy);
+        cudaStreamDestroy(c.copy);
+    }
     c.d_build.release();
     if (c.md_exec) cudaGraphExecDestroy(c.md_exec);
     if (c.md_graph) cudaGraphDestroy(c.md_graph);
@@ -690,6 +874,24 @@ int mdf_fetch(mdf_ctx* ctx, double* forces_out, mdf_energies* e_out)
     return guarded(ctx, [&] {
         MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
         fetch(ctx->c, forces_out, e_out);
+    });
+}
+
+int mdf_submit(mdf_ctx* ctx, uint32_t flags, const double* xyz, double* forces_out)
+{
+    if (!ctx || !xyz) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        submit(ctx->c, flags, xyz, forces_out);
+    });
+}
+
+int mdf_collect(mdf_ctx* ctx, mdf_energies* e_out)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(ctx->c.device));
+        collect(ctx->c, e_out);
     });
 }
 
@@ -919,6 +1121,20 @@ int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
         cudaEventDestroy(e1);
         c.pending = false;
         c.md_stale = true;   // a recorded dynamics graph holds the old shapes
+    });
+}
+
+int mdf_set_collectives(mdf_ctx* ctx, mdf_reduce_scatter_u64 reduce_scatter, mdf_allgather_bytes allgather,
+                        mdf_alltoall_bytes alltoall, void* user)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        const bool all = reduce_scatter && allgather && alltoall, none = !reduce_scatter && !allgather && !alltoall;
+        if (!all && !none) throw ApiError(MDF_ERR_INVALID, "give all three collectives or none");
+        ctx->c.coll_rs = reduce_scatter;
+        ctx->c.coll_ag = allgather;
+        ctx->c.coll_a2a = alltoall;
+        ctx->c.coll_user = user;
     });
 }
 

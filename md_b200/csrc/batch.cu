@@ -165,7 +165,7 @@ struct MultiArgs {
     std::vector<PackArgs<R>> pack;
     std::vector<PruneArgs<R>> prune;
     std::vector<PairF32Args> pf32;
-    std::vector<PairArgs<R>> p64;
+    std::vector<PairF64Args> p64;
     std::vector<ExclArgs> excl;
     std::vector<Pair14Args> p14;
     std::vector<BondedArgs> bonded;
@@ -189,7 +189,7 @@ struct MultiDev {
     const PackArgs<R>* pack;
     const PruneArgs<R>* prune;
     const PairF32Args* pf32;
-    const PairArgs<R>* p64;
+    const PairF64Args* p64;
     const ExclArgs* excl;
     const Pair14Args* p14;
     const BondedArgs* bonded;
@@ -230,7 +230,9 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
             M.pf32.push_back(make_pair_f32_args(c, &dyn));
             M.dyn_pairs = std::max(M.dyn_pairs, dyn);
         } else {
-            M.p64.push_back(make_pair_args<R>(c, false));
+            size_t dyn = 0;
+            M.p64.push_back(make_pair_f64_args(c, &dyn));
+            M.dyn_pairs = std::max(M.dyn_pairs, dyn);
         }
         M.excl.push_back(make_excl_args(c));
         M.p14.push_back(make_pair14_args(c));
@@ -344,8 +346,7 @@ void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D)
         if (sizeof(R) == 4)
             launch_pairs_f32_multi(D.pf32, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, b->main);
         else
-            launch_pairs_multi_fp64(reinterpret_cast<const PairArgs<double>*>(D.p64), n, M.gx_pairs, M.threads,
-                                    M.energy, b->main);
+            launch_pairs_f64_multi(D.p64, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, b->main);
         ++k;
     }
     MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, b->ev_join2, 0));

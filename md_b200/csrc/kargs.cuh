@@ -85,6 +85,39 @@ struct PairF32Args {
     unsigned* st;
 };
 
+// Constants and image offsets of the FP64 PHYSICAL pair kernel (the same
+// structure as the FP32 kernel's, in double).
+struct PairConstD {
+    double rc2, alpha, two_a_spi;
+    double inv_sw, rsw_inv, d30, d60;   // switch: x = r inv_sw - rsw_inv; dS/dr = x^2 (d30 + x (d60 + x d30))
+    double uc6, uc12, rc;               // force-shifted LJ
+};
+
+struct ShiftTableD {
+    double v[27][3];
+};
+
+struct PairF64Args {
+    int gx, gy;
+    int nlist;
+    const ILRange* ilist;
+    const PairEntry* plist;
+    const double4* xq;
+    const int* stype;
+    const double4* center;
+    const double4* lj4;     // (A, B, 12A, 6B) per type pair
+    int ntp;
+    int lj_smem;
+    double kc;
+    PairConstD K;
+    ShiftTableD shifts;
+    unsigned long long* fslot;
+    int nslots;
+    unsigned long long* acc;
+    unsigned long long* npairs;
+    unsigned* st;
+};
+
 template <typename R>
 struct PairArgs {
     int gx, gy;
@@ -297,8 +330,9 @@ PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn);
 void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
                             bool use_switch, cudaStream_t s);
 template <typename R> PairArgs<R> make_pair_args(const Ctx& c, bool count);
-void launch_pairs_multi_fp64(const PairArgs<double>* d_args, int nsys, int gx, int threads, bool energy,
-                             cudaStream_t s);
+PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn);
+void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
+                            bool use_switch, cudaStream_t s);
 int pair_threads(const Ctx& c);
 ExclArgs make_excl_args(const Ctx& c);
 Pair14Args make_pair14_args(const Ctx& c);

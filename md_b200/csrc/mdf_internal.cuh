@@ -127,6 +127,7 @@ struct Ctx {
     DevBuf<double2> ljAB;      // [(ntypes+1)^2] pair table (A,B); last row/col = padding type
     DevBuf<float2> ljAB_f;
     DevBuf<float4> ljAB4_f;        // (A, B, 12A, 6B) per type pair, FP32 pair kernel
+    DevBuf<double4> ljAB4_d;       // the same in FP64 (FP64 PHYSICAL pair kernel)
     DevBuf<double2> lj14AB;    // same indexing, 1-4 tables
     DevBuf<int> ljvalid;       // [(ntypes+1)^2] nb != 0
     int ntp = 0;               // ntypes + 1 (padding type appended)
@@ -245,6 +246,18 @@ struct Ctx {
     bool md_ready = false;
     mdf_allreduce_u64 allreduce = nullptr;   // sum over ranks (nranks > 1)
     void* allreduce_user = nullptr;
+    // distributed reciprocal space and force return (mdf_set_collectives)
+    mdf_reduce_scatter_u64 coll_rs = nullptr;
+    mdf_allgather_bytes coll_ag = nullptr;
+    mdf_alltoall_bytes coll_a2a = nullptr;
+    void* coll_user = nullptr;
+    DevBuf<unsigned long long> q_slab;       // this rank's planes of the charge grid [K0p][K1][K2]
+    DevBuf<unsigned char> pme_slab;          // complex slab [K0p][K1][Kc] (float2 / double2)
+    DevBuf<unsigned char> pme_send, pme_recv;   // transpose blocks [nranks][K0p][K1p][Kc]
+    DevBuf<unsigned char> pme_rslab;         // real potential slab [K0p][K1][K2]
+    DevBuf<unsigned long long> f_stage;      // force blocks for the reduce-scatter [nranks][3][Sb]
+    DevBuf<unsigned long long> f_mine;       // this rank's block [3][Sb]
+    DevBuf<double> f_out_blk, f_out_all;     // finished forces: this rank's slots [Sb][3], all slots [nranks*Sb][3]
     cudaGraph_t md_graph = nullptr;
     cudaGraphExec_t md_exec = nullptr;
     int md_graph_steps = 0;
@@ -260,6 +273,23 @@ struct Ctx {
     long long launches = 0;                   // kernels launched by evaluations
 
     bool counted_live = false;           // counted in the per-device live-context table
+
+    // pipelined evaluations (mdf_submit / mdf_collect): two stages, each with
+    // its staged positions, its forces, its mapped scalar block and events
+    struct Stage {
+        DevBuf<double> xyz;                      // positions copied in on the copy stream
+        DevBuf<double> forces;                   // this stage's evaluation writes its forces here
+        unsigned long long* h_scal = nullptr;    // mapped pinned scalar block of this stage
+        unsigned long long* d_hscal = nullptr;
+        cudaEvent_t h2d = nullptr, consumed = nullptr, done = nullptr, d2h = nullptr;
+        uint32_t flags = 0;
+    };
+    cudaStream_t copy = nullptr;         // host <-> device copies of the pipelined path
+    Stage stage[2];
+    int stage_next = 0, stage_old = 0, inflight = 0;
+    double* fin_forces = nullptr;              // k_finalize targets for this evaluation (nullptr: the defaults)
+    unsigned long long* fin_hscal = nullptr;
+    cudaEvent_t fin_wait = nullptr;            // event the stream waits for before k_finalize
 
     // last evaluation bookkeeping
     bool pending = false;
@@ -292,7 +322,9 @@ void launch_finalize(Ctx& c, double* d_forces, bool pme_ref);
 void mark(Ctx& c, const char* name);
 void eval_async_impl(Ctx& c, uint32_t flags);
 void host_energies(const Ctx& c, uint32_t flags, mdf_energies* e_out);
+void host_energies_from(const Ctx& c, const unsigned long long* hs, uint32_t flags, mdf_energies* e_out);
 void check_host_status(const Ctx& c);
+void check_status_word(const unsigned long long* hs);
 void noalloc_forget_device(int device);
 
 int grid_blocks(long long n, int threads);
@@ -305,6 +337,8 @@ inline void rank_slice(const Ctx& c, long long n, long long& lo, long long& hi)
     hi = n * (r + 1) / P;
 }
 inline bool distributed(const Ctx& c) { return c.p.nranks > 1; }
+// nranks > 1 with the reduce-scatter / all-gather / all-to-all collectives
+inline bool slab_mode(const Ctx& c) { return distributed(c) && c.coll_rs && c.coll_ag && c.coll_a2a; }
 inline bool rank0(const Ctx& c) { return !distributed(c) || c.p.rank == 0; }
 // In-place sum over the ranks through the registered collective, on c.stream.
 void allreduce_u64(Ctx& c, unsigned long long* d, long long n);

@@ -453,6 +453,166 @@ __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force_multi(const P
 }
 #undef MDF_PF32_UNPACK
 
+// ------------------------------------------------ FP64 PHYSICAL pair kernel
+// The FP32 kernel's structure in double precision: the same warp layout and
+// lane rotation, j clusters staged twice in shared memory (compile-time
+// offsets), the lane's mask row rotated once per entry, branch-free
+// selection of the inactive pairs, an (A, B, 12A, 6B) table in shared memory
+// and constants folded on the host.  The arithmetic differs only where
+// precision does: FP64 rsqrt, exp and erfc (the CUDA math library) instead of
+// the SFU forms and the A&S erfc, and FP64 image offsets from FP64 centres.
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
+{
+    extern __shared__ double4 s_lj_d[];
+    __shared__ double4 sx[NB_WARPS][4][2 * CLUSTER];
+    __shared__ int stj[NB_WARPS][4][2 * CLUSTER];
+    __shared__ double sh[27][3];
+    const int nlist = A.nlist;
+    const ILRange* __restrict__ ilist = A.ilist;
+    const PairEntry* __restrict__ plist = A.plist;
+    const double4* __restrict__ xq = A.xq;
+    const int* __restrict__ stype = A.stype;
+    const double4* __restrict__ center = A.center;
+    const int ntp = A.ntp;
+    unsigned long long* __restrict__ fslot = A.fslot;
+    const int nslots = A.nslots;
+    unsigned* st = A.st;
+    const PairConstD K = A.K;
+    for (int k = threadIdx.x; k < 27 * 3; k += blockDim.x) sh[k / 3][k % 3] = A.shifts.v[k / 3][k % 3];
+    if (A.lj_smem)
+        for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj_d[k] = A.lj4[k];
+    __syncthreads();
+    const double4* __restrict__ ljt = A.lj_smem ? s_lj_d : A.lj4;
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int w = blockIdx.x * (blockDim.x >> 5) + wib;
+    const int jslot = lane >> 3, ii = lane & 7;
+    const unsigned FULL = 0xffffffffu;
+    double e_lj = 0, e_dir = 0;
+    int npc = 0;
+    double fix = 0, fiy = 0, fiz = 0;
+
+    if (w < nlist) {
+        const ILRange L = ilist[w];
+        const int I = L.i;
+        const double4 xi = xq[I * CLUSTER + ii];
+        const int trow = stype[I * CLUSTER + ii] * ntp;
+        const double4 cI = center[I];
+        const double qik = A.kc * xi.w;
+        const double qik2 = qik * K.two_a_spi;
+        const int rot_src = (lane & ~7) | ((ii + 1) & 7);
+        for (int b = 0; b < L.count; b += 4) {
+            const int e = b + jslot;
+            PairEntry pe;
+            if (e < L.count) {
+                pe = plist[L.start + e];
+            } else {
+                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+            }
+            const int J = pe.j;
+            const double4 xjj = xq[J * CLUSTER + ii];
+            const int tjj = stype[J * CLUSTER + ii];
+            sx[wib][jslot][ii] = xjj;
+            sx[wib][jslot][ii + CLUSTER] = xjj;
+            stj[wib][jslot][ii] = tjj;
+            stj[wib][jslot][ii + CLUSTER] = tjj;
+            const double4 cJ = center[J];
+            const double* s3 = sh[pe.shift];
+            const double xix = xi.x + ((cI.x - cJ.x) - s3[0]);
+            const double xiy = xi.y + ((cI.y - cJ.y) - s3[1]);
+            const double xiz = xi.z + ((cI.z - cJ.z) - s3[2]);
+            const unsigned rowm = (unsigned)(pe.mask >> (ii * 8)) & 0xffu;
+            const unsigned rot = ((rowm >> ii) | (rowm << (8 - ii))) & 0xffu;
+            __syncwarp();
+            double fjx = 0, fjy = 0, fjz = 0, el = 0, ed = 0;
+            const double4* __restrict__ sxl = &sx[wib][jslot][ii];
+            const int* __restrict__ stl = &stj[wib][jslot][ii];
+#pragma unroll
+            for (int t = 0; t < CLUSTER; ++t) {
+                const double4 xj = sxl[t];
+                const double dx = xix - xj.x, dy = xiy - xj.y, dz = xiz - xj.z;
+                const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
+                const double rinv = rsqrt(r2);
+                const double r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
+                const double4 ab = ljt[trow + stl[t]];      // A, B, 12A, 6B
+                double U = rinv6 * fma(ab.x, rinv6, -ab.y);
+                double G = (rinv6 * rinv2) * fma(ab.z, rinv6, -ab.w);
+                if (SWITCH) {
+                    const double x = fmax(0.0, fma(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
+                    const double S = fma(x2 * x, fma(x, fma(x, -6.0, 15.0), -10.0), 1.0);
+                    const double dSr = x2 * fma(x, fma(x, K.d30, K.d60), K.d30) * rinv;   // dS/dr / r
+                    G = fma(S, G, -U * dSr);
+                    U = U * S;
+                } else {
+                    const double uc = ab.x * K.uc12 - ab.y * K.uc6;
+                    const double gc = (ab.z * K.uc12 - ab.w * K.uc6) / K.rc2;
+                    U = U - uc + (r - K.rc) * (gc * K.rc);
+                    G = G - gc * K.rc * rinv;
+                }
+                const double ar = K.alpha * r;
+                const double ex = exp(-ar * ar);
+                const double ec = (qik * xj.w) * erfc(ar) * rinv;
+                double g = fma(fma(qik2 * xj.w, ex, ec), rinv2, G);
+                g = on ? g : 0.0;
+                if (ENERGY) {
+                    el += on ? U : 0.0;
+                    ed += on ? ec : 0.0;
+                }
+                if (COUNT) npc += on ? 1 : 0;
+                fix = fma(g, dx, fix); fiy = fma(g, dy, fiy); fiz = fma(g, dz, fiz);
+                fjx = fma(-g, dx, fjx); fjy = fma(-g, dy, fjy); fjz = fma(-g, dz, fjz);
+                fjx = __shfl_sync(FULL, fjx, rot_src);
+                fjy = __shfl_sync(FULL, fjy, rot_src);
+                fjz = __shfl_sync(FULL, fjz, rot_src);
+            }
+            if (ENERGY) {
+                e_lj += el;
+                e_dir += ed;
+            }
+            if (e < L.count && (fjx != 0.0 || fjy != 0.0 || fjz != 0.0)) {
+                const int sl = J * CLUSTER + ii;
+                fx_add(fslot + sl, fjx, FORCE_SCALE, st);
+                fx_add(fslot + nslots + sl, fjy, FORCE_SCALE, st);
+                fx_add(fslot + 2 * nslots + sl, fjz, FORCE_SCALE, st);
+            }
+            __syncwarp();
+        }
+        fix += __shfl_xor_sync(FULL, fix, 8); fix += __shfl_xor_sync(FULL, fix, 16);
+        fiy += __shfl_xor_sync(FULL, fiy, 8); fiy += __shfl_xor_sync(FULL, fiy, 16);
+        fiz += __shfl_xor_sync(FULL, fiz, 8); fiz += __shfl_xor_sync(FULL, fiz, 16);
+        if (jslot == 0) {
+            const int sl = I * CLUSTER + ii;
+            fx_add(fslot + sl, fix, FORCE_SCALE, st);
+            fx_add(fslot + nslots + sl, fiy, FORCE_SCALE, st);
+            fx_add(fslot + 2 * nslots + sl, fiz, FORCE_SCALE, st);
+        }
+    }
+    if (ENERGY) {
+        const double v[2] = {e_lj, e_dir};
+        const int idx[2] = {MDF_E_VDW, MDF_E_EE_DIRECT};
+        block_acc_fixed<2>(v, A.acc, idx, ENERGY_SCALE, st);
+    }
+    if (COUNT) {
+        long long np = warp_sum_ll((long long)npc);
+        if (lane == 0 && np) atomicAdd(A.npairs, (unsigned long long)np);
+    }
+}
+
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f64(PairF64Args A)
+{
+    pairs_f64_body<ENERGY, SWITCH, COUNT>(A);
+}
+
+template <bool ENERGY, bool SWITCH>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f64_multi(const PairF64Args* __restrict__ As)
+{
+    const PairF64Args& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs_f64_body<ENERGY, SWITCH, false>(A);
+}
+
 // --------------------------------------------------------------- FP64 pairs
 __device__ __forceinline__ void pair_vec(const double* __restrict__ xyz, int a, int b, const NBParams& P,
                                          double d[3])
@@ -720,13 +880,6 @@ static void launch_pairs_t(Ctx& c, bool energy)
     c.launches += 1;
 }
 
-void launch_pairs_multi_fp64(const PairArgs<double>* d_args, int nsys, int gx, int threads, bool energy,
-                             cudaStream_t s)
-{
-    if (energy) k_pairs_multi<double, MDF_SEM_PHYSICAL, true><<<dim3(gx, 1, nsys), threads, 0, s>>>(d_args);
-    else k_pairs_multi<double, MDF_SEM_PHYSICAL, false><<<dim3(gx, 1, nsys), threads, 0, s>>>(d_args);
-    MDF_CUDA_TRY(cudaGetLastError());
-}
 
 ShiftTable make_shift_table(const Ctx& c)
 {
@@ -831,6 +984,105 @@ void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int thr
     MDF_CUDA_TRY(cudaGetLastError());
 }
 
+// FP64 pair-kernel arguments (PHYSICAL) of this rank's i clusters; *dyn gets
+// the dynamic shared memory of the LJ table (0 when it stays in global memory).
+PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn)
+{
+    PairF64Args A;
+    const NBParams P = make_params(c);
+    for (int code = 0; code < 27; ++code) {
+        const int sv[3] = {code % 3 - 1, (code / 3) % 3 - 1, code / 9 - 1};
+        for (int d = 0; d < 3; ++d) A.shifts.v[code][d] = sv[d] * c.box[d];
+    }
+    PairConstD& K = A.K;
+    K.rc2 = P.rc2;
+    K.alpha = P.alpha;
+    K.two_a_spi = 2.0 * P.alpha / 1.7724538509055160273;
+    K.inv_sw = P.inv_sw;
+    K.rsw_inv = P.rsw * P.inv_sw;
+    K.d30 = -30.0 * P.inv_sw;
+    K.d60 = 60.0 * P.inv_sw;
+    K.uc6 = P.ucut_pow6;
+    K.uc12 = P.ucut_pow12;
+    K.rc = P.rc;
+    const size_t lj_bytes = sizeof(double4) * (size_t)c.ntp * c.ntp;
+    A.lj_smem = lj_bytes <= 96 * 1024 ? 1 : 0;
+    if (dyn) *dyn = A.lj_smem ? lj_bytes : 0;
+    const int wpb = pair_warps(c);
+    long long lo, hi;
+    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    A.nlist = (int)(hi - lo);
+    A.gx = grid_blocks(A.nlist, wpb);
+    A.gy = 1;
+    const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
+    A.ilist = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
+    A.plist = pruned ? c.plist_in.p : c.plist.p;
+    A.xq = c.xq_d.p;
+    A.stype = c.slot_type.p;
+    A.center = c.center.p;
+    A.lj4 = c.ljAB4_d.p;
+    A.ntp = c.ntp;
+    A.kc = P.kc;
+    A.fslot = c.f_slot.p;
+    A.nslots = c.n_slots;
+    A.acc = c.acc.p;
+    A.npairs = c.npairs_dev.p;
+    A.st = c.status.p;
+    return A;
+}
+
+// The table above 48 KB needs the opt-in dynamic shared memory size.
+template <typename KernelT>
+static void allow_smem(KernelT* k, size_t dyn)
+{
+    if (dyn > 48 * 1024)
+        MDF_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+}
+
+static void launch_pairs_f64(Ctx& c, bool energy)
+{
+    const bool count = begin_pair_count(c);
+    size_t dyn = 0;
+    const PairF64Args A = make_pair_f64_args(c, &dyn);
+    if (A.nlist == 0) return;
+    const int th = 32 * pair_warps(c);
+    const bool sw = c.p.switch_radius > 0.0;
+#define MDF_PF64(E, S, K_)                                                                                     \
+    do {                                                                                                       \
+        allow_smem(k_pairs_f64<E, S, K_>, dyn);                                                                \
+        k_pairs_f64<E, S, K_><<<grid_of(A), th, dyn, c.stream>>>(A);                                           \
+    } while (0)
+#define MDF_PF64_K(E, S) \
+    do { if (count) MDF_PF64(E, S, true); else MDF_PF64(E, S, false); } while (0)
+    if (energy) {
+        if (sw) MDF_PF64_K(true, true); else MDF_PF64_K(true, false);
+    } else {
+        if (sw) MDF_PF64_K(false, true); else MDF_PF64_K(false, false);
+    }
+#undef MDF_PF64_K
+#undef MDF_PF64
+    MDF_CUDA_TRY(cudaGetLastError());
+    c.launches += 1;
+}
+
+void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
+                            bool use_switch, cudaStream_t s)
+{
+    const dim3 g(gx, 1, nsys);
+#define MDF_PF64M(E, S)                                                                                        \
+    do {                                                                                                       \
+        allow_smem(k_pairs_f64_multi<E, S>, dyn);                                                              \
+        k_pairs_f64_multi<E, S><<<g, threads, dyn, s>>>(d_args);                                               \
+    } while (0)
+    if (energy) {
+        if (use_switch) MDF_PF64M(true, true); else MDF_PF64M(true, false);
+    } else {
+        if (use_switch) MDF_PF64M(false, true); else MDF_PF64M(false, false);
+    }
+#undef MDF_PF64M
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+
 void launch_nonbonded(Ctx& c, bool energy)
 {
     if (c.n_clusters == 0) return;
@@ -839,7 +1091,7 @@ void launch_nonbonded(Ctx& c, bool energy)
         if (phys) launch_pairs_f32(c, energy);
         else launch_pairs_t<float, MDF_SEM_REFERENCE>(c, energy);
     } else {
-        if (phys) launch_pairs_t<double, MDF_SEM_PHYSICAL>(c, energy);
+        if (phys) launch_pairs_f64(c, energy);
         else launch_pairs_t<double, MDF_SEM_REFERENCE>(c, energy);
     }
 }

@@ -24,6 +24,7 @@
 // is deterministic regardless of atomic ordering.
 #include <algorithm>
 #include <cmath>
+#include <string>
 #include <vector>
 
 #include "kargs.cuh"
@@ -1191,6 +1192,131 @@ static void run_pme(Ctx& c, bool energy)
     c.launches += 7;   // spread, z, y, x+conv, y, z, gather
 }
 
+// ------------------------------------------- distributed reciprocal space
+// x-slab decomposition over nranks (P): rank r owns planes [r K0p, (r+1) K0p)
+// of the charge grid for the z and y passes and the y-range [r K1p, (r+1) K1p)
+// for the x pass and the convolution; K0p = ceil(K0/P), K1p = ceil(K1/P).
+// Transpose blocks are [P][K0p][K1p][Kc]: block t of a rank's send buffer
+// holds its planes restricted to rank t's y-range.
+
+// slab [K0p][K1][Kc] -> blocks [t][x][yl][kc] (y = t K1p + yl; zero past K1)
+template <typename C>
+__global__ void k_slab_to_blocks(const C* __restrict__ slab, C* __restrict__ blocks, int P, int K0p, int K1,
+                                 int K1p, int Kc)
+{
+    const long long n = (long long)P * K0p * K1p * Kc;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int kc = (int)(e % Kc);
+        long long rest = e / Kc;
+        const int yl = (int)(rest % K1p);
+        rest /= K1p;
+        const int x = (int)(rest % K0p);
+        const int t = (int)(rest / K0p);
+        const int y = t * K1p + yl;
+        C v;
+        v.x = 0;
+        v.y = 0;
+        if (y < K1) v = slab[((long long)x * K1 + y) * Kc + kc];
+        blocks[e] = v;
+    }
+}
+
+// blocks [t][x][yl][kc] -> slab [K0p][K1][Kc]
+template <typename C>
+__global__ void k_blocks_to_slab(const C* __restrict__ blocks, C* __restrict__ slab, int K0p, int K1, int K1p, int Kc)
+{
+    const long long n = (long long)K0p * K1 * Kc;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int kc = (int)(e % Kc);
+        const long long rest = e / Kc;
+        const int y = (int)(rest % K1);
+        const int x = (int)(rest / K1);
+        const int t = y / K1p, yl = y - t * K1p;
+        slab[e] = blocks[(((long long)t * K0p + x) * K1p + yl) * Kc + kc];
+    }
+}
+
+static void coll_check(int rc, const char* what)
+{
+    if (rc != 0) throw ApiError(MDF_ERR_CUDA, std::string("the ") + what + " callback failed");
+}
+
+template <typename R>
+static void run_pme_slab(Ctx& c, bool energy)
+{
+    using C = typename CT<R>::type;
+    const int P = c.p.nranks, r = c.p.rank;
+    const int K0 = c.K[0], K1 = c.K[1], K2 = c.K[2], Kc = K2 / 2 + 1;
+    const int K0p = (K0 + P - 1) / P, K1p = (K1 + P - 1) / P;
+    const long long plane = (long long)K1 * K2;
+    const size_t blk = (size_t)K0p * K1p * Kc;
+    // padded to P slabs: the planes past K0 stay zero
+    c.qgrid.alloc((size_t)P * K0p * plane);
+    if (sizeof(R) == 4) c.rgrid_f.alloc((size_t)P * K0p * plane);
+    else c.rgrid_d.alloc((size_t)P * K0p * plane);
+    c.q_slab.alloc((size_t)K0p * plane);
+    c.pme_slab.alloc(sizeof(C) * (size_t)K0p * K1 * Kc);
+    c.pme_send.alloc(sizeof(C) * P * blk);
+    c.pme_recv.alloc(sizeof(C) * P * blk);
+    c.pme_rslab.alloc(sizeof(R) * (size_t)K0p * plane);
+    C* slab = reinterpret_cast<C*>(c.pme_slab.p);
+    C* sendb = reinterpret_cast<C*>(c.pme_send.p);
+    C* recvb = reinterpret_cast<C*>(c.pme_recv.p);
+    R* rslab = reinterpret_cast<R*>(c.pme_rslab.p);
+    const PmeBufs<R> B(c);
+    const int th = 256;
+    MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * (size_t)P * K0p * plane, c.stream));
+    const SpreadArgs S = make_spread_args(c);
+    if (S.s1 > S.s0) k_spread4_rows<R><<<grid_of(S), th, 0, c.stream>>>(S);
+    MDF_CUDA_TRY(cudaGetLastError());
+    coll_check(c.coll_rs(reinterpret_cast<const uint64_t*>(c.qgrid.p), reinterpret_cast<uint64_t*>(c.q_slab.p),
+                         (int64_t)K0p * plane, (void*)c.stream, c.coll_user),
+               "reduce-scatter");
+    mark(c, "pme_spread");
+    FFTChain<R> F = make_fft_chain<R>(c, energy);
+    const int nl = K0p * K1;
+    F.zf.gx = (nl + 2 * F.zf.LP - 1) / (2 * F.zf.LP);
+    F.zf.qgrid = c.q_slab.p;
+    F.zf.cgrid = slab;
+    F.zf.nlines = nl;
+    F.zi = F.zf;
+    F.zi.rgrid = rslab;
+    F.yf.cgrid = slab;
+    F.yf.gy = K0p;
+    F.yi.cgrid = slab;
+    F.yi.gy = K0p;
+    const int ny = std::max(0, std::min(K1p, K1 - r * K1p));   // this rank's y planes
+    F.x.cgrid = recvb;
+    F.x.K1 = K1p;
+    F.x.gy = ny;
+    F.x.infl += (long long)r * K1p * Kc * K0;
+    F.x.my += (long long)r * K1p;
+    k_fft_z_r2c<R><<<grid_of(F.zf), FFT_THREADS, F.smz, c.stream>>>(F.zf);
+    k_fft_y<R><<<grid_of(F.yf), FFT_THREADS, F.smy, c.stream>>>(F.yf);
+    const int nb = (int)std::min<long long>(148 * 8, ((long long)P * blk + th - 1) / th);
+    k_slab_to_blocks<C><<<nb, th, 0, c.stream>>>(slab, sendb, P, K0p, K1, K1p, Kc);
+    MDF_CUDA_TRY(cudaGetLastError());
+    coll_check(c.coll_a2a(sendb, recvb, (int64_t)(sizeof(C) * blk), (void*)c.stream, c.coll_user), "all-to-all");
+    if (ny > 0) {
+        if (energy) k_fft_x_conv<R, true><<<grid_of(F.x), FFT_THREADS, F.smx, c.stream>>>(F.x);
+        else k_fft_x_conv<R, false><<<grid_of(F.x), FFT_THREADS, F.smx, c.stream>>>(F.x);
+    }
+    // back: the x-pass layout [s][x][yl][kc] is already one block per rank
+    coll_check(c.coll_a2a(recvb, sendb, (int64_t)(sizeof(C) * blk), (void*)c.stream, c.coll_user), "all-to-all");
+    k_blocks_to_slab<C><<<nb, th, 0, c.stream>>>(sendb, slab, K0p, K1, K1p, Kc);
+    k_fft_y<R><<<grid_of(F.yi), FFT_THREADS, F.smy, c.stream>>>(F.yi);
+    k_fft_z_c2r<R><<<grid_of(F.zi), FFT_THREADS, F.smz, c.stream>>>(F.zi);
+    MDF_CUDA_TRY(cudaGetLastError());
+    coll_check(c.coll_ag(rslab, B.rg, (int64_t)(sizeof(R) * (size_t)K0p * plane), (void*)c.stream, c.coll_user),
+               "all-gather");
+    mark(c, "pme_fft_conv");
+    const GatherArgs<R> G = make_gather_args<R>(c);
+    if (G.s1 > G.s0) k_gather4<R><<<grid_of(G), th, 0, c.stream>>>(G);
+    MDF_CUDA_TRY(cudaGetLastError());
+    mark(c, "pme_gather");
+    c.launches += 10;   // spread, z, y, pack, x+conv, unpack, y, z, gather (+ memset)
+}
+
 // Many systems: clear the charge grids, spread, the FFT chain, gather.
 template <typename R>
 void launch_pme_multi(const ZeroArgs* d_zero, int zx, const SpreadArgs* d_spread, int sx, const FFTChainDev<R>& D,
@@ -1402,8 +1528,15 @@ void pme_adjoint(Ctx& c, double gE, double)
 
 void launch_pme(Ctx& c, bool energy)
 {
-    if (c.p.semantics == MDF_SEM_PHYSICAL && c.p.precision == MDF_PREC_MIXED) run_pme<float>(c, energy);
-    else run_pme<double>(c, energy);
+    const bool f32 = c.p.semantics == MDF_SEM_PHYSICAL && c.p.precision == MDF_PREC_MIXED;
+    if (slab_mode(c)) {
+        if (f32) run_pme_slab<float>(c, energy);
+        else run_pme_slab<double>(c, energy);
+    } else if (f32) {
+        run_pme<float>(c, energy);
+    } else {
+        run_pme<double>(c, energy);
+    }
 }
 
 }  // namespace mdf

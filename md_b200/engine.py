@@ -19,13 +19,13 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libmdf.so")
 EXPORTS = [
     "mdf_params_default", "mdf_create", "mdf_destroy", "mdf_last_error", "mdf_status_string",
     "mdf_set_positions", "mdf_set_positions_device", "mdf_set_box", "mdf_build_pairlist", "mdf_compute",
-    "mdf_compute_async", "mdf_fetch", "mdf_forces_device", "mdf_get_pme_forces", "mdf_set_stream",
+    "mdf_compute_async", "mdf_fetch", "mdf_submit", "mdf_collect", "mdf_forces_device", "mdf_get_pme_forces", "mdf_set_stream",
     "mdf_pairlist_info", "mdf_enable_timing", "mdf_kernel_times", "mdf_cmap_coefficients",
     "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_probe_l2_reductions", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_host_buffers", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
-    "mdf_pme_grids", "mdf_set_allreduce", "mdf_autotune", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
+    "mdf_pme_grids", "mdf_set_allreduce", "mdf_set_collectives", "mdf_autotune", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
 
@@ -62,6 +62,8 @@ def library(path=None):
     lib.mdf_compute.argtypes = [C.c_void_p, C.c_uint32, dp, C.POINTER(abi.mdf_energies)]
     lib.mdf_compute_async.argtypes = [C.c_void_p, C.c_uint32]
     lib.mdf_fetch.argtypes = [C.c_void_p, dp, C.POINTER(abi.mdf_energies)]
+    lib.mdf_submit.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+    lib.mdf_collect.argtypes = [C.c_void_p, C.POINTER(abi.mdf_energies)]
     lib.mdf_forces_device.argtypes = [C.c_void_p, C.c_void_p]
     lib.mdf_get_pme_forces.argtypes = [C.c_void_p, dp]
     lib.mdf_pme_grids.argtypes = [C.c_void_p, C.POINTER(C.c_int32), dp, dp]
@@ -80,6 +82,8 @@ def library(path=None):
     lib.mdf_minimize.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.POINTER(abi.mdf_min_report)]
     lib.mdf_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(abi.mdf_tune_report)]
     lib.mdf_set_allreduce.argtypes = [C.c_void_p, abi.MDF_ALLREDUCE_FN, C.c_void_p]
+    lib.mdf_set_collectives.argtypes = [C.c_void_p, abi.MDF_REDUCE_SCATTER_FN, abi.MDF_ALLGATHER_FN,
+                                        abi.MDF_ALLTOALL_FN, C.c_void_p]
     lib.mdf_minimize_lbfgs.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32,
                                        C.POINTER(abi.mdf_min_report)]
     lib.mdf_md_init.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_uint64]
@@ -216,6 +220,18 @@ class Engine:
                                          C.byref(e)), "compute")
         return e
 
+    def submit(self, xyz_ptr, forces_ptr, energy=True):
+        """mdf_submit: positions from and forces to raw host pointers (pinned for
+        overlap); returns at once, mdf_collect finishes the oldest."""
+        flags = abi.MDF_COMPUTE_FORCES | (abi.MDF_COMPUTE_ENERGY if energy else 0)
+        self._check(self.lib.mdf_submit(self.h, flags, C.c_void_p(xyz_ptr), C.c_void_p(forces_ptr or None)), "submit")
+
+    def collect(self):
+        """mdf_collect: waits for the oldest submitted evaluation; its energies."""
+        e = abi.mdf_energies()
+        self._check(self.lib.mdf_collect(self.h, C.byref(e)), "collect")
+        return e.as_dict()
+
     def launches(self):
         return int(self.lib.mdf_kernel_launches(self.h))
 
@@ -236,6 +252,20 @@ class Engine:
         one from a torch.distributed group)."""
         self._allreduce_cb = abi.MDF_ALLREDUCE_FN(fn)   # kept alive with the engine
         self._check(self.lib.mdf_set_allreduce(self.h, self._allreduce_cb, None), "set_allreduce")
+
+    def set_collectives(self, reduce_scatter, allgather, alltoall):
+        """The distributed reciprocal space and force return of a split context
+        (mdf_set_collectives): three callbacks (md_b200.distributed builds them
+        from a torch.distributed group); None for all three goes back to the
+        all-reduce form."""
+        if reduce_scatter is None:
+            self._coll_cb = None
+            self._check(self.lib.mdf_set_collectives(self.h, abi.MDF_REDUCE_SCATTER_FN(), abi.MDF_ALLGATHER_FN(),
+                                                     abi.MDF_ALLTOALL_FN(), None), "set_collectives")
+            return
+        self._coll_cb = (abi.MDF_REDUCE_SCATTER_FN(reduce_scatter), abi.MDF_ALLGATHER_FN(allgather),
+                         abi.MDF_ALLTOALL_FN(alltoall))   # kept alive with the engine
+        self._check(self.lib.mdf_set_collectives(self.h, *self._coll_cb, None), "set_collectives")
 
     def set_box(self, box):
         b = np.ascontiguousarray(box, dtype=np.float64)

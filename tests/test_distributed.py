@@ -6,7 +6,8 @@ place across the ranks, two's-complement wrap-around included.
 
 GPU (gloo, 2 and 3 ranks sharing cuda:0; the collectives run on the host,
 no kernel waits on another rank): every rank ends with forces identical bit
-for bit to one context evaluating everything, mixed and FP64, on the first
+for bit to one context evaluating everything - with the all-reduce form and
+with the slab-distributed reciprocal space and reduce-scatter force return - mixed and FP64, on the first
 evaluation after a list build (pair counting on) and the next; energies agree
 to 1e-12 relative + 1e-8 (per-block FP64 sums are rounded to the 2^-32
 fixed point before they are added, and the blocks differ) and the pair count
@@ -71,7 +72,7 @@ def test_allreduce_callback_two_rank_gloo_cpu():
         assert vals == [3, -3000, wrap, 14]
 
 
-def _eval_worker(rank, world, port, q, cfg, prec):
+def _eval_worker(rank, world, port, q, cfg, prec, slab=False):
     from md_b200 import distributed, engine, synth
     from tests import helpers as H
     dist = _init(rank, world, port)
@@ -80,6 +81,8 @@ def _eval_worker(rank, world, port, q, cfg, prec):
     eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=prec, ewald_tol=1e-5,
                         grid=synth.GRIDS[cfg], rank=rank, nranks=world)
     eng.set_allreduce(distributed.torch_allreduce())
+    if slab:
+        eng.set_collectives(*distributed.torch_collectives())
     eng.set_positions(s.coords)
     eng.build_pairlist()
     out = []
@@ -113,6 +116,25 @@ def _single(cfg, prec):
                                             ("c0", 2, abi.MDF_PREC_MIXED)])
 def test_split_evaluation_matches_one_context(cfg, world, prec):
     res = _run(_eval_worker, world, cfg, prec)
+    ref = _single(cfg, prec)
+    for out in res:
+        for (E, F, npair), (E0, F0, np0) in zip(out, ref):
+            assert np.array_equal(F, F0)
+            assert npair == np0
+            for k in abi.E_NAMES + ["total"]:
+                assert abs(E[k] - E0[k]) <= 1e-12 * abs(E0[k]) + 1e-8, (k, E[k], E0[k])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg,world,prec", [("small", 2, abi.MDF_PREC_MIXED), ("small", 3, abi.MDF_PREC_FP64),
+                                            ("c0", 2, abi.MDF_PREC_MIXED), ("c0", 3, abi.MDF_PREC_MIXED)])
+def test_slab_pme_and_force_scatter_match_one_context(cfg, world, prec):
+    """With mdf_set_collectives the reciprocal space is distributed as x-slabs
+    (reduce-scatter of the charge grid, all-to-all transposes around the x
+    pass, all-gather of the potential) and the forces return by reduce-scatter
+    and all-gather: forces still equal one context's bit for bit, energies to
+    1e-12 relative + 1e-8 (3 ranks: grids whose planes do not divide evenly)."""
+    res = _run(_eval_worker, world, cfg, prec, True)
     ref = _single(cfg, prec)
     for out in res:
         for (E, F, npair), (E0, F0, np0) in zip(out, ref):

@@ -357,3 +357,33 @@ def test_c4_960k_atoms_fp64_and_mixed_match_o2():
     assert H.frel(Fmx, F64) <= 1e-5, H.frel(Fmx, F64)
     tot2 = sum(e2[abi.E_INDEX[k]] for k in E_PHYS_TERMS)
     assert H.rel(Emx["total"], tot2) < 1e-6
+
+
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_pipelined_submit_collect_equals_compute(prec):
+    """mdf_submit / mdf_collect with two evaluations in flight (positions in and
+    forces out on the copy stream) give mdf_compute's forces and energies bit
+    for bit, each evaluation at its own positions."""
+    import torch
+    s = H.system("small")
+    eng, flat = make_engine(s, PHYS, prec, (32, 32, 32))
+    rng = np.random.default_rng(11)
+    frames = [s.coords + rng.uniform(-0.05, 0.05, s.coords.shape) for _ in range(5)]
+    ref = []
+    for x in frames:
+        eng.set_positions(x)
+        ref.append(eng.compute())
+    xs = [torch.from_numpy(np.ascontiguousarray(x.reshape(-1))).pin_memory() for x in frames]
+    fs = [torch.empty(3 * s.natoms, dtype=torch.float64).pin_memory() for _ in frames]
+    out = []
+    eng.submit(xs[0].data_ptr(), fs[0].data_ptr())
+    for k in range(1, len(frames)):
+        eng.submit(xs[k].data_ptr(), fs[k].data_ptr())
+        out.append(eng.collect())
+    out.append(eng.collect())
+    for k, (E, F) in enumerate(ref):
+        assert np.array_equal(fs[k].numpy().reshape(-1, 3), F), k
+        assert all(out[k][t] == E[t] for t in E_PHYS_TERMS), k
+    with pytest.raises(engine.MDFError):
+        eng.collect()                 # nothing in flight
+    eng.close()

@@ -38,8 +38,9 @@ Multi-GPU (torchrun): each rank evaluates its own replica of the system (no
 data-path collective: a single 100k-atom system is not sharded), timings are
 max-reduced over ranks and value is the whole-job rate (weak scaling).  The
 c3 batch is sharded over the ranks by estimated cost, and c4_split times one
-c4 evaluation split over all ranks (int64 NCCL all-reduces through
-mdf_set_allreduce) against one GPU.
+c4 evaluation split over all ranks (x-slab PME with NCCL reduce-scatter,
+all-to-all and all-gather through mdf_set_collectives; energies by
+all-reduce) against one GPU.
 """
 from __future__ import annotations
 
@@ -369,9 +370,10 @@ def cufft_check(eng, dev, s, ours_ms, reps=20):
 
 def split_bench(dev, ws, rank, cfg="c4", steps=20, warmup=3):
     """c4 (960k atoms, PME 216^3; `cfg` another named workload) evaluated by all ranks together: each rank
-    takes its share of the pair, bonded and PME spread/gather work and the
-    int64 charge grid and accumulators are summed with NCCL all-reduces
-    (mdf_params.rank / nranks + mdf_set_allreduce).  Time: CUDA events on each
+    takes its share of the pair, bonded and PME spread/gather work, the
+    reciprocal space is distributed as x-slabs of the grid and the forces
+    come back by reduce-scatter + all-gather (mdf_params.rank / nranks,
+    mdf_set_allreduce + mdf_set_collectives, NCCL).  Time: CUDA events on each
     rank's stream around `steps` evaluations, max over ranks.  Rank 0 also
     times one context doing the whole evaluation, for the speed-up."""
     import torch
@@ -409,10 +411,12 @@ def split_bench(dev, ws, rank, cfg="c4", steps=20, warmup=3):
 
     eng = engine.Engine(flat, s.box, rank=rank, nranks=ws, **kw)
     eng.set_allreduce(distributed.torch_allreduce())
+    eng.set_collectives(*distributed.torch_collectives())
     t_split = timed(eng, True)
     eng.close()
     out = {"workload": "%s: %d atoms, PME %s, cutoff 10 A, mixed precision; one evaluation split over %d ranks "
-                       "(int64 all-reduce of the charge grid and the force/energy accumulators)"
+                       "(x-slab PME: reduce-scatter of the charge grid, all-to-all transposes around the x pass, "
+                       "all-gather of the potential; forces by reduce-scatter + all-gather; energies all-reduced)"
                        % (cfg, s.natoms, "x".join(map(str, synth.GRIDS[cfg])), ws),
            "n_ranks": ws, "evals_per_s": steps / t_split, "ms_per_eval": t_split / steps * 1e3}
     if rank == 0:

@@ -9,7 +9,8 @@
 //                                return at once.
 // A system's blocks run the same code on the same data in both forms, so a
 // batch launch reproduces the single-system results bit for bit (energies
-// included: each block sums the same terms in the same order).
+// included: each block, or each i cluster in the persistent pair kernels,
+// sums the same terms in the same order).
 #pragma once
 
 #include "mdf_device.cuh"
@@ -82,6 +83,7 @@ struct PairF32Args {
     int nslots;
     unsigned long long* acc;
     unsigned long long* npairs;
+    unsigned long long* next;   // work counter of the persistent warps, zero at launch
     unsigned* st;
 };
 
@@ -115,6 +117,7 @@ struct PairF64Args {
     int nslots;
     unsigned long long* acc;
     unsigned long long* npairs;
+    unsigned long long* next;   // work counter of the persistent warps, zero at launch
     unsigned* st;
 };
 

@@ -20,7 +20,8 @@ constexpr double GRID_SCALE = 1099511627776.0;        // 2^40 fixed point for PM
 constexpr double GRID_ISCALE = 1.0 / 1099511627776.0;
 constexpr int NUM_ACC = MDF_E_COUNT + 6;   // energies + 6 virial components
 constexpr int ACC_VIR = MDF_E_COUNT;
-constexpr int NUM_SCAL = NUM_ACC + 2;      // + pairs in cutoff + status word
+constexpr int NUM_SCAL = NUM_ACC + 3;      // + pairs in cutoff + status word + pair-kernel work counter
+constexpr int SCAL_WORK = NUM_ACC + 2;     // work counter of the persistent pair kernels (cleared with the block)
 
 // device status bits
 enum : unsigned {

@@ -20,6 +20,8 @@
 // stay in registers for the whole list; j forces go to int64 fixed-point
 // accumulators once per cluster pair.
 #include <cmath>
+#include <map>
+#include <tuple>
 
 #include "kargs.cuh"
 #include "mdf_device.cuh"
@@ -284,7 +286,8 @@ __device__ __forceinline__ void pairs_f32_body(
     int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
     const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp,
     int lj_smem, float kc, const PairConstF& Kin, const ShiftTable& shifts, unsigned long long* __restrict__ fslot,
-    int nslots, unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs, unsigned* st)
+    int nslots, unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs,
+    unsigned long long* __restrict__ next, unsigned* st)
 {
     const PairConstF K = Kin;   // registers (the multi-system launch reads it from device memory)
     extern __shared__ float4 s_lj[];
@@ -300,14 +303,21 @@ __device__ __forceinline__ void pairs_f32_body(
     __syncthreads();
     const float4* __restrict__ ljt = lj_smem ? s_lj : lj4;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int w = blockIdx.x * (blockDim.x >> 5) + wib;
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
-    double e_lj = 0, e_dir = 0;
     int npc = 0;
-    float fix = 0.f, fiy = 0.f, fiz = 0.f;
-
-    if (w < nlist) {
+    // Persistent warps: each takes the next i cluster from the work counter
+    // until the list is done, so no SM idles behind a slow block or a
+    // partial last wave.  Energies go to fixed point once per i cluster (a
+    // fixed-order FP64 sum), so they do not depend on which warp took which
+    // cluster.
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = (int)atomicAdd(next, 1ull);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= nlist) break;
+        double e_lj = 0, e_dir = 0;
+        float fix = 0.f, fiy = 0.f, fiz = 0.f;
         const ILRange L = ilist[w];
         const int I = L.i;
         const float4 xi = xq[I * CLUSTER + ii];
@@ -402,11 +412,13 @@ __device__ __forceinline__ void pairs_f32_body(
             fx_add_force_f(fslot + nslots + sl, fiy, st);
             fx_add_force_f(fslot + 2 * nslots + sl, fiz, st);
         }
-    }
-    if (ENERGY) {
-        const double v[2] = {e_lj, e_dir};
-        const int idx[2] = {MDF_E_VDW, MDF_E_EE_DIRECT};
-        block_acc_fixed<2>(v, acc, idx, ENERGY_SCALE, st);
+        if (ENERGY) {
+            const double s_lj = warp_sum(e_lj), s_dir = warp_sum(e_dir);
+            if (lane == 0) {
+                if (s_lj != 0.0) fx_add(acc + MDF_E_VDW, s_lj, ENERGY_SCALE, st);
+                if (s_dir != 0.0) fx_add(acc + MDF_E_EE_DIRECT, s_dir, ENERGY_SCALE, st);
+            }
+        }
     }
     if (COUNT) {
         long long np = warp_sum_ll((long long)npc);
@@ -416,7 +428,7 @@ __device__ __forceinline__ void pairs_f32_body(
 
 #define MDF_PF32_UNPACK(A)                                                                                       \
     A.nlist, A.ilist, A.plist, A.xq, A.stype, A.centerf, A.lj4, A.ntp, A.lj_smem, A.kc, A.K, A.shifts, A.fslot,      \
-        A.nslots, A.acc, A.npairs, A.st
+        A.nslots, A.acc, A.npairs, A.next, A.st
 
 // With energies: the compiler's own register choice (72, three blocks per SM;
 // a 64-register cap spills and is slower).
@@ -485,14 +497,17 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
     __syncthreads();
     const double4* __restrict__ ljt = A.lj_smem ? s_lj_d : A.lj4;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int w = blockIdx.x * (blockDim.x >> 5) + wib;
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
-    double e_lj = 0, e_dir = 0;
     int npc = 0;
-    double fix = 0, fiy = 0, fiz = 0;
-
-    if (w < nlist) {
+    // persistent warps and per-cluster energies, as in the FP32 kernel
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = (int)atomicAdd(A.next, 1ull);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= nlist) break;
+        double e_lj = 0, e_dir = 0;
+        double fix = 0, fiy = 0, fiz = 0;
         const ILRange L = ilist[w];
         const int I = L.i;
         const double4 xi = xq[I * CLUSTER + ii];
@@ -587,11 +602,13 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
             fx_add(fslot + nslots + sl, fiy, FORCE_SCALE, st);
             fx_add(fslot + 2 * nslots + sl, fiz, FORCE_SCALE, st);
         }
-    }
-    if (ENERGY) {
-        const double v[2] = {e_lj, e_dir};
-        const int idx[2] = {MDF_E_VDW, MDF_E_EE_DIRECT};
-        block_acc_fixed<2>(v, A.acc, idx, ENERGY_SCALE, st);
+        if (ENERGY) {
+            const double s_lj = warp_sum(e_lj), s_dir = warp_sum(e_dir);
+            if (lane == 0) {
+                if (s_lj != 0.0) fx_add(A.acc + MDF_E_VDW, s_lj, ENERGY_SCALE, st);
+                if (s_dir != 0.0) fx_add(A.acc + MDF_E_EE_DIRECT, s_dir, ENERGY_SCALE, st);
+            }
+        }
     }
     if (COUNT) {
         long long np = warp_sum_ll((long long)npc);
@@ -813,6 +830,35 @@ static int pair_warps(const Ctx& c)
     return (w == 2 || w == 4 || w == 8) ? w : NB_WARPS;
 }
 
+// Blocks of a persistent pair kernel: as many as stay resident on the device
+// at once (SMs x resident blocks per SM for this kernel, block size and
+// shared memory), cached per kernel and launch shape.
+int persistent_blocks(const void* fn, int threads, size_t dyn)
+{
+    struct Key {
+        const void* fn;
+        int threads;
+        size_t dyn;
+        int dev;
+        bool operator<(const Key& o) const
+        {
+            return std::tie(fn, threads, dyn, dev) < std::tie(o.fn, o.threads, o.dyn, o.dev);
+        }
+    };
+    static thread_local std::map<Key, int> cache;
+    int dev = 0;
+    MDF_CUDA_TRY(cudaGetDevice(&dev));
+    const Key k{fn, threads, dyn, dev};
+    auto it = cache.find(k);
+    if (it != cache.end()) return it->second;
+    int sms = 0, per = 0;
+    MDF_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    MDF_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, dyn));
+    const int n = std::max(1, sms * std::max(1, per));
+    cache[k] = n;
+    return n;
+}
+
 int pair_threads(const Ctx& c)
 {
     return 32 * pair_warps(c);
@@ -940,6 +986,7 @@ PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn)
     A.nslots = c.n_slots;
     A.acc = c.acc.p;
     A.npairs = c.npairs_dev.p;
+    A.next = c.scal.p + SCAL_WORK;
     A.st = c.status.p;
     return A;
 }
@@ -954,8 +1001,10 @@ static void launch_pairs_f32(Ctx& c, bool energy)
     const bool sw = c.p.switch_radius > 0.0;
 #define MDF_PF32(E, S, K_)                                                                                     \
     do {                                                                                                       \
-        if (E) k_pairs_f32<S, K_><<<grid_of(A), th, dyn, c.stream>>>(A);                                         \
-        else k_pairs_f32_force<S, K_><<<grid_of(A), th, dyn, c.stream>>>(A);                                     \
+        const void* fn = (E) ? (const void*)k_pairs_f32<S, K_> : (const void*)k_pairs_f32_force<S, K_>;        \
+        const int nb = std::min(A.gx, persistent_blocks(fn, th, dyn));                                          \
+        if (E) k_pairs_f32<S, K_><<<nb, th, dyn, c.stream>>>(A);                                                 \
+        else k_pairs_f32_force<S, K_><<<nb, th, dyn, c.stream>>>(A);                                             \
     } while (0)
 #define MDF_PF32_K(E, S) \
     do { if (count) MDF_PF32(E, S, true); else MDF_PF32(E, S, false); } while (0)
@@ -973,14 +1022,17 @@ static void launch_pairs_f32(Ctx& c, bool energy)
 void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
                             bool use_switch, cudaStream_t s)
 {
-    const dim3 g(gx, 1, nsys);
+#define MDF_PF32M(KERN)                                                                                        \
+    do {                                                                                                       \
+        const dim3 g(std::min(gx, persistent_blocks((const void*)KERN, threads, dyn)), 1, nsys);                \
+        KERN<<<g, threads, dyn, s>>>(d_args);                                                                  \
+    } while (0)
     if (energy) {
-        if (use_switch) k_pairs_f32_multi<true><<<g, threads, dyn, s>>>(d_args);
-        else k_pairs_f32_multi<false><<<g, threads, dyn, s>>>(d_args);
+        if (use_switch) MDF_PF32M(k_pairs_f32_multi<true>); else MDF_PF32M(k_pairs_f32_multi<false>);
     } else {
-        if (use_switch) k_pairs_f32_force_multi<true><<<g, threads, dyn, s>>>(d_args);
-        else k_pairs_f32_force_multi<false><<<g, threads, dyn, s>>>(d_args);
+        if (use_switch) MDF_PF32M(k_pairs_f32_force_multi<true>); else MDF_PF32M(k_pairs_f32_force_multi<false>);
     }
+#undef MDF_PF32M
     MDF_CUDA_TRY(cudaGetLastError());
 }
 
@@ -1027,6 +1079,7 @@ PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn)
     A.nslots = c.n_slots;
     A.acc = c.acc.p;
     A.npairs = c.npairs_dev.p;
+    A.next = c.scal.p + SCAL_WORK;
     A.st = c.status.p;
     return A;
 }
@@ -1050,7 +1103,8 @@ static void launch_pairs_f64(Ctx& c, bool energy)
 #define MDF_PF64(E, S, K_)                                                                                     \
     do {                                                                                                       \
         allow_smem(k_pairs_f64<E, S, K_>, dyn);                                                                \
-        k_pairs_f64<E, S, K_><<<grid_of(A), th, dyn, c.stream>>>(A);                                           \
+        const int nb = std::min(A.gx, persistent_blocks((const void*)k_pairs_f64<E, S, K_>, th, dyn));          \
+        k_pairs_f64<E, S, K_><<<nb, th, dyn, c.stream>>>(A);                                                   \
     } while (0)
 #define MDF_PF64_K(E, S) \
     do { if (count) MDF_PF64(E, S, true); else MDF_PF64(E, S, false); } while (0)
@@ -1068,11 +1122,12 @@ static void launch_pairs_f64(Ctx& c, bool energy)
 void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
                             bool use_switch, cudaStream_t s)
 {
-    const dim3 g(gx, 1, nsys);
 #define MDF_PF64M(E, S)                                                                                        \
     do {                                                                                                       \
         allow_smem(k_pairs_f64_multi<E, S>, dyn);                                                              \
-        k_pairs_f64_multi<E, S><<<g, threads, dyn, s>>>(d_args);                                               \
+        const dim3 gp(std::min(gx, persistent_blocks((const void*)k_pairs_f64_multi<E, S>, threads, dyn)), 1,  \
+                      nsys);                                                                                   \
+        k_pairs_f64_multi<E, S><<<gp, threads, dyn, s>>>(d_args);                                              \
     } while (0)
     if (energy) {
         if (use_switch) MDF_PF64M(true, true); else MDF_PF64M(true, false);

@@ -97,16 +97,28 @@ def parse():
     ap.add_argument("--no-md", action="store_true")
     ap.add_argument("--no-split", action="store_true", help="skip the c4 evaluation split over the ranks (N > 1)")
     ap.add_argument("--profile", metavar="CONFIG", default=None,
-                    help="profiling run: build CONFIG (tiny, small, c0, c1, c4), run --warmup + --steps "
+                    help="profiling run: build CONFIG (tiny, small, c0, c1, c4, or c3: the batch), run --warmup + --steps "
                          "evaluations, print the per-phase times and exit (for ncu)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     return ap.parse_args()
 
 
 def run_profile(args):
-    """Plain evaluation loop for profilers: no timing bookkeeping of our own."""
+    """Plain evaluation loop for profilers: no timing bookkeeping of our own.
+    c3 runs the 256-system batch (one graph launch per evaluation)."""
     import torch
     from md_b200 import abi, engine, synth, topology
+    if args.profile == "c3":
+        members = make_batch_workload(range(256))
+        ss = [m[0] for m in members]
+        b = engine.Batch([m[1] for m in members], [x.box for x in ss], [x.meta["grid"] for x in ss],
+                         precision=abi.MDF_PREC_MIXED, cutoff=9.0, skin=2.0, switch_radius=8.0, ewald_tol=1e-5)
+        b.set_positions([x.coords for x in ss])
+        for _ in range(args.warmup + args.steps):
+            b.compute(energy=True, forces=True)
+        print(json.dumps({"profile": "c3", "systems": len(ss), "info": b.info()}))
+        b.close()
+        return
     s = synth.make_config(args.profile)
     flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
     prec = abi.MDF_PREC_MIXED if args.precision == "mixed" else abi.MDF_PREC_FP64

@@ -547,10 +547,11 @@ static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
         MDF_CUDA_TRY(cudaMemcpy(forces_out, c.forces_out.p, sizeof(double) * 3 * (size_t)c.N, cudaMemcpyDeviceToHost));
 }
 
-// Pipelined evaluation: the positions go in on the copy stream (into the
+// Pipelined evaluation: the positions go in on one copy stream (into the
 // stage's buffer, then one device copy on the evaluation stream), the
 // evaluation runs on the context's stream and writes the stage's forces and
-// scalar block, and the forces go out on the copy stream.  With two stages the
+// scalar block, and the forces go out on a second copy stream (so the next
+// evaluation's positions never queue behind this one's forces).  With two stages the
 // copies of one evaluation overlap the computation of the other.
 static void submit(Ctx& c, uint32_t flags, const double* xyz, double* forces_out)
 {
@@ -558,6 +559,7 @@ static void submit(Ctx& c, uint32_t flags, const double* xyz, double* forces_out
     if (distributed(c)) throw ApiError(MDF_ERR_UNSUPPORTED, "not available with nranks > 1");
     const size_t n3 = 3 * (size_t)c.N;
     if (!c.copy) MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.copy, cudaStreamNonBlocking));
+    if (!c.copy_out) MDF_CUDA_TRY(cudaStreamCreateWithFlags(&c.copy_out, cudaStreamNonBlocking));
     Ctx::Stage& S = c.stage[c.stage_next];
     if (!S.h_scal) {
         MDF_CUDA_TRY(cudaHostAlloc((void**)&S.h_scal, sizeof(unsigned long long) * NUM_SCAL, cudaHostAllocMapped));
@@ -591,10 +593,11 @@ static void submit(Ctx& c, uint32_t flags, const double* xyz, double* forces_out
     c.pending = false;   // results belong to the stage, not to mdf_fetch
     MDF_CUDA_TRY(cudaEventRecord(S.done, c.stream));
     // forces out
-    MDF_CUDA_TRY(cudaStreamWaitEvent(c.copy, S.done, 0));
+    MDF_CUDA_TRY(cudaStreamWaitEvent(c.copy_out, S.done, 0));
     if (forces_out)
-        MDF_CUDA_TRY(cudaMemcpyAsync(forces_out, S.forces.p, sizeof(double) * n3, cudaMemcpyDeviceToHost, c.copy));
-    MDF_CUDA_TRY(cudaEventRecord(S.d2h, c.copy));
+        MDF_CUDA_TRY(cudaMemcpyAsync(forces_out, S.forces.p, sizeof(double) * n3, cudaMemcpyDeviceToHost,
+                                     c.copy_out));
+    MDF_CUDA_TRY(cudaEventRecord(S.d2h, c.copy_out));
     S.flags = flags;
     c.stage_next ^= 1;
     ++c.inflight;
@@ -793,10 +796,11 @@ void mdf_destroy(mdf_ctx* ctx)
         S.xyz.release();
         S.forces.release();
     }
-    if (c.copy) {
-        cudaStreamSynchronize(c.copy);
-        cudaStreamDestroy(c.copy);
-    }
+    for (cudaStream_t cs : {c.copy, c.copy_out})
+        if (cs) {
+            cudaStreamSynchronize(cs);
+            cudaStreamDestroy(cs);
+        }
     c.d_build.release();
     if (c.md_exec) cudaGraphExecDestroy(c.md_exec);
     if (c.md_graph) cudaGraphDestroy(c.md_graph);

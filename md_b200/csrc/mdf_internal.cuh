@@ -285,7 +285,9 @@ struct Ctx {
         cudaEvent_t h2d = nullptr, consumed = nullptr, done = nullptr, d2h = nullptr;
         uint32_t flags = 0;
     };
-    cudaStream_t copy = nullptr;         // host <-> device copies of the pipelined path
+    cudaStream_t copy = nullptr;         // host -> device copies of the pipelined path
+    cudaStream_t copy_out = nullptr;     // device -> host copies (its own stream, so the next
+                                         // evaluation's positions need not wait behind them)
     Stage stage[2];
     int stage_next = 0, stage_old = 0, inflight = 0;
     double* fin_forces = nullptr;              // k_finalize targets for this evaluation (nullptr: the defaults)

@@ -505,16 +505,16 @@ __device__ __forceinline__ R bspline4_one(R w, int j)
     return v * (R)(1.0 / 6.0);
 }
 
-// Charge spread with 16 lanes per atom: lane (i, j) of the atom's 4 x 4 (x, y)
-// stencil rows adds the row's 4 consecutive z points, so each lane's four
-// int64 reductions fall in one 32-byte sector (two at the periodic z edge)
-// and the 16 lanes of an atom touch 16 distinct rows.  Against one thread per
-// atom (64 reductions scattered over 16 rows by one thread) this keeps more
-// reductions in flight per warp and spreads them over more L2 slices.  Each
-// lane computes only the weights it uses: theta_x[i], theta_y[j] and the four
-// theta_z.  The grid words are identical to the per-atom form's (the same
-// rounded fixed-point values, summed in any order).  Launched with a multiple
-// of 16 threads per block.
+// Charge spread with 16 lanes per atom, four lanes per z run: lane (r, z)
+// of an atom's group adds, in four steps t, the point (x = t, y = r, z) of the
+// atom's 4 x 4 x 4 stencil.  At every step the 16 lanes of an atom hit four
+// (x, y) rows with four consecutive z words each, so the L2 merges the
+// reductions of a row (one or two 32-byte sectors per four words) instead of
+// taking four separate requests from one lane.  Lane 0 of the group computes
+// the atom's grid position and fractional offsets once and shares them.  The
+// grid words are identical to the one-thread-per-atom form's (the same
+// rounded fixed-point values, summed in any order).  Launched with a
+// multiple of 16 threads per block.
 template <typename R>
 __device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A)
 {
@@ -525,48 +525,61 @@ __device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A)
     const GridGeom& g = A.g;
     unsigned long long* __restrict__ qgrid = A.qgrid;
     unsigned* st = A.st;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = s0 + (int)(t >> 4);
-    const int row = (int)(t & 15), i = row >> 2, j = row & 3;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = s0 + (int)(t0 >> 4);
+    const int l = (int)(t0 & 15), r = l >> 2, zz = l & 3;
+    // the whole group of 16 lanes leaves together (same atom)
     if (s >= s1) return;
     const int a = slot_atom[s];
     if (a < 0) return;
     const double qa = q[a];
     if (qa == 0.0) return;
-    int base[3];
+    const unsigned grp = 0xffffu << (threadIdx.x & 16);
+    int base[3] = {0, 0, 0};
+    double u[3] = {0, 0, 0};
+    int bad = 0;
+    if (l == 0) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double v = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
+            if (!(v >= 0.0 && v <= (double)g.K[d])) bad = 1;   // non-finite position
+            if (v >= g.K[d]) v -= g.K[d];
+            const int b = bad ? 0 : min((int)floor(v), g.K[d] - 1);
+            base[d] = b;
+            u[d] = v - b;
+        }
+    }
+    bad = __shfl_sync(grp, bad, 0, 16);
+    if (bad) {
+        if (l == 0) status_set(st, ST_NONFINITE);
+        return;
+    }
     R w[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        double u = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
-        if (!(u >= 0.0 && u <= (double)g.K[d])) {   // non-finite position
-            if (row == 0) status_set(st, ST_NONFINITE);
-            return;
-        }
-        if (u >= g.K[d]) u -= g.K[d];
-        const int b = min((int)floor(u), g.K[d] - 1);
-        base[d] = b;
-        w[d] = (R)(u - b);
+        base[d] = __shfl_sync(grp, base[d], 0, 16);
+        w[d] = (R)__shfl_sync(grp, u[d], 0, 16);
     }
-    int kx = base[0] - 1 + i;
-    kx += (kx < 0) ? g.K[0] : 0;
-    kx -= (kx >= g.K[0]) ? g.K[0] : 0;
-    int ky = base[1] - 1 + j;
+    R thx[4];
+    bspline4<R>(w[0], thx, nullptr);
+    const R thy = bspline4_one<R>(w[1], r), thz = bspline4_one<R>(w[2], zz);
+    int ky = base[1] - 1 + r;
     ky += (ky < 0) ? g.K[1] : 0;
     ky -= (ky >= g.K[1]) ? g.K[1] : 0;
-    const R wxy = (R)qa * bspline4_one<R>(w[0], i) * bspline4_one<R>(w[1], j);
-    R th[4];
-    bspline4<R>(w[2], th, nullptr);
-    unsigned long long* rowp = qgrid + ((long long)kx * g.K[1] + ky) * g.K[2];
+    int kz = base[2] - 1 + zz;
+    kz += (kz < 0) ? g.K[2] : 0;
+    kz -= (kz >= g.K[2]) ? g.K[2] : 0;
+    const R qr = (R)qa;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int kz = base[2] - 1 + k;
-        kz += (kz < 0) ? g.K[2] : 0;
-        kz -= (kz >= g.K[2]) ? g.K[2] : 0;
-        const R v = wxy * th[k];
+    for (int t = 0; t < 4; ++t) {
+        int kx = base[0] - 1 + t;
+        kx += (kx < 0) ? g.K[0] : 0;
+        kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+        const R v = qr * thx[t] * thy * thz;
         long long fx;
         if (sizeof(R) == 4) fx = __float2ll_rn((float)v * 1099511627776.0f);   // exact 2^40 scaling
         else fx = __double2ll_rn((double)v * GRID_SCALE);
-        atomicAdd(rowp + kz, (unsigned long long)fx);
+        atomicAdd(qgrid + ((long long)kx * g.K[1] + ky) * g.K[2] + kz, (unsigned long long)fx);
     }
 }
 

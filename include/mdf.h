@@ -162,6 +162,13 @@ typedef struct {
      * ends with the full forces and energies, bit-identical to one context. */
     int32_t rank;
     int32_t nranks;
+    /* How the pair kernel's warps find their i clusters (results do not
+     * depend on it): 0 = one warp per i cluster over a grid of all of them;
+     * 1 = persistent warps, as many as stay resident, that take the next
+     * i cluster from a work counter (no partial last wave, but they hold
+     * every SM slot until the list is done, so kernels queued beside them
+     * wait).  mdf_autotune picks. */
+    int32_t pair_schedule;
 } mdf_params;
 
 /* Sum of `count` 64-bit integers at d_buf (device memory of the context's
@@ -404,6 +411,8 @@ typedef struct {
     int32_t n_tried;      /* candidates timed */
     double best_ms;       /* one batch evaluation with the chosen shapes */
     double default_ms;    /* ... with the shapes the batch was created with */
+    int32_t pair_schedule;
+    int32_t reserved;
 } mdf_tune_report;
 
 int mdf_batch_create(int nsys, const mdf_topology *const *topos, const mdf_params *params, mdf_batch **out);
@@ -432,7 +441,7 @@ int mdf_batch_fetch(mdf_batch *b, uint32_t flags, double *forces, mdf_energies *
  * and keep the fastest.  report may be NULL. */
 int mdf_batch_autotune(mdf_batch *b, int reps, mdf_tune_report *report);
 /* The same for one context: pair_warps {2, 4, 8} x fft_lines {1, 2, 4} x
- * prune_every {0, 1} at the current positions (reps energy + force
+ * prune_every {0, 1} x pair_schedule {0, 1} at the current positions (reps energy + force
  * evaluations each, CUDA events on the context's stream); the fastest stays
  * in the context's parameters.  Forces do not depend on the choice.  Not
  * available with nranks > 1. */

@@ -1061,16 +1061,17 @@ int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
         if (!c.have_list) build_pairlist(c);
         const int R = reps > 0 ? reps : 5;
         const uint32_t flags = MDF_COMPUTE_ENERGY | MDF_COMPUTE_FORCES;
-        const int warps[3] = {2, 4, 8}, lines[3] = {1, 2, 4}, prune[2] = {0, 1};
+        const int warps[3] = {2, 4, 8}, lines[3] = {1, 2, 4}, prune[2] = {0, 1}, sched[2] = {0, 1};
         const bool timing = c.timing;
         c.timing = false;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         try {
             MDF_CUDA_TRY(cudaEventCreate(&e0));
             MDF_CUDA_TRY(cudaEventCreate(&e1));
-            auto apply = [&](int w, int l, int p) {
+            auto apply = [&](int w, int l, int p, int sc) {
                 c.p.pair_warps = w;
                 c.p.fft_lines = l;
+                c.p.pair_schedule = sc;
                 if (c.p.prune_every != p) {
                     c.p.prune_every = p;
                     c.pruned_valid = false;
@@ -1090,26 +1091,28 @@ int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
                 MDF_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
                 return (double)ms / R;
             };
-            const int w0 = c.p.pair_warps, l0 = c.p.fft_lines, p0 = c.p.prune_every;
+            const int w0 = c.p.pair_warps, l0 = c.p.fft_lines, p0 = c.p.prune_every, s0 = c.p.pair_schedule;
             const double t_default = time_it();
             double best = t_default;
-            int bw = w0, bl = l0, bp = p0, tried = 0;
-            for (int p : prune)
-                for (int w : warps)
-                    for (int l : lines) {
-                        apply(w, l, p);
-                        const double t = time_it();
-                        ++tried;
-                        if (t < best) {
-                            best = t;
-                            bw = w; bl = l; bp = p;
+            int bw = w0, bl = l0, bp = p0, bs = s0, tried = 0;
+            for (int sc : sched)
+                for (int p : prune)
+                    for (int w : warps)
+                        for (int l : lines) {
+                            apply(w, l, p, sc);
+                            const double t = time_it();
+                            ++tried;
+                            if (t < best) {
+                                best = t;
+                                bw = w; bl = l; bp = p; bs = sc;
+                            }
                         }
-                    }
-            apply(bw, bl, bp);
+            apply(bw, bl, bp, bs);
             if (rep) {
                 rep->pair_warps = bw;
                 rep->fft_lines = bl;
                 rep->prune_every = bp;
+            rep->pair_schedule = bs;
                 rep->n_tried = tried;
                 rep->best_ms = best;
                 rep->default_ms = t_default;

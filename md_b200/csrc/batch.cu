@@ -152,7 +152,7 @@ bool uniform_launches(const mdf_batch* b)
         const mdf_params& p = x->c.p;
         if (p.precision != p0.precision || (p.switch_radius > 0) != (p0.switch_radius > 0) ||
             (p.prune_every > 0) != (p0.prune_every > 0) || p.pair_warps != p0.pair_warps ||
-            p.fft_lines != p0.fft_lines || p.nranks > 1)
+            p.fft_lines != p0.fft_lines || p.pair_schedule != p0.pair_schedule || p.nranks > 1)
             return false;
     }
     return true;
@@ -181,7 +181,7 @@ struct MultiArgs {
         gx_gather = 0, gx_fin = 0;
     size_t dyn_pairs = 0;
     int threads = 256;
-    bool prune_on = false, use_switch = false, energy = false;
+    bool prune_on = false, use_switch = false, energy = false, persist = false;
 };
 
 template <typename R>
@@ -220,6 +220,7 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
     M.prune_on = c0.p.prune_every > 0;
     M.use_switch = c0.p.switch_radius > 0;
     M.threads = pair_threads(c0);
+    M.persist = c0.p.pair_schedule == 1;
     for (int s = 0; s < n; ++s) {
         Ctx& c = b->sys[s]->c;
         if (M.prune_on) c.pruned_valid = true;   // the captured chain prunes before the pair kernel
@@ -344,9 +345,11 @@ void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D)
     }
     if (M.gx_pairs > 0) {
         if (sizeof(R) == 4)
-            launch_pairs_f32_multi(D.pf32, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, b->main);
+            launch_pairs_f32_multi(D.pf32, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, M.persist,
+                                   b->main);
         else
-            launch_pairs_f64_multi(D.p64, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, b->main);
+            launch_pairs_f64_multi(D.p64, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, M.persist,
+                                   b->main);
         ++k;
     }
     MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, b->ev_join2, 0));
@@ -602,15 +605,16 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
         if (!b->have_lists) build_lists(b);
         const int R = reps > 0 ? reps : 5;
         const uint32_t flags = MDF_COMPUTE_ENERGY | MDF_COMPUTE_FORCES;
-        const int warps[3] = {2, 4, 8}, lines[3] = {1, 2, 4}, prune[2] = {0, 1};
+        const int warps[3] = {2, 4, 8}, lines[3] = {1, 2, 4}, prune[2] = {0, 1}, sched[2] = {0, 1};
         cudaEvent_t e0, e1;
         MDF_CUDA_TRY(cudaEventCreate(&e0));
         MDF_CUDA_TRY(cudaEventCreate(&e1));
-        auto apply = [&](int w, int l, int p) {
+        auto apply = [&](int w, int l, int p, int sc) {
             for (mdf_ctx* x : b->sys) {
                 Ctx& c = x->c;
                 c.p.pair_warps = w;
                 c.p.fft_lines = l;
+                c.p.pair_schedule = sc;
                 if (c.p.prune_every != p) {
                     c.p.prune_every = p;
                     c.pruned_valid = false;
@@ -631,22 +635,23 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
             return (double)ms / R;
         };
         const Ctx& c0 = b->sys[0]->c;
-        const int w0 = c0.p.pair_warps, l0 = c0.p.fft_lines, p0 = c0.p.prune_every;
+        const int w0 = c0.p.pair_warps, l0 = c0.p.fft_lines, p0 = c0.p.prune_every, s0 = c0.p.pair_schedule;
         double t_default = time_it();
         double best = 1e300;
-        int bw = w0, bl = l0, bp = p0, tried = 0;
-        for (int p : prune)
-            for (int w : warps)
-                for (int l : lines) {
-                    apply(w, l, p);
-                    const double t = time_it();
-                    ++tried;
-                    if (t < best) {
-                        best = t;
-                        bw = w; bl = l; bp = p;
+        int bw = w0, bl = l0, bp = p0, bs = s0, tried = 0;
+        for (int sc : sched)
+            for (int p : prune)
+                for (int w : warps)
+                    for (int l : lines) {
+                        apply(w, l, p, sc);
+                        const double t = time_it();
+                        ++tried;
+                        if (t < best) {
+                            best = t;
+                            bw = w; bl = l; bp = p; bs = sc;
+                        }
                     }
-                }
-        apply(bw, bl, bp);
+        apply(bw, bl, bp, bs);
         run(b, flags);
         MDF_CUDA_TRY(cudaStreamSynchronize(b->main));
         cudaEventDestroy(e0);
@@ -655,6 +660,7 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
             rep->pair_warps = bw;
             rep->fft_lines = bl;
             rep->prune_every = bp;
+            rep->pair_schedule = bs;
             rep->n_tried = tried;
             rep->best_ms = best;
             rep->default_ms = t_default;

@@ -287,7 +287,7 @@ __device__ __forceinline__ void pairs_f32_body(
     const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp,
     int lj_smem, float kc, const PairConstF& Kin, const ShiftTable& shifts, unsigned long long* __restrict__ fslot,
     int nslots, unsigned long long* __restrict__ acc, unsigned long long* __restrict__ npairs,
-    unsigned long long* __restrict__ next, unsigned* st)
+    unsigned long long* __restrict__ next, int persist, unsigned* st)
 {
     const PairConstF K = Kin;   // registers (the multi-system launch reads it from device memory)
     extern __shared__ float4 s_lj[];
@@ -306,15 +306,20 @@ __device__ __forceinline__ void pairs_f32_body(
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
     int npc = 0;
-    // Persistent warps: each takes the next i cluster from the work counter
-    // until the list is done, so no SM idles behind a slow block or a
-    // partial last wave.  Energies go to fixed point once per i cluster (a
-    // fixed-order FP64 sum), so they do not depend on which warp took which
-    // cluster.
-    for (;;) {
+    // persist: persistent warps, each taking the next i cluster from the work
+    // counter until the list is done (no SM idles behind a slow block or a
+    // partial last wave); otherwise warp w takes i cluster w.  Energies go to
+    // fixed point once per i cluster (a fixed-order FP64 sum), so they do not
+    // depend on which warp took which cluster.
+    for (int round = 0;; ++round) {
         int w = 0;
-        if (lane == 0) w = (int)atomicAdd(next, 1ull);
-        w = __shfl_sync(FULL, w, 0);
+        if (persist) {
+            if (lane == 0) w = (int)atomicAdd(next, 1ull);
+            w = __shfl_sync(FULL, w, 0);
+        } else {
+            if (round) break;
+            w = blockIdx.x * (blockDim.x >> 5) + wib;
+        }
         if (w >= nlist) break;
         double e_lj = 0, e_dir = 0;
         float fix = 0.f, fiy = 0.f, fiz = 0.f;
@@ -428,7 +433,7 @@ __device__ __forceinline__ void pairs_f32_body(
 
 #define MDF_PF32_UNPACK(A)                                                                                       \
     A.nlist, A.ilist, A.plist, A.xq, A.stype, A.centerf, A.lj4, A.ntp, A.lj_smem, A.kc, A.K, A.shifts, A.fslot,      \
-        A.nslots, A.acc, A.npairs, A.next, A.st
+        A.nslots, A.acc, A.npairs, A.next, A.persist, A.st
 
 // With energies: the compiler's own register choice (72, three blocks per SM;
 // a 64-register cap spills and is slower).
@@ -500,11 +505,16 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
     int npc = 0;
-    // persistent warps and per-cluster energies, as in the FP32 kernel
-    for (;;) {
+    // warp schedule and per-cluster energies as in the FP32 kernel
+    for (int round = 0;; ++round) {
         int w = 0;
-        if (lane == 0) w = (int)atomicAdd(A.next, 1ull);
-        w = __shfl_sync(FULL, w, 0);
+        if (A.persist) {
+            if (lane == 0) w = (int)atomicAdd(A.next, 1ull);
+            w = __shfl_sync(FULL, w, 0);
+        } else {
+            if (round) break;
+            w = blockIdx.x * (blockDim.x >> 5) + wib;
+        }
         if (w >= nlist) break;
         double e_lj = 0, e_dir = 0;
         double fix = 0, fiy = 0, fiz = 0;
@@ -987,6 +997,7 @@ PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn)
     A.acc = c.acc.p;
     A.npairs = c.npairs_dev.p;
     A.next = c.scal.p + SCAL_WORK;
+    A.persist = c.p.pair_schedule == 1 ? 1 : 0;
     A.st = c.status.p;
     return A;
 }
@@ -1002,7 +1013,7 @@ static void launch_pairs_f32(Ctx& c, bool energy)
 #define MDF_PF32(E, S, K_)                                                                                     \
     do {                                                                                                       \
         const void* fn = (E) ? (const void*)k_pairs_f32<S, K_> : (const void*)k_pairs_f32_force<S, K_>;        \
-        const int nb = std::min(A.gx, persistent_blocks(fn, th, dyn));                                          \
+        const int nb = A.persist ? std::min(A.gx, persistent_blocks(fn, th, dyn)) : A.gx;                       \
         if (E) k_pairs_f32<S, K_><<<nb, th, dyn, c.stream>>>(A);                                                 \
         else k_pairs_f32_force<S, K_><<<nb, th, dyn, c.stream>>>(A);                                             \
     } while (0)
@@ -1020,11 +1031,11 @@ static void launch_pairs_f32(Ctx& c, bool energy)
 }
 
 void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, cudaStream_t s)
+                            bool use_switch, bool persist, cudaStream_t s)
 {
 #define MDF_PF32M(KERN)                                                                                        \
     do {                                                                                                       \
-        const dim3 g(std::min(gx, persistent_blocks((const void*)KERN, threads, dyn)), 1, nsys);                \
+        const dim3 g(persist ? std::min(gx, persistent_blocks((const void*)KERN, threads, dyn)) : gx, 1, nsys); \
         KERN<<<g, threads, dyn, s>>>(d_args);                                                                  \
     } while (0)
     if (energy) {
@@ -1080,6 +1091,7 @@ PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn)
     A.acc = c.acc.p;
     A.npairs = c.npairs_dev.p;
     A.next = c.scal.p + SCAL_WORK;
+    A.persist = c.p.pair_schedule == 1 ? 1 : 0;
     A.st = c.status.p;
     return A;
 }
@@ -1103,7 +1115,8 @@ static void launch_pairs_f64(Ctx& c, bool energy)
 #define MDF_PF64(E, S, K_)                                                                                     \
     do {                                                                                                       \
         allow_smem(k_pairs_f64<E, S, K_>, dyn);                                                                \
-        const int nb = std::min(A.gx, persistent_blocks((const void*)k_pairs_f64<E, S, K_>, th, dyn));          \
+        const int nb = A.persist ? std::min(A.gx, persistent_blocks((const void*)k_pairs_f64<E, S, K_>, th, dyn)) \
+                                 : A.gx;                                                                       \
         k_pairs_f64<E, S, K_><<<nb, th, dyn, c.stream>>>(A);                                                   \
     } while (0)
 #define MDF_PF64_K(E, S) \
@@ -1120,13 +1133,14 @@ static void launch_pairs_f64(Ctx& c, bool energy)
 }
 
 void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, cudaStream_t s)
+                            bool use_switch, bool persist, cudaStream_t s)
 {
 #define MDF_PF64M(E, S)                                                                                        \
     do {                                                                                                       \
         allow_smem(k_pairs_f64_multi<E, S>, dyn);                                                              \
-        const dim3 gp(std::min(gx, persistent_blocks((const void*)k_pairs_f64_multi<E, S>, threads, dyn)), 1,  \
-                      nsys);                                                                                   \
+        const dim3 gp(persist ? std::min(gx, persistent_blocks((const void*)k_pairs_f64_multi<E, S>, threads, dyn)) \
+                              : gx,                                                                            \
+                      1, nsys);                                                                                \
         k_pairs_f64_multi<E, S><<<gp, threads, dyn, s>>>(d_args);                                              \
     } while (0)
     if (energy) {

@@ -242,7 +242,8 @@ class Engine:
         """mdf_autotune: the fastest launch shapes for this context (kept)."""
         r = abi.mdf_tune_report()
         self._check(self.lib.mdf_autotune(self.h, int(reps), C.byref(r)), "autotune")
-        return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every, n_tried=r.n_tried,
+        return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every,
+                    pair_schedule=r.pair_schedule, n_tried=r.n_tried,
                     best_ms=r.best_ms, default_ms=r.default_ms)
 
     def set_allreduce(self, fn):
@@ -519,7 +520,8 @@ class Batch:
     def autotune(self, reps=5):
         r = abi.mdf_tune_report()
         self._check(self.lib.mdf_batch_autotune(self.h, int(reps), C.byref(r)), "autotune")
-        return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every, n_tried=r.n_tried,
+        return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every,
+                    pair_schedule=r.pair_schedule, n_tried=r.n_tried,
                     best_ms=r.best_ms, default_ms=r.default_ms)
 
     def info(self):

@@ -284,7 +284,8 @@ def test_autotune_keeps_forces_and_reports(prec):
     eng, _ = make_engine(s, PHYS, prec, synth.GRIDS["small"])
     E0, F0 = eng.compute()
     rep = eng.autotune(reps=2)
-    assert rep["n_tried"] == 18 and rep["best_ms"] > 0 and rep["best_ms"] <= rep["default_ms"]
+    assert rep["n_tried"] == 36 and rep["best_ms"] > 0 and rep["best_ms"] <= rep["default_ms"]
+    assert rep["pair_schedule"] in (0, 1)
     assert rep["pair_warps"] in (2, 4, 8) and rep["fft_lines"] in (1, 2, 4) and rep["prune_every"] in (0, 1)
     E1, F1 = eng.compute()
     assert np.array_equal(F0, F1)

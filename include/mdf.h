@@ -169,6 +169,12 @@ typedef struct {
      * every SM slot until the list is done, so kernels queued beside them
      * wait).  mdf_autotune picks. */
     int32_t pair_schedule;
+    /* Unit of the pruned list the pair kernel walks (results do not depend
+     * on it): 0 = whole 8 x 8 cluster pairs; 1 = half entries, each half of
+     * an i cluster (atoms 0-3, 4-7) with the j clusters within the cutoff
+     * of that half (fewer atom pairs outside the cutoff, more list work).
+     * Needs pruning (prune_every > 0).  mdf_autotune picks. */
+    int32_t pair_layout;
 } mdf_params;
 
 /* Sum of `count` 64-bit integers at d_buf (device memory of the context's
@@ -412,7 +418,7 @@ typedef struct {
     double best_ms;       /* one batch evaluation with the chosen shapes */
     double default_ms;    /* ... with the shapes the batch was created with */
     int32_t pair_schedule;
-    int32_t reserved;
+    int32_t pair_layout;
 } mdf_tune_report;
 
 int mdf_batch_create(int nsys, const mdf_topology *const *topos, const mdf_params *params, mdf_batch **out);
@@ -441,7 +447,8 @@ int mdf_batch_fetch(mdf_batch *b, uint32_t flags, double *forces, mdf_energies *
  * and keep the fastest.  report may be NULL. */
 int mdf_batch_autotune(mdf_batch *b, int reps, mdf_tune_report *report);
 /* The same for one context: pair_warps {2, 4, 8} x fft_lines {1, 2, 4} x
- * prune_every {0, 1} x pair_schedule {0, 1} at the current positions (reps energy + force
+ * prune_every {0, 1} x pair_schedule {0, 1} x pair_layout {0, 1} (layout 1
+ * only with pruning) at the current positions (reps energy + force
  * evaluations each, CUDA events on the context's stream); the fastest stays
  * in the context's parameters.  Forces do not depend on the choice.  Not
  * available with nranks > 1. */

@@ -66,13 +66,14 @@ class mdf_params(C.Structure):
         ("pme_order", C.c_int32), ("coulomb_const", C.c_double), ("device", C.c_int32),
         ("prune_every", C.c_int32), ("prune_margin", C.c_double), ("pair_warps", C.c_int32),
         ("fft_lines", C.c_int32), ("rank", C.c_int32), ("nranks", C.c_int32), ("pair_schedule", C.c_int32),
+        ("pair_layout", C.c_int32),
     ]
 
 
 class mdf_tune_report(C.Structure):
     _fields_ = [("pair_warps", C.c_int32), ("fft_lines", C.c_int32), ("prune_every", C.c_int32),
                 ("n_tried", C.c_int32), ("best_ms", C.c_double), ("default_ms", C.c_double),
-                ("pair_schedule", C.c_int32), ("reserved", C.c_int32)]
+                ("pair_schedule", C.c_int32), ("pair_layout", C.c_int32)]
 
 
 class mdf_md_report(C.Structure):

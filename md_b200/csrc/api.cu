@@ -1068,12 +1068,13 @@ int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
         try {
             MDF_CUDA_TRY(cudaEventCreate(&e0));
             MDF_CUDA_TRY(cudaEventCreate(&e1));
-            auto apply = [&](int w, int l, int p, int sc) {
+            auto apply = [&](int w, int l, int p, int sc, int ly) {
                 c.p.pair_warps = w;
                 c.p.fft_lines = l;
                 c.p.pair_schedule = sc;
-                if (c.p.prune_every != p) {
+                if (c.p.prune_every != p || c.p.pair_layout != ly) {
                     c.p.prune_every = p;
+                    c.p.pair_layout = ly;
                     c.pruned_valid = false;
                     c.since_prune = 0;
                 }
@@ -1091,28 +1092,31 @@ int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
                 MDF_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
                 return (double)ms / R;
             };
-            const int w0 = c.p.pair_warps, l0 = c.p.fft_lines, p0 = c.p.prune_every, s0 = c.p.pair_schedule;
+            const int w0 = c.p.pair_warps, l0 = c.p.fft_lines, p0 = c.p.prune_every, s0 = c.p.pair_schedule,
+                      y0 = c.p.pair_layout;
             const double t_default = time_it();
             double best = t_default;
-            int bw = w0, bl = l0, bp = p0, bs = s0, tried = 0;
+            int bw = w0, bl = l0, bp = p0, bs = s0, by = y0, tried = 0;
             for (int sc : sched)
                 for (int p : prune)
-                    for (int w : warps)
-                        for (int l : lines) {
-                            apply(w, l, p, sc);
-                            const double t = time_it();
-                            ++tried;
-                            if (t < best) {
-                                best = t;
-                                bw = w; bl = l; bp = p; bs = sc;
+                    for (int ly = 0; ly <= (p > 0 ? 1 : 0); ++ly)   // the half layout runs on pruned lists only
+                        for (int w : warps)
+                            for (int l : lines) {
+                                apply(w, l, p, sc, ly);
+                                const double t = time_it();
+                                ++tried;
+                                if (t < best) {
+                                    best = t;
+                                    bw = w; bl = l; bp = p; bs = sc; by = ly;
+                                }
                             }
-                        }
-            apply(bw, bl, bp, bs);
+            apply(bw, bl, bp, bs, by);
             if (rep) {
                 rep->pair_warps = bw;
                 rep->fft_lines = bl;
                 rep->prune_every = bp;
-            rep->pair_schedule = bs;
+                rep->pair_schedule = bs;
+                rep->pair_layout = by;
                 rep->n_tried = tried;
                 rep->best_ms = best;
                 rep->default_ms = t_default;

@@ -152,7 +152,8 @@ bool uniform_launches(const mdf_batch* b)
         const mdf_params& p = x->c.p;
         if (p.precision != p0.precision || (p.switch_radius > 0) != (p0.switch_radius > 0) ||
             (p.prune_every > 0) != (p0.prune_every > 0) || p.pair_warps != p0.pair_warps ||
-            p.fft_lines != p0.fft_lines || p.pair_schedule != p0.pair_schedule || p.nranks > 1)
+            p.fft_lines != p0.fft_lines || p.pair_schedule != p0.pair_schedule ||
+            half_layout(x->c) != half_layout(b->sys[0]->c) || p.nranks > 1)
             return false;
     }
     return true;
@@ -181,7 +182,7 @@ struct MultiArgs {
         gx_gather = 0, gx_fin = 0;
     size_t dyn_pairs = 0;
     int threads = 256;
-    bool prune_on = false, use_switch = false, energy = false, persist = false;
+    bool prune_on = false, use_switch = false, energy = false, persist = false, half = false;
 };
 
 template <typename R>
@@ -221,11 +222,17 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
     M.use_switch = c0.p.switch_radius > 0;
     M.threads = pair_threads(c0);
     M.persist = c0.p.pair_schedule == 1;
+    M.half = half_layout(c0);
     for (int s = 0; s < n; ++s) {
         Ctx& c = b->sys[s]->c;
-        if (M.prune_on) c.pruned_valid = true;   // the captured chain prunes before the pair kernel
+        if (M.prune_on) {
+            // the captured chain prunes before the pair kernel
+            c.pruned_valid = true;
+            c.pruned_half = M.half;
+        }
+        if (M.half) ensure_half_lists(c);
         M.pack.push_back(make_pack_args<R>(c));
-        M.prune.push_back(make_prune_args<R>(c));
+        M.prune.push_back(M.half ? make_prune_half_args<R>(c) : make_prune_args<R>(c));
         if (sizeof(R) == 4) {
             size_t dyn = 0;
             M.pf32.push_back(make_pair_f32_args(c, &dyn));
@@ -340,16 +347,16 @@ void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D)
     launch_pack_multi<R>(D.pack, n, M.gx_pack, b->main);
     ++k;
     if (M.prune_on) {
-        launch_prune_multi<R>(D.prune, n, M.gx_prune, b->main);
+        launch_prune_multi<R>(D.prune, n, M.gx_prune, M.half, b->main);
         ++k;
     }
     if (M.gx_pairs > 0) {
         if (sizeof(R) == 4)
             launch_pairs_f32_multi(D.pf32, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, M.persist,
-                                   b->main);
+                                   M.half, b->main);
         else
             launch_pairs_f64_multi(D.p64, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, M.persist,
-                                   b->main);
+                                   M.half, b->main);
         ++k;
     }
     MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, b->ev_join2, 0));
@@ -609,14 +616,15 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
         cudaEvent_t e0, e1;
         MDF_CUDA_TRY(cudaEventCreate(&e0));
         MDF_CUDA_TRY(cudaEventCreate(&e1));
-        auto apply = [&](int w, int l, int p, int sc) {
+        auto apply = [&](int w, int l, int p, int sc, int ly) {
             for (mdf_ctx* x : b->sys) {
                 Ctx& c = x->c;
                 c.p.pair_warps = w;
                 c.p.fft_lines = l;
                 c.p.pair_schedule = sc;
-                if (c.p.prune_every != p) {
+                if (c.p.prune_every != p || c.p.pair_layout != ly) {
                     c.p.prune_every = p;
+                    c.p.pair_layout = ly;
                     c.pruned_valid = false;
                     c.since_prune = 0;
                 }
@@ -635,23 +643,25 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
             return (double)ms / R;
         };
         const Ctx& c0 = b->sys[0]->c;
-        const int w0 = c0.p.pair_warps, l0 = c0.p.fft_lines, p0 = c0.p.prune_every, s0 = c0.p.pair_schedule;
+        const int w0 = c0.p.pair_warps, l0 = c0.p.fft_lines, p0 = c0.p.prune_every, s0 = c0.p.pair_schedule,
+                  y0 = c0.p.pair_layout;
         double t_default = time_it();
         double best = 1e300;
-        int bw = w0, bl = l0, bp = p0, bs = s0, tried = 0;
+        int bw = w0, bl = l0, bp = p0, bs = s0, by = y0, tried = 0;
         for (int sc : sched)
             for (int p : prune)
-                for (int w : warps)
-                    for (int l : lines) {
-                        apply(w, l, p, sc);
-                        const double t = time_it();
-                        ++tried;
-                        if (t < best) {
-                            best = t;
-                            bw = w; bl = l; bp = p; bs = sc;
+                for (int ly = 0; ly <= (p > 0 ? 1 : 0); ++ly)   // the half layout runs on pruned lists only
+                    for (int w : warps)
+                        for (int l : lines) {
+                            apply(w, l, p, sc, ly);
+                            const double t = time_it();
+                            ++tried;
+                            if (t < best) {
+                                best = t;
+                                bw = w; bl = l; bp = p; bs = sc; by = ly;
+                            }
                         }
-                    }
-        apply(bw, bl, bp, bs);
+        apply(bw, bl, bp, bs, by);
         run(b, flags);
         MDF_CUDA_TRY(cudaStreamSynchronize(b->main));
         cudaEventDestroy(e0);
@@ -661,6 +671,7 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
             rep->fft_lines = bl;
             rep->prune_every = bp;
             rep->pair_schedule = bs;
+            rep->pair_layout = by;
             rep->n_tried = tried;
             rep->best_ms = best;
             rep->default_ms = t_default;

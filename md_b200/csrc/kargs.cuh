@@ -84,7 +84,8 @@ struct PairF32Args {
     unsigned long long* acc;
     unsigned long long* npairs;
     unsigned long long* next;   // work counter of the persistent warps, zero at launch
-    int persist;                // 1: persistent warps on the counter; 0: warp w takes i cluster w
+    int persist;                // 1: persistent warps on the counter; 0: warp w takes item w
+    int half;                   // items are half entries (the 4 x 8 kernel)
     unsigned* st;
 };
 
@@ -119,7 +120,8 @@ struct PairF64Args {
     unsigned long long* acc;
     unsigned long long* npairs;
     unsigned long long* next;   // work counter of the persistent warps, zero at launch
-    int persist;                // 1: persistent warps on the counter; 0: warp w takes i cluster w
+    int persist;                // 1: persistent warps on the counter; 0: warp w takes item w
+    int half;                   // items are half entries (the 4 x 8 kernel)
     unsigned* st;
 };
 
@@ -330,14 +332,17 @@ struct FinalizeArgs {
 template <typename R> PackArgs<R> make_pack_args(const Ctx& c);
 template <typename R> void launch_pack_multi(const PackArgs<R>* d_args, int nsys, int gx, cudaStream_t s);
 template <typename R> PruneArgs<R> make_prune_args(const Ctx& c);
-template <typename R> void launch_prune_multi(const PruneArgs<R>* d_args, int nsys, int gx, cudaStream_t s);
+template <typename R> PruneArgs<R> make_prune_half_args(const Ctx& c);
+void ensure_half_lists(Ctx& c);
+template <typename R>
+void launch_prune_multi(const PruneArgs<R>* d_args, int nsys, int gx, bool half, cudaStream_t s);
 PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn);
 void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, cudaStream_t s);
+                            bool use_switch, bool persist, bool half, cudaStream_t s);
 template <typename R> PairArgs<R> make_pair_args(const Ctx& c, bool count);
 PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn);
 void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, cudaStream_t s);
+                            bool use_switch, bool persist, bool half, cudaStream_t s);
 int pair_threads(const Ctx& c);
 ExclArgs make_excl_args(const Ctx& c);
 Pair14Args make_pair14_args(const Ctx& c);

@@ -181,6 +181,9 @@ struct Ctx {
     DevBuf<PairEntry> plist_in;    // pruned list the pair kernel walks (same offsets as plist)
     DevBuf<ILRange> ilist_in;
     DevBuf<unsigned long long> n_in;   // [1] entries kept by the last prune
+    DevBuf<ILRange> ilist_h;       // half layout: [2 n_clusters] items (ILRange.pad = half)
+    DevBuf<PairEntry> plist_h;     // half layout: [2 x outer capacity]
+    bool pruned_half = false;      // the last prune wrote the half lists
     int since_prune = 0;
     bool pruned_valid = false;
     DevBuf<int> scan_tmp;
@@ -314,7 +317,9 @@ void backward(Ctx& c, const double* dL_dF, double dL_dE, double* dL_dq, double* 
 void pme_adjoint(Ctx& c, double gE, double vscale);
 void build_pairlist(Ctx& c);
 void pack_positions(Ctx& c);
-void prune_pairlist(Ctx& c);
+void prune_pairlist(Ctx& c, bool whole_entries = false);
+// half-entry lists in use by the pair kernel (layout 1, pruned)
+inline bool half_layout(const Ctx& c) { return c.p.pair_layout == 1 && c.p.prune_every > 0; }
 void launch_nonbonded(Ctx& c, bool energy);
 void launch_exclusions(Ctx& c, bool energy);
 void launch_bonded(Ctx& c, bool energy);

@@ -431,6 +431,166 @@ __device__ __forceinline__ void pairs_f32_body(
     }
 }
 
+// ---------------------------------------- half-cluster (4 x 8) FP32 kernel
+// The same pair arithmetic over half entries: an item is (i cluster, half h)
+// with the list of j clusters that have an atom pair within the cutoff of
+// i atoms 4h..4h+3 (the half prune builds it, ILRange.pad = h).  At c1 half
+// entries keep 45% of their atom pairs inside the cutoff against 39% for
+// whole 8 x 8 entries.  Lane (e, jj) owns j atom jj of entry e of a batch of
+// four; in step t it meets i atom 4h + ((jj + t) & 3), read from shared
+// memory (stored twice so the step's atom sits at a compile-time offset), so
+// the j force stays in the lane's registers and the i-force accumulators
+// rotate one lane per step (the lane's i atom repeats every four lanes, so
+// the same shuffle as the whole-entry kernel works).  After the item the
+// eight partial sums of each i atom are reduced by three butterfly steps.
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
+{
+    extern __shared__ float4 s_lj[];
+    __shared__ float4 sxi[NB_WARPS][8];    // the item's four i atoms (I frame, charge x kc), twice
+    __shared__ int sti[NB_WARPS][8];       // their LJ table rows
+    __shared__ float sh[27][6];
+    const int nlist = A.nlist, ntp = A.ntp, nslots = A.nslots;
+    const ILRange* __restrict__ ilist = A.ilist;
+    const PairEntry* __restrict__ plist = A.plist;
+    const float4* __restrict__ xq = A.xq;
+    const int* __restrict__ stype = A.stype;
+    const float4* __restrict__ centerf = A.centerf;
+    unsigned long long* __restrict__ fslot = A.fslot;
+    unsigned* st = A.st;
+    const PairConstF K = A.K;
+    for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = A.shifts.v[k / 6][k % 6];
+    if (A.lj_smem)
+        for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj[k] = A.lj4[k];
+    __syncthreads();
+    const float4* __restrict__ ljt = A.lj_smem ? s_lj : A.lj4;
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int eslot = lane >> 3, jj = lane & 7, i4 = jj & 3;
+    const unsigned FULL = 0xffffffffu;
+    const int rot_src = (lane & ~7) | ((jj + 1) & 7);
+    int npc = 0;
+    for (int round = 0;; ++round) {
+        int w = 0;
+        if (A.persist) {
+            if (lane == 0) w = (int)atomicAdd(A.next, 1ull);
+            w = __shfl_sync(FULL, w, 0);
+        } else {
+            if (round) break;
+            w = blockIdx.x * (blockDim.x >> 5) + wib;
+        }
+        if (w >= nlist) break;
+        const ILRange L = ilist[w];
+        const int I = L.i, h = L.pad;
+        if (lane < 8) {
+            float4 v = xq[I * CLUSTER + 4 * h + (lane & 3)];
+            v.w *= A.kc;
+            sxi[wib][lane] = v;
+            sti[wib][lane] = stype[I * CLUSTER + 4 * h + (lane & 3)] * ntp;
+        }
+        __syncwarp();
+        const float4 cI = centerf[I];
+        const float4* __restrict__ sxl = &sxi[wib][i4];
+        const int* __restrict__ stl = &sti[wib][i4];
+        double e_lj = 0, e_dir = 0;
+        float fix = 0.f, fiy = 0.f, fiz = 0.f;   // the i atom (jj + t) & 3 at step t
+        for (int b = 0; b < L.count; b += 4) {
+            const int e = b + eslot;
+            PairEntry pe;
+            if (e < L.count) {
+                pe = plist[L.start + e];
+            } else {
+                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+            }
+            const int J = pe.j;
+            const float4 xj = xq[J * CLUSTER + jj];
+            const int tj = stype[J * CLUSTER + jj];
+            const float4 cJ = centerf[J];
+            const float* s6 = sh[pe.shift];
+            // the j atom in I's frame: x_j - D, D = (c_I - c_J) - image offset
+            const float pjx = xj.x - (((cI.x - cJ.x) - s6[0]) - s6[3]);
+            const float pjy = xj.y - (((cI.y - cJ.y) - s6[1]) - s6[4]);
+            const float pjz = xj.z - (((cI.z - cJ.z) - s6[2]) - s6[5]);
+            // mask bits (4h + i) * 8 + jj, i = 0..3, rotated so step t tests bit t
+            const unsigned long long mc = pe.mask >> (32 * h + jj);
+            const unsigned nib = (unsigned)((mc & 1ull) | ((mc >> 7) & 2ull) | ((mc >> 14) & 4ull) | ((mc >> 21) & 8ull));
+            const unsigned rot = ((nib >> i4) | (nib << (4 - i4))) & 0xfu;
+            float fjx = 0.f, fjy = 0.f, fjz = 0.f, el = 0.f, ed = 0.f;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const float4 xi = sxl[t];
+                const float dx = xi.x - pjx, dy = xi.y - pjy, dz = xi.z - pjz;
+                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
+                const float rinv = rsqrt_ftz(r2);
+                const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
+                const float4 ab = ljt[stl[t] + tj];      // A, B, 12A, 6B
+                float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
+                float G = (rinv6 * rinv2) * fmaf(ab.z, rinv6, -ab.w);
+                if (SWITCH) {
+                    const float x = fmaxf(0.f, fmaf(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
+                    const float S = fmaf(x2 * x, fmaf(x, fmaf(x, -6.f, 15.f), -10.f), 1.f);
+                    const float dSr = x2 * fmaf(x, fmaf(x, K.d30, K.d60), K.d30) * rinv;   // dS/dr / r
+                    G = fmaf(S, G, -U * dSr);
+                    U = U * S;
+                } else {
+                    const float uc = ab.x * K.uc12 - ab.y * K.uc6;
+                    const float gc = (ab.z * K.uc12 - ab.w * K.uc6) / K.rc2f;
+                    U = U - uc + (r - K.rcf) * (gc * K.rcf);
+                    G = G - gc * K.rcf * rinv;
+                }
+                const float ex = ex2_approx(K.kex * r2);
+                const float erfcv = erfc_as(rcp_ftz(fmaf(K.pa, r, 1.0f)), ex);
+                const float qq = xi.w * xj.w;
+                const float ec = qq * erfcv * rinv;
+                float g = fmaf(fmaf(qq * K.two_a_spi, ex, ec), rinv2, G);
+                g = on ? g : 0.f;
+                if (ENERGY) {
+                    el += on ? U : 0.f;
+                    ed += on ? ec : 0.f;
+                }
+                if (COUNT) npc += on ? 1 : 0;
+                fix = fmaf(g, dx, fix); fiy = fmaf(g, dy, fiy); fiz = fmaf(g, dz, fiz);
+                fjx = fmaf(-g, dx, fjx); fjy = fmaf(-g, dy, fjy); fjz = fmaf(-g, dz, fjz);
+                fix = __shfl_sync(FULL, fix, rot_src);
+                fiy = __shfl_sync(FULL, fiy, rot_src);
+                fiz = __shfl_sync(FULL, fiz, rot_src);
+            }
+            if (ENERGY) {
+                e_lj += (double)el;
+                e_dir += (double)ed;
+            }
+            if (e < L.count && (fjx != 0.f || fjy != 0.f || fjz != 0.f)) {
+                const int sl = J * CLUSTER + jj;
+                fx_add_force_f(fslot + sl, fjx, st);
+                fx_add_force_f(fslot + nslots + sl, fjy, st);
+                fx_add_force_f(fslot + 2 * nslots + sl, fjz, st);
+            }
+        }
+        // lane jj holds a partial sum for i atom jj & 3: eight per atom
+        fix += __shfl_xor_sync(FULL, fix, 4); fix += __shfl_xor_sync(FULL, fix, 8); fix += __shfl_xor_sync(FULL, fix, 16);
+        fiy += __shfl_xor_sync(FULL, fiy, 4); fiy += __shfl_xor_sync(FULL, fiy, 8); fiy += __shfl_xor_sync(FULL, fiy, 16);
+        fiz += __shfl_xor_sync(FULL, fiz, 4); fiz += __shfl_xor_sync(FULL, fiz, 8); fiz += __shfl_xor_sync(FULL, fiz, 16);
+        if (lane < 4) {
+            const int sl = I * CLUSTER + 4 * h + lane;
+            fx_add_force_f(fslot + sl, fix, st);
+            fx_add_force_f(fslot + nslots + sl, fiy, st);
+            fx_add_force_f(fslot + 2 * nslots + sl, fiz, st);
+        }
+        if (ENERGY) {
+            const double s_lj = warp_sum(e_lj), s_dir = warp_sum(e_dir);
+            if (lane == 0) {
+                if (s_lj != 0.0) fx_add(A.acc + MDF_E_VDW, s_lj, ENERGY_SCALE, st);
+                if (s_dir != 0.0) fx_add(A.acc + MDF_E_EE_DIRECT, s_dir, ENERGY_SCALE, st);
+            }
+        }
+        __syncwarp();   // the next item overwrites this warp's i atoms
+    }
+    if (COUNT) {
+        long long np = warp_sum_ll((long long)npc);
+        if (lane == 0 && np) atomicAdd(A.npairs, (unsigned long long)np);
+    }
+}
+
 #define MDF_PF32_UNPACK(A)                                                                                       \
     A.nlist, A.ilist, A.plist, A.xq, A.stype, A.centerf, A.lj4, A.ntp, A.lj_smem, A.kc, A.K, A.shifts, A.fslot,      \
         A.nslots, A.acc, A.npairs, A.next, A.persist, A.st
@@ -449,6 +609,35 @@ template <bool SWITCH, bool COUNT>
 __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force(PairF32Args A)
 {
     pairs_f32_body<false, SWITCH, COUNT>(MDF_PF32_UNPACK(A));
+}
+
+// The half-entry (4 x 8) forms, same register budgets.
+template <bool SWITCH, bool COUNT>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32_half(PairF32Args A)
+{
+    pairs_f32_half_body<true, SWITCH, COUNT>(A);
+}
+
+template <bool SWITCH, bool COUNT>
+__global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_half_force(PairF32Args A)
+{
+    pairs_f32_half_body<false, SWITCH, COUNT>(A);
+}
+
+template <bool SWITCH>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32_half_multi(const PairF32Args* __restrict__ As)
+{
+    const PairF32Args& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs_f32_half_body<true, SWITCH, false>(A);
+}
+
+template <bool SWITCH>
+__global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_half_force_multi(const PairF32Args* __restrict__ As)
+{
+    const PairF32Args& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs_f32_half_body<false, SWITCH, false>(A);
 }
 
 // Many systems in one launch (blockIdx.z = system), with the same register
@@ -624,6 +813,167 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
         long long np = warp_sum_ll((long long)npc);
         if (lane == 0 && np) atomicAdd(A.npairs, (unsigned long long)np);
     }
+}
+
+// The half-entry (4 x 8) layout in FP64: the FP32 half kernel's structure
+// with the FP64 kernel's arithmetic.
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
+{
+    extern __shared__ double4 s_lj_d[];
+    __shared__ double4 sxi[NB_WARPS][8];
+    __shared__ int sti[NB_WARPS][8];
+    __shared__ double sh[27][3];
+    const int nlist = A.nlist, ntp = A.ntp, nslots = A.nslots;
+    const ILRange* __restrict__ ilist = A.ilist;
+    const PairEntry* __restrict__ plist = A.plist;
+    const double4* __restrict__ xq = A.xq;
+    const int* __restrict__ stype = A.stype;
+    const double4* __restrict__ center = A.center;
+    unsigned long long* __restrict__ fslot = A.fslot;
+    unsigned* st = A.st;
+    const PairConstD K = A.K;
+    for (int k = threadIdx.x; k < 27 * 3; k += blockDim.x) sh[k / 3][k % 3] = A.shifts.v[k / 3][k % 3];
+    if (A.lj_smem)
+        for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj_d[k] = A.lj4[k];
+    __syncthreads();
+    const double4* __restrict__ ljt = A.lj_smem ? s_lj_d : A.lj4;
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int eslot = lane >> 3, jj = lane & 7, i4 = jj & 3;
+    const unsigned FULL = 0xffffffffu;
+    const int rot_src = (lane & ~7) | ((jj + 1) & 7);
+    int npc = 0;
+    for (int round = 0;; ++round) {
+        int w = 0;
+        if (A.persist) {
+            if (lane == 0) w = (int)atomicAdd(A.next, 1ull);
+            w = __shfl_sync(FULL, w, 0);
+        } else {
+            if (round) break;
+            w = blockIdx.x * (blockDim.x >> 5) + wib;
+        }
+        if (w >= nlist) break;
+        const ILRange L = ilist[w];
+        const int I = L.i, h = L.pad;
+        if (lane < 8) {
+            double4 v = xq[I * CLUSTER + 4 * h + (lane & 3)];
+            v.w *= A.kc;
+            sxi[wib][lane] = v;
+            sti[wib][lane] = stype[I * CLUSTER + 4 * h + (lane & 3)] * ntp;
+        }
+        __syncwarp();
+        const double4 cI = center[I];
+        const double4* __restrict__ sxl = &sxi[wib][i4];
+        const int* __restrict__ stl = &sti[wib][i4];
+        double e_lj = 0, e_dir = 0;
+        double fix = 0, fiy = 0, fiz = 0;
+        for (int b = 0; b < L.count; b += 4) {
+            const int e = b + eslot;
+            PairEntry pe;
+            if (e < L.count) {
+                pe = plist[L.start + e];
+            } else {
+                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+            }
+            const int J = pe.j;
+            const double4 xj = xq[J * CLUSTER + jj];
+            const int tj = stype[J * CLUSTER + jj];
+            const double4 cJ = center[J];
+            const double* s3 = sh[pe.shift];
+            const double pjx = xj.x - ((cI.x - cJ.x) - s3[0]);
+            const double pjy = xj.y - ((cI.y - cJ.y) - s3[1]);
+            const double pjz = xj.z - ((cI.z - cJ.z) - s3[2]);
+            const unsigned long long mc = pe.mask >> (32 * h + jj);
+            const unsigned nib = (unsigned)((mc & 1ull) | ((mc >> 7) & 2ull) | ((mc >> 14) & 4ull) | ((mc >> 21) & 8ull));
+            const unsigned rot = ((nib >> i4) | (nib << (4 - i4))) & 0xfu;
+            double fjx = 0, fjy = 0, fjz = 0, el = 0, ed = 0;
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const double4 xi = sxl[t];
+                const double dx = xi.x - pjx, dy = xi.y - pjy, dz = xi.z - pjz;
+                const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
+                const double rinv = rsqrt(r2);
+                const double r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
+                const double4 ab = ljt[stl[t] + tj];      // A, B, 12A, 6B
+                double U = rinv6 * fma(ab.x, rinv6, -ab.y);
+                double G = (rinv6 * rinv2) * fma(ab.z, rinv6, -ab.w);
+                if (SWITCH) {
+                    const double x = fmax(0.0, fma(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
+                    const double S = fma(x2 * x, fma(x, fma(x, -6.0, 15.0), -10.0), 1.0);
+                    const double dSr = x2 * fma(x, fma(x, K.d30, K.d60), K.d30) * rinv;   // dS/dr / r
+                    G = fma(S, G, -U * dSr);
+                    U = U * S;
+                } else {
+                    const double uc = ab.x * K.uc12 - ab.y * K.uc6;
+                    const double gc = (ab.z * K.uc12 - ab.w * K.uc6) / K.rc2;
+                    U = U - uc + (r - K.rc) * (gc * K.rc);
+                    G = G - gc * K.rc * rinv;
+                }
+                const double ar = K.alpha * r;
+                const double ex = exp(-ar * ar);
+                const double qq = xi.w * xj.w;
+                const double ec = qq * erfc(ar) * rinv;
+                double g = fma(fma(qq * K.two_a_spi, ex, ec), rinv2, G);
+                g = on ? g : 0.0;
+                if (ENERGY) {
+                    el += on ? U : 0.0;
+                    ed += on ? ec : 0.0;
+                }
+                if (COUNT) npc += on ? 1 : 0;
+                fix = fma(g, dx, fix); fiy = fma(g, dy, fiy); fiz = fma(g, dz, fiz);
+                fjx = fma(-g, dx, fjx); fjy = fma(-g, dy, fjy); fjz = fma(-g, dz, fjz);
+                fix = __shfl_sync(FULL, fix, rot_src);
+                fiy = __shfl_sync(FULL, fiy, rot_src);
+                fiz = __shfl_sync(FULL, fiz, rot_src);
+            }
+            if (ENERGY) {
+                e_lj += el;
+                e_dir += ed;
+            }
+            if (e < L.count && (fjx != 0.0 || fjy != 0.0 || fjz != 0.0)) {
+                const int sl = J * CLUSTER + jj;
+                fx_add(fslot + sl, fjx, FORCE_SCALE, st);
+                fx_add(fslot + nslots + sl, fjy, FORCE_SCALE, st);
+                fx_add(fslot + 2 * nslots + sl, fjz, FORCE_SCALE, st);
+            }
+        }
+        fix += __shfl_xor_sync(FULL, fix, 4); fix += __shfl_xor_sync(FULL, fix, 8); fix += __shfl_xor_sync(FULL, fix, 16);
+        fiy += __shfl_xor_sync(FULL, fiy, 4); fiy += __shfl_xor_sync(FULL, fiy, 8); fiy += __shfl_xor_sync(FULL, fiy, 16);
+        fiz += __shfl_xor_sync(FULL, fiz, 4); fiz += __shfl_xor_sync(FULL, fiz, 8); fiz += __shfl_xor_sync(FULL, fiz, 16);
+        if (lane < 4) {
+            const int sl = I * CLUSTER + 4 * h + lane;
+            fx_add(fslot + sl, fix, FORCE_SCALE, st);
+            fx_add(fslot + nslots + sl, fiy, FORCE_SCALE, st);
+            fx_add(fslot + 2 * nslots + sl, fiz, FORCE_SCALE, st);
+        }
+        if (ENERGY) {
+            const double s_lj = warp_sum(e_lj), s_dir = warp_sum(e_dir);
+            if (lane == 0) {
+                if (s_lj != 0.0) fx_add(A.acc + MDF_E_VDW, s_lj, ENERGY_SCALE, st);
+                if (s_dir != 0.0) fx_add(A.acc + MDF_E_EE_DIRECT, s_dir, ENERGY_SCALE, st);
+            }
+        }
+        __syncwarp();
+    }
+    if (COUNT) {
+        long long np = warp_sum_ll((long long)npc);
+        if (lane == 0 && np) atomicAdd(A.npairs, (unsigned long long)np);
+    }
+}
+
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f64_half(PairF64Args A)
+{
+    pairs_f64_half_body<ENERGY, SWITCH, COUNT>(A);
+}
+
+template <bool ENERGY, bool SWITCH>
+__global__ void __launch_bounds__(NB_THREADS) k_pairs_f64_half_multi(const PairF64Args* __restrict__ As)
+{
+    const PairF64Args& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    pairs_f64_half_body<ENERGY, SWITCH, false>(A);
 }
 
 template <bool ENERGY, bool SWITCH, bool COUNT>
@@ -984,8 +1334,13 @@ PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn)
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
-    A.ilist = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
-    A.plist = pruned ? c.plist_in.p : c.plist.p;
+    A.half = pruned && c.pruned_half ? 1 : 0;
+    A.ilist = A.half ? c.ilist_h.p + 2 * lo : (pruned ? c.ilist_in.p : c.ilist.p) + lo;
+    A.plist = pruned ? (A.half ? c.plist_h.p : c.plist_in.p) : c.plist.p;
+    if (A.half) {
+        A.nlist *= 2;   // two half items per i cluster
+        A.gx = grid_blocks(A.nlist, wpb);
+    }
     A.xq = c.xq_f.p;
     A.stype = c.slot_type.p;
     A.centerf = c.centerf.p;
@@ -1012,10 +1367,17 @@ static void launch_pairs_f32(Ctx& c, bool energy)
     const bool sw = c.p.switch_radius > 0.0;
 #define MDF_PF32(E, S, K_)                                                                                     \
     do {                                                                                                       \
-        const void* fn = (E) ? (const void*)k_pairs_f32<S, K_> : (const void*)k_pairs_f32_force<S, K_>;        \
+        const void* fn = A.half ? ((E) ? (const void*)k_pairs_f32_half<S, K_>                                  \
+                                       : (const void*)k_pairs_f32_half_force<S, K_>)                           \
+                                : ((E) ? (const void*)k_pairs_f32<S, K_> : (const void*)k_pairs_f32_force<S, K_>); \
         const int nb = A.persist ? std::min(A.gx, persistent_blocks(fn, th, dyn)) : A.gx;                       \
-        if (E) k_pairs_f32<S, K_><<<nb, th, dyn, c.stream>>>(A);                                                 \
-        else k_pairs_f32_force<S, K_><<<nb, th, dyn, c.stream>>>(A);                                             \
+        if (A.half) {                                                                                          \
+            if (E) k_pairs_f32_half<S, K_><<<nb, th, dyn, c.stream>>>(A);                                        \
+            else k_pairs_f32_half_force<S, K_><<<nb, th, dyn, c.stream>>>(A);                                    \
+        } else {                                                                                               \
+            if (E) k_pairs_f32<S, K_><<<nb, th, dyn, c.stream>>>(A);                                             \
+            else k_pairs_f32_force<S, K_><<<nb, th, dyn, c.stream>>>(A);                                         \
+        }                                                                                                      \
     } while (0)
 #define MDF_PF32_K(E, S) \
     do { if (count) MDF_PF32(E, S, true); else MDF_PF32(E, S, false); } while (0)
@@ -1031,14 +1393,21 @@ static void launch_pairs_f32(Ctx& c, bool energy)
 }
 
 void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, cudaStream_t s)
+                            bool use_switch, bool persist, bool half, cudaStream_t s)
 {
 #define MDF_PF32M(KERN)                                                                                        \
     do {                                                                                                       \
         const dim3 g(persist ? std::min(gx, persistent_blocks((const void*)KERN, threads, dyn)) : gx, 1, nsys); \
         KERN<<<g, threads, dyn, s>>>(d_args);                                                                  \
     } while (0)
-    if (energy) {
+    if (half) {
+        if (energy) {
+            if (use_switch) MDF_PF32M(k_pairs_f32_half_multi<true>); else MDF_PF32M(k_pairs_f32_half_multi<false>);
+        } else {
+            if (use_switch) MDF_PF32M(k_pairs_f32_half_force_multi<true>);
+            else MDF_PF32M(k_pairs_f32_half_force_multi<false>);
+        }
+    } else if (energy) {
         if (use_switch) MDF_PF32M(k_pairs_f32_multi<true>); else MDF_PF32M(k_pairs_f32_multi<false>);
     } else {
         if (use_switch) MDF_PF32M(k_pairs_f32_force_multi<true>); else MDF_PF32M(k_pairs_f32_force_multi<false>);
@@ -1078,8 +1447,13 @@ PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn)
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;
     const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
-    A.ilist = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
-    A.plist = pruned ? c.plist_in.p : c.plist.p;
+    A.half = pruned && c.pruned_half ? 1 : 0;
+    A.ilist = A.half ? c.ilist_h.p + 2 * lo : (pruned ? c.ilist_in.p : c.ilist.p) + lo;
+    A.plist = pruned ? (A.half ? c.plist_h.p : c.plist_in.p) : c.plist.p;
+    if (A.half) {
+        A.nlist *= 2;   // two half items per i cluster
+        A.gx = grid_blocks(A.nlist, wpb);
+    }
     A.xq = c.xq_d.p;
     A.stype = c.slot_type.p;
     A.center = c.center.p;
@@ -1114,10 +1488,19 @@ static void launch_pairs_f64(Ctx& c, bool energy)
     const bool sw = c.p.switch_radius > 0.0;
 #define MDF_PF64(E, S, K_)                                                                                     \
     do {                                                                                                       \
-        allow_smem(k_pairs_f64<E, S, K_>, dyn);                                                                \
-        const int nb = A.persist ? std::min(A.gx, persistent_blocks((const void*)k_pairs_f64<E, S, K_>, th, dyn)) \
-                                 : A.gx;                                                                       \
-        k_pairs_f64<E, S, K_><<<nb, th, dyn, c.stream>>>(A);                                                   \
+        if (A.half) {                                                                                          \
+            allow_smem(k_pairs_f64_half<E, S, K_>, dyn);                                                       \
+            const int nb = A.persist                                                                           \
+                               ? std::min(A.gx, persistent_blocks((const void*)k_pairs_f64_half<E, S, K_>, th, dyn)) \
+                               : A.gx;                                                                         \
+            k_pairs_f64_half<E, S, K_><<<nb, th, dyn, c.stream>>>(A);                                          \
+        } else {                                                                                               \
+            allow_smem(k_pairs_f64<E, S, K_>, dyn);                                                            \
+            const int nb = A.persist                                                                           \
+                               ? std::min(A.gx, persistent_blocks((const void*)k_pairs_f64<E, S, K_>, th, dyn))  \
+                               : A.gx;                                                                         \
+            k_pairs_f64<E, S, K_><<<nb, th, dyn, c.stream>>>(A);                                               \
+        }                                                                                                      \
     } while (0)
 #define MDF_PF64_K(E, S) \
     do { if (count) MDF_PF64(E, S, true); else MDF_PF64(E, S, false); } while (0)
@@ -1133,15 +1516,18 @@ static void launch_pairs_f64(Ctx& c, bool energy)
 }
 
 void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, cudaStream_t s)
+                            bool use_switch, bool persist, bool half, cudaStream_t s)
 {
+#define MDF_PF64K(KERN)                                                                                        \
+    do {                                                                                                       \
+        allow_smem(KERN, dyn);                                                                                 \
+        const dim3 gp(persist ? std::min(gx, persistent_blocks((const void*)KERN, threads, dyn)) : gx, 1, nsys); \
+        KERN<<<gp, threads, dyn, s>>>(d_args);                                                                 \
+    } while (0)
 #define MDF_PF64M(E, S)                                                                                        \
     do {                                                                                                       \
-        allow_smem(k_pairs_f64_multi<E, S>, dyn);                                                              \
-        const dim3 gp(persist ? std::min(gx, persistent_blocks((const void*)k_pairs_f64_multi<E, S>, threads, dyn)) \
-                              : gx,                                                                            \
-                      1, nsys);                                                                                \
-        k_pairs_f64_multi<E, S><<<gp, threads, dyn, s>>>(d_args);                                              \
+        if (half) MDF_PF64K((k_pairs_f64_half_multi<E, S>));                                                   \
+        else MDF_PF64K((k_pairs_f64_multi<E, S>));                                                             \
     } while (0)
     if (energy) {
         if (use_switch) MDF_PF64M(true, true); else MDF_PF64M(true, false);
@@ -1149,6 +1535,7 @@ void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int thr
         if (use_switch) MDF_PF64M(false, true); else MDF_PF64M(false, false);
     }
 #undef MDF_PF64M
+#undef MDF_PF64K
     MDF_CUDA_TRY(cudaGetLastError());
 }
 

@@ -612,6 +612,107 @@ __device__ __forceinline__ void prune_dev(const PruneArgs<R>& A)
     }
 }
 
+// Half prune (the 4 x 8 pair layout): the same box test, then each half of
+// the i cluster (atoms 0-3, 4-7) is tested on its own; an entry goes to the
+// list of every half that has an atom pair within the radius.  One lane per
+// outer entry, two j atoms at a time, stopping once both halves are found.
+// The outer range [start, start + count) of i cluster I owns the slots
+// [2 start + h count, 2 start + (h + 1) count) of the half list; item 2 w + h
+// of this launch describes half h (ILRange.pad = h).
+template <typename R>
+__device__ __forceinline__ void prune_half_dev(const PruneArgs<R>& A)
+{
+    using V4t = typename V4<R>::type;
+    __shared__ float sh[27][6];
+    for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = A.shifts.v[k / 6][k % 6];
+    __syncthreads();
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= A.ncl) return;
+    const unsigned below = (1u << lane) - 1u;
+    const ILRange L = A.ilist[w];
+    const int I = L.i;
+    const V4t* __restrict__ xq = A.xq;
+    R ax[CLUSTER], ay[CLUSTER], az[CLUSTER], an[CLUSTER];   // -2 x_i and |x_i|^2
+#pragma unroll
+    for (int k = 0; k < CLUSTER; ++k) {
+        const V4t v = xq[I * CLUSTER + k];
+        ax[k] = (R)-2 * v.x; ay[k] = (R)-2 * v.y; az[k] = (R)-2 * v.z;
+        an[k] = v.x * v.x + v.y * v.y + v.z * v.z;
+    }
+    const float4 cI = A.centerf[I], ilo = A.cur_lo[I], ihi = A.cur_hi[I];
+    const R rc2 = (R)A.rcut2;
+    const long long out0 = 2LL * L.start, out1 = 2LL * L.start + L.count;
+    int kept0 = 0, kept1 = 0;
+    for (int base = 0; base < L.count; base += 32) {
+        const bool have = base + lane < L.count;
+        PairEntry my;
+        my.j = I; my.shift = 13; my.mask = 0ull;
+        if (have) my = A.plist[L.start + base + lane];
+        const float4 cJ = A.centerf[my.j], jlo = A.cur_lo[my.j], jhi = A.cur_hi[my.j];
+        const float* s6 = sh[my.shift];
+        const float ox = -(((cI.x - cJ.x) - s6[0]) - s6[3]);
+        const float oy = -(((cI.y - cJ.y) - s6[1]) - s6[4]);
+        const float oz = -(((cI.z - cJ.z) - s6[2]) - s6[5]);
+        const float gx = fmaxf(0.f, fmaxf(jlo.x + ox - ihi.x, ilo.x - (jhi.x + ox)));
+        const float gy = fmaxf(0.f, fmaxf(jlo.y + oy - ihi.y, ilo.y - (jhi.y + oy)));
+        const float gz = fmaxf(0.f, fmaxf(jlo.z + oz - ihi.z, ilo.z - (jhi.z + oz)));
+        const bool cand = have && my.mask != 0ull && gx * gx + gy * gy + gz * gz < A.rcut2;
+        bool k0 = false, k1 = false;
+        if (cand) {
+            const R px = (R)ox, py = (R)oy, pz = (R)oz;
+            const V4t* __restrict__ xj = xq + (size_t)my.j * CLUSTER;
+#pragma unroll 1
+            for (int j = 0; j < CLUSTER && !(k0 && k1); j += 2) {
+                V4t v[2];
+                v[0] = xj[j];
+                v[1] = xj[j + 1];
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const R qx = v[u].x + px, qy = v[u].y + py, qz = v[u].z + pz;
+                    const R thr = rc2 - (qx * qx + qy * qy + qz * qz);
+                    R m0 = fma(ax[0], qx, fma(ay[0], qy, fma(az[0], qz, an[0])));
+                    R m1 = fma(ax[4], qx, fma(ay[4], qy, fma(az[4], qz, an[4])));
+#pragma unroll
+                    for (int ii = 1; ii < 4; ++ii) {
+                        m0 = fmin(m0, fma(ax[ii], qx, fma(ay[ii], qy, fma(az[ii], qz, an[ii]))));
+                        m1 = fmin(m1, fma(ax[ii + 4], qx, fma(ay[ii + 4], qy, fma(az[ii + 4], qz, an[ii + 4]))));
+                    }
+                    k0 = k0 || m0 < thr;
+                    k1 = k1 || m1 < thr;
+                }
+            }
+        }
+        const unsigned b0 = __ballot_sync(0xffffffffu, k0), b1 = __ballot_sync(0xffffffffu, k1);
+        if (k0) A.plist_in[out0 + kept0 + __popc(b0 & below)] = my;
+        if (k1) A.plist_in[out1 + kept1 + __popc(b1 & below)] = my;
+        kept0 += __popc(b0);
+        kept1 += __popc(b1);
+    }
+    if (lane == 0) {
+        ILRange r;
+        r.i = I; r.start = (int)out0; r.count = kept0; r.pad = 0;
+        A.ilist_in[2 * w] = r;
+        r.start = (int)out1; r.count = kept1; r.pad = 1;
+        A.ilist_in[2 * w + 1] = r;
+        if (kept0 + kept1) atomicAdd(A.n_in, (unsigned long long)(kept0 + kept1));
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune_half(PruneArgs<R> A)
+{
+    prune_half_dev(A);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune_half_multi(const PruneArgs<R>* __restrict__ As)
+{
+    const PruneArgs<R>& A = As[blockIdx.z];
+    if ((int)blockIdx.x >= A.gx) return;
+    prune_half_dev(A);
+}
+
 template <typename R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 3) k_prune(PruneArgs<R> A)
 {
@@ -659,31 +760,64 @@ PruneArgs<R> make_prune_args(const Ctx& c)
     A.n_in = c.n_in.p;
     return A;
 }
+
+// The half-layout lists (two items per i cluster, twice the outer capacity).
+void ensure_half_lists(Ctx& c)
+{
+    c.ilist_h.alloc(2 * (size_t)std::max(c.n_clusters, 1));
+    c.plist_h.alloc(2 * (size_t)std::max<size_t>(c.plist.n, 1));
+}
+
+// Prune arguments writing the half lists (item 2 w + h of this rank's range).
+template <typename R>
+PruneArgs<R> make_prune_half_args(const Ctx& c)
+{
+    PruneArgs<R> A = make_prune_args<R>(c);
+    long long lo, hi;
+    rank_slice(c, c.n_clusters, lo, hi);
+    A.ilist_in = c.ilist_h.p + 2 * lo;
+    A.plist_in = c.plist_h.p;
+    return A;
+}
+template PruneArgs<float> make_prune_half_args<float>(const Ctx&);
+template PruneArgs<double> make_prune_half_args<double>(const Ctx&);
 template PruneArgs<float> make_prune_args<float>(const Ctx&);
 template PruneArgs<double> make_prune_args<double>(const Ctx&);
 
 template <typename R>
-void launch_prune_multi(const PruneArgs<R>* d_args, int nsys, int gx, cudaStream_t s)
+void launch_prune_multi(const PruneArgs<R>* d_args, int nsys, int gx, bool half, cudaStream_t s)
 {
-    k_prune_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    if (half) k_prune_half_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    else k_prune_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
     MDF_CUDA_TRY(cudaGetLastError());
 }
-template void launch_prune_multi<float>(const PruneArgs<float>*, int, int, cudaStream_t);
-template void launch_prune_multi<double>(const PruneArgs<double>*, int, int, cudaStream_t);
+template void launch_prune_multi<float>(const PruneArgs<float>*, int, int, bool, cudaStream_t);
+template void launch_prune_multi<double>(const PruneArgs<double>*, int, int, bool, cudaStream_t);
 
-void prune_pairlist(Ctx& c)
+// whole_entries: build the 8 x 8 pruned list even in the half layout (the
+// adjoint walks whole entries).
+void prune_pairlist(Ctx& c, bool whole_entries)
 {
     MDF_CUDA_TRY(cudaMemsetAsync(c.n_in.p, 0, sizeof(unsigned long long), c.stream));
+    const bool half = half_layout(c) && !whole_entries;
+    if (half) ensure_half_lists(c);
     if (c.p.precision == MDF_PREC_MIXED) {
-        const PruneArgs<float> A = make_prune_args<float>(c);
-        if (A.ncl > 0) k_prune<float><<<grid_of(A), 256, 0, c.stream>>>(A);
+        const PruneArgs<float> A = half ? make_prune_half_args<float>(c) : make_prune_args<float>(c);
+        if (A.ncl > 0) {
+            if (half) k_prune_half<float><<<grid_of(A), 256, 0, c.stream>>>(A);
+            else k_prune<float><<<grid_of(A), 256, 0, c.stream>>>(A);
+        }
     } else {
-        const PruneArgs<double> A = make_prune_args<double>(c);
-        if (A.ncl > 0) k_prune<double><<<grid_of(A), 256, 0, c.stream>>>(A);
+        const PruneArgs<double> A = half ? make_prune_half_args<double>(c) : make_prune_args<double>(c);
+        if (A.ncl > 0) {
+            if (half) k_prune_half<double><<<grid_of(A), 256, 0, c.stream>>>(A);
+            else k_prune<double><<<grid_of(A), 256, 0, c.stream>>>(A);
+        }
     }
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
     c.pruned_valid = true;
+    c.pruned_half = half;
 }
 
 // ------------------------------------------------------------------ host

@@ -164,7 +164,8 @@ class Engine:
 
     def __init__(self, flat, box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, cutoff=10.0,
                  skin=2.0, switch_radius=9.0, ewald_tol=1e-5, ewald_alpha=0.0, grid=(0, 0, 0), pme_order=4,
-                 device=0, prune_every=1, prune_margin=0.0, rank=0, nranks=1):
+                 device=0, prune_every=1, prune_margin=0.0, rank=0, nranks=1, pair_warps=0, fft_lines=0,
+                 pair_schedule=0, pair_layout=0):
         self.lib = library()
         self.flat = flat
         self.natoms = flat.natoms
@@ -178,6 +179,8 @@ class Engine:
         p.ewald_tol, p.ewald_alpha, p.pme_order, p.device = float(ewald_tol), float(ewald_alpha), int(pme_order), int(device)
         p.prune_every, p.prune_margin = int(prune_every), float(prune_margin)
         p.rank, p.nranks = int(rank), int(nranks)
+        p.pair_warps, p.fft_lines = int(pair_warps), int(fft_lines)
+        p.pair_schedule, p.pair_layout = int(pair_schedule), int(pair_layout)
         self.params = p
         h = C.c_void_p()
         rc = self.lib.mdf_create(C.byref(flat.struct()), C.byref(p), C.byref(h))
@@ -243,7 +246,7 @@ class Engine:
         r = abi.mdf_tune_report()
         self._check(self.lib.mdf_autotune(self.h, int(reps), C.byref(r)), "autotune")
         return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every,
-                    pair_schedule=r.pair_schedule, n_tried=r.n_tried,
+                    pair_schedule=r.pair_schedule, pair_layout=r.pair_layout, n_tried=r.n_tried,
                     best_ms=r.best_ms, default_ms=r.default_ms)
 
     def set_allreduce(self, fn):
@@ -422,7 +425,7 @@ class Batch:
     (mdf_batch_*).  flats / boxes / grids: one per system."""
 
     def __init__(self, flats, boxes, grids, precision=abi.MDF_PREC_MIXED, cutoff=9.0, skin=2.0, switch_radius=8.0,
-                 ewald_tol=1e-5, device=0, prune_every=1):
+                 ewald_tol=1e-5, device=0, prune_every=1, pair_schedule=0, pair_layout=0):
         self.lib = library()
         self.flats = list(flats)
         n = len(self.flats)
@@ -439,6 +442,7 @@ class Batch:
             p.cutoff, p.skin, p.switch_radius = float(cutoff), float(skin), float(switch_radius)
             p.ewald_tol, p.device = float(ewald_tol), int(device)
             p.prune_every = int(prune_every)
+            p.pair_schedule, p.pair_layout = int(pair_schedule), int(pair_layout)
             params[k] = p
         self._tops, self._params = tops, params
         h = C.c_void_p()
@@ -521,7 +525,7 @@ class Batch:
         r = abi.mdf_tune_report()
         self._check(self.lib.mdf_batch_autotune(self.h, int(reps), C.byref(r)), "autotune")
         return dict(pair_warps=r.pair_warps, fft_lines=r.fft_lines, prune_every=r.prune_every,
-                    pair_schedule=r.pair_schedule, n_tried=r.n_tried,
+                    pair_schedule=r.pair_schedule, pair_layout=r.pair_layout, n_tried=r.n_tried,
                     best_ms=r.best_ms, default_ms=r.default_ms)
 
     def info(self):

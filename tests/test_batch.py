@@ -2,10 +2,12 @@
 graph launch, one kernel launch per evaluation step for all systems, must give
 exactly the single-system results (same kernel bodies on the same data,
 fixed-point sums) across graph replays and position updates.  After
-autotuning the launch shapes the forces are still bit-identical (each pair
-force is converted to fixed point on its own); energies, summed in FP64 per
-block before their fixed-point conversion, may move in the last bits
-(1e-12 relative + 1e-8 absolute).  The FP64 batch matches the oracle."""
+autotuning, the batch equals single systems run with the chosen launch shape
+(pruning and the pair layout set the order of the FP32 sums of each i
+cluster's forces; warps per block, the warp schedule and FFT lines change no
+bit of the forces); energies, summed in FP64 per warp before their
+fixed-point conversion, may move in the last bits (1e-12 relative + 1e-8
+absolute).  The FP64 and mixed batches match the oracle."""
 import numpy as np
 import pytest
 
@@ -33,10 +35,10 @@ def _flats(ss):
     return [H.flat(s, PHYS, engine.cmap_coefficients) for s in ss]
 
 
-def _singles(ss, flats, prec, coords=None):
+def _singles(ss, flats, prec, coords=None, **shape):
     out = []
     for k, (s, f) in enumerate(zip(ss, flats)):
-        eng = engine.Engine(f, s.box, semantics=PHYS, precision=prec, grid=s.meta["grid"], **KW)
+        eng = engine.Engine(f, s.box, semantics=PHYS, precision=prec, grid=s.meta["grid"], **KW, **shape)
         eng.set_positions(s.coords)
         eng.build_pairlist()
         if coords is not None:
@@ -55,14 +57,16 @@ def _same(res, ref, etol=0.0):
             assert abs(E[t] - E1[t]) <= etol * abs(E1[t]) + (1e-8 if etol else 0.0), (t, E[t], E1[t])
 
 
+@pytest.mark.parametrize("layout", [0, 1])
 @pytest.mark.parametrize("prec", [MIXED, FP64])
-def test_batch_equals_single_systems(prec):
+def test_batch_equals_single_systems(prec, layout):
     ss = systems()
     flats = _flats(ss)
-    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=prec, **KW)
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=prec, pair_layout=layout,
+                     **KW)
     b.set_positions([s.coords for s in ss])
     res = b.compute()
-    ref = _singles(ss, flats, prec)
+    ref = _singles(ss, flats, prec, pair_layout=layout)
     _same(res, ref)
     _same(b.compute(), ref)           # a graph replay
     info = b.info()
@@ -97,16 +101,17 @@ def test_batch_autotune_keeps_results_and_follows_positions():
     flats = _flats(ss)
     b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
     b.set_positions([s.coords for s in ss])
-    ref = _singles(ss, flats, MIXED)
     rep = b.autotune(reps=2)
-    assert rep["n_tried"] == 36 and rep["best_ms"] > 0 and rep["pair_schedule"] in (0, 1)
+    assert rep["n_tried"] == 54 and rep["best_ms"] > 0
+    assert rep["pair_schedule"] in (0, 1) and rep["pair_layout"] in (0, 1)
     assert rep["pair_warps"] in (2, 4, 8) and rep["fft_lines"] in (1, 2, 4) and rep["prune_every"] in (0, 1)
-    _same(b.compute(), ref, 1e-12)
+    shape = dict(prune_every=rep["prune_every"], pair_layout=rep["pair_layout"])
+    _same(b.compute(), _singles(ss, flats, MIXED, **shape), 1e-12)
     # moved positions (within the skin): the graph uploads them at every launch
     rng = np.random.default_rng(3)
     moved = [s.coords + rng.uniform(-0.2, 0.2, s.coords.shape) for s in ss]
     b.set_positions(moved)
-    _same(b.compute(), _singles(ss, flats, MIXED, coords=moved), 1e-12)
+    _same(b.compute(), _singles(ss, flats, MIXED, coords=moved, **shape), 1e-12)
     b.close()
 
 
@@ -125,14 +130,16 @@ def test_fp64_batch_matches_oracle():
     b.close()
 
 
-def test_mixed_batch_matches_oracle_every_system():
+@pytest.mark.parametrize("layout", [0, 1])
+def test_mixed_batch_matches_oracle_every_system(layout):
     """The mixed-precision batch (the c3 workload's precision) against the FP64
     oracle on every member: forces <= 1e-5 rms relative (the mixed-path
     target), total energy 1e-6 relative, each system with its own box and
-    PME grid."""
+    PME grid; whole-entry and half-entry pair kernels."""
     ss = systems()
     flats = _flats(ss)
-    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, pair_layout=layout,
+                     **KW)
     b.set_positions([s.coords for s in ss])
     res = b.compute()
     for (E, F), s, f in zip(res, ss, flats):

@@ -100,6 +100,10 @@ def parse():
                     help="profiling run: build CONFIG (tiny, small, c0, c1, c4, or c3: the batch), run --warmup + --steps "
                          "evaluations, print the per-phase times and exit (for ncu)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--pair-layout", type=int, default=0, choices=[0, 1],
+                    help="profiling run: pair-kernel layout (0 whole 8x8 entries, 1 half entries)")
+    ap.add_argument("--pair-schedule", type=int, default=0, choices=[0, 1],
+                    help="profiling run: pair-kernel schedule (0 one warp per item, 1 persistent warps)")
     return ap.parse_args()
 
 
@@ -112,7 +116,8 @@ def run_profile(args):
         members = make_batch_workload(range(256))
         ss = [m[0] for m in members]
         b = engine.Batch([m[1] for m in members], [x.box for x in ss], [x.meta["grid"] for x in ss],
-                         precision=abi.MDF_PREC_MIXED, cutoff=9.0, skin=2.0, switch_radius=8.0, ewald_tol=1e-5)
+                         precision=abi.MDF_PREC_MIXED, cutoff=9.0, skin=2.0, switch_radius=8.0, ewald_tol=1e-5,
+                         pair_layout=args.pair_layout, pair_schedule=args.pair_schedule)
         b.set_positions([x.coords for x in ss])
         for _ in range(args.warmup + args.steps):
             b.compute(energy=True, forces=True)
@@ -123,7 +128,8 @@ def run_profile(args):
     flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
     prec = abi.MDF_PREC_MIXED if args.precision == "mixed" else abi.MDF_PREC_FP64
     eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=prec, ewald_tol=1e-5,
-                        grid=synth.GRIDS[args.profile])
+                        grid=synth.GRIDS[args.profile], pair_layout=args.pair_layout,
+                        pair_schedule=args.pair_schedule)
     eng.set_positions(s.coords)
     eng.build_pairlist()
     for _ in range(args.warmup + args.steps):
@@ -132,6 +138,7 @@ def run_profile(args):
     eng.enable_timing(True)
     eng.compute()
     print(json.dumps({"profile": args.profile, "natoms": s.natoms, "precision": args.precision,
+                      "pair_layout": args.pair_layout, "pair_schedule": args.pair_schedule,
                       "pairlist": eng.pairlist_info(), "phase_ms": dict(eng.kernel_times())}))
     eng.close()
 

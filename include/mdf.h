@@ -149,8 +149,9 @@ typedef struct {
     int32_t prune_every;
     double prune_margin;
     /* Launch shapes (results do not depend on them; mdf_batch_autotune picks
-     * them): warps per block of the pair kernel (2, 4 or 8; 0 = 8) and the
-     * most FFT lines per block (1, 2 or 4; 0 = 4). */
+     * them): warps per block of the pair kernel (2, 4 or 8; 0 = 8) and FFT
+     * lines per block (1, 2, 4, 8, 16 or 32; 0 = chosen per grid size: 4 for
+     * 100 or 216 points, 16 for 32, so small grids keep every thread busy). */
     int32_t pair_warps;
     int32_t fft_lines;
     /* Work split over nranks contexts (one per GPU, PHYSICAL semantics; 0 or
@@ -446,7 +447,7 @@ int mdf_batch_fetch(mdf_batch *b, uint32_t flags, double *forces, mdf_energies *
 /* Time every candidate launch shape on this batch (reps graph launches each)
  * and keep the fastest.  report may be NULL. */
 int mdf_batch_autotune(mdf_batch *b, int reps, mdf_tune_report *report);
-/* The same for one context: pair_warps {2, 4, 8} x fft_lines {1, 2, 4} x
+/* The same for one context: pair_warps {2, 4, 8} x fft_lines {2, 4, 8, 16} x
  * prune_every {0, 1} x pair_schedule {0, 1} x pair_layout {0, 1} (layout 1
  * only with pruning) at the current positions (reps energy + force
  * evaluations each, CUDA events on the context's stream); the fastest stays

@@ -1061,7 +1061,7 @@ int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
         if (!c.have_list) build_pairlist(c);
         const int R = reps > 0 ? reps : 5;
         const uint32_t flags = MDF_COMPUTE_ENERGY | MDF_COMPUTE_FORCES;
-        const int warps[3] = {2, 4, 8}, lines[3] = {1, 2, 4}, prune[2] = {0, 1}, sched[2] = {0, 1};
+        const int warps[3] = {2, 4, 8}, lines[4] = {2, 4, 8, 16}, prune[2] = {0, 1}, sched[2] = {0, 1};
         const bool timing = c.timing;
         c.timing = false;
         cudaEvent_t e0 = nullptr, e1 = nullptr;

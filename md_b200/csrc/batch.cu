@@ -612,7 +612,7 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
         if (!b->have_lists) build_lists(b);
         const int R = reps > 0 ? reps : 5;
         const uint32_t flags = MDF_COMPUTE_ENERGY | MDF_COMPUTE_FORCES;
-        const int warps[3] = {2, 4, 8}, lines[3] = {1, 2, 4}, prune[2] = {0, 1}, sched[2] = {0, 1};
+        const int warps[3] = {2, 4, 8}, lines[4] = {2, 4, 8, 16}, prune[2] = {0, 1}, sched[2] = {0, 1};
         cudaEvent_t e0, e1;
         MDF_CUDA_TRY(cudaEventCreate(&e0));
         MDF_CUDA_TRY(cudaEventCreate(&e1));

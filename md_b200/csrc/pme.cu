@@ -854,11 +854,19 @@ static double cardinal_bspline(int n, double x)
     return (x * cardinal_bspline(n - 1, x) + (n - x) * cardinal_bspline(n - 1, x - 1.0)) / (n - 1);
 }
 
-// lines per block (power of two dividing FFT_THREADS) within 46 KB of shared
-// memory, at most cap (mdf_params.fft_lines: 1, 2 or 4; 0 = 4)
-static int lines_per_block(const FFTPlan1D& p, size_t csize, int cap = 4)
+// Lines per block (a power of two dividing FFT_THREADS) within 46 KB of
+// shared memory: mdf_params.fft_lines (1, 2, 4, 8, 16 or 32), or for 0 the
+// most lines (at least 4) that leave every line as many threads as its
+// radix-4 stages have butterflies (n/4): 4 at n = 100 or 216, 16 at n = 32.
+static int lines_per_block(const FFTPlan1D& p, size_t csize, int cap = 0)
 {
-    const int top = (cap == 1 || cap == 2) ? cap : 4;
+    int top = 4;
+    if (cap == 1 || cap == 2 || cap == 4 || cap == 8 || cap == 16 || cap == 32) {
+        top = cap;
+    } else {
+        const int need = (p.n + 3) / 4;
+        while (top < 32 && FFT_THREADS / (2 * top) >= need) top *= 2;
+    }
     for (int lp = top; lp >= 1; lp >>= 1) {
         size_t bytes = csize * ((size_t)p.n + 2 * (size_t)lp * p.n) + sizeof(int2) * (size_t)p.ntab;
         if (bytes <= 46 * 1024) return lp;

@@ -102,9 +102,9 @@ def test_batch_autotune_keeps_results_and_follows_positions():
     b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
     b.set_positions([s.coords for s in ss])
     rep = b.autotune(reps=2)
-    assert rep["n_tried"] == 54 and rep["best_ms"] > 0
+    assert rep["n_tried"] == 72 and rep["best_ms"] > 0
     assert rep["pair_schedule"] in (0, 1) and rep["pair_layout"] in (0, 1)
-    assert rep["pair_warps"] in (2, 4, 8) and rep["fft_lines"] in (1, 2, 4) and rep["prune_every"] in (0, 1)
+    assert rep["pair_warps"] in (2, 4, 8) and rep["fft_lines"] in (2, 4, 8, 16) and rep["prune_every"] in (0, 1)
     shape = dict(prune_every=rep["prune_every"], pair_layout=rep["pair_layout"])
     _same(b.compute(), _singles(ss, flats, MIXED, **shape), 1e-12)
     # moved positions (within the skin): the graph uploads them at every launch

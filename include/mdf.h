@@ -444,6 +444,18 @@ int mdf_batch_compute(mdf_batch *b, uint32_t flags, double *forces, mdf_energies
  * `stream` after it) and fetch (waits, then copies out). */
 int mdf_batch_launch(mdf_batch *b, uint32_t flags, void *stream);
 int mdf_batch_fetch(mdf_batch *b, uint32_t flags, double *forces, mdf_energies *energies);
+/* Pipelined batch evaluation: submit queues one evaluation of the positions
+ * at xyz (all systems concatenated, 3 * total atoms doubles; pinned host
+ * memory for asynchronous copies) and returns; the forces go to `forces`
+ * (may be NULL).  At most two evaluations are in flight: the positions of
+ * the next one go in on one copy stream and the forces of the previous one
+ * come out on another while the GPU computes.  collect waits for the oldest
+ * and writes its energies (one per system, may be NULL); xyz and forces of a
+ * submission must stay valid until it is collected.  Needs the same launch
+ * parameters (precision, switch, pruning, launch shapes) in every system.
+ * The first submission builds the pairlists from its positions. */
+int mdf_batch_submit(mdf_batch *b, uint32_t flags, const double *xyz, double *forces);
+int mdf_batch_collect(mdf_batch *b, mdf_energies *energies);
 /* Time every candidate launch shape on this batch (reps graph launches each)
  * and keep the fastest.  report may be NULL. */
 int mdf_batch_autotune(mdf_batch *b, int reps, mdf_tune_report *report);

@@ -60,6 +60,23 @@ struct mdf_batch {
     // per-kernel argument arrays of the multi form (rebuilt before each capture)
     DevBuf<unsigned char> args;          // one allocation, the arrays below point into it
     size_t args_cap = 0;
+    // pipelined evaluation (mdf_batch_submit / mdf_batch_collect): two stages,
+    // each with its own graph (no copies inside), device position and force
+    // buffers and host scalar blocks; the copies run on two copy streams
+    struct Stage {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        uint32_t graph_flags = 0;
+        DevBuf<double> d_pos, d_forces;
+        DevBuf<unsigned char> args;
+        unsigned long long* h_scal = nullptr;    // mapped pinned [nsys][NUM_SCAL]
+        unsigned long long* d_hscal = nullptr;
+        cudaEvent_t h2d = nullptr, consumed = nullptr, done = nullptr, d2h = nullptr;
+        uint32_t flags = 0;
+    };
+    Stage stage[2];
+    int stage_next = 0, stage_old = 0, inflight = 0;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;
 };
 
 namespace {
@@ -111,6 +128,13 @@ void drop_graph(mdf_batch* b)
     b->exec = nullptr;
     b->graph = nullptr;
     b->have_graph = false;
+    if (b->inflight) cudaStreamSynchronize(b->main);   // stage graphs still queued finish first
+    for (auto& S : b->stage) {
+        if (S.exec) cudaGraphExecDestroy(S.exec);
+        if (S.graph) cudaGraphDestroy(S.graph);
+        S.exec = nullptr;
+        S.graph = nullptr;
+    }
 }
 
 // Enqueue one batch evaluation on b->main (used both plainly and under capture).
@@ -211,8 +235,13 @@ size_t arr_bytes(const std::vector<T>& v)
 // (synchronously, outside any capture); returns the device arrays.  (The
 // prune kernel's kept-entry counter is not cleared per evaluation here: a
 // batch does not report it.)
+// d_forces: the concatenated force buffer the finalize kernels write;
+// hscal: per-system host scalar blocks ([nsys][NUM_SCAL], device view of
+// mapped memory; nullptr = each context's own); args: the device allocation
+// of the argument arrays.
 template <typename R>
-MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
+MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M, double* d_forces,
+                          unsigned long long* hscal, DevBuf<unsigned char>& args)
 {
     const int n = b->nsys;
     const bool energy = (flags & MDF_COMPUTE_ENERGY) != 0;
@@ -269,7 +298,8 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
         M.fm.smx = std::max(M.fm.smx, F.smx);
         M.gather.push_back(make_gather_args<R>(c));
         // forces straight into the batch's concatenated device buffer
-        M.fin.push_back(make_finalize_args(c, b->d_forces.p + b->off[s]));
+        M.fin.push_back(make_finalize_args(c, d_forces + b->off[s]));
+        if (hscal) M.fin.back().host_scal = hscal + (size_t)s * NUM_SCAL;
     }
     auto gmax = [](const auto& v) {
         int g = 0;
@@ -292,13 +322,13 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
                          arr_bytes(M.spread) + arr_bytes(M.zf) + arr_bytes(M.yf) + arr_bytes(M.x) +
                          arr_bytes(M.yi) + arr_bytes(M.zi) + arr_bytes(M.gather) + arr_bytes(M.fin);
     std::vector<unsigned char> host(total);
-    b->args.alloc(total);
+    args.alloc(total);
     size_t off = 0;
     MultiDev<R> D;
     auto put = [&](const auto& v, auto*& dptr) {
         using T = typename std::decay_t<decltype(v)>::value_type;
         if (!v.empty()) memcpy(host.data() + off, v.data(), v.size() * sizeof(T));
-        dptr = reinterpret_cast<T*>(b->args.p + off);
+        dptr = reinterpret_cast<T*>(args.p + off);
         off += arr_bytes(v);
     };
     put(M.pack, D.pack);
@@ -317,18 +347,24 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M)
     put(M.zi, D.fft.zi);
     put(M.gather, D.gather);
     put(M.fin, D.fin);
-    MDF_CUDA_TRY(cudaMemcpyAsync(b->args.p, host.data(), total, cudaMemcpyHostToDevice, b->main));
+    MDF_CUDA_TRY(cudaMemcpyAsync(args.p, host.data(), total, cudaMemcpyHostToDevice, b->main));
     MDF_CUDA_TRY(cudaStreamSynchronize(b->main));
     return D;
 }
 
+// One batch evaluation in the multi form.  copies: the host<->device copies
+// of the batch's own pinned buffers at both ends (the plain graph); without
+// them the evaluation reads positions from d_pos and leaves forces where the
+// finalize arguments point (the pipelined stages).
 template <typename R>
-void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D)
+void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D, const double* d_pos, bool copies)
 {
     const int n = b->nsys, th = 256;
     const dim3 grid((unsigned)((b->max_len + th - 1) / th), (unsigned)n);
-    MDF_CUDA_TRY(cudaMemcpyAsync(b->d_pos.p, b->h_pos, sizeof(double) * b->total, cudaMemcpyHostToDevice, b->main));
-    k_batch_scatter<<<grid, th, 0, b->main>>>(b->d_off.p, b->d_pos.p, b->d_xyz_ptr.p);
+    if (copies)
+        MDF_CUDA_TRY(cudaMemcpyAsync(b->d_pos.p, b->h_pos, sizeof(double) * b->total, cudaMemcpyHostToDevice,
+                                     b->main));
+    k_batch_scatter<<<grid, th, 0, b->main>>>(b->d_off.p, d_pos, b->d_xyz_ptr.p);
     MDF_CUDA_TRY(cudaGetLastError());
     long long k = 2;   // scatter + finalize
     // side stream: exclusions, 1-4, bonded terms, PME (they only read positions
@@ -361,8 +397,9 @@ void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D)
     }
     MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, b->ev_join2, 0));
     launch_finalize_multi(D.fin, n, M.gx_fin, b->main);
-    MDF_CUDA_TRY(cudaMemcpyAsync(b->h_forces, b->d_forces.p, sizeof(double) * b->total, cudaMemcpyDeviceToHost,
-                                 b->main));
+    if (copies)
+        MDF_CUDA_TRY(cudaMemcpyAsync(b->h_forces, b->d_forces.p, sizeof(double) * b->total, cudaMemcpyDeviceToHost,
+                                     b->main));
     b->graph_kernels = k;
 }
 
@@ -376,14 +413,14 @@ void capture(mdf_batch* b, uint32_t flags)
     MultiDev<float> Df{};
     MultiDev<double> Dd{};
     if (b->multi) {
-        if (fp32) Df = prepare_multi<float>(b, flags, Mf);
-        else Dd = prepare_multi<double>(b, flags, Md);
+        if (fp32) Df = prepare_multi<float>(b, flags, Mf, b->d_forces.p, nullptr, b->args);
+        else Dd = prepare_multi<double>(b, flags, Md, b->d_forces.p, nullptr, b->args);
     }
     MDF_CUDA_TRY(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
     try {
         if (!b->multi) enqueue(b, flags);
-        else if (fp32) enqueue_multi<float>(b, Mf, Df);
-        else enqueue_multi<double>(b, Md, Dd);
+        else if (fp32) enqueue_multi<float>(b, Mf, Df, b->d_pos.p, true);
+        else enqueue_multi<double>(b, Md, Dd, b->d_pos.p, true);
     } catch (...) {
         cudaGraph_t g = nullptr;
         cudaStreamEndCapture(b->main, &g);
@@ -434,6 +471,101 @@ void collect(mdf_batch* b, uint32_t flags, double* forces, mdf_energies* e)
         if (e) host_energies(c, flags, e + s);
     }
     if (forces) memcpy(forces, b->h_forces, sizeof(double) * b->total);
+}
+
+// The graph of pipeline stage st: the multi-form evaluation reading the
+// stage's device positions and writing its device forces and host scalar blocks.
+void capture_stage(mdf_batch* b, uint32_t flags, int st)
+{
+    mdf_batch::Stage& S = b->stage[st];
+    if (S.exec) cudaGraphExecDestroy(S.exec);
+    if (S.graph) cudaGraphDestroy(S.graph);
+    S.exec = nullptr;
+    S.graph = nullptr;
+    if (!uniform_launches(b))
+        throw ApiError(MDF_ERR_UNSUPPORTED, "pipelined batches need the same launch parameters in every system");
+    const bool fp32 = b->sys[0]->c.p.precision == MDF_PREC_MIXED;
+    MultiArgs<float> Mf;
+    MultiArgs<double> Md;
+    MultiDev<float> Df{};
+    MultiDev<double> Dd{};
+    if (fp32) Df = prepare_multi<float>(b, flags, Mf, S.d_forces.p, S.d_hscal, S.args);
+    else Dd = prepare_multi<double>(b, flags, Md, S.d_forces.p, S.d_hscal, S.args);
+    MDF_CUDA_TRY(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
+    try {
+        if (fp32) enqueue_multi<float>(b, Mf, Df, S.d_pos.p, false);
+        else enqueue_multi<double>(b, Md, Dd, S.d_pos.p, false);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(b->main, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    MDF_CUDA_TRY(cudaStreamEndCapture(b->main, &S.graph));
+    MDF_CUDA_TRY(cudaGraphInstantiate(&S.exec, S.graph, 0));
+    S.graph_flags = flags;
+}
+
+void submit(mdf_batch* b, uint32_t flags, const double* xyz, double* forces)
+{
+    if (b->inflight >= 2) throw ApiError(MDF_ERR_STATE, "two batch evaluations in flight: collect one first");
+    if (!b->have_lists) {
+        // the first evaluation: lists from these positions (through the batch's own buffer)
+        if (xyz != b->h_pos) memcpy(b->h_pos, xyz, sizeof(double) * b->total);
+        b->have_positions = true;
+        build_lists(b);
+    }
+    if (!b->copy_in) MDF_CUDA_TRY(cudaStreamCreateWithFlags(&b->copy_in, cudaStreamNonBlocking));
+    if (!b->copy_out) MDF_CUDA_TRY(cudaStreamCreateWithFlags(&b->copy_out, cudaStreamNonBlocking));
+    mdf_batch::Stage& S = b->stage[b->stage_next];
+    if (!S.h_scal) {
+        MDF_CUDA_TRY(cudaHostAlloc((void**)&S.h_scal, sizeof(unsigned long long) * NUM_SCAL * (size_t)b->nsys,
+                                   cudaHostAllocMapped));
+        memset(S.h_scal, 0, sizeof(unsigned long long) * NUM_SCAL * (size_t)b->nsys);
+        MDF_CUDA_TRY(cudaHostGetDevicePointer((void**)&S.d_hscal, S.h_scal, 0));
+        for (cudaEvent_t* e : {&S.h2d, &S.consumed, &S.done, &S.d2h})
+            MDF_CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        S.d_pos.alloc(b->total);
+        S.d_forces.alloc(b->total);
+    }
+    if (!S.exec || S.graph_flags != flags) capture_stage(b, flags, b->stage_next);
+    // positions in (the stage buffer is free once its last evaluation ran)
+    MDF_CUDA_TRY(cudaStreamWaitEvent(b->copy_in, S.consumed, 0));
+    MDF_CUDA_TRY(cudaMemcpyAsync(S.d_pos.p, xyz, sizeof(double) * b->total, cudaMemcpyHostToDevice, b->copy_in));
+    MDF_CUDA_TRY(cudaEventRecord(S.h2d, b->copy_in));
+    // the evaluation, after its positions and after the stage's last forces left
+    MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, S.h2d, 0));
+    MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, S.d2h, 0));
+    MDF_CUDA_TRY(cudaGraphLaunch(S.exec, b->main));
+    MDF_CUDA_TRY(cudaEventRecord(S.consumed, b->main));
+    MDF_CUDA_TRY(cudaEventRecord(S.done, b->main));
+    // forces out
+    MDF_CUDA_TRY(cudaStreamWaitEvent(b->copy_out, S.done, 0));
+    if (forces)
+        MDF_CUDA_TRY(cudaMemcpyAsync(forces, S.d_forces.p, sizeof(double) * b->total, cudaMemcpyDeviceToHost,
+                                     b->copy_out));
+    MDF_CUDA_TRY(cudaEventRecord(S.d2h, b->copy_out));
+    S.flags = flags;
+    b->stage_next ^= 1;
+    ++b->inflight;
+}
+
+void collect_stage(mdf_batch* b, mdf_energies* e)
+{
+    if (b->inflight == 0) throw ApiError(MDF_ERR_STATE, "no submitted batch evaluation to collect");
+    mdf_batch::Stage& S = b->stage[b->stage_old];
+    b->stage_old ^= 1;
+    --b->inflight;
+    MDF_CUDA_TRY(cudaEventSynchronize(S.d2h));
+    for (int s = 0; s < b->nsys; ++s) {
+        const unsigned long long* hs = S.h_scal + (size_t)s * NUM_SCAL;
+        try {
+            check_status_word(hs);
+        } catch (const ApiError& err) {
+            throw ApiError(err.status, "system " + std::to_string(s) + ": " + err.msg);
+        }
+        if (e) host_energies_from(b->sys[s]->c, hs, S.flags, e + s);
+    }
 }
 
 }  // namespace
@@ -520,6 +652,19 @@ void mdf_batch_destroy(mdf_batch* b)
     if (b->ev_join2) cudaEventDestroy(b->ev_join2);
     if (b->side) cudaStreamDestroy(b->side);
     b->args.release();
+    for (auto& S : b->stage) {
+        if (S.h_scal) cudaFreeHost(S.h_scal);
+        for (cudaEvent_t e : {S.h2d, S.consumed, S.done, S.d2h})
+            if (e) cudaEventDestroy(e);
+        S.d_pos.release();
+        S.d_forces.release();
+        S.args.release();
+    }
+    for (cudaStream_t cs : {b->copy_in, b->copy_out})
+        if (cs) {
+            cudaStreamSynchronize(cs);
+            cudaStreamDestroy(cs);
+        }
     if (b->main) cudaStreamDestroy(b->main);
     delete b;
 }
@@ -591,6 +736,24 @@ int mdf_batch_launch(mdf_batch* b, uint32_t flags, void* stream)
             MDF_CUDA_TRY(cudaEventRecord(b->join[0], b->main));
             MDF_CUDA_TRY(cudaStreamWaitEvent((cudaStream_t)stream, b->join[0], 0));
         }
+    });
+}
+
+int mdf_batch_submit(mdf_batch* b, uint32_t flags, const double* xyz, double* forces)
+{
+    if (!b || !xyz) return MDF_ERR_INVALID;
+    return batch_guard(b, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(b->device));
+        submit(b, flags, xyz, forces);
+    });
+}
+
+int mdf_batch_collect(mdf_batch* b, mdf_energies* energies)
+{
+    if (!b) return MDF_ERR_INVALID;
+    return batch_guard(b, [&] {
+        MDF_CUDA_TRY(cudaSetDevice(b->device));
+        collect_stage(b, energies);
     });
 }
 

@@ -222,23 +222,9 @@ struct ZeroArgs {
     long long n;
 };
 
-// One work item of the charge spread: the clusters of up to four
-// neighbouring pairlist columns (a tile of TX x TY columns) whose centres lie
-// in one window of W grid planes along z.  cb/ce: cluster range per column of
-// the tile (empty where the tile is narrower); ref: the grid point the
-// item's box is laid out from (the tile's lower x, y grid line and the
-// window's first plane).
-struct SpreadItem {
-    int cb[4];
-    int ce[4];
-    int ref[4];
-};
-
 struct SpreadArgs {
     int gx, gy;
-    int i0, i1;                  // this launch's items
-    const SpreadItem* items;
-    int cap;                     // grid points of the shared-memory box
+    int s0, s1;
     const int* slot_atom;
     const double* xyz;
     const double* q;
@@ -366,8 +352,6 @@ BondedArgs make_bonded_args(const Ctx& c, bool whole, unsigned long long* f, uns
 void launch_bonded_multi(const BondedArgs* d_args, int nsys, int gx, bool energy, cudaStream_t s);
 template <typename R> FFTChain<R> make_fft_chain(const Ctx& c, bool energy);
 SpreadArgs make_spread_args(const Ctx& c);
-void build_spread_items(Ctx& c);
-size_t spread_smem_bytes();
 template <typename R> GatherArgs<R> make_gather_args(const Ctx& c);
 template <typename R>
 void launch_pme_multi(const ZeroArgs* d_zero, int zx, const SpreadArgs* d_spread, int sx, const FFTChainDev<R>& D,

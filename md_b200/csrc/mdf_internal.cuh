@@ -184,8 +184,6 @@ struct Ctx {
     DevBuf<ILRange> ilist_h;       // half layout: [2 n_clusters] items (ILRange.pad = half)
     DevBuf<PairEntry> plist_h;     // half layout: [2 x outer capacity]
     bool pruned_half = false;      // the last prune wrote the half lists
-    DevBuf<unsigned char> spread_items;   // SpreadItem [n_spread_items], rebuilt with the pairlist
-    int n_spread_items = 0;
     int since_prune = 0;
     bool pruned_valid = false;
     DevBuf<int> scan_tmp;

@@ -1009,7 +1009,6 @@ void build_pairlist(Ctx& c)
         c.n_in.alloc(1);
         c.pruned_valid = false;
         c.since_prune = 0;
-        build_spread_items(c);
         c.have_list = true;
         return;
     }

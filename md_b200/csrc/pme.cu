@@ -515,267 +515,86 @@ __device__ __forceinline__ R bspline4_one(R w, int j)
 // grid words are identical to the one-thread-per-atom form's (the same
 // rounded fixed-point values, summed in any order).  Launched with a
 // multiple of 16 threads per block.
-// ------------------------------------------------------------ charge spread
-// Work items are tiles of TX x TY pairlist columns times windows of W grid
-// planes along z (built with the pairlist).  One block per item: the item's
-// atoms are spread into a box of the grid in shared memory (the union of
-// their 4 x 4 x 4 stencils), and the box is then added to the global grid
-// one z run per warp instruction, each grid point of the box once.  The
-// fixed-point value of every stencil point (2^-40, the same int64 as a direct
-// spread) is split as hi * 2^20 + lo with lo in [0, 2^20), and the two parts
-// are summed with 32-bit shared atomics, so the box holds the exact int64 sum
-// and the grid receives bit for bit the sum that direct int64 reductions of
-// every point would give.  The hi sums stay inside int32 while the item's sum
-// of |q| stays below 6000 (|hi| <= 0.3 |q| 2^20 per point), the lo sums while
-// it has at most 2048 charged atoms; an item beyond either bound, or whose
-// box exceeds the shared memory, adds its points straight to the global grid.
-constexpr int SPREAD_THREADS = 256;
-constexpr int SPREAD_BOX_CAP = 6912;   // grid points of the shared box (54 KB: four blocks per SM)
-
-size_t spread_smem_bytes() { return 2 * sizeof(int) * (size_t)SPREAD_BOX_CAP; }
-
-// z stride of the box: the four rows of one atom's 16 lanes (4 rows x 4
-// consecutive z) land in distinct banks when k S mod 32 stays at least 4 away
-// from 0 for k = 1, 2, 3
-__host__ __device__ __forceinline__ int spread_zstride(int ez)
-{
-    int S = ez;
-    for (int it = 0; it < 32; ++it, ++S) {
-        bool ok = true;
-        for (int k = 1; k <= 3; ++k) {
-            const int m = (k * S) & 31;
-            if (m <= 3 || m >= 29) ok = false;
-        }
-        if (ok) break;
-    }
-    return S;
-}
-
-// Stencil base of atom a (points base - 1 .. base + 2 per dimension) and the
-// fraction past it; false for a non-finite position.
-__device__ __forceinline__ bool spread_point(const double* __restrict__ xyz, int a, const GridGeom& g, int base[3],
-                                             double u[3])
-{
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        double v = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
-        if (!(v >= 0.0 && v <= (double)g.K[d])) return false;
-        if (v >= g.K[d]) v -= g.K[d];
-        const int b = min((int)floor(v), g.K[d] - 1);
-        base[d] = b;
-        u[d] = v - b;
-    }
-    return true;
-}
-
-// Grid offset of base from the item's reference point, in [-K/2, K - K/2).
-__device__ __forceinline__ int spread_rel(int base, int ref, int K)
-{
-    int r = base - ref;
-    const int half = K >> 1;
-    if (r >= K - half) r -= K;
-    if (r < -half) r += K;
-    return r;
-}
-
-__device__ __forceinline__ int wrap_index(int v, int K)
-{
-    v %= K;
-    return v < 0 ? v + K : v;
-}
-
 template <typename R>
-__device__ __forceinline__ long long spread_fixed(R v)
+__device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A)
 {
-    if (sizeof(R) == 4) return __float2ll_rn((float)v * 1099511627776.0f);   // exact 2^40 scaling
-    return __double2ll_rn((double)v * GRID_SCALE);
-}
-
-template <typename R>
-__device__ __forceinline__ void spread_tiles_dev(const SpreadArgs& A, int item)
-{
-    extern __shared__ int s_box[];   // hi parts [cap] | lo parts [cap]
-    __shared__ int s_mn[3], s_mx[3], s_cnt, s_pre[5], s_cb[4], s_ref[3], s_mode, s_S;
-    __shared__ unsigned s_aq;
+    const int s0 = A.s0, s1 = A.s1;
     const int* __restrict__ slot_atom = A.slot_atom;
     const double* __restrict__ xyz = A.xyz;
     const double* __restrict__ q = A.q;
     const GridGeom& g = A.g;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const unsigned FULL = 0xffffffffu;
-    if (tid == 0) {
-        const SpreadItem it = A.items[item];
-        int pre = 0;
-        for (int j = 0; j < 4; ++j) {
-            s_pre[j] = pre;
-            s_cb[j] = it.cb[j];
-            pre += CLUSTER * max(0, it.ce[j] - it.cb[j]);
-        }
-        s_pre[4] = pre;
-        for (int d = 0; d < 3; ++d) {
-            s_ref[d] = it.ref[d];
-            s_mn[d] = INT_MAX;
-            s_mx[d] = INT_MIN;
-        }
-        s_cnt = 0;
-        s_aq = 0u;
-    }
-    __syncthreads();
-    const int ns = s_pre[4];
-    auto slot_of = [&](int k) {
-        const int j = (k >= s_pre[1]) + (k >= s_pre[2]) + (k >= s_pre[3]);
-        return s_cb[j] * CLUSTER + (k - s_pre[j]);
-    };
-    // pass 1: the box (extent of the item's stencils around its reference
-    // point), the number of charged atoms and their sum of |q| (1/1024 units)
-    for (int k0 = 0; k0 < ns; k0 += SPREAD_THREADS) {
-        const int k = k0 + tid;
-        int mn[3] = {INT_MAX, INT_MAX, INT_MAX}, mx[3] = {INT_MIN, INT_MIN, INT_MIN}, cnt = 0;
-        unsigned aq = 0u;
-        if (k < ns) {
-            const int a = slot_atom[slot_of(k)];
-            const double qa = a >= 0 ? q[a] : 0.0;
-            if (qa != 0.0) {
-                int b[3];
-                double u[3];
-                if (spread_point(xyz, a, g, b, u)) {
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) mn[d] = mx[d] = spread_rel(b[d], s_ref[d], g.K[d]);
-                    cnt = 1;
-                    aq = (unsigned)fmin(ceil(fabs(qa) * 1024.0), 1048576.0);
-                } else {
-                    status_set(A.st, ST_NONFINITE);
-                }
-            }
-        }
+    unsigned long long* __restrict__ qgrid = A.qgrid;
+    unsigned* st = A.st;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = s0 + (int)(t0 >> 4);
+    const int l = (int)(t0 & 15), r = l >> 2, zz = l & 3;
+    // the whole group of 16 lanes leaves together (same atom)
+    if (s >= s1) return;
+    const int a = slot_atom[s];
+    if (a < 0) return;
+    const double qa = q[a];
+    if (qa == 0.0) return;
+    const unsigned grp = 0xffffu << (threadIdx.x & 16);
+    int base[3] = {0, 0, 0};
+    double u[3] = {0, 0, 0};
+    int bad = 0;
+    if (l == 0) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-            mn[d] = __reduce_min_sync(FULL, mn[d]);
-            mx[d] = __reduce_max_sync(FULL, mx[d]);
-        }
-        cnt = __reduce_add_sync(FULL, cnt);
-        aq = __reduce_add_sync(FULL, aq);
-        if (lane == 0 && cnt) {
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                atomicMin(&s_mn[d], mn[d]);
-                atomicMax(&s_mx[d], mx[d]);
-            }
-            atomicAdd(&s_cnt, cnt);
-            atomicAdd(&s_aq, aq);
+            double v = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
+            if (!(v >= 0.0 && v <= (double)g.K[d])) bad = 1;   // non-finite position
+            if (v >= g.K[d]) v -= g.K[d];
+            const int b = bad ? 0 : min((int)floor(v), g.K[d] - 1);
+            base[d] = b;
+            u[d] = v - b;
         }
     }
-    __syncthreads();
-    if (tid == 0) {
-        int mode = 0;   // 0: nothing to spread, 1: shared box, 2: straight to the grid
-        int S = 0;
-        if (s_cnt > 0) {
-            const int ex = s_mx[0] - s_mn[0] + 4, ey = s_mx[1] - s_mn[1] + 4, ez = s_mx[2] - s_mn[2] + 4;
-            S = spread_zstride(ez);
-            const long long vol = (long long)ex * ey * S;
-            mode = (vol <= A.cap && s_cnt <= 2048 && s_aq <= 6000u * 1024u) ? 1 : 2;
-        }
-        s_mode = mode;
-        s_S = S;
+    bad = __shfl_sync(grp, bad, 0, 16);
+    if (bad) {
+        if (l == 0) status_set(st, ST_NONFINITE);
+        return;
     }
-    __syncthreads();
-    const int mode = s_mode;
-    if (mode == 0) return;
-    const int S = s_S;
-    const int ey = s_mx[1] - s_mn[1] + 4, ez = s_mx[2] - s_mn[2] + 4, ex = s_mx[0] - s_mn[0] + 4;
-    int* __restrict__ sH = s_box;
-    unsigned* __restrict__ sL = reinterpret_cast<unsigned*>(s_box + A.cap);
-    if (mode == 1) {
-        const int vol = ex * ey * S;
-        for (int i = tid; i < vol; i += SPREAD_THREADS) {
-            sH[i] = 0;
-            sL[i] = 0u;
-        }
-        __syncthreads();
+    R w[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        base[d] = __shfl_sync(grp, base[d], 0, 16);
+        w[d] = (R)__shfl_sync(grp, u[d], 0, 16);
     }
-    // pass 2: 16 lanes per atom, lane (r, zz) adds points (t, r, zz), t = 0..3
-    {
-        const int grp = tid >> 4, l = tid & 15, r = l >> 2, zz = l & 3;
-        const unsigned gmask = 0xffffu << (tid & 16);
-        for (int k0 = 0; k0 < ns; k0 += SPREAD_THREADS / 16) {
-            const int k = k0 + grp;
-            if (k >= ns) break;
-            const int a = slot_atom[slot_of(k)];
-            if (a < 0) continue;
-            const double qa = q[a];
-            if (qa == 0.0) continue;
-            int base[3] = {0, 0, 0};
-            double u[3] = {0, 0, 0};
-            int ok = 0;
-            if (l == 0) ok = spread_point(xyz, a, g, base, u) ? 1 : 0;
-            ok = __shfl_sync(gmask, ok, 0, 16);
-            if (!ok) continue;
-            R w[3];
+    R thx[4];
+    bspline4<R>(w[0], thx, nullptr);
+    const R thy = bspline4_one<R>(w[1], r), thz = bspline4_one<R>(w[2], zz);
+    int ky = base[1] - 1 + r;
+    ky += (ky < 0) ? g.K[1] : 0;
+    ky -= (ky >= g.K[1]) ? g.K[1] : 0;
+    int kz = base[2] - 1 + zz;
+    kz += (kz < 0) ? g.K[2] : 0;
+    kz -= (kz >= g.K[2]) ? g.K[2] : 0;
+    const R qr = (R)qa;
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                base[d] = __shfl_sync(gmask, base[d], 0, 16);
-                w[d] = (R)__shfl_sync(gmask, u[d], 0, 16);
-            }
-            R thx[4];
-            bspline4<R>(w[0], thx, nullptr);
-            const R thy = bspline4_one<R>(w[1], r), thz = bspline4_one<R>(w[2], zz);
-            const R qr = (R)qa;
-            if (mode == 1) {
-                const int ix = spread_rel(base[0], s_ref[0], g.K[0]) - s_mn[0];
-                const int iy = spread_rel(base[1], s_ref[1], g.K[1]) - s_mn[1] + r;
-                const int iz = spread_rel(base[2], s_ref[2], g.K[2]) - s_mn[2] + zz;
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    const long long fx = spread_fixed<R>(qr * thx[t] * thy * thz);
-                    const int idx = ((ix + t) * ey + iy) * S + iz;
-                    atomicAdd(sH + idx, (int)(fx >> 20));
-                    atomicAdd(sL + idx, (unsigned)(fx & 0xfffffLL));
-                }
-            } else {
-                const int ky = wrap_index(base[1] - 1 + r, g.K[1]), kz = wrap_index(base[2] - 1 + zz, g.K[2]);
-#pragma unroll
-                for (int t = 0; t < 4; ++t) {
-                    const int kx = wrap_index(base[0] - 1 + t, g.K[0]);
-                    const long long fx = spread_fixed<R>(qr * thx[t] * thy * thz);
-                    atomicAdd(A.qgrid + ((long long)kx * g.K[1] + ky) * g.K[2] + kz, (unsigned long long)fx);
-                }
-            }
-        }
-    }
-    if (mode != 1) return;
-    __syncthreads();
-    // the box into the grid: one (x, y) row per warp, lanes along z
-    const int rows = ex * ey;
-    for (int row = warp; row < rows; row += SPREAD_THREADS / 32) {
-        const int x = row / ey, y = row - x * ey;
-        const int gx = wrap_index(s_ref[0] + s_mn[0] - 1 + x, g.K[0]);
-        const int gy = wrap_index(s_ref[1] + s_mn[1] - 1 + y, g.K[1]);
-        const int gz0 = wrap_index(s_ref[2] + s_mn[2] - 1, g.K[2]);
-        unsigned long long* __restrict__ rowp = A.qgrid + ((long long)gx * g.K[1] + gy) * g.K[2];
-        for (int z = lane; z < ez; z += 32) {
-            const int hv = sH[row * S + z];
-            const unsigned lv = sL[row * S + z];
-            if (hv != 0 || lv != 0u) {
-                int gz = gz0 + z;
-                while (gz >= g.K[2]) gz -= g.K[2];
-                atomicAdd(rowp + gz, (unsigned long long)((long long)hv * 1048576LL + (long long)lv));
-            }
-        }
+    for (int t = 0; t < 4; ++t) {
+        int kx = base[0] - 1 + t;
+        kx += (kx < 0) ? g.K[0] : 0;
+        kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+        const R v = qr * thx[t] * thy * thz;
+        long long fx;
+        if (sizeof(R) == 4) fx = __float2ll_rn((float)v * 1099511627776.0f);   // exact 2^40 scaling
+        else fx = __double2ll_rn((double)v * GRID_SCALE);
+        atomicAdd(qgrid + ((long long)kx * g.K[1] + ky) * g.K[2] + kz, (unsigned long long)fx);
     }
 }
 
 template <typename R>
-__global__ void __launch_bounds__(SPREAD_THREADS, 4) k_spread_tiles(SpreadArgs A)
+__global__ void __launch_bounds__(256) k_spread4_rows(SpreadArgs A)
 {
-    spread_tiles_dev<R>(A, A.i0 + (int)blockIdx.x);
+    spread4_rows_dev<R>(A);
 }
 
 template <typename R>
-__global__ void __launch_bounds__(SPREAD_THREADS, 4) k_spread_tiles_multi(const SpreadArgs* __restrict__ As)
+__global__ void __launch_bounds__(256) k_spread4_rows_multi(const SpreadArgs* __restrict__ As)
 {
     const SpreadArgs& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;
-    spread_tiles_dev<R>(A, A.i0 + (int)blockIdx.x);
+    spread4_rows_dev<R>(A);
 }
 
 // Clear many systems' charge grids in one launch.
@@ -1315,95 +1134,16 @@ template void launch_fft_chain_multi<float>(const FFTChainDev<float>&, int, cons
 template void launch_fft_chain_multi<double>(const FFTChainDev<double>&, int, const FFTChainMax&, bool,
                                              cudaStream_t);
 
-template <typename R>
-static void launch_spread(const SpreadArgs& S, cudaStream_t st)
-{
-    if (S.gx <= 0) return;
-    MDF_CUDA_TRY(cudaFuncSetAttribute(k_spread_tiles<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)spread_smem_bytes()));
-    k_spread_tiles<R><<<S.gx, SPREAD_THREADS, spread_smem_bytes(), st>>>(S);
-    MDF_CUDA_TRY(cudaGetLastError());
-}
-
-// The spread's work items: thread per pairlist column; it walks its column's
-// clusters (ordered by z) once and cuts them at the window boundaries.
-__global__ void k_spread_items(int ncx, int ncy, int TX, int TY, int ntx, int nw, int W, int K0, int K1,
-                               double zstep, const int* __restrict__ col_cstart, const double4* __restrict__ center,
-                               SpreadItem* __restrict__ items)
-{
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= ncx * ncy) return;
-    const int cx = col % ncx, cy = col / ncx;
-    const int tx = cx / TX, ty = cy / TY, j = (cx - tx * TX) + TX * (cy - ty * TY);
-    const int c1 = col_cstart[col + 1];
-    int p = col_cstart[col];
-    SpreadItem* __restrict__ it = items + (size_t)(ty * ntx + tx) * nw;
-    for (int w = 0; w < nw; ++w) {
-        const int b = p;
-        if (w == nw - 1) {
-            p = c1;
-        } else {
-            const double zt = (w + 1) * zstep;
-            while (p < c1 && center[p].z < zt) ++p;
-        }
-        it[w].cb[j] = b;
-        it[w].ce[j] = p;
-        if (j == 0) {
-            it[w].ref[0] = (int)floor((double)(tx * TX) * K0 / ncx);
-            it[w].ref[1] = (int)floor((double)(ty * TY) * K1 / ncy);
-            it[w].ref[2] = w * W;
-            it[w].ref[3] = 0;
-        }
-    }
-}
-
-// Tile shape and window height: the largest (2 x 2 columns, 16 planes first)
-// whose box around a tile's atoms, with a skin's drift, fills at most 80% of
-// the shared box; boxes that still overflow at run time go straight to the grid.
-void build_spread_items(Ctx& c)
-{
-    c.n_spread_items = 0;
-    if (c.K[0] <= 0 || c.ncols <= 0) return;
-    const double drift = 0.5 * std::max(0.0, c.p.skin);
-    auto extent = [&](int T, int d, int nc) {
-        return (int)std::ceil(T * (double)c.K[d] / nc) + 4 + 2 * (int)std::ceil(drift * c.K[d] / c.box[d]);
-    };
-    const int shapes[4][3] = {{2, 2, 16}, {2, 2, 8}, {1, 1, 16}, {1, 1, 8}};
-    int TX = 1, TY = 1, W = 8;
-    for (const auto& sh : shapes) {
-        TX = std::min(sh[0], c.ncol_x);
-        TY = std::min(sh[1], c.ncol_y);
-        W = std::min(sh[2], c.K[2]);
-        const int ez = W + 4 + 2 * (int)std::ceil(drift * c.K[2] / c.box[2]);
-        const long long vol = (long long)extent(TX, 0, c.ncol_x) * extent(TY, 1, c.ncol_y) * spread_zstride(ez);
-        if (vol <= (long long)(0.8 * SPREAD_BOX_CAP)) break;
-    }
-    const int ntx = (c.ncol_x + TX - 1) / TX, nty = (c.ncol_y + TY - 1) / TY, nw = (c.K[2] + W - 1) / W;
-    const long long n = (long long)ntx * nty * nw;
-    c.spread_items.alloc(sizeof(SpreadItem) * (size_t)n);
-    MDF_CUDA_TRY(cudaMemsetAsync(c.spread_items.p, 0, sizeof(SpreadItem) * (size_t)n, c.stream));
-    const double zstep = W * c.box[2] / c.K[2];
-    k_spread_items<<<grid_blocks(c.ncols, 128), 128, 0, c.stream>>>(
-        c.ncol_x, c.ncol_y, TX, TY, ntx, nw, W, c.K[0], c.K[1], zstep, c.col_cstart.p, c.center.p,
-        reinterpret_cast<SpreadItem*>(c.spread_items.p));
-    MDF_CUDA_TRY(cudaGetLastError());
-    c.n_spread_items = (int)n;
-}
-
-// Spread arguments of this rank's work items and gather arguments of its
-// slots (PHYSICAL, order 4).  The items partition the clusters, so any split
-// over ranks sums to the same grid.
+// Spread and gather arguments of this rank's slots (PHYSICAL, order 4).
 SpreadArgs make_spread_args(const Ctx& c)
 {
     SpreadArgs A;
-    long long i0, i1;
-    rank_slice(c, c.n_spread_items, i0, i1);   // this rank's items (all of them with one rank)
-    A.i0 = (int)i0;
-    A.i1 = (int)i1;
-    A.gx = (int)(i1 - i0);
+    long long s0, s1;
+    rank_slice(c, c.n_slots, s0, s1);   // this rank's slots (all of them with one rank)
+    A.s0 = (int)s0;
+    A.s1 = (int)s1;
+    A.gx = grid_blocks(16 * (s1 - s0), 256);
     A.gy = 1;
-    A.items = reinterpret_cast<const SpreadItem*>(c.spread_items.p);
-    A.cap = SPREAD_BOX_CAP;
     A.slot_atom = c.slot_atom.p;
     A.xyz = c.xyz.p;
     A.q = c.q.p;
@@ -1451,7 +1191,7 @@ static void run_pme(Ctx& c, bool energy)
     const int th = 256;
     if (!ref) {
         const SpreadArgs S = make_spread_args(c);
-        launch_spread<R>(S, c.stream);
+        if (S.s1 > S.s0) k_spread4_rows<R><<<grid_of(S), th, 0, c.stream>>>(S);
         if (distributed(c)) allreduce_u64(c, c.qgrid.p, ntot);   // the whole charge grid on every rank
     } else {
         k_spread_ref5<<<grid_blocks(c.N, th), th, 0, c.stream>>>(c.N, c.xyz.p, c.q.p, B.g, c.qgrid.p);
@@ -1548,7 +1288,8 @@ static void run_pme_slab(Ctx& c, bool energy)
     const int th = 256;
     MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * (size_t)P * K0p * plane, c.stream));
     const SpreadArgs S = make_spread_args(c);
-    launch_spread<R>(S, c.stream);
+    if (S.s1 > S.s0) k_spread4_rows<R><<<grid_of(S), th, 0, c.stream>>>(S);
+    MDF_CUDA_TRY(cudaGetLastError());
     coll_check(c.coll_rs(reinterpret_cast<const uint64_t*>(c.qgrid.p), reinterpret_cast<uint64_t*>(c.q_slab.p),
                          (int64_t)K0p * plane, (void*)c.stream, c.coll_user),
                "reduce-scatter");
@@ -1604,11 +1345,7 @@ void launch_pme_multi(const ZeroArgs* d_zero, int zx, const SpreadArgs* d_spread
                       cudaStream_t s)
 {
     k_zero_multi<<<dim3(zx, 1, nsys), 256, 0, s>>>(d_zero);
-    if (sx > 0) {
-        MDF_CUDA_TRY(cudaFuncSetAttribute(k_spread_tiles_multi<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)spread_smem_bytes()));
-        k_spread_tiles_multi<R><<<dim3(sx, 1, nsys), SPREAD_THREADS, spread_smem_bytes(), s>>>(d_spread);
-    }
+    k_spread4_rows_multi<R><<<dim3(sx, 1, nsys), 256, 0, s>>>(d_spread);
     MDF_CUDA_TRY(cudaGetLastError());
     launch_fft_chain_multi<R>(D, nsys, M, energy, s);
     k_gather4_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_gather);

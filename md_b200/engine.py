@@ -24,7 +24,7 @@ EXPORTS = [
     "mdf_kernel_launches", "mdf_probe_fma_tflops", "mdf_probe_l2_reductions", "mdf_compute_bonded_noalloc", "mdf_set_parameters",
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_host_buffers", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
-    "mdf_batch_fetch", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
+    "mdf_batch_fetch", "mdf_batch_submit", "mdf_batch_collect", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
     "mdf_pme_grids", "mdf_set_allreduce", "mdf_set_collectives", "mdf_autotune", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
@@ -105,6 +105,8 @@ def library(path=None):
     lib.mdf_batch_compute.argtypes = [vp, C.c_uint32, dp, C.POINTER(abi.mdf_energies)]
     lib.mdf_batch_launch.argtypes = [vp, C.c_uint32, vp]
     lib.mdf_batch_fetch.argtypes = [vp, C.c_uint32, dp, C.POINTER(abi.mdf_energies)]
+    lib.mdf_batch_submit.argtypes = [vp, C.c_uint32, dp, dp]
+    lib.mdf_batch_collect.argtypes = [vp, C.POINTER(abi.mdf_energies)]
     lib.mdf_batch_autotune.argtypes = [vp, C.c_int, C.POINTER(abi.mdf_tune_report)]
     lib.mdf_compute_bonded_noalloc.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.POINTER(abi.mdf_energies)]
     _LIB = lib
@@ -520,6 +522,21 @@ class Batch:
         flags = abi.MDF_COMPUTE_FORCES | (abi.MDF_COMPUTE_ENERGY if energy else 0)
         self._check(self.lib.mdf_batch_fetch(self.h, flags, C.cast(forces_ptr, C.POINTER(C.c_double))
                                              if forces_ptr else None, None), "fetch")
+
+    def submit(self, xyz_ptr, forces_ptr, energy=True):
+        """Pipelined evaluation (mdf_batch_submit): positions from the pinned
+        host buffer at xyz_ptr (all systems, concatenated), forces into the one
+        at forces_ptr; at most two in flight, collect() in order."""
+        flags = abi.MDF_COMPUTE_FORCES | (abi.MDF_COMPUTE_ENERGY if energy else 0)
+        self._check(self.lib.mdf_batch_submit(self.h, flags, C.cast(xyz_ptr, C.POINTER(C.c_double)),
+                                              C.cast(forces_ptr, C.POINTER(C.c_double)) if forces_ptr else None),
+                    "submit")
+
+    def collect(self, energy=True):
+        """Wait for the oldest submitted evaluation; its energies per system."""
+        E = (abi.mdf_energies * self.n)() if energy else None
+        self._check(self.lib.mdf_batch_collect(self.h, E), "collect")
+        return [E[k].as_dict() for k in range(self.n)] if energy else None
 
     def autotune(self, reps=5):
         r = abi.mdf_tune_report()

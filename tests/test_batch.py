@@ -149,3 +149,52 @@ def test_mixed_batch_matches_oracle_every_system(layout):
         tot2 = sum(e2[abi.E_INDEX[t]] for t in TERMS[:-1])
         assert H.rel(E["total"], tot2) < 1e-6, (s.name, E["total"], tot2)
     b.close()
+
+
+def test_batch_submit_collect_pipelined_equals_compute():
+    """Pipelined batches (mdf_batch_submit / mdf_batch_collect, two in flight,
+    copies on their own streams) give the plain batch's forces and energies
+    bit for bit, frame by frame; a fresh batch's first submission builds its
+    lists from the submitted positions."""
+    ss = systems()
+    flats = _flats(ss)
+    rng = np.random.default_rng(21)
+    frames = [np.concatenate([s.coords + rng.uniform(-0.1, 0.1, s.coords.shape) for s in ss]) for _ in range(4)]
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
+    b.set_positions(frames[0])
+    b.build_pairlists()
+    ref = []
+    for x in frames:
+        b.set_positions(x)
+        res = b.compute()
+        ref.append((np.concatenate([f for _, f in res]), [e for e, _ in res]))
+    outs = [np.zeros_like(x) for x in frames]
+    got = []
+    b.submit(frames[0].ctypes.data, outs[0].ctypes.data)
+    for k in range(1, len(frames)):
+        b.submit(frames[k].ctypes.data, outs[k].ctypes.data)
+        got.append(b.collect())
+    got.append(b.collect())
+    for k in range(len(frames)):
+        assert np.array_equal(outs[k].reshape(-1, 3), ref[k][0]), k
+        for e, e_ref in zip(got[k], ref[k][1]):
+            assert e["total"] == e_ref["total"] and e["ee_recip"] == e_ref["ee_recip"], k
+    # a third submission without a collect is refused
+    b.submit(frames[0].ctypes.data, outs[0].ctypes.data)
+    b.submit(frames[1].ctypes.data, outs[1].ctypes.data)
+    with pytest.raises(engine.MDFError):
+        b.submit(frames[2].ctypes.data, outs[2].ctypes.data)
+    b.collect(); b.collect()
+    b.close()
+    # fresh batch: the first submission builds the lists
+    b2 = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
+    out = np.zeros_like(frames[0])
+    b2.submit(frames[0].ctypes.data, out.ctypes.data)
+    e = b2.collect()
+    b2.close()
+    b3 = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **KW)
+    b3.set_positions(frames[0])
+    res = b3.compute()
+    b3.close()
+    assert np.array_equal(out.reshape(-1, 3), np.concatenate([f for _, f in res]))
+    assert all(x["total"] == r[0]["total"] for x, r in zip(e, res))

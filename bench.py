@@ -604,7 +604,7 @@ def batch_bench(dev, members, stream, steps=20):
     # positions in and forces out through pinned buffers on their own copy
     # streams while the GPU computes; wall clock of the whole loop
     xin = [torch.from_numpy(pos_h.copy()).pin_memory() for _ in range(2)]
-    fout = [torch.empty(len(pos_h), dtype=torch.float64).pin_memory() for _ in range(2)]
+    fout = [torch.empty(pos_h.size, dtype=torch.float64).pin_memory() for _ in range(2)]
     for k in range(4):
         b.submit(xin[k % 2].data_ptr(), fout[k % 2].data_ptr())
         if k >= 1:

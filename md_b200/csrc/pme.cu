@@ -419,8 +419,10 @@ __global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv(FFTXArgs<R> A)
     fft_x_conv_dev<R, ENERGY>(A);
 }
 
+// 64 registers (eight blocks per SM): the many-system grids are small and the
+// pass is latency bound, so resident warps matter more than registers here
 template <typename R, bool ENERGY>
-__global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv_multi(const FFTXArgs<R>* __restrict__ As)
+__global__ void __launch_bounds__(FFT_THREADS, 8) k_fft_x_conv_multi(const FFTXArgs<R>* __restrict__ As)
 {
     const FFTXArgs<R>& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx || (int)blockIdx.y >= A.gy) return;

@@ -461,11 +461,14 @@ def md_bench(dev, steps=1000, equil=200):
     Steps/s is the host wall time of mdf_md_run (graph chunks of 10 steps,
     list rebuilds and the per-chunk energy read-back included); the energy
     drift is last minus first sample of the total energy over the measured
-    steps, mixed against FP64 from the same start."""
+    steps, mixed against FP64 from the same start.  The pair lists prune
+    themselves on the device (prune_every < 0, 0.2 A margin: the prune kernel
+    runs when an atom moved more than 0.1 A since the last prune)."""
     from md_b200 import abi, engine, synth, topology
     s = synth.make_config("c4")
     flat = topology.flatten(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
-    kw = dict(semantics=abi.MDF_SEM_PHYSICAL, ewald_tol=1e-5, grid=synth.GRIDS["c4"], device=dev)
+    kw = dict(semantics=abi.MDF_SEM_PHYSICAL, ewald_tol=1e-5, grid=synth.GRIDS["c4"], device=dev,
+              prune_every=-1, prune_margin=0.2)
     eng = engine.Engine(flat, s.box, precision=abi.MDF_PREC_MIXED, **kw)
     eng.set_positions(s.coords)
     eng.build_pairlist()
@@ -507,8 +510,8 @@ def md_bench(dev, steps=1000, equil=200):
                    "charged atom) is bound by L2 reduction throughput, spread_l2_frac is against the measured "
                    "L2 reduction peak; the gather by L1/L2 latency of its 64 loads per atom")
     out = {"workload": "c4: %d atoms (320,000 flexible waters), 215 A box, PME 216^3, cutoff 10 A, skin 2 A, "
-                       "dt 0.5 fs, NVE, list rebuilt every 10 steps, %d measured steps after %d equilibration "
-                       "steps" % (s.natoms, steps, equil),
+                       "dt 0.5 fs, NVE, list rebuilt every 10 steps and pruned on the device when an atom moved "
+                       "0.1 A, %d measured steps after %d equilibration steps" % (s.natoms, steps, equil),
            "minimiser": mrep, "pme_spread_gather": pme}
     for name, prec in (("mixed", abi.MDF_PREC_MIXED), ("fp64", abi.MDF_PREC_FP64)):
         if prec != abi.MDF_PREC_MIXED:

@@ -145,7 +145,12 @@ typedef struct {
      * them).  prune_every = 1, prune_margin = 0 prunes against the current
      * positions at every evaluation (exact); larger intervals need a margin
      * of at least twice the largest displacement between prunes.
-     * prune_every = 0 disables pruning. */
+     * prune_every < 0 (self-pruning): the pack kernel measures at every
+     * evaluation the largest displacement of an atom since the last prune,
+     * and the prune kernel runs only when it exceeds prune_margin / 2 (or the
+     * list changed), so every pair within the cutoff stays in the list
+     * without a host decision (dynamics graphs, batches); with nranks > 1 it
+     * prunes at every evaluation.  prune_every = 0 disables pruning. */
     int32_t prune_every;
     double prune_margin;
     /* Launch shapes (results do not depend on them; mdf_batch_autotune picks

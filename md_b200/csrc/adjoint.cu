@@ -289,7 +289,7 @@ template <typename R>
 static void launch_adj_pairs(Ctx& c, const NBParams& P, double gE)
 {
     using V4t = typename V4<R>::type;
-    const bool pruned = c.p.prune_every > 0 && c.pruned_valid && !c.pruned_half;
+    const bool pruned = c.p.prune_every != 0 && c.pruned_valid && !c.pruned_half;
     const ILRange* il = pruned ? c.ilist_in.p : c.ilist.p;
     const PairEntry* pl = pruned ? c.plist_in.p : c.plist.p;
     const V4t* xq = sizeof(R) == 4 ? reinterpret_cast<const V4t*>(c.xq_f.p) : reinterpret_cast<const V4t*>(c.xq_d.p);
@@ -359,9 +359,10 @@ void backward(Ctx& c, const double* dL_dF, double dL_dE, double* dL_dq, double* 
     const int th = 256;
     // current cluster frame and pruned list, as a forward evaluation builds them
     pack_positions(c);
-    if (c.p.prune_every > 0) {
+    if (c.p.prune_every != 0) {
         prune_pairlist(c, true);   // whole entries: the adjoint kernel walks 8 x 8 cluster pairs
-        c.since_prune = half_layout(c) ? c.p.prune_every : 1;   // the forward rebuilds its half lists
+        c.since_prune = 1;
+        if (half_layout(c)) c.pruned_valid = false;   // the next forward prunes its half lists again
     }
     if (mixed) {
         c.adj_vs_f.alloc(c.n_slots);

@@ -431,6 +431,9 @@ void eval_async_impl(Ctx& c, uint32_t flags)
         }
         ++c.since_prune;
         mark(c, "prune");
+    } else if (c.p.prune_every < 0) {
+        prune_pairlist(c);   // self-pruning: the kernel returns at once while the last lists hold
+        mark(c, "prune");
     }
     launch_nonbonded(c, energy);
     mark(c, "pairs");
@@ -778,7 +781,7 @@ void mdf_destroy(mdf_ctx* ctx)
     c.col_atoms.release(); c.slot_atom.release(); c.atom_slot.release(); c.slot_type.release(); c.center.release(); c.centerf.release();
     c.bb_lo.release(); c.bb_hi.release(); c.xq_f.release(); c.xq_d.release(); c.cluster_col.release();
     c.ilist.release(); c.plist.release(); c.scan_tmp.release(); c.f_slot.release();
-    c.plist_in.release(); c.ilist_in.release(); c.n_in.release(); c.cur_lo.release(); c.cur_hi.release();
+    c.plist_in.release(); c.ilist_in.release(); c.cur_lo.release(); c.cur_hi.release(); c.xq_snap.release();
     c.q_slab.release(); c.pme_slab.release(); c.pme_send.release(); c.pme_recv.release(); c.pme_rslab.release();
     c.f_stage.release(); c.f_mine.release(); c.f_out_blk.release(); c.f_out_all.release();
     c.f_atom.release(); c.scal.release(); c.npairs_dev.release(); c.forces_out.release(); c.forces_pme_ref.release();
@@ -995,11 +998,20 @@ int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pair
         if (n_clusters) *n_clusters = c.have_list ? c.n_clusters : -1;
         if (n_cluster_pairs) *n_cluster_pairs = c.have_list ? c.n_entries : -1;
         if (n_cluster_pairs_pruned) {
-            unsigned long long v = 0;
-            bool ok = c.have_list && c.pruned_valid && c.p.prune_every > 0;
+            // entries the pair kernel walks: the counts of the last prune's item ranges
+            long long v = 0;
+            const bool ok = c.have_list && c.pruned_valid && c.p.prune_every != 0;
             if (ok) {
+                long long lo, hi;
+                rank_slice(c, c.n_clusters, lo, hi);
+                const bool half = c.pruned_half;
+                const size_t n = (size_t)(hi - lo) * (half ? 2 : 1);
+                std::vector<ILRange> r(n);
                 MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
-                MDF_CUDA_TRY(cudaMemcpy(&v, c.n_in.p, sizeof(v), cudaMemcpyDeviceToHost));
+                if (n)
+                    MDF_CUDA_TRY(cudaMemcpy(r.data(), half ? c.ilist_h.p + 2 * lo : c.ilist_in.p + lo,
+                                            sizeof(ILRange) * n, cudaMemcpyDeviceToHost));
+                for (const ILRange& x : r) v += x.count;
             }
             *n_cluster_pairs_pruned = ok ? (int64_t)v : -1;
         }
@@ -1097,9 +1109,13 @@ int mdf_autotune(mdf_ctx* ctx, int reps, mdf_tune_report* rep)
             const double t_default = time_it();
             double best = t_default;
             int bw = w0, bl = l0, bp = p0, bs = s0, by = y0, tried = 0;
+            // a self-pruning context (prune_every < 0) keeps that mode
+            const int prune_self[1] = {c.p.prune_every};
+            const int* popts = c.p.prune_every < 0 ? prune_self : prune;
+            const int np = c.p.prune_every < 0 ? 1 : 2;
             for (int sc : sched)
-                for (int p : prune)
-                    for (int ly = 0; ly <= (p > 0 ? 1 : 0); ++ly)   // the half layout runs on pruned lists only
+                for (int pi = 0; pi < np; ++pi)
+                    for (int ly = 0, p = popts[pi]; ly <= (p != 0 ? 1 : 0); ++ly)   // half layout: pruned lists only
                         for (int w : warps)
                             for (int l : lines) {
                                 apply(w, l, p, sc, ly);

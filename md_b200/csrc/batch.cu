@@ -175,7 +175,7 @@ bool uniform_launches(const mdf_batch* b)
     for (const mdf_ctx* x : b->sys) {
         const mdf_params& p = x->c.p;
         if (p.precision != p0.precision || (p.switch_radius > 0) != (p0.switch_radius > 0) ||
-            (p.prune_every > 0) != (p0.prune_every > 0) || p.pair_warps != p0.pair_warps ||
+            (p.prune_every != 0) != (p0.prune_every != 0) || p.pair_warps != p0.pair_warps ||
             p.fft_lines != p0.fft_lines || p.pair_schedule != p0.pair_schedule ||
             half_layout(x->c) != half_layout(b->sys[0]->c) || p.nranks > 1)
             return false;
@@ -247,7 +247,7 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M, double*
     const bool energy = (flags & MDF_COMPUTE_ENERGY) != 0;
     M.energy = energy;
     const Ctx& c0 = b->sys[0]->c;
-    M.prune_on = c0.p.prune_every > 0;
+    M.prune_on = c0.p.prune_every != 0;
     M.use_switch = c0.p.switch_radius > 0;
     M.threads = pair_threads(c0);
     M.persist = c0.p.pair_schedule == 1;
@@ -811,9 +811,13 @@ int mdf_batch_autotune(mdf_batch* b, int reps, mdf_tune_report* rep)
         double t_default = time_it();
         double best = 1e300;
         int bw = w0, bl = l0, bp = p0, bs = s0, by = y0, tried = 0;
+        // self-pruning systems (prune_every < 0) keep that mode
+        const int prune_self[1] = {p0};
+        const int* popts = p0 < 0 ? prune_self : prune;
+        const int np = p0 < 0 ? 1 : 2;
         for (int sc : sched)
-            for (int p : prune)
-                for (int ly = 0; ly <= (p > 0 ? 1 : 0); ++ly)   // the half layout runs on pruned lists only
+            for (int pi = 0; pi < np; ++pi)
+                for (int ly = 0, p = popts[pi]; ly <= (p != 0 ? 1 : 0); ++ly)   // half layout: pruned lists only
                     for (int w : warps)
                         for (int l : lines) {
                             apply(w, l, p, sc, ly);

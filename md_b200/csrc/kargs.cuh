@@ -31,6 +31,8 @@ struct PackArgs {
     double L[3];
     typename V4<R>::type* xq;
     float4 *cur_lo, *cur_hi;
+    const typename V4<R>::type* snap;   // self-pruning: positions of the last prune (nullptr: off)
+    unsigned* disp;                     // largest squared displacement from snap (FP32 bits, atomicMax)
     unsigned* st;
 };
 
@@ -50,7 +52,13 @@ struct PruneArgs {
     float rcut2;
     ILRange* ilist_in;
     PairEntry* plist_in;
-    unsigned long long* n_in;
+    // self-pruning: prune only when force is set or the displacement since the
+    // last prune (written by the pack kernel) exceeds disp_thr2; a prune that
+    // runs records the positions it used in snap
+    typename V4<R>::type* snap;
+    const unsigned* disp;
+    float disp_thr2;
+    int force;
 };
 
 // ------------------------------------------------------------- pair kernels

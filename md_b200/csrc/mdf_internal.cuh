@@ -20,8 +20,9 @@ constexpr double GRID_SCALE = 1099511627776.0;        // 2^40 fixed point for PM
 constexpr double GRID_ISCALE = 1.0 / 1099511627776.0;
 constexpr int NUM_ACC = MDF_E_COUNT + 6;   // energies + 6 virial components
 constexpr int ACC_VIR = MDF_E_COUNT;
-constexpr int NUM_SCAL = NUM_ACC + 3;      // + pairs in cutoff + status word + pair-kernel work counter
+constexpr int NUM_SCAL = NUM_ACC + 4;      // + pairs in cutoff + status word + pair-kernel work counter + displacement
 constexpr int SCAL_WORK = NUM_ACC + 2;     // work counter of the persistent pair kernels (cleared with the block)
+constexpr int SCAL_DISP = NUM_ACC + 3;     // largest squared displacement since the last prune (FP32 bits; self-pruning mode)
 
 // device status bits
 enum : unsigned {
@@ -180,10 +181,10 @@ struct Ctx {
     long long n_entries = 0;
     DevBuf<PairEntry> plist_in;    // pruned list the pair kernel walks (same offsets as plist)
     DevBuf<ILRange> ilist_in;
-    DevBuf<unsigned long long> n_in;   // [1] entries kept by the last prune
     DevBuf<ILRange> ilist_h;       // half layout: [2 n_clusters] items (ILRange.pad = half)
     DevBuf<PairEntry> plist_h;     // half layout: [2 x outer capacity]
     bool pruned_half = false;      // the last prune wrote the half lists
+    DevBuf<unsigned char> xq_snap; // self-pruning mode: the cluster-frame positions of the last prune, per slot
     int since_prune = 0;
     bool pruned_valid = false;
     DevBuf<int> scan_tmp;
@@ -319,7 +320,10 @@ void build_pairlist(Ctx& c);
 void pack_positions(Ctx& c);
 void prune_pairlist(Ctx& c, bool whole_entries = false);
 // half-entry lists in use by the pair kernel (layout 1, pruned)
-inline bool half_layout(const Ctx& c) { return c.p.pair_layout == 1 && c.p.prune_every > 0; }
+inline bool half_layout(const Ctx& c) { return c.p.pair_layout == 1 && c.p.prune_every != 0; }
+// prune_every < 0: the device prunes when an atom moved more than prune_margin / 2
+// since the last prune (one context per system; with several ranks it prunes every evaluation)
+inline bool self_pruning(const Ctx& c) { return c.p.prune_every < 0 && c.p.nranks <= 1; }
 void launch_nonbonded(Ctx& c, bool energy);
 void launch_exclusions(Ctx& c, bool energy);
 void launch_bonded(Ctx& c, bool energy);

@@ -1249,7 +1249,7 @@ PairArgs<R> make_pair_args(const Ctx& c, bool count)
     A.nlist = (int)(hi - lo);
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;
-    const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
+    const bool pruned = c.p.prune_every != 0 && c.pruned_valid;
     A.ilist = (pruned ? c.ilist_in.p : c.ilist.p) + lo;
     A.plist = pruned ? c.plist_in.p : c.plist.p;
     if (sizeof(R) == 4) {
@@ -1333,7 +1333,7 @@ PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn)
     A.nlist = (int)(hi - lo);
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;
-    const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
+    const bool pruned = c.p.prune_every != 0 && c.pruned_valid;
     A.half = pruned && c.pruned_half ? 1 : 0;
     A.ilist = A.half ? c.ilist_h.p + 2 * lo : (pruned ? c.ilist_in.p : c.ilist.p) + lo;
     A.plist = pruned ? (A.half ? c.plist_h.p : c.plist_in.p) : c.plist.p;
@@ -1446,7 +1446,7 @@ PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn)
     A.nlist = (int)(hi - lo);
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;
-    const bool pruned = c.p.prune_every > 0 && c.pruned_valid;
+    const bool pruned = c.p.prune_every != 0 && c.pruned_valid;
     A.half = pruned && c.pruned_half ? 1 : 0;
     A.ilist = A.half ? c.ilist_h.p + 2 * lo : (pruned ? c.ilist_in.p : c.ilist.p) + lo;
     A.plist = pruned ? (A.half ? c.plist_h.p : c.plist_in.p) : c.plist.p;

@@ -251,6 +251,18 @@ __device__ __forceinline__ void pack_dev(const PackArgs<R>& A)
         }
     }
     if (inside) xq[s] = v;
+    if (A.snap) {
+        // self-pruning: the largest squared displacement since the last prune
+        float d2 = 0.f;
+        if (a >= 0) {
+            const typename V4<R>::type o = A.snap[s];
+            const double ex = (double)v.x - (double)o.x, ey = (double)v.y - (double)o.y, ez = (double)v.z - (double)o.z;
+            d2 = __double2float_ru(ex * ex + ey * ey + ez * ez);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d2 = fmaxf(d2, __shfl_xor_sync(0xffffffffu, d2, o));
+        if ((threadIdx.x & 31) == 0 && d2 > 0.f) atomicMax(A.disp, __float_as_uint(d2));
+    }
     // min/max over the 8 slots of the cluster (8 consecutive lanes)
 #pragma unroll
     for (int o = 1; o < CLUSTER; o <<= 1)
@@ -503,8 +515,9 @@ __device__ __forceinline__ void prune_dev(const PruneArgs<R>& A)
     const float rcut2 = A.rcut2;
     ILRange* __restrict__ ilist_in = A.ilist_in;
     PairEntry* __restrict__ plist_in = A.plist_in;
-    unsigned long long* __restrict__ n_in = A.n_in;
     using V4t = typename V4<R>::type;
+    // self-pruning: the list pruned last time still holds every pair within the cutoff
+    if (!A.force && __uint_as_float(*A.disp) <= A.disp_thr2) return;
     __shared__ float sh[27][6];
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
     __syncthreads();
@@ -514,6 +527,7 @@ __device__ __forceinline__ void prune_dev(const PruneArgs<R>& A)
     const unsigned below = (1u << lane) - 1u;
     const ILRange L = ilist[w];
     const int I = L.i;
+    if (A.snap && lane < CLUSTER) A.snap[I * CLUSTER + lane] = xq[I * CLUSTER + lane];
     R ax[CLUSTER], ay[CLUSTER], az[CLUSTER], an[CLUSTER];   // -2 x_i and |x_i|^2
 #pragma unroll
     for (int k = 0; k < CLUSTER; ++k) {
@@ -608,7 +622,6 @@ __device__ __forceinline__ void prune_dev(const PruneArgs<R>& A)
         ILRange r;
         r.i = I; r.start = L.start; r.count = kept; r.pad = 0;
         ilist_in[w] = r;
-        if (kept) atomicAdd(n_in, (unsigned long long)kept);
     }
 }
 
@@ -623,6 +636,7 @@ template <typename R>
 __device__ __forceinline__ void prune_half_dev(const PruneArgs<R>& A)
 {
     using V4t = typename V4<R>::type;
+    if (!A.force && __uint_as_float(*A.disp) <= A.disp_thr2) return;   // self-pruning: the lists still hold
     __shared__ float sh[27][6];
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = A.shifts.v[k / 6][k % 6];
     __syncthreads();
@@ -633,6 +647,7 @@ __device__ __forceinline__ void prune_half_dev(const PruneArgs<R>& A)
     const ILRange L = A.ilist[w];
     const int I = L.i;
     const V4t* __restrict__ xq = A.xq;
+    if (A.snap && lane < CLUSTER) A.snap[I * CLUSTER + lane] = xq[I * CLUSTER + lane];
     R ax[CLUSTER], ay[CLUSTER], az[CLUSTER], an[CLUSTER];   // -2 x_i and |x_i|^2
 #pragma unroll
     for (int k = 0; k < CLUSTER; ++k) {
@@ -695,7 +710,6 @@ __device__ __forceinline__ void prune_half_dev(const PruneArgs<R>& A)
         A.ilist_in[2 * w] = r;
         r.start = (int)out1; r.count = kept1; r.pad = 1;
         A.ilist_in[2 * w + 1] = r;
-        if (kept0 + kept1) atomicAdd(A.n_in, (unsigned long long)(kept0 + kept1));
     }
 }
 
@@ -757,7 +771,12 @@ PruneArgs<R> make_prune_args(const Ctx& c)
     A.rcut2 = (float)(rc * rc);
     A.ilist_in = c.ilist_in.p + lo;
     A.plist_in = c.plist_in.p;
-    A.n_in = c.n_in.p;
+    const bool selfp = self_pruning(c);
+    A.snap = selfp ? reinterpret_cast<typename V4<R>::type*>(c.xq_snap.p) : nullptr;
+    A.disp = reinterpret_cast<const unsigned*>(c.scal.p + SCAL_DISP);
+    const float half_margin = (float)(0.5 * std::max(0.0, c.p.prune_margin));
+    A.disp_thr2 = half_margin * half_margin;
+    A.force = (!selfp || !c.pruned_valid) ? 1 : 0;
     return A;
 }
 
@@ -795,10 +814,10 @@ template void launch_prune_multi<float>(const PruneArgs<float>*, int, int, bool,
 template void launch_prune_multi<double>(const PruneArgs<double>*, int, int, bool, cudaStream_t);
 
 // whole_entries: build the 8 x 8 pruned list even in the half layout (the
-// adjoint walks whole entries).
+// adjoint walks whole entries); it also prunes unconditionally.
 void prune_pairlist(Ctx& c, bool whole_entries)
 {
-    MDF_CUDA_TRY(cudaMemsetAsync(c.n_in.p, 0, sizeof(unsigned long long), c.stream));
+    if (whole_entries) c.pruned_valid = false;   // a self-pruning launch prunes when the list is not valid
     const bool half = half_layout(c) && !whole_entries;
     if (half) ensure_half_lists(c);
     if (c.p.precision == MDF_PREC_MIXED) {
@@ -841,6 +860,8 @@ PackArgs<R> make_pack_args(const Ctx& c)
     A.xq = reinterpret_cast<typename V4<R>::type*>(sizeof(R) == 4 ? (void*)c.xq_f.p : (void*)c.xq_d.p);
     A.cur_lo = c.cur_lo.p;
     A.cur_hi = c.cur_hi.p;
+    A.snap = self_pruning(c) ? reinterpret_cast<const typename V4<R>::type*>(c.xq_snap.p) : nullptr;
+    A.disp = reinterpret_cast<unsigned*>(c.scal.p + SCAL_DISP);
     A.st = c.status.p;
     return A;
 }
@@ -1002,11 +1023,12 @@ void build_pairlist(Ctx& c)
         c.cur_hi.alloc(ncl);
         if (c.p.precision == MDF_PREC_MIXED) c.xq_f.alloc(c.n_slots);
         else c.xq_d.alloc(c.n_slots);
+        if (c.p.prune_every < 0)
+            c.xq_snap.alloc((c.p.precision == MDF_PREC_MIXED ? sizeof(float4) : sizeof(double4)) * (size_t)c.n_slots);
         c.f_slot.alloc((size_t)3 * c.n_slots);
         c.need_clear = true;   // slot layout changed: clear the accumulators before the next evaluation
         c.plist_in.alloc(c.plist.n);
         c.ilist_in.alloc(ncl);
-        c.n_in.alloc(1);
         c.pruned_valid = false;
         c.since_prune = 0;
         c.have_list = true;

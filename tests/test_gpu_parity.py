@@ -242,6 +242,38 @@ def test_prune_interval_with_margin_tracks_moving_atoms():
     a.close(); b.close()
 
 
+@pytest.mark.parametrize("layout", [0, 1])
+@pytest.mark.parametrize("prec", [FP64, MIXED])
+def test_self_pruning_tracks_moving_atoms(prec, layout):
+    """prune_every < 0: the pack kernel measures the largest displacement
+    since the last prune and the prune kernel re-prunes only beyond
+    prune_margin / 2.  Atoms drift up to 0.05 A per evaluation against a
+    0.3 A margin, so the lists are reused for some evaluations and re-pruned
+    on the device for others: forces equal an exact prune at every evaluation
+    (FP64 to 1e-12; mixed to the order of the FP32 sums) and the reported list
+    holds at least the exact prune's entries."""
+    s = H.system("small")
+    flat = H.flat(s, PHYS, engine.cmap_coefficients)
+    kw = dict(semantics=PHYS, precision=prec, ewald_tol=1e-5, grid=(32, 32, 32), pair_layout=layout)
+    a = engine.Engine(flat, s.box, prune_every=-1, prune_margin=0.3, **kw)
+    b = engine.Engine(flat, s.box, prune_every=1, **kw)
+    rng = np.random.default_rng(12)
+    x = s.coords.copy()
+    a.set_positions(x); a.build_pairlist()
+    b.set_positions(x); b.build_pairlist()
+    tol = 1e-12 if prec == FP64 else 1e-6
+    for step in range(12):
+        a.set_positions(x)
+        b.set_positions(x)
+        Ea, Fa = a.compute()
+        Eb, Fb = b.compute()
+        assert H.frel(Fa, Fb) < tol, step
+        assert abs(Ea["total"] - Eb["total"]) <= tol * abs(Eb["total"]) + 1e-8, step
+        assert a.pairlist_info()["cluster_pairs_pruned"] >= b.pairlist_info()["cluster_pairs_pruned"]
+        x = x + rng.uniform(-0.03, 0.03, x.shape)
+    a.close(); b.close()
+
+
 @pytest.mark.parametrize("prec", [FP64, MIXED])
 @pytest.mark.parametrize("n,charged", [(1, True), (2, True), (2, False), (9, True), (17, False)])
 def test_few_atoms_match_o2(n, charged, prec):

@@ -323,7 +323,7 @@ void prune_pairlist(Ctx& c, bool whole_entries = false);
 inline bool half_layout(const Ctx& c) { return c.p.pair_layout == 1 && c.p.prune_every != 0; }
 // prune_every < 0: the device prunes when an atom moved more than prune_margin / 2
 // since the last prune (one context per system; with several ranks it prunes every evaluation)
-inline bool self_pruning(const Ctx& c) { return c.p.prune_every < 0 && c.p.nranks <= 1; }
+inline bool self_pruning(const Ctx& c) { return c.p.prune_every < 0 && c.p.nranks <= 1 && c.xq_snap.p != nullptr; }
 void launch_nonbonded(Ctx& c, bool energy);
 void launch_exclusions(Ctx& c, bool energy);
 void launch_bonded(Ctx& c, bool energy);

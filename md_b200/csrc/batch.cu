@@ -254,12 +254,18 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M, double*
     M.half = half_layout(c0);
     for (int s = 0; s < n; ++s) {
         Ctx& c = b->sys[s]->c;
+        if (M.half) ensure_half_lists(c);
         if (M.prune_on) {
-            // the captured chain prunes before the pair kernel
+            // the captured chain prunes before the pair kernel.  A self-pruning
+            // system whose lists are not valid (new list, new layout) prunes once
+            // here, so the captured prunes can leave the decision to the device.
+            if (self_pruning(c) && (!c.pruned_valid || c.pruned_half != M.half)) {
+                prune_pairlist(c);
+                MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+            }
             c.pruned_valid = true;
             c.pruned_half = M.half;
         }
-        if (M.half) ensure_half_lists(c);
         M.pack.push_back(make_pack_args<R>(c));
         M.prune.push_back(M.half ? make_prune_half_args<R>(c) : make_prune_args<R>(c));
         if (sizeof(R) == 4) {

@@ -1025,6 +1025,7 @@ void build_pairlist(Ctx& c)
         else c.xq_d.alloc(c.n_slots);
         if (c.p.prune_every < 0)
             c.xq_snap.alloc((c.p.precision == MDF_PREC_MIXED ? sizeof(float4) : sizeof(double4)) * (size_t)c.n_slots);
+        if (half_layout(c)) ensure_half_lists(c);   // sized here, not inside a later stream capture
         c.f_slot.alloc((size_t)3 * c.n_slots);
         c.need_clear = true;   // slot layout changed: clear the accumulators before the next evaluation
         c.plist_in.alloc(c.plist.n);

@@ -198,3 +198,36 @@ def test_batch_submit_collect_pipelined_equals_compute():
     b3.close()
     assert np.array_equal(out.reshape(-1, 3), np.concatenate([f for _, f in res]))
     assert all(x["total"] == r[0]["total"] for x, r in zip(e, res))
+
+
+def test_self_pruning_batch_equals_single_systems():
+    """Self-pruning systems (prune_every < 0) in a batch: the captured prune
+    kernels decide on the device, frame by frame, exactly as single contexts
+    in the same mode do (forces bit for bit over frames that move by up to
+    0.05 A against a 0.3 A margin), and within the mixed bound of the oracle."""
+    ss = systems()[:3]
+    flats = _flats(ss)
+    kw = dict(KW, prune_every=-1, prune_margin=0.3)
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=MIXED, **kw)
+    rng = np.random.default_rng(8)
+    frames = [[s.coords for s in ss]]
+    for _ in range(4):
+        frames.append([x + rng.uniform(-0.03, 0.03, x.shape) for x in frames[-1]])
+    b.set_positions(frames[0])
+    got = []
+    for fr in frames:
+        b.set_positions(fr)
+        got.append(b.compute())
+    b.close()
+    for k, (s, f) in enumerate(zip(ss, flats)):
+        eng = engine.Engine(f, s.box, semantics=PHYS, precision=MIXED, grid=s.meta["grid"], **kw)
+        eng.set_positions(frames[0][k])
+        eng.build_pairlist()
+        for n, fr in enumerate(frames):
+            eng.set_positions(fr[k])
+            E, F = eng.compute()
+            assert np.array_equal(F, got[n][k][1]), (k, n)
+        eng.close()
+    p = O.make_params(PHYS, ss[0].box, ss[0].meta["grid"], H.alpha_for(1e-5, 9.0), H.KC, cutoff=9.0, switch=8.0)
+    e2, f2, _, _, _ = O.evaluate(flats[0], p, frames[-1][0])
+    assert H.frel(got[-1][0][1], f2) <= 1e-5

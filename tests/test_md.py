@@ -64,14 +64,19 @@ def test_one_step_is_velocity_verlet():
 def test_self_pruning_dynamics_matches_pruning_every_step(prec):
     """Dynamics in graph-captured chunks with device-decided pruning
     (prune_every < 0, 0.2 A margin) follows the trajectory of pruning at
-    every step: 60 steps of 0.5 fs, positions to 1e-9 A (FP64) / 1e-4 A
-    (mixed: FP32 sums in another order, amplified over the trajectory)."""
+    every step: 80 steps of 0.25 fs from a minimised start, positions to
+    1e-9 A (FP64) / 1e-4 A (mixed: FP32 sums in another order, amplified
+    over the trajectory)."""
     s = H.system("small")
+    e0 = _engine(s, FP64)
+    e0.minimize(max_iter=300, fmax_tol=5.0)
+    x0, _ = e0.md_state(velocities=False)
+    e0.close()
     out = []
     for kw in (dict(prune_every=-1, prune_margin=0.2), dict(prune_every=1)):
-        eng = _engine(s, prec, **kw)
+        eng = _engine(s, prec, coords=x0, **kw)
         eng.md_init(s.mass, _v0(s))
-        eng.md_run(60, 0.0005, chunk=10)
+        eng.md_run(80, 0.00025, chunk=10)
         out.append(eng.md_state()[0])
         eng.close()
     tol = 1e-9 if prec == FP64 else 1e-4

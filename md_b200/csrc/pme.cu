@@ -609,11 +609,6 @@ __global__ void k_zero_multi(const ZeroArgs* __restrict__ As)
         A.p[i] = 0ull;
 }
 
-// Force gather with four lanes per atom: lane i of an atom's group takes the
-// stencil plane x = base - 1 + i (16 potential loads), lane 0 computes the
-// grid position and shares it, and the four partial forces are summed by two
-// butterfly steps before lane 0 adds them (four times the loads in flight per
-// atom of a one-thread-per-atom gather).
 template <typename R>
 __device__ __forceinline__ void gather4_dev(const GatherArgs<R>& A)
 {
@@ -625,84 +620,53 @@ __device__ __forceinline__ void gather4_dev(const GatherArgs<R>& A)
     const R* __restrict__ phi = A.phi;
     unsigned long long* __restrict__ fslot = A.fslot;
     unsigned* st = A.st;
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = s0 + (int)(t >> 2);   // slots [s0, s1) of nslots
-    const int i = (int)(t & 3);
-    const unsigned grp = 0xfu << (threadIdx.x & 28);
-    // the four lanes of a slot leave together
+    int s = s0 + blockIdx.x * blockDim.x + threadIdx.x;   // slots [s0, s1) of nslots
     if (s >= s1) return;
-    const int a = slot_atom[s];
+    int a = slot_atom[s];
     if (a < 0) return;
-    const double qa = q[a];
+    double qa = q[a];
     if (qa == 0.0) return;
-    int base[3] = {0, 0, 0};
-    double u[3] = {0, 0, 0};
-    int bad = 0;
-    if (i == 0) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            double v = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
-            if (!(v >= 0.0 && v <= (double)g.K[d])) bad = 1;   // non-finite position
-            if (v >= g.K[d]) v -= g.K[d];
-            const int b = bad ? 0 : min((int)floor(v), g.K[d] - 1);
-            base[d] = b;
-            u[d] = v - b;
-        }
-    }
-    bad = __shfl_sync(grp, bad, 0, 4);
-    if (bad) {
-        if (i == 0) status_set(st, ST_NONFINITE);
-        return;
-    }
+    int base[3];
     R th[3][4], dth[3][4];
-#pragma unroll
     for (int d = 0; d < 3; ++d) {
-        base[d] = __shfl_sync(grp, base[d], 0, 4);
-        bspline4<R>((R)__shfl_sync(grp, u[d], 0, 4), th[d], dth[d]);
-    }
-    // this lane's x weight and derivative (selected, so the arrays stay in registers)
-    R tx = th[0][0], dtx = dth[0][0];
-#pragma unroll
-    for (int m = 1; m < 4; ++m)
-        if (i == m) {
-            tx = th[0][m];
-            dtx = dth[0][m];
+        double u = wrap_coord(xyz[3 * a + d], g.L[d]) * g.scale[d];
+        if (!(u >= 0.0 && u <= (double)g.K[d])) {   // non-finite position
+            status_set(st, ST_NONFINITE);
+            return;
         }
-    int kx = base[0] - 1 + i;
-    kx += (kx < 0) ? g.K[0] : 0;
-    kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+        if (u >= g.K[d]) u -= g.K[d];
+        int b = min((int)floor(u), g.K[d] - 1);
+        base[d] = b;
+        bspline4<R>((R)(u - b), th[d], dth[d]);
+    }
     R gx = 0, gy = 0, gz = 0;
-    for (int j = 0; j < 4; ++j) {
-        int ky = base[1] - 1 + j;
-        ky += (ky < 0) ? g.K[1] : 0;
-        ky -= (ky >= g.K[1]) ? g.K[1] : 0;
-        const long long row = ((long long)kx * g.K[1] + ky) * g.K[2];
-        R sz = 0, dz = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            int kz = base[2] - 1 + k;
-            kz += (kz < 0) ? g.K[2] : 0;
-            kz -= (kz >= g.K[2]) ? g.K[2] : 0;
-            const R p = phi[row + kz];
-            sz += th[2][k] * p;
-            dz += dth[2][k] * p;
+    for (int i = 0; i < 4; ++i) {
+        int kx = base[0] - 1 + i;
+        kx += (kx < 0) ? g.K[0] : 0;
+        kx -= (kx >= g.K[0]) ? g.K[0] : 0;
+        for (int j = 0; j < 4; ++j) {
+            int ky = base[1] - 1 + j;
+            ky += (ky < 0) ? g.K[1] : 0;
+            ky -= (ky >= g.K[1]) ? g.K[1] : 0;
+            long long row = ((long long)kx * g.K[1] + ky) * g.K[2];
+            R sz = 0, dz = 0;
+            for (int k = 0; k < 4; ++k) {
+                int kz = base[2] - 1 + k;
+                kz += (kz < 0) ? g.K[2] : 0;
+                kz -= (kz >= g.K[2]) ? g.K[2] : 0;
+                R p = phi[row + kz];
+                sz += th[2][k] * p;
+                dz += dth[2][k] * p;
+            }
+            gx += dth[0][i] * th[1][j] * sz;
+            gy += th[0][i] * dth[1][j] * sz;
+            gz += th[0][i] * th[1][j] * dz;
         }
-        gx += dtx * th[1][j] * sz;
-        gy += tx * dth[1][j] * sz;
-        gz += tx * th[1][j] * dz;
     }
-#pragma unroll
-    for (int o = 1; o < 4; o <<= 1) {
-        gx += __shfl_xor_sync(grp, gx, o, 4);
-        gy += __shfl_xor_sync(grp, gy, o, 4);
-        gz += __shfl_xor_sync(grp, gz, o, 4);
-    }
-    if (i == 0) {
-        const R qr = (R)qa;
-        fx_add(fslot + s, -qr * gx * (R)g.scale[0], FORCE_SCALE, st);
-        fx_add(fslot + nslots + s, -qr * gy * (R)g.scale[1], FORCE_SCALE, st);
-        fx_add(fslot + 2 * nslots + s, -qr * gz * (R)g.scale[2], FORCE_SCALE, st);
-    }
+    const R qr = (R)qa;
+    fx_add(fslot + s, -qr * gx * (R)g.scale[0], FORCE_SCALE, st);
+    fx_add(fslot + nslots + s, -qr * gy * (R)g.scale[1], FORCE_SCALE, st);
+    fx_add(fslot + 2 * nslots + s, -qr * gz * (R)g.scale[2], FORCE_SCALE, st);
 }
 
 template <typename R>
@@ -1205,7 +1169,7 @@ GatherArgs<R> make_gather_args(const Ctx& c)
     A.s0 = (int)s0;
     A.s1 = (int)s1;
     A.nslots = c.n_slots;
-    A.gx = grid_blocks(4 * (s1 - s0), 256);   // four lanes per slot
+    A.gx = grid_blocks(s1 - s0, 256);
     A.gy = 1;
     A.slot_atom = c.slot_atom.p;
     A.xyz = c.xyz.p;

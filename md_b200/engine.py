@@ -427,7 +427,7 @@ class Batch:
     (mdf_batch_*).  flats / boxes / grids: one per system."""
 
     def __init__(self, flats, boxes, grids, precision=abi.MDF_PREC_MIXED, cutoff=9.0, skin=2.0, switch_radius=8.0,
-                 ewald_tol=1e-5, device=0, prune_every=1, pair_schedule=0, pair_layout=0):
+                 ewald_tol=1e-5, device=0, prune_every=1, pair_schedule=0, pair_layout=0, prune_margin=0.0):
         self.lib = library()
         self.flats = list(flats)
         n = len(self.flats)
@@ -443,7 +443,7 @@ class Batch:
                 p.grid[d] = int(grids[k][d])
             p.cutoff, p.skin, p.switch_radius = float(cutoff), float(skin), float(switch_radius)
             p.ewald_tol, p.device = float(ewald_tol), int(device)
-            p.prune_every = int(prune_every)
+            p.prune_every, p.prune_margin = int(prune_every), float(prune_margin)
             p.pair_schedule, p.pair_layout = int(pair_schedule), int(pair_layout)
             params[k] = p
         self._tops, self._params = tops, params

@@ -14,9 +14,11 @@
 // rebuild or a change of launch shapes.
 //
 // mdf_batch_autotune times the candidate launch shapes (pair-kernel warps per
-// block, FFT lines per block, per-evaluation pruning on or off) on the batch
-// itself and keeps the fastest; results do not depend on the choice (all
-// sums are fixed point).
+// block, FFT lines per block, per-evaluation pruning on or off, pair-kernel
+// schedule and layout) on the batch itself and keeps the fastest; the choice
+// changes results only through the order of the floating-point sums of each
+// i cluster's forces (pruning, layout), never through the atomics (fixed
+// point).  mdf_batch_submit / mdf_batch_collect pipeline consecutive batches.
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -640,7 +642,10 @@ void mdf_batch_destroy(mdf_batch* b)
 {
     if (!b) return;
     cudaSetDevice(b->device);
-    if (b->main) cudaStreamSynchronize(b->main);
+    // submitted evaluations (and their copies) finish before anything is freed
+    for (cudaStream_t cs : {b->main, b->copy_in, b->copy_out})
+        if (cs) cudaStreamSynchronize(cs);
+    b->inflight = 0;
     drop_graph(b);
     for (mdf_ctx* c : b->sys)
         if (c) mdf_destroy(c);

@@ -43,9 +43,7 @@ void mark(Ctx& c, const char* name)
 
 // Forces out in atom order, and every accumulator cleared for the next
 // evaluation (read-and-clear: an evaluation needs no memsets).  The scalar
-// block goes to the host (mapped memory) and is cleared here too.  One
-// thread per atom and component (blockIdx.y = component): three times the
-// loads in flight of a thread per atom, for a latency-bound pass.
+// block was copied to the host before this kernel runs.
 __device__ __forceinline__ void finalize_dev(const FinalizeArgs& A)
 {
     const int N = A.N, nslots = A.nslots;
@@ -55,20 +53,25 @@ __device__ __forceinline__ void finalize_dev(const FinalizeArgs& A)
     double* __restrict__ out = A.out;
     unsigned long long* __restrict__ scal = A.scal;
     unsigned long long* __restrict__ host_scal = A.host_scal;
-    const int a = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y;
-    if (k == 0 && a < NUM_SCAL) {
+    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    if (a < NUM_SCAL) {
         host_scal[a] = scal[a];   // mapped pinned memory: no copy-engine round trip
         scal[a] = 0ull;
     }
     if (a >= N) return;
     const int s = atom_slot[a];
-    unsigned long long* fa = fatom + (long long)k * N + a;
-    unsigned long long* fs = fslot + (long long)k * nslots + s;
-    const long long v = (long long)*fa + (long long)*fs;
-    *fa = 0ull;
-    *fs = 0ull;
-    out[3 * a + k] = (double)v * FORCE_ISCALE;
+    // all loads before any store, so the six loads are in flight together
+    long long v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+        v[k] = (long long)fatom[(long long)k * N + a] + (long long)fslot[(long long)k * nslots + s];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        fatom[(long long)k * N + a] = 0ull;
+        fslot[(long long)k * nslots + s] = 0ull;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[3 * a + k] = (double)v[k] * FORCE_ISCALE;
 }
 
 __global__ void k_finalize(FinalizeArgs A)
@@ -167,7 +170,7 @@ FinalizeArgs make_finalize_args(const Ctx& c, double* d_forces)
 {
     FinalizeArgs A;
     A.gx = grid_blocks(std::max(c.N, NUM_SCAL), 256);
-    A.gy = 3;   // x, y, z
+    A.gy = 1;
     A.N = c.N;
     A.nslots = c.n_slots;
     A.fatom = c.f_atom.p;
@@ -191,7 +194,7 @@ void launch_finalize(Ctx& c, double* d_forces, bool)
 
 void launch_finalize_multi(const FinalizeArgs* d_args, int nsys, int gx, cudaStream_t s)
 {
-    k_finalize_multi<<<dim3(gx, 3, nsys), 256, 0, s>>>(d_args);
+    k_finalize_multi<<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
     MDF_CUDA_TRY(cudaGetLastError());
 }
 

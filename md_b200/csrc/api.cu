@@ -44,7 +44,7 @@ void mark(Ctx& c, const char* name)
 // Forces out in atom order, and every accumulator cleared for the next
 // evaluation (read-and-clear: an evaluation needs no memsets).  The scalar
 // block was copied to the host before this kernel runs.
-__device__ __forceinline__ void finalize_dev(const FinalizeArgs& A)
+__device__ __forceinline__ void finalize_dev(const FinalizeArgs& A, int bx, int by)
 {
     const int N = A.N, nslots = A.nslots;
     unsigned long long* __restrict__ fatom = A.fatom;
@@ -53,7 +53,7 @@ __device__ __forceinline__ void finalize_dev(const FinalizeArgs& A)
     double* __restrict__ out = A.out;
     unsigned long long* __restrict__ scal = A.scal;
     unsigned long long* __restrict__ host_scal = A.host_scal;
-    int a = blockIdx.x * blockDim.x + threadIdx.x;
+    int a = bx * blockDim.x + threadIdx.x;
     if (a < NUM_SCAL) {
         host_scal[a] = scal[a];   // mapped pinned memory: no copy-engine round trip
         scal[a] = 0ull;
@@ -76,14 +76,13 @@ __device__ __forceinline__ void finalize_dev(const FinalizeArgs& A)
 
 __global__ void k_finalize(FinalizeArgs A)
 {
-    finalize_dev(A);
+    finalize_dev(A, blockIdx.x, 0);
 }
 
-__global__ void k_finalize_multi(const FinalizeArgs* __restrict__ As)
+__global__ void k_finalize_multi(const FinalizeArgs* __restrict__ As, const int2* __restrict__ bmap)
 {
-    const FinalizeArgs& A = As[blockIdx.z];
-    if ((int)blockIdx.x >= A.gx) return;
-    finalize_dev(A);
+    const int2 m = bmap[blockIdx.x];
+    finalize_dev(As[m.x], m.y, 0);
 }
 
 // Distributed force return.  Fold the per-atom accumulators into slot order
@@ -192,9 +191,10 @@ void launch_finalize(Ctx& c, double* d_forces, bool)
     c.launches += 1;
 }
 
-void launch_finalize_multi(const FinalizeArgs* d_args, int nsys, int gx, cudaStream_t s)
+void launch_finalize_multi(const FinalizeArgs* d_args, BlockMap bm, cudaStream_t s)
 {
-    k_finalize_multi<<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    if (bm.n <= 0) return;
+    k_finalize_multi<<<bm.n, 256, 0, s>>>(d_args, bm.map);
     MDF_CUDA_TRY(cudaGetLastError());
 }
 

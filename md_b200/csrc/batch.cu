@@ -203,9 +203,11 @@ struct MultiArgs {
     std::vector<FFTXArgs<R>> x;
     std::vector<GatherArgs<R>> gather;
     std::vector<FinalizeArgs> fin;
+    // block maps of the kernels whose per-system grids differ most between
+    // systems (one entry per block actually needed: no idle blocks)
+    std::vector<int2> map_pack, map_zero, map_spread, map_z, map_y, map_x, map_gather, map_fin;
     FFTChainMax fm{};
-    int gx_pack = 0, gx_prune = 0, gx_pairs = 0, gx_excl = 0, gx_14 = 0, gx_bonded = 0, gx_zero = 0, gx_spread = 0,
-        gx_gather = 0, gx_fin = 0;
+    int gx_prune = 0, gx_pairs = 0, gx_excl = 0, gx_14 = 0, gx_bonded = 0;
     size_t dyn_pairs = 0;
     int threads = 256;
     bool prune_on = false, use_switch = false, energy = false, persist = false, half = false;
@@ -225,7 +227,14 @@ struct MultiDev {
     FFTChainDev<R> fft;
     const GatherArgs<R>* gather;
     const FinalizeArgs* fin;
+    BlockMap pack_m, zero_m, spread_m, gather_m, fin_m;
 };
+
+// Append system s's blocks (a gx x gy grid, linear index) to a block map.
+inline void add_blocks(std::vector<int2>& map, int s, int gx, int gy)
+{
+    for (int b = 0; b < gx * gy; ++b) map.push_back(make_int2(s, b));
+}
 
 template <typename T>
 size_t arr_bytes(const std::vector<T>& v)
@@ -296,11 +305,9 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M, double*
         M.x.push_back(F.x);
         M.yi.push_back(F.yi);
         M.zi.push_back(F.zi);
-        M.fm.zx = std::max(M.fm.zx, F.zf.gx);
-        M.fm.yx = std::max(M.fm.yx, F.yf.gx);
-        M.fm.yy = std::max(M.fm.yy, F.yf.gy);
-        M.fm.xx = std::max(M.fm.xx, F.x.gx);
-        M.fm.xy = std::max(M.fm.xy, F.x.gy);
+        add_blocks(M.map_z, s, F.zf.gx, F.zf.gy);
+        add_blocks(M.map_y, s, F.yf.gx, F.yf.gy);
+        add_blocks(M.map_x, s, F.x.gx, F.x.gy);
         M.fm.smz = std::max(M.fm.smz, F.smz);
         M.fm.smy = std::max(M.fm.smy, F.smy);
         M.fm.smx = std::max(M.fm.smx, F.smx);
@@ -314,21 +321,26 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M, double*
         for (const auto& a : v) g = std::max(g, a.gx);
         return g;
     };
-    M.gx_pack = gmax(M.pack);
     M.gx_prune = gmax(M.prune);
     M.gx_pairs = sizeof(R) == 4 ? gmax(M.pf32) : gmax(M.p64);
     M.gx_excl = gmax(M.excl);
     M.gx_14 = gmax(M.p14);
     M.gx_bonded = gmax(M.bonded);
-    M.gx_zero = gmax(M.zero);
-    M.gx_spread = gmax(M.spread);
-    M.gx_gather = gmax(M.gather);
-    M.gx_fin = gmax(M.fin);
+    for (int s = 0; s < n; ++s) {
+        add_blocks(M.map_pack, s, M.pack[s].gx, 1);
+        add_blocks(M.map_zero, s, M.zero[s].gx, 1);
+        add_blocks(M.map_spread, s, M.spread[s].gx, 1);
+        add_blocks(M.map_gather, s, M.gather[s].gx, 1);
+        add_blocks(M.map_fin, s, M.fin[s].gx, 1);
+    }
     // one device allocation for every array
     const size_t total = arr_bytes(M.pack) + arr_bytes(M.prune) + arr_bytes(M.pf32) + arr_bytes(M.p64) +
                          arr_bytes(M.excl) + arr_bytes(M.p14) + arr_bytes(M.bonded) + arr_bytes(M.zero) +
                          arr_bytes(M.spread) + arr_bytes(M.zf) + arr_bytes(M.yf) + arr_bytes(M.x) +
-                         arr_bytes(M.yi) + arr_bytes(M.zi) + arr_bytes(M.gather) + arr_bytes(M.fin);
+                         arr_bytes(M.yi) + arr_bytes(M.zi) + arr_bytes(M.gather) + arr_bytes(M.fin) +
+                         arr_bytes(M.map_pack) + arr_bytes(M.map_zero) + arr_bytes(M.map_spread) +
+                         arr_bytes(M.map_z) + arr_bytes(M.map_y) + arr_bytes(M.map_x) + arr_bytes(M.map_gather) +
+                         arr_bytes(M.map_fin);
     std::vector<unsigned char> host(total);
     args.alloc(total);
     size_t off = 0;
@@ -355,6 +367,20 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M, double*
     put(M.zi, D.fft.zi);
     put(M.gather, D.gather);
     put(M.fin, D.fin);
+    auto putmap = [&](const std::vector<int2>& v, BlockMap& bm) {
+        const int2* p = nullptr;
+        put(v, p);
+        bm.map = p;
+        bm.n = (int)v.size();
+    };
+    putmap(M.map_pack, D.pack_m);
+    putmap(M.map_zero, D.zero_m);
+    putmap(M.map_spread, D.spread_m);
+    putmap(M.map_gather, D.gather_m);
+    putmap(M.map_fin, D.fin_m);
+    putmap(M.map_z, D.fft.mz);
+    putmap(M.map_y, D.fft.my);
+    putmap(M.map_x, D.fft.mx);
     MDF_CUDA_TRY(cudaMemcpyAsync(args.p, host.data(), total, cudaMemcpyHostToDevice, b->main));
     MDF_CUDA_TRY(cudaStreamSynchronize(b->main));
     return D;
@@ -383,12 +409,12 @@ void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D, co
     k += (M.gx_excl > 0) + (M.gx_14 > 0);
     launch_bonded_multi(D.bonded, n, M.gx_bonded, M.energy, b->side);
     k += M.gx_bonded > 0;
-    launch_pme_multi<R>(D.zero, M.gx_zero, D.spread, M.gx_spread, D.fft, M.fm, D.gather, M.gx_gather, n, M.energy,
+    launch_pme_multi<R>(D.zero, D.zero_m, D.spread, D.spread_m, D.fft, M.fm, D.gather, D.gather_m, M.energy,
                         b->side);
     k += 8;   // grid clear, spread, five FFT passes, gather
     MDF_CUDA_TRY(cudaEventRecord(b->ev_join2, b->side));
     // main stream: pack, prune, pair kernel
-    launch_pack_multi<R>(D.pack, n, M.gx_pack, b->main);
+    launch_pack_multi<R>(D.pack, D.pack_m, b->main);
     ++k;
     if (M.prune_on) {
         launch_prune_multi<R>(D.prune, n, M.gx_prune, M.half, b->main);
@@ -404,7 +430,7 @@ void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D, co
         ++k;
     }
     MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, b->ev_join2, 0));
-    launch_finalize_multi(D.fin, n, M.gx_fin, b->main);
+    launch_finalize_multi(D.fin, D.fin_m, b->main);
     if (copies)
         MDF_CUDA_TRY(cudaMemcpyAsync(b->h_forces, b->d_forces.p, sizeof(double) * b->total, cudaMemcpyDeviceToHost,
                                      b->main));

@@ -19,6 +19,14 @@
 
 namespace mdf {
 
+// The blocks of a many-system launch: a one-dimensional grid of n blocks,
+// block b running block map[b].y (linear in the system's own gx x gy grid)
+// of system map[b].x.
+struct BlockMap {
+    const int2* map;
+    int n;
+};
+
 // ---------------------------------------------------------------- pairlist
 template <typename R>
 struct PackArgs {
@@ -314,11 +322,11 @@ struct FFTChainDev {
     const FFTXArgs<R>* x;
     const FFTYArgs<R>* yi;
     const FFTZArgs<R>* zi;
+    BlockMap mz, my, mx;   // the blocks of the z, y and x passes (forward and inverse share them)
 };
 
-// ... and the largest grid and shared memory of each pass over the systems.
+// ... and the largest shared memory of each pass over the systems.
 struct FFTChainMax {
-    int zx, yx, yy, xx, xy;
     size_t smz, smy, smx;
 };
 
@@ -338,7 +346,7 @@ struct FinalizeArgs {
 // The arguments of one system's launch (from its context) and the
 // many-system launchers (device arrays of arguments, the largest grid).
 template <typename R> PackArgs<R> make_pack_args(const Ctx& c);
-template <typename R> void launch_pack_multi(const PackArgs<R>* d_args, int nsys, int gx, cudaStream_t s);
+template <typename R> void launch_pack_multi(const PackArgs<R>* d_args, BlockMap bm, cudaStream_t s);
 template <typename R> PruneArgs<R> make_prune_args(const Ctx& c);
 template <typename R> PruneArgs<R> make_prune_half_args(const Ctx& c);
 void ensure_half_lists(Ctx& c);
@@ -362,11 +370,11 @@ template <typename R> FFTChain<R> make_fft_chain(const Ctx& c, bool energy);
 SpreadArgs make_spread_args(const Ctx& c);
 template <typename R> GatherArgs<R> make_gather_args(const Ctx& c);
 template <typename R>
-void launch_pme_multi(const ZeroArgs* d_zero, int zx, const SpreadArgs* d_spread, int sx, const FFTChainDev<R>& D,
-                      const FFTChainMax& M, const GatherArgs<R>* d_gather, int gx, int nsys, bool energy,
-                      cudaStream_t s);
+void launch_pme_multi(const ZeroArgs* d_zero, BlockMap mzero, const SpreadArgs* d_spread, BlockMap mspread,
+                      const FFTChainDev<R>& D, const FFTChainMax& M, const GatherArgs<R>* d_gather, BlockMap mgather,
+                      bool energy, cudaStream_t s);
 FinalizeArgs make_finalize_args(const Ctx& c, double* d_forces);
-void launch_finalize_multi(const FinalizeArgs* d_args, int nsys, int gx, cudaStream_t s);
+void launch_finalize_multi(const FinalizeArgs* d_args, BlockMap bm, cudaStream_t s);
 
 // The grid of a one-system launch from the struct's own extents.
 template <typename A>

@@ -217,7 +217,7 @@ __global__ void k_cluster_geom(const int* __restrict__ d_ncl, const double* __re
 // Also the cluster's current bounding box in its own frame (FP32, rounded
 // outward) for the prune's box test.  blockDim.x must be a multiple of 32.
 template <typename R>
-__device__ __forceinline__ void pack_dev(const PackArgs<R>& A)
+__device__ __forceinline__ void pack_dev(const PackArgs<R>& A, int bx, int by)
 {
     const int nslots = A.nslots;
     const double* __restrict__ xyz = A.xyz;
@@ -229,7 +229,7 @@ __device__ __forceinline__ void pack_dev(const PackArgs<R>& A)
     float4* __restrict__ cur_lo = A.cur_lo;
     float4* __restrict__ cur_hi = A.cur_hi;
     unsigned* st = A.st;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int s = bx * blockDim.x + threadIdx.x;
     const bool inside = s < nslots;
     const int a = inside ? slot_atom[s] : -1;
     typename V4<R>::type v;
@@ -280,15 +280,14 @@ __device__ __forceinline__ void pack_dev(const PackArgs<R>& A)
 template <typename R>
 __global__ void k_pack(PackArgs<R> A)
 {
-    pack_dev(A);
+    pack_dev(A, blockIdx.x, 0);
 }
 
 template <typename R>
-__global__ void k_pack_multi(const PackArgs<R>* __restrict__ As)
+__global__ void k_pack_multi(const PackArgs<R>* __restrict__ As, const int2* __restrict__ bmap)
 {
-    const PackArgs<R>& A = As[blockIdx.z];
-    if ((int)blockIdx.x >= A.gx) return;
-    pack_dev(A);
+    const int2 m = bmap[blockIdx.x];
+    pack_dev(As[m.x], m.y, 0);
 }
 
 __global__ void k_slot_type(const int* __restrict__ d_ncl, const int* __restrict__ slot_atom,
@@ -869,13 +868,14 @@ template PackArgs<float> make_pack_args<float>(const Ctx&);
 template PackArgs<double> make_pack_args<double>(const Ctx&);
 
 template <typename R>
-void launch_pack_multi(const PackArgs<R>* d_args, int nsys, int gx, cudaStream_t s)
+void launch_pack_multi(const PackArgs<R>* d_args, BlockMap bm, cudaStream_t s)
 {
-    k_pack_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_args);
+    if (bm.n <= 0) return;
+    k_pack_multi<R><<<bm.n, 256, 0, s>>>(d_args, bm.map);
     MDF_CUDA_TRY(cudaGetLastError());
 }
-template void launch_pack_multi<float>(const PackArgs<float>*, int, int, cudaStream_t);
-template void launch_pack_multi<double>(const PackArgs<double>*, int, int, cudaStream_t);
+template void launch_pack_multi<float>(const PackArgs<float>*, BlockMap, cudaStream_t);
+template void launch_pack_multi<double>(const PackArgs<double>*, BlockMap, cudaStream_t);
 
 void pack_positions(Ctx& c)
 {

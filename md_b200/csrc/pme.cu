@@ -208,7 +208,7 @@ __device__ __forceinline__ void fft_smem_setup(unsigned char* raw, const FFTDesc
 
 // ------------------------------------------------------------- z passes
 template <typename R>
-__device__ __forceinline__ void fft_z_r2c_dev(const FFTZArgs<R>& A)
+__device__ __forceinline__ void fft_z_r2c_dev(const FFTZArgs<R>& A, int bx, int by)
 {
     const unsigned long long* __restrict__ qgrid = A.qgrid;
     typename CT<R>::type* __restrict__ cgrid = A.cgrid;
@@ -224,7 +224,7 @@ __device__ __forceinline__ void fft_z_r2c_dev(const FFTZArgs<R>& A)
     fft_smem_setup(smem_raw, dz, twz, tabz, LP, tw, tab, bufA, bufB);
     const int K2 = dz.n, Kc = K2 / 2 + 1;
     const int tpl = blockDim.x / LP, line = threadIdx.x / tpl, lt = threadIdx.x - line * tpl;
-    const long long g0 = (long long)blockIdx.x * 2 * LP + 2 * line;   // this thread's pair of real lines
+    const long long g0 = (long long)bx * 2 * LP + 2 * line;   // this thread's pair of real lines
     for (int z = lt; z < K2; z += tpl) {
         C v;
         v.x = g0 < nlines ? (R)((double)(long long)qgrid[g0 * K2 + z] * GRID_ISCALE) : (R)0;
@@ -243,7 +243,7 @@ __device__ __forceinline__ void fft_z_r2c_dev(const FFTZArgs<R>& A)
 }
 
 template <typename R>
-__device__ __forceinline__ void fft_z_c2r_dev(const FFTZArgs<R>& A)
+__device__ __forceinline__ void fft_z_c2r_dev(const FFTZArgs<R>& A, int bx, int by)
 {
     const typename CT<R>::type* __restrict__ cgrid = A.cgrid;
     R* __restrict__ rgrid = A.rgrid;
@@ -259,7 +259,7 @@ __device__ __forceinline__ void fft_z_c2r_dev(const FFTZArgs<R>& A)
     fft_smem_setup(smem_raw, dz, twz, tabz, LP, tw, tab, bufA, bufB);
     const int K2 = dz.n, Kc = K2 / 2 + 1;
     const int tpl = blockDim.x / LP, line = threadIdx.x / tpl, lt = threadIdx.x - line * tpl;
-    const long long g0 = (long long)blockIdx.x * 2 * LP + 2 * line;
+    const long long g0 = (long long)bx * 2 * LP + 2 * line;
     for (int k = lt; k < K2; k += tpl) {
         const int kk = k < Kc ? k : K2 - k;
         C A = {0, 0}, B = {0, 0};
@@ -283,7 +283,7 @@ __device__ __forceinline__ void fft_z_c2r_dev(const FFTZArgs<R>& A)
 
 // ------------------------------------------------------------- y pass
 template <typename R>
-__device__ __forceinline__ void fft_y_dev(const FFTYArgs<R>& A)
+__device__ __forceinline__ void fft_y_dev(const FFTYArgs<R>& A, int bx, int by)
 {
     typename CT<R>::type* __restrict__ cgrid = A.cgrid;
     const int Kc = A.Kc;
@@ -298,7 +298,7 @@ __device__ __forceinline__ void fft_y_dev(const FFTYArgs<R>& A)
     int2* tab;
     fft_smem_setup(smem_raw, dy, twy, taby, LP, tw, tab, bufA, bufB);
     const int K1 = dy.n;
-    const int x = blockIdx.y, kz0 = blockIdx.x * LP;
+    const int x = by, kz0 = bx * LP;
     const long long base = (long long)x * K1 * Kc;
     // loads: consecutive threads take consecutive kz (coalesced)
     for (int e = threadIdx.x; e < LP * K1; e += blockDim.x) {
@@ -319,7 +319,7 @@ __device__ __forceinline__ void fft_y_dev(const FFTYArgs<R>& A)
 // ------------------------------------------- x pass + convolution + inverse
 
 template <typename R, bool ENERGY>
-__device__ __forceinline__ void fft_x_conv_dev(const FFTXArgs<R>& A)
+__device__ __forceinline__ void fft_x_conv_dev(const FFTXArgs<R>& A, int bx, int by)
 {
     typename CT<R>::type* __restrict__ cgrid = A.cgrid;
     const int K1 = A.K1, Kc = A.Kc;
@@ -340,7 +340,7 @@ __device__ __forceinline__ void fft_x_conv_dev(const FFTXArgs<R>& A)
     int2* tab;
     fft_smem_setup(smem_raw, dx, twx, tabx, LP, tw, tab, bufA, bufB);
     const int K0 = dx.n;
-    const int y = blockIdx.y, kz0 = blockIdx.x * LP;
+    const int y = by, kz0 = bx * LP;
     const long long stride = (long long)K1 * Kc;
     for (int e = threadIdx.x; e < LP * K0; e += blockDim.x) {
         const int x = e >> lp_shift, l = e & (LP - 1), kz = kz0 + l;
@@ -393,20 +393,23 @@ __device__ __forceinline__ void fft_x_conv_dev(const FFTXArgs<R>& A)
     }
 }
 
-// One-system kernels (arguments by value) and their many-system forms
-// (blockIdx.z = system; blocks past the system's own grid return).
+// One-system kernels (arguments by value) and their many-system forms: a
+// one-dimensional grid of every system's blocks, block b running block
+// bmap[b].y of system bmap[b].x (so systems of different sizes leave no idle
+// blocks).
 #define MDF_FFT_KERNELS(NAME, DEV, ARGS, ...)                                                                   \
     template <__VA_ARGS__>                                                                                    \
     __global__ void __launch_bounds__(FFT_THREADS) NAME(ARGS A)                                               \
     {                                                                                                         \
-        DEV(A);                                                                                               \
+        DEV(A, blockIdx.x, blockIdx.y);                                                                       \
     }                                                                                                         \
     template <__VA_ARGS__>                                                                                    \
-    __global__ void __launch_bounds__(FFT_THREADS) NAME##_multi(const ARGS* __restrict__ As)                  \
+    __global__ void __launch_bounds__(FFT_THREADS) NAME##_multi(const ARGS* __restrict__ As,                  \
+                                                                const int2* __restrict__ bmap)                \
     {                                                                                                         \
-        const ARGS& A = As[blockIdx.z];                                                                       \
-        if ((int)blockIdx.x >= A.gx || (int)blockIdx.y >= A.gy) return;                                       \
-        DEV(A);                                                                                               \
+        const int2 m = bmap[blockIdx.x];                                                                      \
+        const ARGS& A = As[m.x];                                                                              \
+        DEV(A, m.y % A.gx, m.y / A.gx);                                                                       \
     }
 MDF_FFT_KERNELS(k_fft_z_r2c, fft_z_r2c_dev<R>, FFTZArgs<R>, typename R)
 MDF_FFT_KERNELS(k_fft_z_c2r, fft_z_c2r_dev<R>, FFTZArgs<R>, typename R)
@@ -416,17 +419,18 @@ MDF_FFT_KERNELS(k_fft_y, fft_y_dev<R>, FFTYArgs<R>, typename R)
 template <typename R, bool ENERGY>
 __global__ void __launch_bounds__(FFT_THREADS) k_fft_x_conv(FFTXArgs<R> A)
 {
-    fft_x_conv_dev<R, ENERGY>(A);
+    fft_x_conv_dev<R, ENERGY>(A, blockIdx.x, blockIdx.y);
 }
 
 // 64 registers (eight blocks per SM): the many-system grids are small and the
 // pass is latency bound, so resident warps matter more than registers here
 template <typename R, bool ENERGY>
-__global__ void __launch_bounds__(FFT_THREADS, 8) k_fft_x_conv_multi(const FFTXArgs<R>* __restrict__ As)
+__global__ void __launch_bounds__(FFT_THREADS, 8) k_fft_x_conv_multi(const FFTXArgs<R>* __restrict__ As,
+                                                                     const int2* __restrict__ bmap)
 {
-    const FFTXArgs<R>& A = As[blockIdx.z];
-    if ((int)blockIdx.x >= A.gx || (int)blockIdx.y >= A.gy) return;
-    fft_x_conv_dev<R, ENERGY>(A);
+    const int2 m = bmap[blockIdx.x];
+    const FFTXArgs<R>& A = As[m.x];
+    fft_x_conv_dev<R, ENERGY>(A, m.y % A.gx, m.y / A.gx);
 }
 
 // ------------------------------------------------------ spread / gather
@@ -518,7 +522,7 @@ __device__ __forceinline__ R bspline4_one(R w, int j)
 // rounded fixed-point values, summed in any order).  Launched with a
 // multiple of 16 threads per block.
 template <typename R>
-__device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A)
+__device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A, int bx, int by)
 {
     const int s0 = A.s0, s1 = A.s1;
     const int* __restrict__ slot_atom = A.slot_atom;
@@ -527,7 +531,7 @@ __device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A)
     const GridGeom& g = A.g;
     unsigned long long* __restrict__ qgrid = A.qgrid;
     unsigned* st = A.st;
-    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long t0 = (long long)bx * blockDim.x + threadIdx.x;
     const int s = s0 + (int)(t0 >> 4);
     const int l = (int)(t0 & 15), r = l >> 2, zz = l & 3;
     // the whole group of 16 lanes leaves together (same atom)
@@ -588,29 +592,27 @@ __device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A)
 template <typename R>
 __global__ void __launch_bounds__(256) k_spread4_rows(SpreadArgs A)
 {
-    spread4_rows_dev<R>(A);
+    spread4_rows_dev<R>(A, blockIdx.x, 0);
 }
 
 template <typename R>
-__global__ void __launch_bounds__(256) k_spread4_rows_multi(const SpreadArgs* __restrict__ As)
+__global__ void __launch_bounds__(256) k_spread4_rows_multi(const SpreadArgs* __restrict__ As, const int2* __restrict__ bmap)
 {
-    const SpreadArgs& A = As[blockIdx.z];
-    if ((int)blockIdx.x >= A.gx) return;
-    spread4_rows_dev<R>(A);
+    const int2 m = bmap[blockIdx.x];
+    spread4_rows_dev<R>(As[m.x], m.y, 0);
 }
 
 // Clear many systems' charge grids in one launch.
-__global__ void k_zero_multi(const ZeroArgs* __restrict__ As)
+__global__ void k_zero_multi(const ZeroArgs* __restrict__ As, const int2* __restrict__ bmap)
 {
-    const ZeroArgs& A = As[blockIdx.z];
-    if ((int)blockIdx.x >= A.gx) return;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < A.n;
-         i += (long long)A.gx * blockDim.x)
+    const int2 m = bmap[blockIdx.x];
+    const ZeroArgs& A = As[m.x];
+    for (long long i = (long long)m.y * blockDim.x + threadIdx.x; i < A.n; i += (long long)A.gx * blockDim.x)
         A.p[i] = 0ull;
 }
 
 template <typename R>
-__device__ __forceinline__ void gather4_dev(const GatherArgs<R>& A)
+__device__ __forceinline__ void gather4_dev(const GatherArgs<R>& A, int bx, int by)
 {
     const int s0 = A.s0, s1 = A.s1, nslots = A.nslots;
     const int* __restrict__ slot_atom = A.slot_atom;
@@ -620,7 +622,7 @@ __device__ __forceinline__ void gather4_dev(const GatherArgs<R>& A)
     const R* __restrict__ phi = A.phi;
     unsigned long long* __restrict__ fslot = A.fslot;
     unsigned* st = A.st;
-    int s = s0 + blockIdx.x * blockDim.x + threadIdx.x;   // slots [s0, s1) of nslots
+    int s = s0 + bx * blockDim.x + threadIdx.x;   // slots [s0, s1) of nslots
     if (s >= s1) return;
     int a = slot_atom[s];
     if (a < 0) return;
@@ -672,15 +674,14 @@ __device__ __forceinline__ void gather4_dev(const GatherArgs<R>& A)
 template <typename R>
 __global__ void k_gather4(GatherArgs<R> A)
 {
-    gather4_dev<R>(A);
+    gather4_dev<R>(A, blockIdx.x, 0);
 }
 
 template <typename R>
-__global__ void k_gather4_multi(const GatherArgs<R>* __restrict__ As)
+__global__ void k_gather4_multi(const GatherArgs<R>* __restrict__ As, const int2* __restrict__ bmap)
 {
-    const GatherArgs<R>& A = As[blockIdx.z];
-    if ((int)blockIdx.x >= A.gx) return;
-    gather4_dev<R>(A);
+    const int2 m = bmap[blockIdx.x];
+    gather4_dev<R>(As[m.x], m.y, 0);
 }
 
 // The reference's order-5 weights (src/System/PBC.cpp:329-356 for the spread,
@@ -1120,21 +1121,21 @@ static void conv_chain(Ctx& c, const PmeBufs<R>&, bool energy)
 }
 
 // Many systems' FFT chains, one launch per pass (each struct array holds one
-// entry per system; grids and shared memory are the largest over systems).
+// entry per system; the block maps list every system's blocks; shared memory
+// is the largest over systems).
 template <typename R>
-void launch_fft_chain_multi(const FFTChainDev<R>& D, int nsys, const FFTChainMax& M, bool energy, cudaStream_t s)
+void launch_fft_chain_multi(const FFTChainDev<R>& D, const FFTChainMax& M, bool energy, cudaStream_t s)
 {
-    k_fft_z_r2c_multi<R><<<dim3(M.zx, 1, nsys), FFT_THREADS, M.smz, s>>>(D.zf);
-    k_fft_y_multi<R><<<dim3(M.yx, M.yy, nsys), FFT_THREADS, M.smy, s>>>(D.yf);
-    if (energy) k_fft_x_conv_multi<R, true><<<dim3(M.xx, M.xy, nsys), FFT_THREADS, M.smx, s>>>(D.x);
-    else k_fft_x_conv_multi<R, false><<<dim3(M.xx, M.xy, nsys), FFT_THREADS, M.smx, s>>>(D.x);
-    k_fft_y_multi<R><<<dim3(M.yx, M.yy, nsys), FFT_THREADS, M.smy, s>>>(D.yi);
-    k_fft_z_c2r_multi<R><<<dim3(M.zx, 1, nsys), FFT_THREADS, M.smz, s>>>(D.zi);
+    if (D.mz.n > 0) k_fft_z_r2c_multi<R><<<D.mz.n, FFT_THREADS, M.smz, s>>>(D.zf, D.mz.map);
+    if (D.my.n > 0) k_fft_y_multi<R><<<D.my.n, FFT_THREADS, M.smy, s>>>(D.yf, D.my.map);
+    if (D.mx.n > 0) {
+        if (energy) k_fft_x_conv_multi<R, true><<<D.mx.n, FFT_THREADS, M.smx, s>>>(D.x, D.mx.map);
+        else k_fft_x_conv_multi<R, false><<<D.mx.n, FFT_THREADS, M.smx, s>>>(D.x, D.mx.map);
+    }
+    if (D.my.n > 0) k_fft_y_multi<R><<<D.my.n, FFT_THREADS, M.smy, s>>>(D.yi, D.my.map);
+    if (D.mz.n > 0) k_fft_z_c2r_multi<R><<<D.mz.n, FFT_THREADS, M.smz, s>>>(D.zi, D.mz.map);
     MDF_CUDA_TRY(cudaGetLastError());
 }
-template void launch_fft_chain_multi<float>(const FFTChainDev<float>&, int, const FFTChainMax&, bool, cudaStream_t);
-template void launch_fft_chain_multi<double>(const FFTChainDev<double>&, int, const FFTChainMax&, bool,
-                                             cudaStream_t);
 
 // Spread and gather arguments of this rank's slots (PHYSICAL, order 4).
 SpreadArgs make_spread_args(const Ctx& c)
@@ -1342,21 +1343,22 @@ static void run_pme_slab(Ctx& c, bool energy)
 
 // Many systems: clear the charge grids, spread, the FFT chain, gather.
 template <typename R>
-void launch_pme_multi(const ZeroArgs* d_zero, int zx, const SpreadArgs* d_spread, int sx, const FFTChainDev<R>& D,
-                      const FFTChainMax& M, const GatherArgs<R>* d_gather, int gx, int nsys, bool energy,
-                      cudaStream_t s)
+void launch_pme_multi(const ZeroArgs* d_zero, BlockMap mzero, const SpreadArgs* d_spread, BlockMap mspread,
+                      const FFTChainDev<R>& D, const FFTChainMax& M, const GatherArgs<R>* d_gather, BlockMap mgather,
+                      bool energy, cudaStream_t s)
 {
-    k_zero_multi<<<dim3(zx, 1, nsys), 256, 0, s>>>(d_zero);
-    k_spread4_rows_multi<R><<<dim3(sx, 1, nsys), 256, 0, s>>>(d_spread);
+    if (mzero.n > 0) k_zero_multi<<<mzero.n, 256, 0, s>>>(d_zero, mzero.map);
+    if (mspread.n > 0) k_spread4_rows_multi<R><<<mspread.n, 256, 0, s>>>(d_spread, mspread.map);
     MDF_CUDA_TRY(cudaGetLastError());
-    launch_fft_chain_multi<R>(D, nsys, M, energy, s);
-    k_gather4_multi<R><<<dim3(gx, 1, nsys), 256, 0, s>>>(d_gather);
+    launch_fft_chain_multi<R>(D, M, energy, s);
+    if (mgather.n > 0) k_gather4_multi<R><<<mgather.n, 256, 0, s>>>(d_gather, mgather.map);
     MDF_CUDA_TRY(cudaGetLastError());
 }
-template void launch_pme_multi<float>(const ZeroArgs*, int, const SpreadArgs*, int, const FFTChainDev<float>&,
-                                      const FFTChainMax&, const GatherArgs<float>*, int, int, bool, cudaStream_t);
-template void launch_pme_multi<double>(const ZeroArgs*, int, const SpreadArgs*, int, const FFTChainDev<double>&,
-                                       const FFTChainMax&, const GatherArgs<double>*, int, int, bool, cudaStream_t);
+template void launch_pme_multi<float>(const ZeroArgs*, BlockMap, const SpreadArgs*, BlockMap, const FFTChainDev<float>&,
+                                      const FFTChainMax&, const GatherArgs<float>*, BlockMap, bool, cudaStream_t);
+template void launch_pme_multi<double>(const ZeroArgs*, BlockMap, const SpreadArgs*, BlockMap,
+                                       const FFTChainDev<double>&, const FFTChainMax&, const GatherArgs<double>*,
+                                       BlockMap, bool, cudaStream_t);
 
 // ------------------------------------------------------------- adjoint
 // Reciprocal-space part of mdf_backward.  With E = 1/2 Q^T C Q (Q the charge

@@ -595,10 +595,10 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
     A.nlist, A.ilist, A.plist, A.xq, A.stype, A.centerf, A.lj4, A.ntp, A.lj_smem, A.kc, A.K, A.shifts, A.fslot,      \
         A.nslots, A.acc, A.npairs, A.next, A.persist, A.st
 
-// With energies: the compiler's own register choice (72, three blocks per SM;
-// a 64-register cap spills and is slower).
+// With energies: up to 80 registers, three blocks per SM (left to itself the
+// compiler picks 64 and spills, which measured 1-2% slower).
 template <bool SWITCH, bool COUNT>
-__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32(PairF32Args A)
+__global__ void __launch_bounds__(NB_THREADS, 3) k_pairs_f32(PairF32Args A)
 {
     pairs_f32_body<true, SWITCH, COUNT>(MDF_PF32_UNPACK(A));
 }
@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_half_force_multi(co
 // Many systems in one launch (blockIdx.z = system), with the same register
 // budgets as the one-system kernels above.
 template <bool SWITCH>
-__global__ void __launch_bounds__(NB_THREADS) k_pairs_f32_multi(const PairF32Args* __restrict__ As)
+__global__ void __launch_bounds__(NB_THREADS, 3) k_pairs_f32_multi(const PairF32Args* __restrict__ As)
 {
     const PairF32Args& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;

@@ -133,8 +133,8 @@ typedef struct {
     double cutoff;           /* LJ and Coulomb cutoff (reference: lj_cutoff_ = ee_cutoff_) */
     double skin;             /* pairlist skin; list cutoff = cutoff + skin */
     double switch_radius;    /* LJ potential switch start; <= 0 selects force-shifted LJ */
-    double ewald_tol;        /* alpha = sqrt(-ln(2 tol)) / cutoff (src/System/PBC.cpp:88-91) */
-    double ewald_alpha;      /* > 0 overrides ewald_tol */
+    double ewald_tol;        /* alpha = sqrt(-ln(2 tol)) / cutoff (src/System/PBC.cpp:88-91); (0, 0.5) */
+    double ewald_alpha;      /* > 0 overrides ewald_tol; alpha >= 1e-12 per Angstrom */
     int32_t grid[3];         /* PME mesh; 0 = the reference's formula (src/System/PBC.cpp:93-99) */
     int32_t pme_order;       /* PHYSICAL B-spline order (4); REFERENCE uses its order-5 chain */
     double coulomb_const;    /* 18.2206899283247^2 */

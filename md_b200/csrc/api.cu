@@ -742,6 +742,10 @@ int mdf_create(const mdf_topology* top, const mdf_params* p, mdf_ctx** out)
         for (int d = 0; d < 3; ++d) c.box[d] = c.p.box[d];
         double tol = c.p.ewald_tol > 0 ? c.p.ewald_tol : 1e-6;
         c.alpha = c.p.ewald_alpha > 0 ? c.p.ewald_alpha : std::sqrt(std::log(2 * tol) * -1) / c.p.cutoff;
+        // ewald_tol >= 0.5 gives no splitting parameter; the FP32 pair kernel
+        // also relies on exp(-alpha^2 r^2) vanishing at r^2 = 1e30
+        if (!(std::isfinite(c.alpha) && c.alpha >= 1e-12))
+            throw ApiError(MDF_ERR_INVALID, "Ewald alpha must be finite and >= 1e-12 (ewald_tol in (0, 0.5))");
         upload_topology(c, top);
         if (!(c.box[0] > 0 && c.box[1] > 0 && c.box[2] > 0))
             throw ApiError(MDF_ERR_INVALID, "periodic box required");

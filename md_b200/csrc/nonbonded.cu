@@ -361,15 +361,19 @@ __device__ __forceinline__ void pairs_f32_body(
             for (int t = 0; t < CLUSTER; ++t) {
                 const float4 xj = sxl[t];
                 const float dx = xix - xj.x, dy = xiy - xj.y, dz = xiz - xj.z;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
+                const float r2r = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool on = ((rot >> t) & 1u) && r2r <= K.rc2;
+                // switched LJ: a slot outside the list or the cutoff takes r^2 = 1e30,
+                // at which every term below is exactly zero (r^-6 underflows, the
+                // Gaussian is 0 and the switch is 0 at x = 1), so no result needs a select
+                const float r2 = SWITCH ? (on ? r2r : 1e30f) : r2r;
                 const float rinv = rsqrt_ftz(r2);
                 const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
                 const float4 ab = ljt[trow + stl[t]];      // A, B, 12A, 6B
                 float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
                 float G = (rinv6 * rinv2) * fmaf(ab.z, rinv6, -ab.w);
                 if (SWITCH) {
-                    const float x = fmaxf(0.f, fmaf(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
+                    const float x = __saturatef(fmaf(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
                     const float S = fmaf(x2 * x, fmaf(x, fmaf(x, -6.f, 15.f), -10.f), 1.f);
                     const float dSr = x2 * fmaf(x, fmaf(x, K.d30, K.d60), K.d30) * rinv;   // dS/dr / r
                     G = fmaf(S, G, -U * dSr);
@@ -384,10 +388,10 @@ __device__ __forceinline__ void pairs_f32_body(
                 const float erfcv = erfc_as(rcp_ftz(fmaf(K.pa, r, 1.0f)), ex);
                 const float ec = (qik * xj.w) * erfcv * rinv;
                 float g = fmaf(fmaf(qik2 * xj.w, ex, ec), rinv2, G);
-                g = on ? g : 0.f;
+                if (!SWITCH) g = on ? g : 0.f;
                 if (ENERGY) {
-                    el += on ? U : 0.f;
-                    ed += on ? ec : 0.f;
+                    el += SWITCH ? U : (on ? U : 0.f);
+                    ed += SWITCH ? ec : (on ? ec : 0.f);
                 }
                 if (COUNT) npc += on ? 1 : 0;
                 fix = fmaf(g, dx, fix); fiy = fmaf(g, dy, fiy); fiz = fmaf(g, dz, fiz);
@@ -519,15 +523,16 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
             for (int t = 0; t < 4; ++t) {
                 const float4 xi = sxl[t];
                 const float dx = xi.x - pjx, dy = xi.y - pjy, dz = xi.z - pjz;
-                const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
+                const float r2r = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                const bool on = ((rot >> t) & 1u) && r2r <= K.rc2;
+                const float r2 = SWITCH ? (on ? r2r : 1e30f) : r2r;   // as in the whole-entry kernel
                 const float rinv = rsqrt_ftz(r2);
                 const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
                 const float4 ab = ljt[stl[t] + tj];      // A, B, 12A, 6B
                 float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
                 float G = (rinv6 * rinv2) * fmaf(ab.z, rinv6, -ab.w);
                 if (SWITCH) {
-                    const float x = fmaxf(0.f, fmaf(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
+                    const float x = __saturatef(fmaf(r, K.inv_sw, -K.rsw_inv)), x2 = x * x;
                     const float S = fmaf(x2 * x, fmaf(x, fmaf(x, -6.f, 15.f), -10.f), 1.f);
                     const float dSr = x2 * fmaf(x, fmaf(x, K.d30, K.d60), K.d30) * rinv;   // dS/dr / r
                     G = fmaf(S, G, -U * dSr);
@@ -543,10 +548,10 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
                 const float qq = xi.w * xj.w;
                 const float ec = qq * erfcv * rinv;
                 float g = fmaf(fmaf(qq * K.two_a_spi, ex, ec), rinv2, G);
-                g = on ? g : 0.f;
+                if (!SWITCH) g = on ? g : 0.f;
                 if (ENERGY) {
-                    el += on ? U : 0.f;
-                    ed += on ? ec : 0.f;
+                    el += SWITCH ? U : (on ? U : 0.f);
+                    ed += SWITCH ? ec : (on ? ec : 0.f);
                 }
                 if (COUNT) npc += on ? 1 : 0;
                 fix = fmaf(g, dx, fix); fiy = fmaf(g, dy, fiy); fiz = fmaf(g, dz, fiz);

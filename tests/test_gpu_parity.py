@@ -183,6 +183,16 @@ def test_nacl_madelung_on_gpu():
     eng.close()
 
 
+@pytest.mark.parametrize("tol", [0.5, 0.9])
+def test_ewald_tolerance_without_splitting_rejected(tol):
+    # sqrt(-ln(2 tol)) has no positive value for tol >= 0.5
+    s = H.system("tiny")
+    flat = H.flat(s, PHYS, engine.cmap_coefficients)
+    with pytest.raises(engine.MDFError) as e:
+        engine.Engine(flat, s.box, semantics=PHYS, precision=MIXED, ewald_tol=tol, grid=(24, 24, 24))
+    assert e.value.status == 1
+
+
 def test_nonfinite_position_reported_not_faulted():
     s = H.system("tiny")
     eng, _ = make_engine(s, PHYS, MIXED, (24, 24, 24))

@@ -98,7 +98,7 @@ typedef struct {
     int32_t natoms;
     const double *charge;          /* [natoms], internal charge unit */
     const int32_t *type;           /* [natoms], 0-based atom type */
-    int32_t ntypes;
+    int32_t ntypes;                /* 1..8000 */
     const int32_t *nb_index;       /* [ntypes*ntypes] NONBONDED_PARM_INDEX, 1-based, 0 = none */
     int32_t n_ljpair;
     const double *lj_a, *lj_b;     /* [n_ljpair] */

@@ -259,6 +259,8 @@ void upload_topology(Ctx& c, const mdf_topology* t)
     if (!t || t->natoms <= 0) throw ApiError(MDF_ERR_INVALID, "topology has no atoms");
     if (!t->charge || !t->type || !t->nb_index || t->ntypes <= 0)
         throw ApiError(MDF_ERR_INVALID, "topology misses charges, types or the nonbonded index");
+    // the pair kernels address the (ntypes + 1)^2 table of 32-byte rows with int byte offsets
+    if (t->ntypes > 8000) throw ApiError(MDF_ERR_CAPACITY, "more than 8000 atom types");
     c.N = t->natoms;
     c.ntypes = t->ntypes;
     c.ntp = t->ntypes + 1;

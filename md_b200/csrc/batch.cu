@@ -211,6 +211,7 @@ struct MultiArgs {
     size_t dyn_pairs = 0;
     int threads = 256;
     bool prune_on = false, use_switch = false, energy = false, persist = false, half = false;
+    bool lj_smem = true;   // every system's LJ table in shared memory (one kernel form for the batch)
 };
 
 template <typename R>
@@ -321,6 +322,14 @@ MultiDev<R> prepare_multi(mdf_batch* b, uint32_t flags, MultiArgs<R>& M, double*
         for (const auto& a : v) g = std::max(g, a.gx);
         return g;
     };
+    // the pair kernel reads the LJ tables from shared memory only when all fit
+    for (const auto& a : M.pf32) M.lj_smem = M.lj_smem && a.lj_smem;
+    for (const auto& a : M.p64) M.lj_smem = M.lj_smem && a.lj_smem;
+    if (!M.lj_smem) {
+        for (auto& a : M.pf32) a.lj_smem = 0;
+        for (auto& a : M.p64) a.lj_smem = 0;
+        M.dyn_pairs = 0;
+    }
     M.gx_prune = gmax(M.prune);
     M.gx_pairs = sizeof(R) == 4 ? gmax(M.pf32) : gmax(M.p64);
     M.gx_excl = gmax(M.excl);
@@ -423,10 +432,10 @@ void enqueue_multi(mdf_batch* b, const MultiArgs<R>& M, const MultiDev<R>& D, co
     if (M.gx_pairs > 0) {
         if (sizeof(R) == 4)
             launch_pairs_f32_multi(D.pf32, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, M.persist,
-                                   M.half, b->main);
+                                   M.half, M.lj_smem, b->main);
         else
             launch_pairs_f64_multi(D.p64, n, M.gx_pairs, M.threads, M.dyn_pairs, M.energy, M.use_switch, M.persist,
-                                   M.half, b->main);
+                                   M.half, M.lj_smem, b->main);
         ++k;
     }
     MDF_CUDA_TRY(cudaStreamWaitEvent(b->main, b->ev_join2, 0));

@@ -354,11 +354,11 @@ template <typename R>
 void launch_prune_multi(const PruneArgs<R>* d_args, int nsys, int gx, bool half, cudaStream_t s);
 PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn);
 void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, bool half, cudaStream_t s);
+                            bool use_switch, bool persist, bool half, bool lj_smem, cudaStream_t s);
 template <typename R> PairArgs<R> make_pair_args(const Ctx& c, bool count);
 PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn);
 void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, bool half, cudaStream_t s);
+                            bool use_switch, bool persist, bool half, bool lj_smem, cudaStream_t s);
 int pair_threads(const Ctx& c);
 ExclArgs make_excl_args(const Ctx& c);
 Pair14Args make_pair14_args(const Ctx& c);

@@ -56,6 +56,14 @@ __device__ __forceinline__ float erfc_as(float t, float ex)
     return t * (a1 + t * (a2 + t * (a3 + t * (a4 + t * a5)))) * ex;
 }
 
+// The table row at a byte offset (type indexes are kept pre-multiplied by the
+// row size, so the address is one add).
+template <typename T>
+__device__ __forceinline__ const T& at_bytes(const T* __restrict__ base, int bytes)
+{
+    return *reinterpret_cast<const T*>(reinterpret_cast<const char*>(base) + bytes);
+}
+
 struct ShiftTable {
     float v[27][6];   // hi.x hi.y hi.z lo.x lo.y lo.z
 };

@@ -281,8 +281,31 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_multi(const PairArgs<R>* _
 //  * the LJ table holds (A, B, 12A, 6B) per type pair, in shared memory when it
 //    fits (lj_smem), and the Gaussian uses 2^(kex r^2) on the SFU;
 //  * energies are summed in FP32 per entry and in FP64 across entries.
-template <bool ENERGY, bool SWITCH, bool COUNT>
-__device__ __forceinline__ void pairs_f32_body(
+// Static shared arrays of the pair bodies, declared once per kernel (each
+// kernel inlines two forms of its body, see pairs_f32_body).
+struct SmemF32W {
+    float4 sx[NB_WARPS][4][2 * CLUSTER];
+    int stj[NB_WARPS][4][2 * CLUSTER];
+    float sh[27][6];
+};
+struct SmemF32H {
+    float4 sxi[NB_WARPS][8];    // the item's four i atoms (I frame, charge x kc), twice
+    int sti[NB_WARPS][8];       // their LJ table rows
+    float sh[27][6];
+};
+struct SmemF64W {
+    double4 sx[NB_WARPS][4][2 * CLUSTER];
+    int stj[NB_WARPS][4][2 * CLUSTER];
+    double sh[27][3];
+};
+struct SmemF64H {
+    double4 sxi[NB_WARPS][8];
+    int sti[NB_WARPS][8];
+    double sh[27][3];
+};
+
+template <bool ENERGY, bool SWITCH, bool COUNT, bool LJS>
+__device__ __forceinline__ void pairs_f32_body_t(SmemF32W& S,
     int nlist, const ILRange* __restrict__ ilist, const PairEntry* __restrict__ plist, const float4* __restrict__ xq,
     const int* __restrict__ stype, const float4* __restrict__ centerf, const float4* __restrict__ lj4, int ntp,
     int lj_smem, float kc, const PairConstF& Kin, const ShiftTable& shifts, unsigned long long* __restrict__ fslot,
@@ -294,14 +317,14 @@ __device__ __forceinline__ void pairs_f32_body(
     // each staged j cluster is stored twice in a row, so the atom a lane meets
     // at step t, (ii + t) mod 8, sits at the compile-time offset t from the
     // lane's own slot: no index arithmetic in the pair loop
-    __shared__ float4 sx[NB_WARPS][4][2 * CLUSTER];
-    __shared__ int stj[NB_WARPS][4][2 * CLUSTER];
-    __shared__ float sh[27][6];
+    auto& sx = S.sx;
+    auto& stj = S.stj;
+    auto& sh = S.sh;
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = shifts.v[k / 6][k % 6];
-    if (lj_smem)
+    if (LJS)
         for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj[k] = lj4[k];
     __syncthreads();
-    const float4* __restrict__ ljt = lj_smem ? s_lj : lj4;
+    const float4* __restrict__ ljt = LJS ? s_lj : lj4;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
@@ -326,7 +349,7 @@ __device__ __forceinline__ void pairs_f32_body(
         const ILRange L = ilist[w];
         const int I = L.i;
         const float4 xi = xq[I * CLUSTER + ii];
-        const int trow = stype[I * CLUSTER + ii] * ntp;
+        const int trow = stype[I * CLUSTER + ii] * ntp * (int)sizeof(float4);   // byte offsets
         const float4 cI = centerf[I];
         const float qik = kc * xi.w;
         const float qik2 = qik * K.two_a_spi;
@@ -341,7 +364,7 @@ __device__ __forceinline__ void pairs_f32_body(
             }
             const int J = pe.j;
             const float4 xjj = xq[J * CLUSTER + ii];
-            const int tjj = stype[J * CLUSTER + ii];
+            const int tjj = stype[J * CLUSTER + ii] * (int)sizeof(float4);
             sx[wib][jslot][ii] = xjj;
             sx[wib][jslot][ii + CLUSTER] = xjj;
             stj[wib][jslot][ii] = tjj;
@@ -369,7 +392,7 @@ __device__ __forceinline__ void pairs_f32_body(
                 const float r2 = SWITCH ? (on ? r2r : 1e30f) : r2r;
                 const float rinv = rsqrt_ftz(r2);
                 const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
-                const float4 ab = ljt[trow + stl[t]];      // A, B, 12A, 6B
+                const float4 ab = at_bytes(ljt, trow + stl[t]);      // A, B, 12A, 6B
                 float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
                 float G = (rinv6 * rinv2) * fmaf(ab.z, rinv6, -ab.w);
                 if (SWITCH) {
@@ -447,13 +470,13 @@ __device__ __forceinline__ void pairs_f32_body(
 // rotate one lane per step (the lane's i atom repeats every four lanes, so
 // the same shuffle as the whole-entry kernel works).  After the item the
 // eight partial sums of each i atom are reduced by three butterfly steps.
-template <bool ENERGY, bool SWITCH, bool COUNT>
-__device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
+template <bool ENERGY, bool SWITCH, bool COUNT, bool LJS>
+__device__ __forceinline__ void pairs_f32_half_body_t(SmemF32H& S, const PairF32Args& A)
 {
     extern __shared__ float4 s_lj[];
-    __shared__ float4 sxi[NB_WARPS][8];    // the item's four i atoms (I frame, charge x kc), twice
-    __shared__ int sti[NB_WARPS][8];       // their LJ table rows
-    __shared__ float sh[27][6];
+    auto& sxi = S.sxi;
+    auto& sti = S.sti;
+    auto& sh = S.sh;
     const int nlist = A.nlist, ntp = A.ntp, nslots = A.nslots;
     const ILRange* __restrict__ ilist = A.ilist;
     const PairEntry* __restrict__ plist = A.plist;
@@ -464,10 +487,10 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
     unsigned* st = A.st;
     const PairConstF K = A.K;
     for (int k = threadIdx.x; k < 27 * 6; k += blockDim.x) sh[k / 6][k % 6] = A.shifts.v[k / 6][k % 6];
-    if (A.lj_smem)
+    if (LJS)
         for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj[k] = A.lj4[k];
     __syncthreads();
-    const float4* __restrict__ ljt = A.lj_smem ? s_lj : A.lj4;
+    const float4* __restrict__ ljt = LJS ? s_lj : A.lj4;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int eslot = lane >> 3, jj = lane & 7, i4 = jj & 3;
     const unsigned FULL = 0xffffffffu;
@@ -489,7 +512,7 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
             float4 v = xq[I * CLUSTER + 4 * h + (lane & 3)];
             v.w *= A.kc;
             sxi[wib][lane] = v;
-            sti[wib][lane] = stype[I * CLUSTER + 4 * h + (lane & 3)] * ntp;
+            sti[wib][lane] = stype[I * CLUSTER + 4 * h + (lane & 3)] * ntp * (int)sizeof(float4);   // bytes
         }
         __syncwarp();
         const float4 cI = centerf[I];
@@ -507,7 +530,7 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
             }
             const int J = pe.j;
             const float4 xj = xq[J * CLUSTER + jj];
-            const int tj = stype[J * CLUSTER + jj];
+            const int tj = stype[J * CLUSTER + jj] * (int)sizeof(float4);
             const float4 cJ = centerf[J];
             const float* s6 = sh[pe.shift];
             // the j atom in I's frame: x_j - D, D = (c_I - c_J) - image offset
@@ -528,7 +551,7 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
                 const float r2 = SWITCH ? (on ? r2r : 1e30f) : r2r;   // as in the whole-entry kernel
                 const float rinv = rsqrt_ftz(r2);
                 const float r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
-                const float4 ab = ljt[stl[t] + tj];      // A, B, 12A, 6B
+                const float4 ab = at_bytes(ljt, stl[t] + tj);      // A, B, 12A, 6B
                 float U = rinv6 * fmaf(ab.x, rinv6, -ab.y);
                 float G = (rinv6 * rinv2) * fmaf(ab.z, rinv6, -ab.w);
                 if (SWITCH) {
@@ -600,12 +623,32 @@ __device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
     A.nlist, A.ilist, A.plist, A.xq, A.stype, A.centerf, A.lj4, A.ntp, A.lj_smem, A.kc, A.K, A.shifts, A.fslot,      \
         A.nslots, A.acc, A.npairs, A.next, A.persist, A.st
 
+// Every pair kernel holds two forms of its body: with the LJ table copied to
+// shared memory (lj_smem, when it fits) and read from global memory.  Either
+// way the table loads in the pair loop have a known address space (a generic
+// pointer chosen at run time measured 5% slower at 100k atoms).
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__device__ __forceinline__ void pairs_f32_body(const PairF32Args& A)
+{
+    __shared__ SmemF32W S;
+    if (A.lj_smem) pairs_f32_body_t<ENERGY, SWITCH, COUNT, true>(S, MDF_PF32_UNPACK(A));
+    else pairs_f32_body_t<ENERGY, SWITCH, COUNT, false>(S, MDF_PF32_UNPACK(A));
+}
+
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__device__ __forceinline__ void pairs_f32_half_body(const PairF32Args& A)
+{
+    __shared__ SmemF32H S;
+    if (A.lj_smem) pairs_f32_half_body_t<ENERGY, SWITCH, COUNT, true>(S, A);
+    else pairs_f32_half_body_t<ENERGY, SWITCH, COUNT, false>(S, A);
+}
+
 // With energies: up to 80 registers, three blocks per SM (left to itself the
 // compiler picks 64 and spills, which measured 1-2% slower).
 template <bool SWITCH, bool COUNT>
 __global__ void __launch_bounds__(NB_THREADS, 3) k_pairs_f32(PairF32Args A)
 {
-    pairs_f32_body<true, SWITCH, COUNT>(MDF_PF32_UNPACK(A));
+    pairs_f32_body<true, SWITCH, COUNT>(A);
 }
 
 // Forces only (every dynamics step but the last of a chunk): 64 registers
@@ -613,7 +656,7 @@ __global__ void __launch_bounds__(NB_THREADS, 3) k_pairs_f32(PairF32Args A)
 template <bool SWITCH, bool COUNT>
 __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force(PairF32Args A)
 {
-    pairs_f32_body<false, SWITCH, COUNT>(MDF_PF32_UNPACK(A));
+    pairs_f32_body<false, SWITCH, COUNT>(A);
 }
 
 // The half-entry (4 x 8) forms, same register budgets.
@@ -629,38 +672,44 @@ __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_half_force(PairF32A
     pairs_f32_half_body<false, SWITCH, COUNT>(A);
 }
 
-template <bool SWITCH>
+// The many-system kernels hold one form of the body: LJS is the batch's
+// choice for all its systems (shared memory when every system's table fits).
+template <bool SWITCH, bool LJS>
 __global__ void __launch_bounds__(NB_THREADS) k_pairs_f32_half_multi(const PairF32Args* __restrict__ As)
 {
+    __shared__ SmemF32H S;
     const PairF32Args& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;
-    pairs_f32_half_body<true, SWITCH, false>(A);
+    pairs_f32_half_body_t<true, SWITCH, false, LJS>(S, A);
 }
 
-template <bool SWITCH>
+template <bool SWITCH, bool LJS>
 __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_half_force_multi(const PairF32Args* __restrict__ As)
 {
+    __shared__ SmemF32H S;
     const PairF32Args& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;
-    pairs_f32_half_body<false, SWITCH, false>(A);
+    pairs_f32_half_body_t<false, SWITCH, false, LJS>(S, A);
 }
 
 // Many systems in one launch (blockIdx.z = system), with the same register
 // budgets as the one-system kernels above.
-template <bool SWITCH>
+template <bool SWITCH, bool LJS>
 __global__ void __launch_bounds__(NB_THREADS, 3) k_pairs_f32_multi(const PairF32Args* __restrict__ As)
 {
+    __shared__ SmemF32W S;
     const PairF32Args& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;
-    pairs_f32_body<true, SWITCH, false>(MDF_PF32_UNPACK(A));
+    pairs_f32_body_t<true, SWITCH, false, LJS>(S, MDF_PF32_UNPACK(A));
 }
 
-template <bool SWITCH>
+template <bool SWITCH, bool LJS>
 __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force_multi(const PairF32Args* __restrict__ As)
 {
+    __shared__ SmemF32W S;
     const PairF32Args& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;
-    pairs_f32_body<false, SWITCH, false>(MDF_PF32_UNPACK(A));
+    pairs_f32_body_t<false, SWITCH, false, LJS>(S, MDF_PF32_UNPACK(A));
 }
 #undef MDF_PF32_UNPACK
 
@@ -672,13 +721,13 @@ __global__ void __launch_bounds__(NB_THREADS, 4) k_pairs_f32_force_multi(const P
 // and constants folded on the host.  The arithmetic differs only where
 // precision does: FP64 rsqrt, exp and erfc (the CUDA math library) instead of
 // the SFU forms and the A&S erfc, and FP64 image offsets from FP64 centres.
-template <bool ENERGY, bool SWITCH, bool COUNT>
-__device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
+template <bool ENERGY, bool SWITCH, bool COUNT, bool LJS>
+__device__ __forceinline__ void pairs_f64_body_t(SmemF64W& S, const PairF64Args& A)
 {
     extern __shared__ double4 s_lj_d[];
-    __shared__ double4 sx[NB_WARPS][4][2 * CLUSTER];
-    __shared__ int stj[NB_WARPS][4][2 * CLUSTER];
-    __shared__ double sh[27][3];
+    auto& sx = S.sx;
+    auto& stj = S.stj;
+    auto& sh = S.sh;
     const int nlist = A.nlist;
     const ILRange* __restrict__ ilist = A.ilist;
     const PairEntry* __restrict__ plist = A.plist;
@@ -691,10 +740,10 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
     unsigned* st = A.st;
     const PairConstD K = A.K;
     for (int k = threadIdx.x; k < 27 * 3; k += blockDim.x) sh[k / 3][k % 3] = A.shifts.v[k / 3][k % 3];
-    if (A.lj_smem)
+    if (LJS)
         for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj_d[k] = A.lj4[k];
     __syncthreads();
-    const double4* __restrict__ ljt = A.lj_smem ? s_lj_d : A.lj4;
+    const double4* __restrict__ ljt = LJS ? s_lj_d : A.lj4;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int jslot = lane >> 3, ii = lane & 7;
     const unsigned FULL = 0xffffffffu;
@@ -715,7 +764,7 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
         const ILRange L = ilist[w];
         const int I = L.i;
         const double4 xi = xq[I * CLUSTER + ii];
-        const int trow = stype[I * CLUSTER + ii] * ntp;
+        const int trow = stype[I * CLUSTER + ii] * ntp * (int)sizeof(double4);   // byte offsets
         const double4 cI = center[I];
         const double qik = A.kc * xi.w;
         const double qik2 = qik * K.two_a_spi;
@@ -730,7 +779,7 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
             }
             const int J = pe.j;
             const double4 xjj = xq[J * CLUSTER + ii];
-            const int tjj = stype[J * CLUSTER + ii];
+            const int tjj = stype[J * CLUSTER + ii] * (int)sizeof(double4);
             sx[wib][jslot][ii] = xjj;
             sx[wib][jslot][ii + CLUSTER] = xjj;
             stj[wib][jslot][ii] = tjj;
@@ -754,7 +803,7 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
                 const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
                 const double rinv = rsqrt(r2);
                 const double r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
-                const double4 ab = ljt[trow + stl[t]];      // A, B, 12A, 6B
+                const double4 ab = at_bytes(ljt, trow + stl[t]);      // A, B, 12A, 6B
                 double U = rinv6 * fma(ab.x, rinv6, -ab.y);
                 double G = (rinv6 * rinv2) * fma(ab.z, rinv6, -ab.w);
                 if (SWITCH) {
@@ -822,13 +871,13 @@ __device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
 
 // The half-entry (4 x 8) layout in FP64: the FP32 half kernel's structure
 // with the FP64 kernel's arithmetic.
-template <bool ENERGY, bool SWITCH, bool COUNT>
-__device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
+template <bool ENERGY, bool SWITCH, bool COUNT, bool LJS>
+__device__ __forceinline__ void pairs_f64_half_body_t(SmemF64H& S, const PairF64Args& A)
 {
     extern __shared__ double4 s_lj_d[];
-    __shared__ double4 sxi[NB_WARPS][8];
-    __shared__ int sti[NB_WARPS][8];
-    __shared__ double sh[27][3];
+    auto& sxi = S.sxi;
+    auto& sti = S.sti;
+    auto& sh = S.sh;
     const int nlist = A.nlist, ntp = A.ntp, nslots = A.nslots;
     const ILRange* __restrict__ ilist = A.ilist;
     const PairEntry* __restrict__ plist = A.plist;
@@ -839,10 +888,10 @@ __device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
     unsigned* st = A.st;
     const PairConstD K = A.K;
     for (int k = threadIdx.x; k < 27 * 3; k += blockDim.x) sh[k / 3][k % 3] = A.shifts.v[k / 3][k % 3];
-    if (A.lj_smem)
+    if (LJS)
         for (int k = threadIdx.x; k < ntp * ntp; k += blockDim.x) s_lj_d[k] = A.lj4[k];
     __syncthreads();
-    const double4* __restrict__ ljt = A.lj_smem ? s_lj_d : A.lj4;
+    const double4* __restrict__ ljt = LJS ? s_lj_d : A.lj4;
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int eslot = lane >> 3, jj = lane & 7, i4 = jj & 3;
     const unsigned FULL = 0xffffffffu;
@@ -864,7 +913,7 @@ __device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
             double4 v = xq[I * CLUSTER + 4 * h + (lane & 3)];
             v.w *= A.kc;
             sxi[wib][lane] = v;
-            sti[wib][lane] = stype[I * CLUSTER + 4 * h + (lane & 3)] * ntp;
+            sti[wib][lane] = stype[I * CLUSTER + 4 * h + (lane & 3)] * ntp * (int)sizeof(double4);   // bytes
         }
         __syncwarp();
         const double4 cI = center[I];
@@ -882,7 +931,7 @@ __device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
             }
             const int J = pe.j;
             const double4 xj = xq[J * CLUSTER + jj];
-            const int tj = stype[J * CLUSTER + jj];
+            const int tj = stype[J * CLUSTER + jj] * (int)sizeof(double4);
             const double4 cJ = center[J];
             const double* s3 = sh[pe.shift];
             const double pjx = xj.x - ((cI.x - cJ.x) - s3[0]);
@@ -900,7 +949,7 @@ __device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
                 const bool on = ((rot >> t) & 1u) && r2 <= K.rc2;
                 const double rinv = rsqrt(r2);
                 const double r = r2 * rinv, rinv2 = rinv * rinv, rinv6 = rinv2 * rinv2 * rinv2;
-                const double4 ab = ljt[stl[t] + tj];      // A, B, 12A, 6B
+                const double4 ab = at_bytes(ljt, stl[t] + tj);      // A, B, 12A, 6B
                 double U = rinv6 * fma(ab.x, rinv6, -ab.y);
                 double G = (rinv6 * rinv2) * fma(ab.z, rinv6, -ab.w);
                 if (SWITCH) {
@@ -968,17 +1017,34 @@ __device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
 }
 
 template <bool ENERGY, bool SWITCH, bool COUNT>
-__global__ void __launch_bounds__(NB_THREADS) k_pairs_f64_half(PairF64Args A)
+__device__ __forceinline__ void pairs_f64_body(const PairF64Args& A)
+{
+    __shared__ SmemF64W S;
+    if (A.lj_smem) pairs_f64_body_t<ENERGY, SWITCH, COUNT, true>(S, A);
+    else pairs_f64_body_t<ENERGY, SWITCH, COUNT, false>(S, A);
+}
+
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__device__ __forceinline__ void pairs_f64_half_body(const PairF64Args& A)
+{
+    __shared__ SmemF64H S;
+    if (A.lj_smem) pairs_f64_half_body_t<ENERGY, SWITCH, COUNT, true>(S, A);
+    else pairs_f64_half_body_t<ENERGY, SWITCH, COUNT, false>(S, A);
+}
+
+template <bool ENERGY, bool SWITCH, bool COUNT>
+__global__ void __launch_bounds__(NB_THREADS, 2) k_pairs_f64_half(PairF64Args A)
 {
     pairs_f64_half_body<ENERGY, SWITCH, COUNT>(A);
 }
 
-template <bool ENERGY, bool SWITCH>
+template <bool ENERGY, bool SWITCH, bool LJS>
 __global__ void __launch_bounds__(NB_THREADS) k_pairs_f64_half_multi(const PairF64Args* __restrict__ As)
 {
+    __shared__ SmemF64H S;
     const PairF64Args& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;
-    pairs_f64_half_body<ENERGY, SWITCH, false>(A);
+    pairs_f64_half_body_t<ENERGY, SWITCH, false, LJS>(S, A);
 }
 
 template <bool ENERGY, bool SWITCH, bool COUNT>
@@ -987,12 +1053,13 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_f64(PairF64Args A)
     pairs_f64_body<ENERGY, SWITCH, COUNT>(A);
 }
 
-template <bool ENERGY, bool SWITCH>
+template <bool ENERGY, bool SWITCH, bool LJS>
 __global__ void __launch_bounds__(NB_THREADS) k_pairs_f64_multi(const PairF64Args* __restrict__ As)
 {
+    __shared__ SmemF64W S;
     const PairF64Args& A = As[blockIdx.z];
     if ((int)blockIdx.x >= A.gx) return;
-    pairs_f64_body<ENERGY, SWITCH, false>(A);
+    pairs_f64_body_t<ENERGY, SWITCH, false, LJS>(S, A);
 }
 
 // --------------------------------------------------------------- FP64 pairs
@@ -1398,25 +1465,29 @@ static void launch_pairs_f32(Ctx& c, bool energy)
 }
 
 void launch_pairs_f32_multi(const PairF32Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, bool half, cudaStream_t s)
+                            bool use_switch, bool persist, bool half, bool lj_smem, cudaStream_t s)
 {
 #define MDF_PF32M(KERN)                                                                                        \
     do {                                                                                                       \
         const dim3 g(persist ? std::min(gx, persistent_blocks((const void*)KERN, threads, dyn)) : gx, 1, nsys); \
         KERN<<<g, threads, dyn, s>>>(d_args);                                                                  \
     } while (0)
-    if (half) {
-        if (energy) {
-            if (use_switch) MDF_PF32M(k_pairs_f32_half_multi<true>); else MDF_PF32M(k_pairs_f32_half_multi<false>);
-        } else {
-            if (use_switch) MDF_PF32M(k_pairs_f32_half_force_multi<true>);
-            else MDF_PF32M(k_pairs_f32_half_force_multi<false>);
-        }
-    } else if (energy) {
-        if (use_switch) MDF_PF32M(k_pairs_f32_multi<true>); else MDF_PF32M(k_pairs_f32_multi<false>);
+#define MDF_PF32S(S, L)                                                                                        \
+    do {                                                                                                       \
+        if (half) {                                                                                            \
+            if (energy) MDF_PF32M((k_pairs_f32_half_multi<S, L>));                                             \
+            else MDF_PF32M((k_pairs_f32_half_force_multi<S, L>));                                              \
+        } else {                                                                                               \
+            if (energy) MDF_PF32M((k_pairs_f32_multi<S, L>));                                                  \
+            else MDF_PF32M((k_pairs_f32_force_multi<S, L>));                                                   \
+        }                                                                                                      \
+    } while (0)
+    if (use_switch) {
+        if (lj_smem) MDF_PF32S(true, true); else MDF_PF32S(true, false);
     } else {
-        if (use_switch) MDF_PF32M(k_pairs_f32_force_multi<true>); else MDF_PF32M(k_pairs_f32_force_multi<false>);
+        if (lj_smem) MDF_PF32S(false, true); else MDF_PF32S(false, false);
     }
+#undef MDF_PF32S
 #undef MDF_PF32M
     MDF_CUDA_TRY(cudaGetLastError());
 }
@@ -1521,7 +1592,7 @@ static void launch_pairs_f64(Ctx& c, bool energy)
 }
 
 void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int threads, size_t dyn, bool energy,
-                            bool use_switch, bool persist, bool half, cudaStream_t s)
+                            bool use_switch, bool persist, bool half, bool lj_smem, cudaStream_t s)
 {
 #define MDF_PF64K(KERN)                                                                                        \
     do {                                                                                                       \
@@ -1531,8 +1602,13 @@ void launch_pairs_f64_multi(const PairF64Args* d_args, int nsys, int gx, int thr
     } while (0)
 #define MDF_PF64M(E, S)                                                                                        \
     do {                                                                                                       \
-        if (half) MDF_PF64K((k_pairs_f64_half_multi<E, S>));                                                   \
-        else MDF_PF64K((k_pairs_f64_multi<E, S>));                                                             \
+        if (half) {                                                                                            \
+            if (lj_smem) MDF_PF64K((k_pairs_f64_half_multi<E, S, true>));                                      \
+            else MDF_PF64K((k_pairs_f64_half_multi<E, S, false>));                                             \
+        } else {                                                                                               \
+            if (lj_smem) MDF_PF64K((k_pairs_f64_multi<E, S, true>));                                           \
+            else MDF_PF64K((k_pairs_f64_multi<E, S, false>));                                                  \
+        }                                                                                                      \
     } while (0)
     if (energy) {
         if (use_switch) MDF_PF64M(true, true); else MDF_PF64M(true, false);

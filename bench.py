@@ -389,12 +389,14 @@ def cufft_check(eng, dev, s, ours_ms, reps=20):
 
 def split_bench(dev, ws, rank, cfg="c4", steps=20, warmup=3):
     """c4 (960k atoms, PME 216^3; `cfg` another named workload) evaluated by all ranks together: each rank
-    takes its share of the pair, bonded and PME spread/gather work, the
-    reciprocal space is distributed as x-slabs of the grid and the forces
-    come back by reduce-scatter + all-gather (mdf_params.rank / nranks,
-    mdf_set_allreduce + mdf_set_collectives, NCCL).  Time: CUDA events on each
-    rank's stream around `steps` evaluations, max over ranks.  Rank 0 also
-    times one context doing the whole evaluation, for the speed-up."""
+    takes the pair and PME spread/gather work of its band of space (and its
+    share of the bonded lists), the reciprocal space is distributed as x-slabs
+    of the grid whose charge and potential planes cross between neighbouring
+    bands as halos, and the forces come back by reduce-scatter + all-gather
+    (mdf_params.rank / nranks, mdf_set_allreduce + mdf_set_collectives +
+    mdf_set_halo_exchange, NCCL).  Time: CUDA events on each rank's stream
+    around `steps` evaluations, max over ranks.  Rank 0 also times one context
+    doing the whole evaluation, for the speed-up."""
     import torch
     import torch.distributed as dist
     from md_b200 import abi, distributed, engine, synth, topology
@@ -431,11 +433,13 @@ def split_bench(dev, ws, rank, cfg="c4", steps=20, warmup=3):
     eng = engine.Engine(flat, s.box, rank=rank, nranks=ws, **kw)
     eng.set_allreduce(distributed.torch_allreduce())
     eng.set_collectives(*distributed.torch_collectives())
+    eng.set_halo_exchange(distributed.torch_alltoallv())
     t_split = timed(eng, True)
     eng.close()
     out = {"workload": "%s: %d atoms, PME %s, cutoff 10 A, mixed precision; one evaluation split over %d ranks "
-                       "(x-slab PME: reduce-scatter of the charge grid, all-to-all transposes around the x pass, "
-                       "all-gather of the potential; forces by reduce-scatter + all-gather; energies all-reduced)"
+                       "(bands of space; x-slab PME: halo planes of the charge grid to their owners, all-to-all "
+                       "transposes around the x pass, halo planes of the potential back; forces by reduce-scatter "
+                       "+ all-gather; energies all-reduced)"
                        % (cfg, s.natoms, "x".join(map(str, synth.GRIDS[cfg])), ws),
            "n_ranks": ws, "evals_per_s": steps / t_split, "ms_per_eval": t_split / steps * 1e3}
     if rank == 0:

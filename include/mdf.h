@@ -161,8 +161,10 @@ typedef struct {
     int32_t fft_lines;
     /* Work split over nranks contexts (one per GPU, PHYSICAL semantics; 0 or
      * 1 = one context does everything).  Every rank holds all positions;
-     * rank r takes its share of the i clusters (prune + pair kernel), of the
-     * exclusion, 1-4 and bonded lists and of the PME spread and gather; the
+     * rank r takes its share of the i clusters (prune + pair kernel: the
+     * x-columns of atoms whose centres lie in its x-slab of the PME grid,
+     * a band of space), of the exclusion, 1-4 and bonded lists and of the
+     * PME spread and gather (its band's atoms); the
      * charge grid and the fixed-point force/energy accumulators are summed
      * over the ranks through the mdf_set_allreduce callback, so every rank
      * ends with the full forces and energies, bit-identical to one context. */
@@ -205,6 +207,14 @@ typedef int (*mdf_reduce_scatter_u64)(const uint64_t *d_send, uint64_t *d_recv, 
                                       void *user);
 typedef int (*mdf_allgather_bytes)(const void *d_send, void *d_recv, int64_t bytes, void *stream, void *user);
 typedef int (*mdf_alltoall_bytes)(const void *d_send, void *d_recv, int64_t bytes, void *stream, void *user);
+/* All-to-all with per-rank sizes (mdf_set_halo_exchange), ordered on `stream`
+ * like the others: send_bytes[k] bytes for rank k lie in send one after the
+ * other in rank order, and recv receives recv_bytes[k] bytes from rank k the
+ * same way (ncclSend / ncclRecv grouped, or MPI_Alltoallv).  Zero-size blocks
+ * are frequent: a rank exchanges grid planes with its spatial neighbours
+ * only.  send_bytes and recv_bytes are host arrays of nranks entries. */
+typedef int (*mdf_alltoallv_bytes)(const void *d_send, const int64_t *send_bytes, void *d_recv,
+                                   const int64_t *recv_bytes, void *stream, void *user);
 
 /* Flags for mdf_compute. */
 #define MDF_COMPUTE_ENERGY 1u
@@ -250,6 +260,20 @@ int mdf_set_allreduce(mdf_ctx *ctx, mdf_allreduce_u64 fn, void *user);
  * pair count are still summed by the all-reduce. */
 int mdf_set_collectives(mdf_ctx *ctx, mdf_reduce_scatter_u64 reduce_scatter, mdf_allgather_bytes allgather,
                         mdf_alltoall_bytes alltoall, void *user);
+/* With the collectives set, also register an all-to-all with per-rank sizes
+ * (NULL to go back): the charge grid and the potential then cross between
+ * ranks as halo planes instead of whole grids.  A split context gives rank r
+ * the i clusters of the x-columns whose centres lie in its x-slab of the PME
+ * grid, so its atoms' spread stencils reach only the planes of that slab and
+ * a few around it (half the skin of drift and the stencil's reach); rank r
+ * sends the planes it spread outside its slab to their owners, which add
+ * them, and after the FFTs receives the potential of those planes back.  At
+ * 960k atoms and 8 ranks that is ~6 MB per rank per evaluation instead of the
+ * 80 MB reduce-scatter and 40 MB all-gather.  An atom farther than half the
+ * skin outside its band since the last list build makes the evaluation fail
+ * with MDF_ERR_STATE on the rank that owns it (rebuild the list, as for the
+ * pair list itself).  Forces are still exact and identical to one context. */
+int mdf_set_halo_exchange(mdf_ctx *ctx, mdf_alltoallv_bytes alltoallv, void *user);
 
 /* Cell sort + cluster-pair list with exclusion masks (replaces
  * setup_pairlists / build_lj_pairlist, src/System/NonBondedUtils.cpp:49-57,185-282). */

@@ -532,6 +532,9 @@ void check_status_word(const unsigned long long* hs)
     const unsigned st = (unsigned)hs[NUM_ACC + 1];
     if (st & ST_NONFINITE) throw ApiError(MDF_ERR_NONFINITE, "non-finite force or energy contribution");
     if (st & ST_OVERFLOW) throw ApiError(MDF_ERR_OVERFLOW, "fixed-point accumulator range exceeded");
+    if (st & ST_STALE)
+        throw ApiError(MDF_ERR_STATE, "an atom drifted more than half the skin out of this rank's band since the list "
+                                      "build: rebuild the pair list");
 }
 
 static void fetch(Ctx& c, double* forces_out, mdf_energies* e_out)
@@ -1009,7 +1012,7 @@ int mdf_pairlist_info(mdf_ctx* ctx, int64_t* n_clusters, int64_t* n_cluster_pair
             const bool ok = c.have_list && c.pruned_valid && c.p.prune_every != 0;
             if (ok) {
                 long long lo, hi;
-                rank_slice(c, c.n_clusters, lo, hi);
+                cluster_share(c, lo, hi);
                 const bool half = c.pruned_half;
                 const size_t n = (size_t)(hi - lo) * (half ? 2 : 1);
                 std::vector<ILRange> r(n);
@@ -1168,6 +1171,15 @@ int mdf_set_collectives(mdf_ctx* ctx, mdf_reduce_scatter_u64 reduce_scatter, mdf
         ctx->c.coll_ag = allgather;
         ctx->c.coll_a2a = alltoall;
         ctx->c.coll_user = user;
+    });
+}
+
+int mdf_set_halo_exchange(mdf_ctx* ctx, mdf_alltoallv_bytes alltoallv, void* user)
+{
+    if (!ctx) return MDF_ERR_INVALID;
+    return guarded(ctx, [&] {
+        ctx->c.coll_a2av = alltoallv;
+        ctx->c.coll_a2av_user = user;
     });
 }
 

@@ -247,6 +247,7 @@ struct SpreadArgs {
     GridGeom g;
     unsigned long long* qgrid;
     unsigned* st;
+    int win_lo, win_n;   // halo exchange: stencil bases must lie in win_lo .. +win_n-1 (mod K0); win_n = 0: any
 };
 
 template <typename R>

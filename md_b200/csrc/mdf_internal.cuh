@@ -31,6 +31,7 @@ enum : unsigned {
     ST_CAPACITY_PAIRS = 4u,
     ST_CAPACITY_COLUMN = 8u,
     ST_BAD_INDEX = 16u,
+    ST_STALE = 32u,   // an atom left its rank's band (halo exchange): the list needs a rebuild
 };
 
 struct PairEntry {          // one cluster pair of the half list (16 B)
@@ -260,6 +261,25 @@ struct Ctx {
     DevBuf<unsigned char> pme_slab;          // complex slab [K0p][K1][Kc] (float2 / double2)
     DevBuf<unsigned char> pme_send, pme_recv;   // transpose blocks [nranks][K0p][K1p][Kc]
     DevBuf<unsigned char> pme_rslab;         // real potential slab [K0p][K1][K2]
+    // Bands of a split evaluation (set by the list build, nranks > 1): rank r
+    // owns the i clusters [band_cl[r], band_cl[r+1]), the x-columns whose
+    // centres lie in its x-slab of the PME grid.  Its atoms' spread stencils
+    // start at grid planes (base) within win_lo[r] .. win_lo[r] + win_n[r] - 1
+    // (mod K0) while no atom drifted more than half the skin.
+    std::vector<long long> band_cl;
+    std::vector<int> win_lo, win_n;
+    // halo exchange of grid planes (mdf_set_halo_exchange): this rank's
+    // planes sent to / received from each rank (absolute plane indexes,
+    // concatenated in rank order), the planes of its own window inside its
+    // slab, and the window's plane ranges (at most two after wrapping)
+    mdf_alltoallv_bytes coll_a2av = nullptr;
+    void* coll_a2av_user = nullptr;
+    DevBuf<int> halo_send_pl, halo_recv_pl, halo_local_pl;
+    std::vector<int64_t> halo_send_n, halo_recv_n;   // planes per rank
+    int halo_n_send = 0, halo_n_recv = 0, halo_n_local = 0;
+    int halo_rng[2][2] = {{0, 0}, {0, 0}};           // (first plane, count) of the window
+    std::vector<int64_t> halo_bytes_a, halo_bytes_b;  // per-rank byte counts of the current exchange
+    DevBuf<unsigned char> halo_sendbuf, halo_recvbuf;
     DevBuf<unsigned long long> f_stage;      // force blocks for the reduce-scatter [nranks][3][Sb]
     DevBuf<unsigned long long> f_mine;       // this rank's block [3][Sb]
     DevBuf<double> f_out_blk, f_out_all;     // finished forces: this rank's slots [Sb][3], all slots [nranks*Sb][3]
@@ -317,6 +337,7 @@ void minimize_lbfgs(Ctx& c, int max_iter, double fmax_tol, double max_step, int 
 void backward(Ctx& c, const double* dL_dF, double dL_dE, double* dL_dq, double* dL_dA, double* dL_dB);
 void pme_adjoint(Ctx& c, double gE, double vscale);
 void build_pairlist(Ctx& c);
+void build_bands(Ctx& c);   // rank bands and halo plane lists of a split evaluation
 void pack_positions(Ctx& c);
 void prune_pairlist(Ctx& c, bool whole_entries = false);
 // half-entry lists in use by the pair kernel (layout 1, pruned)
@@ -349,8 +370,27 @@ inline void rank_slice(const Ctx& c, long long n, long long& lo, long long& hi)
     hi = n * (r + 1) / P;
 }
 inline bool distributed(const Ctx& c) { return c.p.nranks > 1; }
+// This rank's i clusters: its band (all of them with one rank).
+inline void cluster_share(const Ctx& c, long long& lo, long long& hi)
+{
+    if (distributed(c) && (int)c.band_cl.size() == c.p.nranks + 1) {
+        lo = c.band_cl[c.p.rank];
+        hi = c.band_cl[c.p.rank + 1];
+    } else {
+        rank_slice(c, c.n_clusters, lo, hi);
+    }
+}
+// This rank's atom slots (PME spread and gather): its band's clusters.
+inline void slot_share(const Ctx& c, long long& lo, long long& hi)
+{
+    cluster_share(c, lo, hi);
+    lo *= CLUSTER;
+    hi *= CLUSTER;
+}
 // nranks > 1 with the reduce-scatter / all-gather / all-to-all collectives
 inline bool slab_mode(const Ctx& c) { return distributed(c) && c.coll_rs && c.coll_ag && c.coll_a2a; }
+// slab mode with the grid planes exchanged as halos (mdf_set_halo_exchange)
+inline bool halo_mode(const Ctx& c) { return slab_mode(c) && c.coll_a2av != nullptr; }
 inline bool rank0(const Ctx& c) { return !distributed(c) || c.p.rank == 0; }
 // In-place sum over the ranks through the registered collective, on c.stream.
 void allreduce_u64(Ctx& c, unsigned long long* d, long long n);

@@ -1317,7 +1317,7 @@ PairArgs<R> make_pair_args(const Ctx& c, bool count)
     A.P = make_params(c);
     const int wpb = pair_warps(c);
     long long lo, hi;
-    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    cluster_share(c, lo, hi);   // this rank's i clusters
     A.nlist = (int)(hi - lo);
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;
@@ -1401,7 +1401,7 @@ PairF32Args make_pair_f32_args(const Ctx& c, size_t* dyn)
     if (dyn) *dyn = A.lj_smem ? lj_bytes : 0;
     const int wpb = pair_warps(c);
     long long lo, hi;
-    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    cluster_share(c, lo, hi);   // this rank's i clusters
     A.nlist = (int)(hi - lo);
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;
@@ -1518,7 +1518,7 @@ PairF64Args make_pair_f64_args(const Ctx& c, size_t* dyn)
     if (dyn) *dyn = A.lj_smem ? lj_bytes : 0;
     const int wpb = pair_warps(c);
     long long lo, hi;
-    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    cluster_share(c, lo, hi);   // this rank's i clusters
     A.nlist = (int)(hi - lo);
     A.gx = grid_blocks(A.nlist, wpb);
     A.gy = 1;

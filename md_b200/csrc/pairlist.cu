@@ -87,7 +87,9 @@ __global__ void k_assign_columns(int N, const double* __restrict__ xyz, double L
     int cx = (int)(x * ncx / Lx), cy = (int)(y * ncy / Ly);
     cx = min(max(cx, 0), ncx - 1);
     cy = min(max(cy, 0), ncy - 1);
-    int col = cx + ncx * cy;
+    // x-major: consecutive columns run along y, so a contiguous range of
+    // clusters is a band of x (a split evaluation's share of space)
+    int col = cy + ncy * cx;
     atom_col[i] = col;
     atomicAdd(&col_count[col], 1);
 }
@@ -343,7 +345,7 @@ __global__ void __launch_bounds__(256) k_pair_search(const int* __restrict__ d_n
     const int lane = threadIdx.x & 31;
     if (I >= *d_ncl) return;
     const int col = cluster_col[I];
-    const int cx = col % g.ncx, cy = col / g.ncx;
+    const int cx = col / g.ncy, cy = col % g.ncy;
     const float4 lo = bb_lo[I], hi = bb_hi[I];
     const int nvi = (int)center[I].w;
     const int nxc = 2 * g.Rx + 1, nyc = 2 * g.Ry + 1;
@@ -393,7 +395,7 @@ __global__ void __launch_bounds__(256) k_pair_search(const int* __restrict__ d_n
             if (gx * gx + gy * gy > g.rlist2) continue;
             const float zmin = lo.z - g.rlist - sz * Lz, zmax = hi.z + g.rlist - sz * Lz;
             if (zmax < -1.0f || zmin > Lz + 1.0f) continue;
-            const int jcol = jx + g.ncx * jy;
+            const int jcol = jy + g.ncy * jx;
             const int c0 = col_cstart[jcol], c1 = col_cstart[jcol + 1];
             // first cluster whose hi.z >= zmin
             int a = c0, b = c1;
@@ -757,7 +759,7 @@ PruneArgs<R> make_prune_args(const Ctx& c)
         }
     }
     long long lo, hi;
-    rank_slice(c, c.n_clusters, lo, hi);   // this rank's i clusters
+    cluster_share(c, lo, hi);   // this rank's i clusters
     A.ncl = (int)(hi - lo);
     A.gx = grid_blocks((long long)A.ncl * 32, 256);
     A.gy = 1;
@@ -792,7 +794,7 @@ PruneArgs<R> make_prune_half_args(const Ctx& c)
 {
     PruneArgs<R> A = make_prune_args<R>(c);
     long long lo, hi;
-    rank_slice(c, c.n_clusters, lo, hi);
+    cluster_share(c, lo, hi);
     A.ilist_in = c.ilist_h.p + 2 * lo;
     A.plist_in = c.plist_h.p;
     return A;
@@ -889,6 +891,107 @@ void pack_positions(Ctx& c)
     MDF_CUDA_TRY(cudaGetLastError());
     c.launches += 1;
 }
+
+// Bands of a split evaluation.  Rank r takes the x-columns whose centres lie
+// in its x-slab of the PME grid (planes [r K0p, (r+1) K0p), K0p = ceil(K0 /
+// nranks)); the columns are x-major, so those are the contiguous clusters
+// [band_cl[r], band_cl[r+1]).  Its atoms were binned at x in [ca, cb) column
+// widths, so with at most half the skin of drift their stencil bases lie in
+// grid planes floor(ca K0/ncx - m) - 1 .. floor(cb K0/ncx + m) + 1 (m = half
+// the skin in planes; one plane each side for rounding), and the stencils
+// touch one plane below and two above those: the rank's window.  Every rank
+// computes every window (all hold all positions and the same list), so the
+// planes a rank sends to each owner and receives from each rank follow
+// without communication.
+void build_bands(Ctx& c)
+{
+    const int P = c.p.nranks, me = c.p.rank, K0 = c.K[0];
+    const int K0p = (K0 + P - 1) / P;
+    const int ncx = c.ncol_x, ncy = c.ncol_y;
+    std::vector<int> cst(c.ncols + 1);
+    MDF_CUDA_TRY(cudaMemcpyAsync(cst.data(), c.col_cstart.p, sizeof(int) * (c.ncols + 1), cudaMemcpyDeviceToHost,
+                                 c.stream));
+    MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    // first column row (cx) of each rank; columns are assigned by their centre
+    std::vector<int> first(P + 1, ncx);
+    for (int cx = ncx - 1; cx >= 0; --cx) {
+        const int t = std::min(P - 1, (int)std::floor((cx + 0.5) * K0 / ncx / K0p));
+        for (int u = 0; u <= t; ++u) first[u] = std::min(first[u], cx);
+    }
+    first[0] = 0;
+    first[P] = ncx;
+    for (int t = 1; t < P; ++t) first[t] = std::max(first[t], first[t - 1]);
+    c.band_cl.assign(P + 1, 0);
+    for (int t = 0; t <= P; ++t) c.band_cl[t] = cst[first[t] * ncy];
+    const double m = 0.5 * c.p.skin * K0 / c.box[0];
+    c.win_lo.assign(P, 0);
+    c.win_n.assign(P, 0);
+    // the real planes of each rank's window, in unwrapped order
+    std::vector<std::vector<int>> W(P);
+    for (int t = 0; t < P; ++t) {
+        const int ca = first[t], cb = first[t + 1];
+        if (cb <= ca) continue;
+        const int blo = (int)std::floor((double)ca * K0 / ncx - m) - 1;
+        const int bhi = (int)std::floor((double)cb * K0 / ncx + m) + 1;
+        c.win_lo[t] = blo;
+        c.win_n[t] = std::min(bhi - blo + 1, K0);
+        const int plo = blo - 1, phi = bhi + 2;   // stencil planes base - 1 .. base + 2
+        if (phi - plo + 1 >= K0) {
+            for (int p = 0; p < K0; ++p) W[t].push_back(p);
+        } else {
+            for (int p = plo; p <= phi; ++p) W[t].push_back(((p % K0) + K0) % K0);
+        }
+    }
+    auto owner = [&](int p) { return p / K0p; };
+    std::vector<int> send, recv, local;
+    c.halo_send_n.assign(P, 0);
+    c.halo_recv_n.assign(P, 0);
+    for (int t = 0; t < P; ++t) {
+        if (t == me) {
+            for (int p : W[me])
+                if (owner(p) == me) local.push_back(p);
+            continue;
+        }
+        for (int p : W[me])
+            if (owner(p) == t) {
+                send.push_back(p);
+                ++c.halo_send_n[t];
+            }
+        for (int p : W[t])
+            if (owner(p) == me) {
+                recv.push_back(p);
+                ++c.halo_recv_n[t];
+            }
+    }
+    auto upload = [&](DevBuf<int>& d, const std::vector<int>& h) {
+        d.alloc(std::max<size_t>(1, h.size()));
+        if (!h.empty())
+            MDF_CUDA_TRY(cudaMemcpyAsync(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, c.stream));
+    };
+    upload(c.halo_send_pl, send);
+    upload(c.halo_recv_pl, recv);
+    upload(c.halo_local_pl, local);
+    c.halo_n_send = (int)send.size();
+    c.halo_n_recv = (int)recv.size();
+    c.halo_n_local = (int)local.size();
+    // the own window as at most two ranges of real planes (for clearing)
+    c.halo_rng[0][0] = c.halo_rng[0][1] = c.halo_rng[1][0] = c.halo_rng[1][1] = 0;
+    if (!W[me].empty()) {
+        if ((int)W[me].size() >= K0) {
+            c.halo_rng[0][0] = 0;
+            c.halo_rng[0][1] = K0;
+        } else {
+            const int p0 = W[me].front(), n = (int)W[me].size();
+            const int n0 = std::min(n, K0 - p0);
+            c.halo_rng[0][0] = p0;
+            c.halo_rng[0][1] = n0;
+            c.halo_rng[1][0] = 0;
+            c.halo_rng[1][1] = n - n0;
+        }
+    }
+    MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));   // the host vectors above are freed on return
+}
+
 
 // The whole build is queued on the context's stream without a host round trip
 // in between: every buffer the build kernels write is sized from bounds known
@@ -1032,6 +1135,7 @@ void build_pairlist(Ctx& c)
         c.ilist_in.alloc(ncl);
         c.pruned_valid = false;
         c.since_prune = 0;
+        if (distributed(c)) build_bands(c);
         c.have_list = true;
         return;
     }

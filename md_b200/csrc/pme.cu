@@ -554,10 +554,16 @@ __device__ __forceinline__ void spread4_rows_dev(const SpreadArgs& A, int bx, in
             base[d] = b;
             u[d] = v - b;
         }
+        if (!bad && A.win_n > 0) {
+            // halo exchange: the stencil must start inside the rank's window
+            int w = (base[0] - A.win_lo) % g.K[0];
+            w += (w < 0) ? g.K[0] : 0;
+            if (w >= A.win_n) bad = 2;
+        }
     }
     bad = __shfl_sync(grp, bad, 0, 16);
     if (bad) {
-        if (l == 0) status_set(st, ST_NONFINITE);
+        if (l == 0) status_set(st, bad == 1 ? ST_NONFINITE : ST_STALE);
         return;
     }
     R w[3];
@@ -1142,7 +1148,7 @@ SpreadArgs make_spread_args(const Ctx& c)
 {
     SpreadArgs A;
     long long s0, s1;
-    rank_slice(c, c.n_slots, s0, s1);   // this rank's slots (all of them with one rank)
+    slot_share(c, s0, s1);   // this rank's slots (all of them with one rank)
     A.s0 = (int)s0;
     A.s1 = (int)s1;
     A.gx = grid_blocks(16 * (s1 - s0), 256);
@@ -1157,6 +1163,12 @@ SpreadArgs make_spread_args(const Ctx& c)
     }
     A.qgrid = c.qgrid.p;
     A.st = c.status.p;
+    A.win_lo = 0;
+    A.win_n = 0;
+    if (halo_mode(c) && (int)c.win_n.size() == c.p.nranks) {
+        A.win_lo = c.win_lo[c.p.rank];
+        A.win_n = c.win_n[c.p.rank];
+    }
     return A;
 }
 
@@ -1166,7 +1178,7 @@ GatherArgs<R> make_gather_args(const Ctx& c)
     GatherArgs<R> A;
     const PmeBufs<R> B(const_cast<Ctx&>(c));
     long long s0, s1;
-    rank_slice(c, c.n_slots, s0, s1);
+    slot_share(c, s0, s1);
     A.s0 = (int)s0;
     A.s1 = (int)s1;
     A.nslots = c.n_slots;
@@ -1265,6 +1277,43 @@ static void coll_check(int rc, const char* what)
     if (rc != 0) throw ApiError(MDF_ERR_CUDA, std::string("the ") + what + " callback failed");
 }
 
+// Move n grid planes of `plane` words: plane k goes from src plane
+// (src_pl ? src_pl[k] - src_off : k) to dst plane (dst_pl ? dst_pl[k] - dst_off
+// : k), added (integer charge planes) or copied.  Packs and unpacks the halo
+// exchange's buffers.
+template <typename T, bool ADD>
+__global__ void k_plane_move(const T* __restrict__ src, const int* __restrict__ src_pl, int src_off,
+                             T* __restrict__ dst, const int* __restrict__ dst_pl, int dst_off, int n, long long plane)
+{
+    const long long total = (long long)n * plane;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(e / plane);
+        const long long i = e - (long long)k * plane;
+        const long long sp = src_pl ? src_pl[k] - src_off : k, dp = dst_pl ? dst_pl[k] - dst_off : k;
+        if (ADD) dst[dp * plane + i] += src[sp * plane + i];
+        else dst[dp * plane + i] = src[sp * plane + i];
+    }
+}
+
+template <typename T, bool ADD>
+static void plane_move(const T* src, const int* src_pl, int src_off, T* dst, const int* dst_pl, int dst_off, int n,
+                       long long plane, cudaStream_t s)
+{
+    if (n <= 0) return;
+    const int nb = (int)std::min<long long>(148 * 8, ((long long)n * plane + 255) / 256);
+    k_plane_move<T, ADD><<<nb, 256, 0, s>>>(src, src_pl, src_off, dst, dst_pl, dst_off, n, plane);
+    MDF_CUDA_TRY(cudaGetLastError());
+}
+
+// Per-rank byte counts of a halo exchange of planes: n[t] planes of `bytes` each.
+static const int64_t* halo_counts(std::vector<int64_t>& out, const std::vector<int64_t>& n, size_t bytes)
+{
+    out.resize(n.size());
+    for (size_t t = 0; t < n.size(); ++t) out[t] = n[t] * (int64_t)bytes;
+    return out.data();
+}
+
 template <typename R>
 static void run_pme_slab(Ctx& c, bool energy)
 {
@@ -1289,13 +1338,42 @@ static void run_pme_slab(Ctx& c, bool energy)
     R* rslab = reinterpret_cast<R*>(c.pme_rslab.p);
     const PmeBufs<R> B(c);
     const int th = 256;
-    MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * (size_t)P * K0p * plane, c.stream));
+    const bool halo = halo_mode(c);
+    const int s_r = r * K0p;   // this rank's first plane
+    const size_t hbytes = (size_t)plane * std::max(sizeof(unsigned long long), sizeof(R));
+    if (halo) {
+        c.halo_sendbuf.alloc(hbytes * (size_t)std::max(1, std::max(c.halo_n_send, c.halo_n_recv)));
+        c.halo_recvbuf.alloc(hbytes * (size_t)std::max(1, std::max(c.halo_n_send, c.halo_n_recv)));
+        // only the window's planes of the full-size grid are spread into
+        for (int k = 0; k < 2; ++k)
+            if (c.halo_rng[k][1] > 0)
+                MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p + (size_t)c.halo_rng[k][0] * plane, 0,
+                                             sizeof(unsigned long long) * (size_t)c.halo_rng[k][1] * plane, c.stream));
+    } else {
+        MDF_CUDA_TRY(cudaMemsetAsync(c.qgrid.p, 0, sizeof(unsigned long long) * (size_t)P * K0p * plane, c.stream));
+    }
     const SpreadArgs S = make_spread_args(c);
     if (S.s1 > S.s0) k_spread4_rows<R><<<grid_of(S), th, 0, c.stream>>>(S);
     MDF_CUDA_TRY(cudaGetLastError());
-    coll_check(c.coll_rs(reinterpret_cast<const uint64_t*>(c.qgrid.p), reinterpret_cast<uint64_t*>(c.q_slab.p),
-                         (int64_t)K0p * plane, (void*)c.stream, c.coll_user),
-               "reduce-scatter");
+    if (halo) {
+        // my slab = my own planes of my window + the planes other ranks spread into it
+        using U = unsigned long long;
+        U* hs = reinterpret_cast<U*>(c.halo_sendbuf.p);
+        U* hr = reinterpret_cast<U*>(c.halo_recvbuf.p);
+        MDF_CUDA_TRY(cudaMemsetAsync(c.q_slab.p, 0, sizeof(U) * (size_t)K0p * plane, c.stream));
+        plane_move<U, true>(c.qgrid.p, c.halo_local_pl.p, 0, c.q_slab.p, c.halo_local_pl.p, s_r, c.halo_n_local, plane,
+                            c.stream);
+        plane_move<U, false>(c.qgrid.p, c.halo_send_pl.p, 0, hs, nullptr, 0, c.halo_n_send, plane, c.stream);
+        coll_check(c.coll_a2av(hs, halo_counts(c.halo_bytes_a, c.halo_send_n, sizeof(U) * plane), hr,
+                               halo_counts(c.halo_bytes_b, c.halo_recv_n, sizeof(U) * plane), (void*)c.stream,
+                               c.coll_a2av_user),
+                   "halo exchange");
+        plane_move<U, true>(hr, nullptr, 0, c.q_slab.p, c.halo_recv_pl.p, s_r, c.halo_n_recv, plane, c.stream);
+    } else {
+        coll_check(c.coll_rs(reinterpret_cast<const uint64_t*>(c.qgrid.p), reinterpret_cast<uint64_t*>(c.q_slab.p),
+                             (int64_t)K0p * plane, (void*)c.stream, c.coll_user),
+                   "reduce-scatter");
+    }
     mark(c, "pme_spread");
     FFTChain<R> F = make_fft_chain<R>(c, energy);
     const int nl = K0p * K1;
@@ -1331,8 +1409,24 @@ static void run_pme_slab(Ctx& c, bool energy)
     k_fft_y<R><<<grid_of(F.yi), FFT_THREADS, F.smy, c.stream>>>(F.yi);
     k_fft_z_c2r<R><<<grid_of(F.zi), FFT_THREADS, F.smz, c.stream>>>(F.zi);
     MDF_CUDA_TRY(cudaGetLastError());
-    coll_check(c.coll_ag(rslab, B.rg, (int64_t)(sizeof(R) * (size_t)K0p * plane), (void*)c.stream, c.coll_user),
-               "all-gather");
+    if (halo) {
+        // the potential of my slab in place, and of my window's other planes from their owners
+        R* ps = reinterpret_cast<R*>(c.halo_sendbuf.p);
+        R* pr = reinterpret_cast<R*>(c.halo_recvbuf.p);
+        const int nown = std::max(0, std::min(K0p, K0 - s_r));
+        if (nown > 0)
+            MDF_CUDA_TRY(cudaMemcpyAsync(B.rg + (size_t)s_r * plane, rslab, sizeof(R) * (size_t)nown * plane,
+                                         cudaMemcpyDeviceToDevice, c.stream));
+        plane_move<R, false>(rslab, c.halo_recv_pl.p, s_r, ps, nullptr, 0, c.halo_n_recv, plane, c.stream);
+        coll_check(c.coll_a2av(ps, halo_counts(c.halo_bytes_a, c.halo_recv_n, sizeof(R) * plane), pr,
+                               halo_counts(c.halo_bytes_b, c.halo_send_n, sizeof(R) * plane), (void*)c.stream,
+                               c.coll_a2av_user),
+                   "halo exchange");
+        plane_move<R, false>(pr, nullptr, 0, B.rg, c.halo_send_pl.p, 0, c.halo_n_send, plane, c.stream);
+    } else {
+        coll_check(c.coll_ag(rslab, B.rg, (int64_t)(sizeof(R) * (size_t)K0p * plane), (void*)c.stream, c.coll_user),
+                   "all-gather");
+    }
     mark(c, "pme_fft_conv");
     const GatherArgs<R> G = make_gather_args<R>(c);
     if (G.s1 > G.s0) k_gather4<R><<<grid_of(G), th, 0, c.stream>>>(G);

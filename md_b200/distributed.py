@@ -11,9 +11,11 @@ for bit, as one context computing everything.
 
 `torch_collectives` builds the reduce-scatter, all-gather and all-to-all of
 mdf_set_collectives (the x-slab distributed reciprocal space and the
-reduce-scatter force return) on the same kind of group.  With gloo the
-buffers are staged through host memory; with NCCL the collectives run on the
-device, ordered on the library's stream.
+reduce-scatter force return) on the same kind of group, and `torch_alltoallv`
+the all-to-all with per-rank sizes of mdf_set_halo_exchange (grid planes to
+and from the spatial neighbours only).  With gloo the buffers are staged
+through host memory; with NCCL the collectives run on the device, ordered on
+the library's stream.
 """
 from __future__ import annotations
 
@@ -129,3 +131,44 @@ def torch_collectives(group=None):
             return 1
 
     return reduce_scatter, allgather, alltoall
+
+
+def torch_alltoallv(group=None, host=False):
+    """fn(send, send_bytes, recv, recv_bytes, stream, user) -> int for
+    Engine.set_halo_exchange on `group` (default: the world): send_bytes[k]
+    bytes of `send` go to rank k and recv_bytes[k] bytes from rank k land in
+    `recv`, both packed in rank order (torch.distributed.all_to_all_single with
+    split sizes).  host=True treats the buffers as host memory (the CPU path
+    of the tests)."""
+    import torch
+    import torch.distributed as dist
+    world = dist.get_world_size(group)
+    nccl = dist.get_backend(group) == "nccl"
+
+    def fn(send, send_bytes, recv, recv_bytes, stream, user):
+        try:
+            ins = [int(send_bytes[k]) for k in range(world)]
+            outs = [int(recv_bytes[k]) for k in range(world)]
+            ni, no = sum(ins), sum(outs)
+            if host:
+                src = torch.from_numpy(np.ctypeslib.as_array(C.cast(C.c_void_p(send), C.POINTER(C.c_uint8)),
+                                                             shape=(max(ni, 1),))[:ni])
+                dst = torch.from_numpy(np.ctypeslib.as_array(C.cast(C.c_void_p(recv), C.POINTER(C.c_uint8)),
+                                                             shape=(max(no, 1),))[:no])
+                dist.all_to_all_single(dst, src, outs, ins, group=group)
+                return 0
+            src = torch.as_tensor(_DeviceBytes(send, ni), device="cuda")
+            dst = torch.as_tensor(_DeviceBytes(recv, no), device="cuda")
+            s = torch.cuda.ExternalStream(int(stream or 0))
+            with torch.cuda.stream(s):
+                if nccl:
+                    dist.all_to_all_single(dst, src, outs, ins, group=group)
+                else:
+                    out = torch.empty(no, dtype=torch.uint8)
+                    dist.all_to_all_single(out, src.cpu(), outs, ins, group=group)
+                    dst.copy_(out)
+                    s.synchronize()
+            return 0
+        except Exception:   # reported to the library as a failed collective
+            return 1
+    return fn

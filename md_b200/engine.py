@@ -25,7 +25,7 @@ EXPORTS = [
     "mdf_backward", "mdf_batch_create", "mdf_batch_destroy", "mdf_batch_last_error", "mdf_batch_info",
     "mdf_batch_set_positions", "mdf_batch_host_buffers", "mdf_batch_build_pairlists", "mdf_batch_compute", "mdf_batch_launch",
     "mdf_batch_fetch", "mdf_batch_submit", "mdf_batch_collect", "mdf_batch_autotune", "mdf_cmap_coefficients_spline",
-    "mdf_pme_grids", "mdf_set_allreduce", "mdf_set_collectives", "mdf_autotune", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
+    "mdf_pme_grids", "mdf_set_allreduce", "mdf_set_collectives", "mdf_set_halo_exchange", "mdf_autotune", "mdf_minimize", "mdf_minimize_lbfgs", "mdf_md_init", "mdf_md_run", "mdf_md_state", "mdf_md_write_rst7",
 ]
 
 
@@ -84,6 +84,7 @@ def library(path=None):
     lib.mdf_set_allreduce.argtypes = [C.c_void_p, abi.MDF_ALLREDUCE_FN, C.c_void_p]
     lib.mdf_set_collectives.argtypes = [C.c_void_p, abi.MDF_REDUCE_SCATTER_FN, abi.MDF_ALLGATHER_FN,
                                         abi.MDF_ALLTOALL_FN, C.c_void_p]
+    lib.mdf_set_halo_exchange.argtypes = [C.c_void_p, abi.MDF_ALLTOALLV_FN, C.c_void_p]
     lib.mdf_minimize_lbfgs.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_double, C.c_int32,
                                        C.POINTER(abi.mdf_min_report)]
     lib.mdf_md_init.argtypes = [C.c_void_p, dp, dp, C.c_double, C.c_uint64]
@@ -272,6 +273,18 @@ class Engine:
         self._coll_cb = (abi.MDF_REDUCE_SCATTER_FN(reduce_scatter), abi.MDF_ALLGATHER_FN(allgather),
                          abi.MDF_ALLTOALL_FN(alltoall))   # kept alive with the engine
         self._check(self.lib.mdf_set_collectives(self.h, *self._coll_cb, None), "set_collectives")
+
+    def set_halo_exchange(self, alltoallv):
+        """Exchange only halo planes of the PME grids between the ranks of a
+        split context (mdf_set_halo_exchange): an all-to-all with per-rank
+        sizes (md_b200.distributed.torch_alltoallv); None goes back to the
+        whole-grid reduce-scatter and all-gather."""
+        if alltoallv is None:
+            self._a2av_cb = None
+            self._check(self.lib.mdf_set_halo_exchange(self.h, abi.MDF_ALLTOALLV_FN(), None), "set_halo_exchange")
+            return
+        self._a2av_cb = abi.MDF_ALLTOALLV_FN(alltoallv)   # kept alive with the engine
+        self._check(self.lib.mdf_set_halo_exchange(self.h, self._a2av_cb, None), "set_halo_exchange")
 
     def set_box(self, box):
         b = np.ascontiguousarray(box, dtype=np.float64)

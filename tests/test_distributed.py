@@ -64,6 +64,36 @@ def _cb_worker(rank, world, port, q):
     dist.destroy_process_group()
 
 
+def _a2av_worker(rank, world, port, q):
+    from md_b200 import distributed
+    dist = _init(rank, world, port)
+    fn = abi.MDF_ALLTOALLV_FN(distributed.torch_alltoallv(host=True))
+    # rank r sends k + r bytes of value 16 r + k to rank k (none to itself when k + r == 0)
+    send_n = [k + rank for k in range(world)]
+    recv_n = [rank + k for k in range(world)]
+    send = np.concatenate([np.full(send_n[k], 16 * rank + k, np.uint8) for k in range(world)] + [np.zeros(1, np.uint8)])
+    recv = np.full(sum(recv_n) + 1, 255, np.uint8)
+    sb = (C.c_int64 * world)(*send_n)
+    rb = (C.c_int64 * world)(*recv_n)
+    rc = fn(send.ctypes.data, sb, recv.ctypes.data, rb, None, None)   # as the library would call it
+    q.put((rank, (rc, recv[:-1].tolist(), int(recv[-1]))))
+    dist.destroy_process_group()
+
+
+def test_alltoallv_callback_three_rank_gloo_cpu():
+    """The halo exchange's all-to-all with per-rank sizes (zero-size blocks
+    included) through the C function pointer, 3 gloo ranks on the CPU."""
+    world = 3
+    res = _run(_a2av_worker, world)
+    for r, (rc, got, tail) in enumerate(res):
+        assert rc == 0
+        want = []
+        for k in range(world):
+            want += [16 * k + r] * (r + k)
+        assert got == want
+        assert tail == 255   # nothing past the received bytes
+
+
 def test_allreduce_callback_two_rank_gloo_cpu():
     res = _run(_cb_worker, 2)
     wrap = -2 ** 63   # 2^62 + 2^62 wraps like an int64 accumulator
@@ -72,7 +102,7 @@ def test_allreduce_callback_two_rank_gloo_cpu():
         assert vals == [3, -3000, wrap, 14]
 
 
-def _eval_worker(rank, world, port, q, cfg, prec, slab=False):
+def _eval_worker(rank, world, port, q, cfg, prec, slab=False, halo=False):
     from md_b200 import distributed, engine, synth
     from tests import helpers as H
     dist = _init(rank, world, port)
@@ -83,6 +113,8 @@ def _eval_worker(rank, world, port, q, cfg, prec, slab=False):
     eng.set_allreduce(distributed.torch_allreduce())
     if slab:
         eng.set_collectives(*distributed.torch_collectives())
+    if halo:
+        eng.set_halo_exchange(distributed.torch_alltoallv())
     eng.set_positions(s.coords)
     eng.build_pairlist()
     out = []
@@ -142,6 +174,86 @@ def test_slab_pme_and_force_scatter_match_one_context(cfg, world, prec):
             assert npair == np0
             for k in abi.E_NAMES + ["total"]:
                 assert abs(E[k] - E0[k]) <= 1e-12 * abs(E0[k]) + 1e-8, (k, E[k], E0[k])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cfg,world,prec", [("small", 2, abi.MDF_PREC_MIXED), ("small", 3, abi.MDF_PREC_FP64),
+                                            ("c0", 2, abi.MDF_PREC_MIXED), ("c0", 3, abi.MDF_PREC_MIXED),
+                                            ("c0", 4, abi.MDF_PREC_FP64)])
+def test_halo_exchange_matches_one_context(cfg, world, prec):
+    """With mdf_set_halo_exchange the charge grid and the potential cross
+    between the ranks as halo planes around each rank's band (all-to-all with
+    per-rank sizes) instead of the whole-grid reduce-scatter and all-gather:
+    forces still equal one context's bit for bit."""
+    res = _run(_eval_worker, world, cfg, prec, True, True)
+    ref = _single(cfg, prec)
+    for out in res:
+        for (E, F, npair), (E0, F0, np0) in zip(out, ref):
+            assert np.array_equal(F, F0)
+            assert npair == np0
+            for k in abi.E_NAMES + ["total"]:
+                assert abs(E[k] - E0[k]) <= 1e-12 * abs(E0[k]) + 1e-8, (k, E[k], E0[k])
+
+
+def _stale_worker(rank, world, port, q, cfg, shift):
+    from md_b200 import distributed, engine, synth
+    from tests import helpers as H
+    dist = _init(rank, world, port)
+    try:
+        s = H.system(cfg)
+        flat = H.flat(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+        eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED,
+                            ewald_tol=1e-5, grid=synth.GRIDS[cfg], rank=rank, nranks=world)
+        eng.set_allreduce(distributed.torch_allreduce())
+        eng.set_collectives(*distributed.torch_collectives())
+        eng.set_halo_exchange(distributed.torch_alltoallv())
+        eng.set_positions(s.coords)
+        eng.build_pairlist()
+        eng.compute()
+        x = s.coords.copy()
+        x[:, 0] += shift   # the whole system moves: every atom leaves its band
+        eng.set_positions(x)
+        status = 0
+        try:
+            eng.compute()
+        except engine.MDFError as e:
+            status = e.status
+        eng.build_pairlist()   # every rank: the list and the bands follow the atoms
+        E, F = eng.compute()
+        eng.close()
+        q.put((rank, (status, F)))
+    except Exception as e:   # reported, not left to the queue's timeout
+        q.put((rank, ("error", repr(e))))
+    dist.destroy_process_group()
+
+
+@pytest.mark.gpu
+def test_halo_exchange_reports_atoms_outside_their_band():
+    """Atoms moved out of their rank's band since the list build (here the
+    whole system, by half a box in x: the same physics, no atom within half
+    the skin of its old band) are reported - MDF_ERR_STATE on the ranks that
+    own them - instead of being spread into planes nobody receives; after a
+    list rebuild the split evaluation equals one context again."""
+    from md_b200 import engine, synth
+    from tests import helpers as H
+    world, cfg = 2, "c0"
+    s = H.system(cfg)
+    shift = 0.5 * s.box[0]
+    res = _run(_stale_worker, world, cfg, shift)
+    for st, F in res:
+        assert st != "error", F
+    assert all(st == abi.MDF_ERR_STATE for st, _ in res)
+    flat = H.flat(s, abi.MDF_SEM_PHYSICAL, engine.cmap_coefficients)
+    eng = engine.Engine(flat, s.box, semantics=abi.MDF_SEM_PHYSICAL, precision=abi.MDF_PREC_MIXED, ewald_tol=1e-5,
+                        grid=synth.GRIDS[cfg])
+    x = s.coords.copy()
+    x[:, 0] += shift
+    eng.set_positions(x)
+    eng.build_pairlist()
+    _, F0 = eng.compute()
+    eng.close()
+    for _, F in res:
+        assert np.array_equal(F, F0)
 
 
 @pytest.mark.gpu

@@ -293,7 +293,7 @@ def _bench_worker(rank, world, port, q):
 
 @pytest.mark.gpu
 def test_bench_split_line_runs():
-    """bench.py's split measurement (run by the driver at N > 1 with NCCL)
+    """bench.py's split measurement (run at N > 1 with NCCL under torchrun)
     end to end with 2 gloo ranks on one GPU and a small workload."""
     res = _run(_bench_worker, 2)
     assert res[0]["n_ranks"] == 2 and res[0]["evals_per_s"] > 0 and res[0]["speedup"] > 0

@@ -3,7 +3,8 @@
 //
 // Atoms are binned into x-y columns whose cross-section holds about one
 // cluster-height of atoms, sorted by z inside each column, and cut into
-// clusters of 8.  Every i cluster then gets the list of j clusters (j >= i,
+// clusters of 8; columns are numbered x-major (y fastest), so consecutive
+// clusters sweep a band of x.  Every i cluster then gets the list of j clusters (j >= i,
 // half list) whose bounding boxes, in some periodic image, come within the
 // list cutoff (cutoff + skin).  Each entry carries a 64-bit mask of the atom
 // pairs that interact: padding slots, the lower triangle of the self pair and

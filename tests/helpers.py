@@ -136,3 +136,28 @@ def nacl_crystal(ncell=4, a=5.64):
 
 
 MADELUNG_NACL = 1.747564594633
+
+
+def many_types(flat, ntypes=60, seed=5):
+    """A copy of a flat topology with `ntypes` LJ types (atom i gets type
+    i mod ntypes; per-type well depths and radii seeded, Lorentz-Berthelot
+    pairs A = eps R^12, B = 2 eps R^6): a pair table too large for the pair
+    kernels' shared memory (more than 51 types in FP32, 55 in FP64)."""
+    from md_b200 import topology
+    rng = np.random.default_rng(seed)
+    eps = rng.uniform(0.05, 0.3, ntypes)
+    rhalf = rng.uniform(0.6, 1.0, ntypes)
+    nb = np.zeros((ntypes, ntypes), np.int32)
+    a, b = [], []
+    for i in range(ntypes):
+        for j in range(i, ntypes):
+            e, r = np.sqrt(eps[i] * eps[j]), rhalf[i] + rhalf[j]
+            a.append(e * r ** 12)
+            b.append(2.0 * e * r ** 6)
+            nb[i, j] = nb[j, i] = len(a)   # 1-based
+    arrays = dict(flat.__dict__)
+    arrays.pop("_struct", None)
+    arrays.update(type=(np.arange(flat.natoms) % ntypes).astype(np.int32), ntypes=ntypes,
+                  nb_index=np.ascontiguousarray(nb.ravel()), lj_a=np.array(a), lj_b=np.array(b),
+                  lj14_a=0.5 * np.array(a), lj14_b=0.5 * np.array(b))
+    return topology.FlatTopology(**arrays)

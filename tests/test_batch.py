@@ -231,3 +231,18 @@ def test_self_pruning_batch_equals_single_systems():
     p = O.make_params(PHYS, ss[0].box, ss[0].meta["grid"], H.alpha_for(1e-5, 9.0), H.KC, cutoff=9.0, switch=8.0)
     e2, f2, _, _, _ = O.evaluate(flats[0], p, frames[-1][0])
     assert H.frel(got[-1][0][1], f2) <= 1e-5
+
+
+@pytest.mark.parametrize("prec", [MIXED, FP64])
+def test_batch_with_a_large_lj_table_equals_single_systems(prec):
+    """One member with 60 LJ types (its pair table does not fit the pair
+    kernels' shared memory): the whole batch reads the tables from global
+    memory and still equals the single systems bit for bit."""
+    ss = systems()[:3]
+    flats = _flats(ss)
+    flats[1] = H.many_types(flats[1])
+    b = engine.Batch(flats, [s.box for s in ss], [s.meta["grid"] for s in ss], precision=prec, **KW)
+    b.set_positions([s.coords for s in ss])
+    res = b.compute()
+    _same(res, _singles(ss, flats, prec))
+    b.close()

@@ -183,6 +183,35 @@ def test_nacl_madelung_on_gpu():
     eng.close()
 
 
+@pytest.mark.parametrize("prec", [MIXED, FP64])
+def test_many_lj_types_table_in_global_memory(prec):
+    """60 LJ types: the 61 x 61 pair table exceeds the shared-memory budget
+    of the pair kernels (40 KB FP32, 96 KB FP64), so they read it from global
+    memory (the other form of their body); both precisions against O2."""
+    s = H.system("small")
+    flat = H.many_types(H.flat(s, PHYS, engine.cmap_coefficients))
+    grid = synth.GRIDS["small"]
+    eng = engine.Engine(flat, s.box, semantics=PHYS, precision=prec, ewald_tol=1e-5, grid=grid)
+    eng.set_positions(s.coords)
+    eng.build_pairlist()
+    E, F = eng.compute()
+    p = O.make_params(PHYS, s.box, grid, H.alpha_for(1e-5), H.KC)
+    e2, f2, _, _, np2 = O.evaluate(flat, p, s.coords)
+    if prec == FP64:
+        assert H.frel(F, f2) < 1e-9
+        for k in ("vdw", "vdw14", "ee_direct"):
+            ref = e2[abi.E_INDEX[k]]
+            assert abs(E[k] - ref) <= 1e-9 * max(abs(ref), 1.0), (k, E[k], ref)
+    else:
+        assert H.frel(F, f2) < 1e-5
+        ref = e2[abi.E_INDEX["vdw"]]
+        assert abs(E["vdw"] - ref) <= 1e-5 * max(abs(ref), 1.0), (E["vdw"], ref)
+    # FP32 distances may put a pair within an ulp of the cutoff on the other side
+    slack = 0 if prec == FP64 else 2
+    assert abs(eng.pairlist_info()["pairs_in_cutoff"] - np2) <= slack
+    eng.close()
+
+
 @pytest.mark.parametrize("tol", [0.5, 0.9])
 def test_ewald_tolerance_without_splitting_rejected(tol):
     # sqrt(-ln(2 tol)) has no positive value for tol >= 0.5

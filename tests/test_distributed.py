@@ -195,6 +195,21 @@ def test_halo_exchange_matches_one_context(cfg, world, prec):
                 assert abs(E[k] - E0[k]) <= 1e-12 * abs(E0[k]) + 1e-8, (k, E[k], E0[k])
 
 
+@pytest.mark.gpu
+def test_halo_exchange_at_960k_atoms():
+    """The band decomposition at c4 scale (960,000 atoms, 49 x-columns, PME
+    216^3; 4 ranks, bands of 6-7 columns, 7-12 halo planes each): forces equal
+    one context's bit for bit."""
+    world, cfg, prec = 4, "c4", abi.MDF_PREC_MIXED
+    res = _run(_eval_worker, world, cfg, prec, True, True)
+    ref = _single(cfg, prec)
+    for out in res:
+        for (E, F, npair), (E0, F0, np0) in zip(out, ref):
+            assert np.array_equal(F, F0)
+            assert npair == np0
+            assert abs(E["total"] - E0["total"]) <= 1e-12 * abs(E0["total"]) + 1e-8
+
+
 def _stale_worker(rank, world, port, q, cfg, shift):
     from md_b200 import distributed, engine, synth
     from tests import helpers as H

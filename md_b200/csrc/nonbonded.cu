@@ -354,13 +354,20 @@ __device__ __forceinline__ void pairs_f32_body_t(SmemF32W& S,
         const float qik = kc * xi.w;
         const float qik2 = qik * K.two_a_spi;
         const int rot_src = (lane & ~7) | ((ii + 1) & 7);
+        // the lane's entry of the next batch is loaded one batch ahead
+        PairEntry pn;
+        if (jslot < L.count) {
+            pn = plist[L.start + jslot];
+        } else {
+            pn.j = I; pn.shift = 13; pn.mask = 0ull;
+        }
         for (int b = 0; b < L.count; b += 4) {
             const int e = b + jslot;
-            PairEntry pe;
-            if (e < L.count) {
-                pe = plist[L.start + e];
+            const PairEntry pe = pn;
+            if (e + 4 < L.count) {
+                pn = plist[L.start + e + 4];
             } else {
-                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+                pn.j = I; pn.shift = 13; pn.mask = 0ull;
             }
             const int J = pe.j;
             const float4 xjj = xq[J * CLUSTER + ii];
@@ -520,13 +527,20 @@ __device__ __forceinline__ void pairs_f32_half_body_t(SmemF32H& S, const PairF32
         const int* __restrict__ stl = &sti[wib][i4];
         double e_lj = 0, e_dir = 0;
         float fix = 0.f, fiy = 0.f, fiz = 0.f;   // the i atom (jj + t) & 3 at step t
+        // the lane's entry of the next batch is loaded one batch ahead
+        PairEntry pn;
+        if (eslot < L.count) {
+            pn = plist[L.start + eslot];
+        } else {
+            pn.j = I; pn.shift = 13; pn.mask = 0ull;
+        }
         for (int b = 0; b < L.count; b += 4) {
             const int e = b + eslot;
-            PairEntry pe;
-            if (e < L.count) {
-                pe = plist[L.start + e];
+            const PairEntry pe = pn;
+            if (e + 4 < L.count) {
+                pn = plist[L.start + e + 4];
             } else {
-                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+                pn.j = I; pn.shift = 13; pn.mask = 0ull;
             }
             const int J = pe.j;
             const float4 xj = xq[J * CLUSTER + jj];
@@ -769,13 +783,20 @@ __device__ __forceinline__ void pairs_f64_body_t(SmemF64W& S, const PairF64Args&
         const double qik = A.kc * xi.w;
         const double qik2 = qik * K.two_a_spi;
         const int rot_src = (lane & ~7) | ((ii + 1) & 7);
+        // the lane's entry of the next batch is loaded one batch ahead
+        PairEntry pn;
+        if (jslot < L.count) {
+            pn = plist[L.start + jslot];
+        } else {
+            pn.j = I; pn.shift = 13; pn.mask = 0ull;
+        }
         for (int b = 0; b < L.count; b += 4) {
             const int e = b + jslot;
-            PairEntry pe;
-            if (e < L.count) {
-                pe = plist[L.start + e];
+            const PairEntry pe = pn;
+            if (e + 4 < L.count) {
+                pn = plist[L.start + e + 4];
             } else {
-                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+                pn.j = I; pn.shift = 13; pn.mask = 0ull;
             }
             const int J = pe.j;
             const double4 xjj = xq[J * CLUSTER + ii];
@@ -921,13 +942,20 @@ __device__ __forceinline__ void pairs_f64_half_body_t(SmemF64H& S, const PairF64
         const int* __restrict__ stl = &sti[wib][i4];
         double e_lj = 0, e_dir = 0;
         double fix = 0, fiy = 0, fiz = 0;
+        // the lane's entry of the next batch is loaded one batch ahead
+        PairEntry pn;
+        if (eslot < L.count) {
+            pn = plist[L.start + eslot];
+        } else {
+            pn.j = I; pn.shift = 13; pn.mask = 0ull;
+        }
         for (int b = 0; b < L.count; b += 4) {
             const int e = b + eslot;
-            PairEntry pe;
-            if (e < L.count) {
-                pe = plist[L.start + e];
+            const PairEntry pe = pn;
+            if (e + 4 < L.count) {
+                pn = plist[L.start + e + 4];
             } else {
-                pe.j = I; pe.shift = 13; pe.mask = 0ull;
+                pn.j = I; pn.shift = 13; pn.mask = 0ull;
             }
             const int J = pe.j;
             const double4 xj = xq[J * CLUSTER + jj];

@@ -152,8 +152,8 @@ def dist_setup(args):
 
 class ClockSampler:
     """SM clock, power and clock-event reasons sampled during the timed region:
-    NVML every 10 ms in a thread (read-only queries), else nvidia-smi every
-    200 ms."""
+    NVML every 2 ms in a thread (read-only queries; the c1 region lasts
+    ~10 ms), else nvidia-smi every 200 ms."""
 
     # NVML clock-event reason bits
     REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
@@ -189,7 +189,7 @@ class ClockSampler:
                                              int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
                     except Exception:
                         pass
-                    self.stop.wait(0.01)
+                    self.stop.wait(0.002)
             self.t = threading.Thread(target=run, daemon=True)
             self.t.start()
             return self
@@ -228,7 +228,7 @@ class ClockSampler:
             sm = [c for c, _ in self.samples]
             reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS.items() if r & bit})
             return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": self.max_mhz, "reasons": reasons,
-                    "samples": len(sm), "source": "NVML, 10 ms"}
+                    "samples": len(sm), "source": "NVML, 2 ms"}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for l in self.lines:

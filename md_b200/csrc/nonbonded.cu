@@ -276,11 +276,16 @@ __global__ void __launch_bounds__(NB_THREADS) k_pairs_multi(const PairArgs<R>* _
 //    vector carries ~1e-6 A rounding, not the 1e-5 A of raw FP32 coordinates;
 //  * the lane's row of the 8x8 mask is rotated once per entry so step t tests
 //    bit t;
-//  * the pair arithmetic is branch-free (inactive pairs are selected out at
-//    the end, so a masked pair at r = 0 only produces values that are dropped);
+//  * the pair arithmetic is branch-free: with the LJ switch an inactive pair
+//    (masked, or beyond the cutoff) is evaluated at r^2 = 1e30, where every
+//    term is exactly zero; with the force-shifted LJ its results are selected
+//    out at the end (a masked pair at r = 0 only produces values that are
+//    dropped);
 //  * the LJ table holds (A, B, 12A, 6B) per type pair, in shared memory when it
 //    fits (lj_smem), and the Gaussian uses 2^(kex r^2) on the SFU;
+//  * each lane loads its entry of the next batch of four one batch ahead;
 //  * energies are summed in FP32 per entry and in FP64 across entries.
+
 // Static shared arrays of the pair bodies, declared once per kernel (each
 // kernel inlines two forms of its body, see pairs_f32_body).
 struct SmemF32W {

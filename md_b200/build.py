@@ -30,7 +30,8 @@ def sources():
 
 def _digest():
     h = hashlib.sha256()
-    for p in sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [os.path.join(REPO, "include", "mdf.h")] + \
+    for p in sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(glob.glob(os.path.join(CSRC, "*.hpp"))) + \
+            [os.path.join(REPO, "include", "mdf.h")] + \
             sorted(glob.glob(os.path.join(HOST, "*.?pp"))):
         with open(p, "rb") as f:
             h.update(p.encode())

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "bands.hpp"
 #include "kargs.cuh"
 #include "mdf_device.cuh"
 #include "mdf_internal.cuh"
@@ -893,104 +894,39 @@ void pack_positions(Ctx& c)
     c.launches += 1;
 }
 
-// Bands of a split evaluation.  Rank r takes the x-columns whose centres lie
-// in its x-slab of the PME grid (planes [r K0p, (r+1) K0p), K0p = ceil(K0 /
-// nranks)); the columns are x-major, so those are the contiguous clusters
-// [band_cl[r], band_cl[r+1]).  Its atoms were binned at x in [ca, cb) column
-// widths, so with at most half the skin of drift their stencil bases lie in
-// grid planes floor(ca K0/ncx - m) - 1 .. floor(cb K0/ncx + m) + 1 (m = half
-// the skin in planes; one plane each side for rounding), and the stencils
-// touch one plane below and two above those: the rank's window.  Every rank
-// computes every window (all hold all positions and the same list), so the
-// planes a rank sends to each owner and receives from each rank follow
-// without communication.
+// Bands of a split evaluation (the arithmetic in bands.hpp): this rank's
+// clusters, its stencil window and its halo plane lists, uploaded once per
+// build.
 void build_bands(Ctx& c)
 {
     const int P = c.p.nranks, me = c.p.rank, K0 = c.K[0];
-    const int K0p = (K0 + P - 1) / P;
-    const int ncx = c.ncol_x, ncy = c.ncol_y;
+    const int ncy = c.ncol_y;
     std::vector<int> cst(c.ncols + 1);
     MDF_CUDA_TRY(cudaMemcpyAsync(cst.data(), c.col_cstart.p, sizeof(int) * (c.ncols + 1), cudaMemcpyDeviceToHost,
                                  c.stream));
     MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));
-    // first column row (cx) of each rank; columns are assigned by their centre
-    std::vector<int> first(P + 1, ncx);
-    for (int cx = ncx - 1; cx >= 0; --cx) {
-        const int t = std::min(P - 1, (int)std::floor((cx + 0.5) * K0 / ncx / K0p));
-        for (int u = 0; u <= t; ++u) first[u] = std::min(first[u], cx);
-    }
-    first[0] = 0;
-    first[P] = ncx;
-    for (int t = 1; t < P; ++t) first[t] = std::max(first[t], first[t - 1]);
+    const BandPlan B = plan_bands(P, K0, c.ncol_x, c.box[0], c.p.skin);
     c.band_cl.assign(P + 1, 0);
-    for (int t = 0; t <= P; ++t) c.band_cl[t] = cst[first[t] * ncy];
-    const double m = 0.5 * c.p.skin * K0 / c.box[0];
-    c.win_lo.assign(P, 0);
-    c.win_n.assign(P, 0);
-    // the real planes of each rank's window, in unwrapped order
-    std::vector<std::vector<int>> W(P);
-    for (int t = 0; t < P; ++t) {
-        const int ca = first[t], cb = first[t + 1];
-        if (cb <= ca) continue;
-        const int blo = (int)std::floor((double)ca * K0 / ncx - m) - 1;
-        const int bhi = (int)std::floor((double)cb * K0 / ncx + m) + 1;
-        c.win_lo[t] = blo;
-        c.win_n[t] = std::min(bhi - blo + 1, K0);
-        const int plo = blo - 1, phi = bhi + 2;   // stencil planes base - 1 .. base + 2
-        if (phi - plo + 1 >= K0) {
-            for (int p = 0; p < K0; ++p) W[t].push_back(p);
-        } else {
-            for (int p = plo; p <= phi; ++p) W[t].push_back(((p % K0) + K0) % K0);
-        }
-    }
-    auto owner = [&](int p) { return p / K0p; };
-    std::vector<int> send, recv, local;
-    c.halo_send_n.assign(P, 0);
-    c.halo_recv_n.assign(P, 0);
-    for (int t = 0; t < P; ++t) {
-        if (t == me) {
-            for (int p : W[me])
-                if (owner(p) == me) local.push_back(p);
-            continue;
-        }
-        for (int p : W[me])
-            if (owner(p) == t) {
-                send.push_back(p);
-                ++c.halo_send_n[t];
-            }
-        for (int p : W[t])
-            if (owner(p) == me) {
-                recv.push_back(p);
-                ++c.halo_recv_n[t];
-            }
-    }
+    for (int t = 0; t <= P; ++t) c.band_cl[t] = cst[B.first[t] * ncy];
+    c.win_lo = B.win_lo;
+    c.win_n = B.win_n;
+    const HaloLists H = halo_lists(B, P, me, K0);
     auto upload = [&](DevBuf<int>& d, const std::vector<int>& h) {
         d.alloc(std::max<size_t>(1, h.size()));
         if (!h.empty())
             MDF_CUDA_TRY(cudaMemcpyAsync(d.p, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice, c.stream));
     };
-    upload(c.halo_send_pl, send);
-    upload(c.halo_recv_pl, recv);
-    upload(c.halo_local_pl, local);
-    c.halo_n_send = (int)send.size();
-    c.halo_n_recv = (int)recv.size();
-    c.halo_n_local = (int)local.size();
-    // the own window as at most two ranges of real planes (for clearing)
-    c.halo_rng[0][0] = c.halo_rng[0][1] = c.halo_rng[1][0] = c.halo_rng[1][1] = 0;
-    if (!W[me].empty()) {
-        if ((int)W[me].size() >= K0) {
-            c.halo_rng[0][0] = 0;
-            c.halo_rng[0][1] = K0;
-        } else {
-            const int p0 = W[me].front(), n = (int)W[me].size();
-            const int n0 = std::min(n, K0 - p0);
-            c.halo_rng[0][0] = p0;
-            c.halo_rng[0][1] = n0;
-            c.halo_rng[1][0] = 0;
-            c.halo_rng[1][1] = n - n0;
-        }
-    }
-    MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));   // the host vectors above are freed on return
+    upload(c.halo_send_pl, H.send);
+    upload(c.halo_recv_pl, H.recv);
+    upload(c.halo_local_pl, H.local);
+    c.halo_send_n = H.send_n;
+    c.halo_recv_n = H.recv_n;
+    c.halo_n_send = (int)H.send.size();
+    c.halo_n_recv = (int)H.recv.size();
+    c.halo_n_local = (int)H.local.size();
+    for (int k = 0; k < 2; ++k)
+        for (int l = 0; l < 2; ++l) c.halo_rng[k][l] = H.rng[k][l];
+    MDF_CUDA_TRY(cudaStreamSynchronize(c.stream));   // the host lists are freed on return
 }
 
 
